@@ -1,0 +1,203 @@
+"""Seeded synthetic microstructures in the reference's voxelised input format.
+
+The reference reads a voxelised microstructure with ``MicrostructureGenMode=4``
+(grainhdl.cpp:404-578): a ``Container.raw`` file of N^3 little-endian uint32
+grain IDs, x fastest, then y, then z (grainhdl.cpp:534-557), plus a ``.uds``
+text file with a 12-line header (line 2 = ID offset, lines 6-8 = NX, NY, NZ,
+line 9 = number of grains, grainhdl.cpp:421-463) and one row per grain
+``id x y z phi1 PHI phi2 xmin xmax ymin ymax zmin zmax count storedEnergy``
+(grainhdl.cpp:484-490; extents are inclusive domain voxel indices).
+
+Everything here is deterministic: a splitmix64 stream (seeded per config) drives
+the seed points, orientations and energies, and each voxel (centre at
+``index + 0.5``) belongs to the nearest seed (Voronoi) or the seed of smallest
+power distance ``|x - s|^2 - r^2`` (Laguerre).  The same files feed the oracle
+and the GPU path, so both start from byte-identical state.
+"""
+from __future__ import annotations
+
+import dataclasses
+import os
+from typing import Optional
+
+import numpy as np
+
+_MASK = np.uint64(0xFFFFFFFFFFFFFFFF)
+
+
+def splitmix64(seed: int, count: int) -> np.ndarray:
+    """``count`` consecutive outputs of splitmix64 started at ``seed``."""
+    with np.errstate(over="ignore"):
+        idx = np.arange(1, count + 1, dtype=np.uint64)
+        z = (np.uint64(seed) + idx * np.uint64(0x9E3779B97F4A7C15)) & _MASK
+        z = ((z ^ (z >> np.uint64(30))) * np.uint64(0xBF58476D1CE4E5B9)) & _MASK
+        z = ((z ^ (z >> np.uint64(27))) * np.uint64(0x94D049BB133111EB)) & _MASK
+        return z ^ (z >> np.uint64(31))
+
+
+def uniform01(seed: int, count: int) -> np.ndarray:
+    """Doubles in [0, 1) from the top 53 bits of splitmix64."""
+    return (splitmix64(seed, count) >> np.uint64(11)).astype(np.float64) * (1.0 / 9007199254740992.0)
+
+
+def normal(seed: int, count: int) -> np.ndarray:
+    """Standard normals by Box-Muller from two splitmix64 streams."""
+    u1 = uniform01(seed, count)
+    u2 = uniform01(seed ^ 0x5DEECE66D, count)
+    return np.sqrt(-2.0 * np.log1p(-u1)) * np.cos(2.0 * np.pi * u2)
+
+
+@dataclasses.dataclass
+class Microstructure:
+    """A labelled voxel domain plus per-grain attributes (IDs are 1..n_grains)."""
+
+    labels: np.ndarray            # (N, N, N) uint32, [z][y][x]; 0 never occurs
+    euler: np.ndarray             # (G, 3) Bunge angles, radians
+    stored_energy: np.ndarray     # (G,) value written in the .uds column
+    seeds: np.ndarray             # (G, 3) seed points (x, y, z), voxel units
+
+    @property
+    def n(self) -> int:
+        return int(self.labels.shape[0])
+
+    @property
+    def n_grains(self) -> int:
+        return int(self.euler.shape[0])
+
+    def grain_extents(self):
+        """Per grain (1..G): inclusive xmin,xmax,ymin,ymax,zmin,zmax and voxel count.
+
+        Grains that own no voxel get count 0 (the reference skips them)."""
+        G = self.n_grains
+        lab = self.labels
+        counts = np.bincount(lab.ravel(), minlength=G + 1)[1:].astype(np.int64)
+        ext = np.zeros((G, 6), dtype=np.int64)
+        z, y, x = np.indices(lab.shape, sparse=True)
+        for axis, coord in ((0, x), (2, y), (4, z)):
+            full = np.broadcast_to(coord, lab.shape).ravel()
+            lo = np.full(G + 1, np.iinfo(np.int64).max, dtype=np.int64)
+            hi = np.full(G + 1, -1, dtype=np.int64)
+            np.minimum.at(lo, lab.ravel(), full)
+            np.maximum.at(hi, lab.ravel(), full)
+            ext[:, axis] = lo[1:]
+            ext[:, axis + 1] = hi[1:]
+        ext[counts == 0] = 0
+        return ext, counts
+
+
+def _uniform_orientations(seed: int, G: int) -> np.ndarray:
+    """Uniformly random orientations (Haar measure) as Bunge Euler angles."""
+    u = uniform01(seed, 3 * G).reshape(G, 3)
+    phi1 = 2.0 * np.pi * u[:, 0]
+    PHI = np.arccos(np.clip(2.0 * u[:, 1] - 1.0, -1.0, 1.0))
+    phi2 = 2.0 * np.pi * u[:, 2]
+    return np.stack([phi1, PHI, phi2], axis=1)
+
+
+def _label_nearest(N: int, seeds: np.ndarray, weights: Optional[np.ndarray]) -> np.ndarray:
+    """Label every voxel centre by its nearest seed (power distance if weighted)."""
+    from scipy.spatial import cKDTree
+
+    G = seeds.shape[0]
+    labels = np.empty((N, N, N), dtype=np.uint32)
+    ax = np.arange(N, dtype=np.float64) + 0.5
+    yy, xx = np.meshgrid(ax, ax, indexing="ij")
+    plane = np.stack([xx.ravel(), yy.ravel()], axis=1)
+    if weights is None:
+        tree = cKDTree(seeds)
+        for z in range(N):
+            pts = np.column_stack([plane, np.full(plane.shape[0], ax[z])])
+            _, idx = tree.query(pts, k=1, workers=-1)
+            labels[z] = (idx.astype(np.uint32) + 1).reshape(N, N)
+        return labels
+    # Laguerre: lift to 4D so that the power distance is a Euclidean distance,
+    # |x-s|^2 - r^2 = |(x,0) - (s, sqrt(R^2 - r^2))|^2 - R^2.
+    R2 = float(np.max(weights ** 2))
+    lift = np.sqrt(np.maximum(R2 - weights ** 2, 0.0))
+    tree = cKDTree(np.column_stack([seeds, lift]))
+    for z in range(N):
+        pts = np.column_stack([plane, np.full(plane.shape[0], ax[z]), np.zeros(plane.shape[0])])
+        _, idx = tree.query(pts, k=1, workers=-1)
+        labels[z] = (idx.astype(np.uint32) + 1).reshape(N, N)
+    del G
+    return labels
+
+
+def voronoi(N: int, n_grains: int, seed: int) -> Microstructure:
+    """Voronoi tessellation of ``n_grains`` uniform random seeds in an N^3 domain."""
+    pts = uniform01(seed, 3 * n_grains).reshape(n_grains, 3) * N
+    labels = _label_nearest(N, pts, None)
+    return Microstructure(labels, _uniform_orientations(seed + 1, n_grains),
+                          np.zeros(n_grains), pts)
+
+
+def laguerre(N: int, n_grains: int, seed: int, sigma: float = 0.3) -> Microstructure:
+    """Laguerre tessellation with lognormal radii (median 1, log-sd ``sigma``),
+    scaled so that the mean cell volume is N^3 / n_grains."""
+    pts = uniform01(seed, 3 * n_grains).reshape(n_grains, 3) * N
+    r = np.exp(sigma * normal(seed + 2, n_grains))
+    r *= (N ** 3 / n_grains * 3.0 / (4.0 * np.pi)) ** (1.0 / 3.0) / np.mean(r)
+    labels = _label_nearest(N, pts, r)
+    return Microstructure(labels, _uniform_orientations(seed + 1, n_grains),
+                          np.zeros(n_grains), pts)
+
+
+def write_mode4(ms: Microstructure, directory: str, raw_name: str = "Container.raw",
+                uds_name: str = "Microstructure.uds", id_offset: int = 1) -> tuple[str, str]:
+    """Write ``Container.raw`` + ``.uds`` in the layout grainhdl.cpp:404-578 reads."""
+    os.makedirs(directory, exist_ok=True)
+    raw_path = os.path.join(directory, raw_name)
+    uds_path = os.path.join(directory, uds_name)
+    (ms.labels.astype("<u4") + np.uint32(id_offset - 1)).tofile(raw_path)
+    ext, counts = ms.grain_extents()
+    N = ms.n
+    lines = [
+        "gg-b200 synthetic microstructure",
+        f"ID_offset\t{id_offset}",
+        "DX\t1", "DY\t1", "DZ\t1",
+        f"NX\t{N}", f"NY\t{N}", f"NZ\t{N}",
+        f"NumberOfGrains\t{ms.n_grains}",
+        "", "",
+        "id\tx\ty\tz\tphi1\tPHI\tphi2\txmin\txmax\tymin\tymax\tzmin\tzmax\tcount\tstoredEnergy",
+    ]
+    rows = []
+    for g in range(ms.n_grains):
+        sx, sy, sz = (int(v) for v in np.floor(ms.seeds[g]))
+        e = ms.euler[g]
+        x0, x1, y0, y1, z0, z1 = (int(v) for v in ext[g])
+        rows.append(f"{g + id_offset}\t{sx}\t{sy}\t{sz}\t{e[0]:.17g}\t{e[1]:.17g}\t{e[2]:.17g}\t"
+                    f"{x0}\t{x1}\t{y0}\t{y1}\t{z0}\t{z1}\t{int(counts[g])}\t{ms.stored_energy[g]:.17g}")
+    with open(uds_path, "w") as f:
+        f.write("\n".join(lines) + "\n")
+        f.write("\n".join(rows) + "\n")
+    return raw_path, uds_path
+
+
+def write_parameters(path: str, *, n_grains: int, border: int = 10, steps: int = 10, time_step: float = 0.2,
+                     raw_name: str = "Container.raw", uds_name: str = "Microstructure.uds",
+                     breakup: int = 0, threads: int = 8, correction: bool = False,
+                     unique_energies: bool = True, mobility_factor: bool = False,
+                     stored_energy: bool = False, analysis_every: int = 1000000) -> None:
+    """A ``parameters.xml`` for the reference (Settings.cpp:81-270) in mode 4.
+
+    ``NumberOfParticles`` must already hold the grain count: the reference sizes
+    its thread work lists from it (grainhdl.cpp:1300-1311) before the mode-4
+    header overrides it (grainhdl.cpp:159-224)."""
+    p = {
+        "StartTime": 0, "NumberOfParticles": n_grains, "NumberOfPointsPerGrain": 10,
+        "AnalysisTimestep": analysis_every, "NumberOfTimesteps": steps,
+        "PlotInterval": 1000000, "TimeStepSize": repr(float(time_step)),
+        "BreakupNumber": breakup, "DiscreteSamplingRate": 25, "DomainBorderSize": border,
+        "MicrostructureGenMode": 4, "ReadFromFilename": raw_name, "AdditionalFilename": uds_name,
+        "HAGB_Energy": "1.", "HAGB_Mobility": "7.5e-14", "DislocEnPerM": "2.5e-10",
+        "Physical_Domain_Size": "2.52e-4", "TripleLineDrag": "1.e6",
+        "UseMobilityFactor": int(mobility_factor), "UseStoredElasticEnergy": int(stored_energy),
+        "UseMagneticField": 0, "DisableConvolutionCorrection": int(not correction),
+        "UseTexture": 0, "ExecuteInParallel": 1, "MaximumNumberOfThreads": threads,
+        "GridCoarsement": 0, "GridCoarsementGradient": 0.95, "ConvolutionMode": 2,
+        "UniqueGBEnergies": int(unique_energies), "GrainScheduler": 0, "DecoupleGrains": 0,
+        "NeighborTracking": 0, "StoreTaskDistribution": 0,
+    }
+    body = "\n".join(f"   <{k}>{v}</{k}>" for k, v in p.items())
+    with open(path, "w") as f:
+        f.write('<?xml version="1.0" encoding="utf-8"?>\n<Parameters>\n' + body + "\n</Parameters>\n")
