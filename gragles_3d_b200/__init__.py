@@ -1,0 +1,260 @@
+"""B200-native GraGLeS_3D level-set timestep.
+
+Python mirror of the reference's ``grainhdl`` driver (grainhdl.cpp:821-943) on
+top of the C ABI in ``include/gg_b200.h`` (``libgg_b200.so``, built in-tree by
+``gragles_3d_b200.build``).  The library is required: there is no CPU path, and
+loading fails loudly when the extension is missing.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import dataclasses
+import os
+from typing import Optional
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libgg_b200.so")
+
+GG_OK = 0
+GG_ERR_INVALID = -1
+GG_ERR_CUDA = -2
+GG_ERR_POOL_EXHAUSTED = -3
+GG_ERR_LIST_OVERFLOW = -4
+GG_ERR_UNSUPPORTED = -5
+PRECISION_FP64 = 0
+PRECISION_MIXED = 1
+
+EXPORTED = [
+    "gg_create", "gg_destroy", "gg_last_error", "gg_load_state", "gg_set_lists", "gg_default_lists", "gg_step",
+    "gg_stage_convolution", "gg_stage_update_lists", "gg_stage_comparison", "gg_stage_level_set",
+    "gg_stage_redistancing", "gg_get_grain_stats", "gg_get_neighbors", "gg_get_list", "gg_get_sdf",
+    "gg_get_idlocal", "gg_grain_count", "gg_loop", "gg_convolve_boxes_f64",
+]
+
+
+class GGError(RuntimeError):
+    def __init__(self, code: int, msg: str):
+        super().__init__(f"gg error {code}: {msg}")
+        self.code = code
+
+
+class Params(C.Structure):
+    _fields_ = [
+        ("domain_size", C.c_int32), ("border", C.c_int32), ("time_step", C.c_double),
+        ("n_grains", C.c_int32), ("precision", C.c_int32), ("disable_correction", C.c_int32),
+        ("list_capacity", C.c_int32), ("pool_voxels", C.c_int64), ("device", C.c_int32),
+        ("reserved", C.c_int32 * 7),
+    ]
+
+
+class StepStats(C.Structure):
+    _fields_ = [
+        ("loop", C.c_int32), ("grain_count", C.c_int32), ("live_grains", C.c_int32), ("reserved0", C.c_int32),
+        ("voxel_updates", C.c_int64), ("ms_convolution", C.c_float), ("ms_lists", C.c_float),
+        ("ms_comparison", C.c_float), ("ms_levelset", C.c_float), ("ms_redistancing", C.c_float),
+        ("ms_total", C.c_float),
+    ]
+
+    def as_dict(self) -> dict:
+        return {k: getattr(self, k) for k, _ in self._fields_ if not k.startswith("reserved")}
+
+
+_lib = None
+
+
+def load_library(path: str = LIB_PATH):
+    """Load libgg_b200.so (raises if it has not been built)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(path):
+        raise FileNotFoundError(f"{path} is missing: build it with `python -m gragles_3d_b200.build`")
+    L = C.CDLL(path)
+    vp, i32, i64 = C.c_void_p, C.c_int32, C.c_int64
+    L.gg_create.argtypes = [C.POINTER(Params), C.POINTER(vp)]
+    L.gg_destroy.argtypes = [vp]
+    L.gg_last_error.argtypes = [vp]
+    L.gg_last_error.restype = C.c_char_p
+    L.gg_load_state.argtypes = [vp, vp, vp, vp]
+    L.gg_set_lists.argtypes = [vp, vp, vp]
+    L.gg_default_lists.argtypes = [vp]
+    L.gg_step.argtypes = [vp, C.POINTER(StepStats)]
+    for s in ("gg_stage_convolution", "gg_stage_update_lists", "gg_stage_comparison", "gg_stage_level_set",
+              "gg_stage_redistancing", "gg_grain_count", "gg_loop"):
+        getattr(L, s).argtypes = [vp]
+    L.gg_get_grain_stats.argtypes = [vp, vp, vp, vp, vp, vp]
+    L.gg_get_neighbors.argtypes = [vp, i32, vp, i32]
+    L.gg_get_list.argtypes = [vp, i32, vp, i32]
+    L.gg_get_sdf.argtypes = [vp, i32, i32, vp, vp, i64]
+    L.gg_get_sdf.restype = i64
+    L.gg_get_idlocal.argtypes = [vp, i32, vp, vp, i64]
+    L.gg_get_idlocal.restype = i64
+    L.gg_convolve_boxes_f64.argtypes = [vp, vp, vp, vp, i32, i32, C.c_double]
+    _lib = L
+    return L
+
+
+def _p(a: np.ndarray):
+    return a.ctypes.data_as(C.c_void_p)
+
+
+def box_shape(box) -> tuple:
+    x0, x1, y0, y1, z0, z1 = (int(v) for v in box)
+    return (z1 - z0, y1 - y0, x1 - x0)
+
+
+@dataclasses.dataclass
+class GrainStats:
+    exists: np.ndarray      # (G+1,) bool, entry 0 unused
+    volume: np.ndarray
+    surface: np.ndarray
+    boxes: np.ndarray       # (G+1, 6)
+    n_neighbors: np.ndarray
+
+
+class GrainHandler:
+    """One simulation on one GPU: the reference's grainhdl, stage for stage.
+
+    ``labels`` (N^3 uint32, [z][y][x], grain IDs 1..G), ``extents`` (G x 6 inclusive
+    domain extents) and ``counts`` (voxels per grain) are the mode-4 input; see
+    ``gragles_3d_b200.microstructure``.
+    """
+
+    def __init__(self, domain_size: int, border: int, time_step: float, n_grains: int,
+                 precision: int = PRECISION_FP64, list_capacity: int = 0, pool_voxels: int = 0,
+                 device: int = 0):
+        L = load_library()
+        self.G = int(n_grains)
+        self.N = int(domain_size)
+        self.border = int(border)
+        self.M = self.N + 2 * self.border
+        self.precision = precision
+        p = Params(domain_size, border, float(time_step), n_grains, precision, 1, list_capacity, pool_voxels,
+                   device)
+        h = C.c_void_p()
+        rc = L.gg_create(C.byref(p), C.byref(h))
+        self._h = h
+        self._check(rc)
+
+    def _check(self, rc: int) -> int:
+        if rc < 0:
+            msg = load_library().gg_last_error(self._h).decode() if self._h else ""
+            raise GGError(rc, msg)
+        return rc
+
+    def close(self):
+        if getattr(self, "_h", None):
+            load_library().gg_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        self.close()
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    # --- set-up -----------------------------------------------------------
+    def load(self, labels: np.ndarray, extents: np.ndarray, counts: np.ndarray) -> None:
+        lab = np.ascontiguousarray(labels, dtype=np.uint32)
+        ext = np.ascontiguousarray(extents, dtype=np.int32)
+        cnt = np.ascontiguousarray(counts, dtype=np.int64)
+        self._check(load_library().gg_load_state(self._h, _p(lab), _p(ext), _p(cnt)))
+
+    def set_lists(self, offsets: np.ndarray, ids: np.ndarray) -> None:
+        off = np.ascontiguousarray(offsets, dtype=np.int64)
+        ids = np.ascontiguousarray(ids, dtype=np.uint32)
+        self._check(load_library().gg_set_lists(self._h, _p(off), _p(ids)))
+
+    def default_lists(self) -> None:
+        self._check(load_library().gg_default_lists(self._h))
+
+    # --- the loop ---------------------------------------------------------
+    def step(self) -> dict:
+        st = StepStats()
+        self._check(load_library().gg_step(self._h, C.byref(st)))
+        return st.as_dict()
+
+    def stage(self, name: str) -> None:
+        self._check(getattr(load_library(), f"gg_stage_{name}")(self._h))
+
+    @property
+    def grain_count(self) -> int:
+        return self._check(load_library().gg_grain_count(self._h))
+
+    @property
+    def loop(self) -> int:
+        return self._check(load_library().gg_loop(self._h))
+
+    # --- read-back ---------------------------------------------------------
+    def stats(self) -> GrainStats:
+        G1 = self.G + 1
+        ex = np.zeros(G1, np.uint8); vol = np.zeros(G1); sur = np.zeros(G1)
+        box = np.zeros((G1, 6), np.int32); nn = np.zeros(G1, np.int32)
+        self._check(load_library().gg_get_grain_stats(self._h, _p(ex), _p(vol), _p(sur), _p(box), _p(nn)))
+        return GrainStats(ex.astype(bool), vol, sur, box, nn)
+
+    def neighbors(self, gid: int) -> np.ndarray:
+        buf = np.zeros(256, np.uint32)
+        n = self._check(load_library().gg_get_neighbors(self._h, gid, _p(buf), buf.size))
+        return buf[:min(n, buf.size)].copy()
+
+    def comparison_list(self, gid: int) -> np.ndarray:
+        buf = np.zeros(1 << 16, np.uint32)
+        n = self._check(load_library().gg_get_list(self._h, gid, _p(buf), buf.size))
+        return buf[:n].copy()
+
+    def sdf(self, gid: int, which: int = 1):
+        box = np.zeros(6, np.int32)
+        n = self._check(load_library().gg_get_sdf(self._h, gid, which, _p(box), None, 0))
+        out = np.zeros(n, np.float64)
+        load_library().gg_get_sdf(self._h, gid, which, _p(box), _p(out), n)
+        return tuple(int(v) for v in box), out.reshape(box_shape(box))
+
+    def idlocal(self, gid: int):
+        box = np.zeros(6, np.int32)
+        n = self._check(load_library().gg_get_idlocal(self._h, gid, _p(box), None, 0))
+        out = np.zeros(n, np.uint32)
+        load_library().gg_get_idlocal(self._h, gid, _p(box), _p(out), n)
+        return tuple(int(v) for v in box), out
+
+
+def from_microstructure(ms, border: int = 10, time_step: float = 0.2, precision: int = PRECISION_FP64,
+                        lists=None, **kw) -> GrainHandler:
+    """Create a handler, load a ``microstructure.Microstructure`` and its lists."""
+    ext, counts = ms.grain_extents()
+    gh = GrainHandler(ms.n, border, time_step, ms.n_grains, precision=precision, **kw)
+    gh.load(ms.labels, ext, counts)
+    if lists is None:
+        gh.default_lists()
+    else:
+        gh.set_lists(*lists)
+    return gh
+
+
+def convolve_boxes_f64(boxes: list, domain_size: int, time_step: float) -> list:
+    """FP64 Gaussian convolution of cubic boxes on the GPU (torch manages the device memory)."""
+    import torch
+
+    L = load_library()
+    sides = np.array([b.shape[0] for b in boxes], np.int32)
+    offs = np.zeros(len(boxes), np.int64)
+    total = 0
+    for i, b in enumerate(boxes):
+        offs[i] = total
+        total += (b.size + 31) // 32 * 32
+    host = np.zeros(max(total, 1), np.float64)
+    for i, b in enumerate(boxes):
+        host[offs[i]:offs[i] + b.size] = b.ravel()
+    d_in = torch.from_numpy(host).cuda()
+    d_out = torch.zeros_like(d_in)
+    rc = L.gg_convolve_boxes_f64(C.c_void_p(d_in.data_ptr()), C.c_void_p(d_out.data_ptr()), _p(sides), _p(offs),
+                                 len(boxes), domain_size, float(time_step))
+    if rc < 0:
+        raise GGError(rc, "gg_convolve_boxes_f64 failed")
+    out = d_out.cpu().numpy()
+    return [out[offs[i]:offs[i] + b.size].reshape(b.shape).copy() for i, b in enumerate(boxes)]

@@ -1,0 +1,913 @@
+// gg_api.cu -- host orchestration and the C ABI (include/gg_b200.h).
+//
+// This is the B200 replacement of grainhdl's per-timestep driver
+// (grainhdl.cpp:821-943): it owns the device-resident box pool, sequences the
+// batched stage kernels on one stream, and mirrors the reference's in/out buffer
+// swaps with arena parities.  Host code only; the kernels live in the other .cu
+// files.  Compiled without floating-point contraction so that the DFT twiddles
+// and Gaussian tables match the oracle's bit for bit.
+#include <algorithm>
+#include <cmath>
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "../../include/gg_b200.h"
+#include "gg_conv.cuh"
+#include "gg_conv_tc.cuh"
+#include "gg_kernels.cuh"
+
+using namespace gg;
+
+namespace {
+
+constexpr double kPi = 3.14159265358979323846;  // ggLS.h:25
+constexpr int kNbCap = 256;
+constexpr int kSlab64 = 4;   // comparison slab (z-planes per tile), FP64 path
+constexpr int kSlab32 = 8;   // FP32 path
+
+struct Timer {
+    cudaEvent_t e[6];
+};
+
+}  // namespace
+
+struct gg_ctx {
+    gg_params P{};
+    std::string err;
+    int G = 0, N = 0, gb = 0, M = 0;
+    bool fp64 = true;
+    size_t esz = 8;
+    Geometry geo{};
+    cudaStream_t stream = nullptr;
+    int num_sms = 148;
+    int grid = 148 * 8;
+    bool loaded = false;
+    // per-grain device state
+    int *d_present = nullptr, *d_exists = nullptr, *d_newbox = nullptr, *d_nnb = nullptr;
+    double *d_volume = nullptr, *d_surface = nullptr;
+    uint32_t* d_nb = nullptr;
+    uint32_t *d_cmp = nullptr, *d_son = nullptr;
+    int *d_ncmp = nullptr, *d_nson = nullptr;
+    // pool
+    void* d_arena[2] = {nullptr, nullptr};
+    int* d_box[2] = {nullptr, nullptr};
+    long long* d_off[2] = {nullptr, nullptr};
+    uint32_t* d_idarena[2] = {nullptr, nullptr};
+    int* d_idbox[2] = {nullptr, nullptr};
+    long long* d_idoff[2] = {nullptr, nullptr};
+    double2* d_spec = nullptr;
+    long long* d_spec_off = nullptr;
+    long long pool_voxels = 0, spec_capacity = 0;
+    // tiles
+    int *d_toff_n = nullptr, *d_toff_slab = nullptr, *d_toff_one = nullptr, *d_toff_mc = nullptr, *d_toff_red = nullptr;
+    // tables
+    double2* d_tw = nullptr;
+    long long* d_tw_off = nullptr;
+    double* d_gtab = nullptr;
+    long long* d_g_off = nullptr;
+    float* d_circ = nullptr;          // FP32 circulant matrices (mixed path)
+    long long* d_circ_off = nullptr;
+    // scalars
+    int* d_err = nullptr;
+    long long* d_total_vox = nullptr;
+    int* d_count3 = nullptr;
+    int* h_count3 = nullptr;  // pinned
+    long long* h_total_vox = nullptr;
+    // host mirror
+    int p = 0;        // SDF arena holding m_inputDistance
+    int q = 0;        // ID arena holding m_IDLocal
+    int loop = 0;
+    int grain_count = 0, live = 0;
+    int side_max = 0;      // largest box side of the current layout
+    int side_limit = 0;    // largest side the shared-memory kernels accept
+    int list_cap = 4096, slab = kSlab64, hash_cap = 8192;
+    cudaEvent_t ev[7] = {};
+};
+
+namespace {
+
+int fail(gg_ctx* c, int code, const char* fmt, ...) {
+    char buf[512];
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(buf, sizeof buf, fmt, ap);
+    va_end(ap);
+    if (c) c->err = buf;
+    return code;
+}
+
+#define CK(call)                                                                               \
+    do {                                                                                       \
+        cudaError_t e_ = (call);                                                               \
+        if (e_ != cudaSuccess)                                                                 \
+            return fail(ctx, GG_ERR_CUDA, "%s failed: %s (%s:%d)", #call, cudaGetErrorString(e_), \
+                        __FILE__, __LINE__);                                                   \
+    } while (0)
+
+template <typename X>
+cudaError_t dalloc(X** p, size_t count) {
+    return cudaMalloc((void**)p, sizeof(X) * (count ? count : 1));
+}
+
+// Gaussian multiplier of box.cpp:760-761 for every S = i2^2 + j2^2 + k2^2 of side n.
+void gaussian_table(int n, int N, double time_step, std::vector<double>& out) {
+    const double dt = time_step / double(N * N);  // grainhdl.cpp:1431
+    const double nsq = N * N;
+    const double local_nsq = n * n;
+    const int h = n / 2;
+    const int smax = 3 * h * h;
+    for (int S = 0; S <= smax; S++) {
+        const double G = std::exp(-std::sqrt(2 / kPi) * S * 4.0 * dt * nsq / local_nsq * kPi * kPi) / (local_nsq * n);
+        out.push_back(G);
+    }
+}
+
+// Twiddles of the specified DFT: (cos, sin)(2 pi j / n), angle (6.283185307179586 * j) / n.
+void twiddle_table(int n, std::vector<double2>& out) {
+    for (int j = 0; j < n; j++) {
+        const double a = 6.283185307179586476925286766559 * (double)j / (double)n;
+        out.push_back(make_double2(std::cos(a), std::sin(a)));
+    }
+}
+
+int upload_tables(gg_ctx* ctx) {
+    const int M = ctx->M;
+    std::vector<double2> tw;
+    std::vector<long long> tw_off(M + 2, 0);
+    std::vector<double> gt;
+    std::vector<long long> g_off(M + 2, 0);
+    for (int n = 1; n <= M; n++) {
+        tw_off[n] = (long long)tw.size();
+        twiddle_table(n, tw);
+        g_off[n] = (long long)gt.size();
+        gaussian_table(n, ctx->N, ctx->P.time_step, gt);
+    }
+    CK(dalloc(&ctx->d_tw, tw.size()));
+    CK(dalloc(&ctx->d_tw_off, tw_off.size()));
+    CK(dalloc(&ctx->d_gtab, gt.size()));
+    CK(dalloc(&ctx->d_g_off, g_off.size()));
+    CK(cudaMemcpy(ctx->d_tw, tw.data(), tw.size() * sizeof(double2), cudaMemcpyHostToDevice));
+    CK(cudaMemcpy(ctx->d_tw_off, tw_off.data(), tw_off.size() * sizeof(long long), cudaMemcpyHostToDevice));
+    CK(cudaMemcpy(ctx->d_gtab, gt.data(), gt.size() * sizeof(double), cudaMemcpyHostToDevice));
+    CK(cudaMemcpy(ctx->d_g_off, g_off.data(), g_off.size() * sizeof(long long), cudaMemcpyHostToDevice));
+    if (!ctx->fp64) {
+        std::vector<float> circ;
+        std::vector<long long> c_off(M + 2, 0);
+        for (int n = 1; n <= M; n++) {
+            c_off[n] = (long long)circ.size();
+            circulant_matrix(n, ctx->N, ctx->P.time_step, circ);
+        }
+        CK(dalloc(&ctx->d_circ, circ.size()));
+        CK(dalloc(&ctx->d_circ_off, c_off.size()));
+        CK(cudaMemcpy(ctx->d_circ, circ.data(), circ.size() * sizeof(float), cudaMemcpyHostToDevice));
+        CK(cudaMemcpy(ctx->d_circ_off, c_off.data(), c_off.size() * sizeof(long long), cudaMemcpyHostToDevice));
+    }
+    return GG_OK;
+}
+
+int check_err(gg_ctx* ctx, const char* where) {
+    int e = 0;
+    CK(cudaMemcpyAsync(&e, ctx->d_err, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
+    CK(cudaStreamSynchronize(ctx->stream));
+    if (e & ERR_POOL) return fail(ctx, GG_ERR_POOL_EXHAUSTED, "%s: box pool or scratch capacity exceeded", where);
+    if (e & (ERR_LIST | ERR_HASH)) return fail(ctx, GG_ERR_LIST_OVERFLOW, "%s: comparison list capacity exceeded", where);
+    if (e & ERR_NEIGHBORS) return fail(ctx, GG_ERR_LIST_OVERFLOW, "%s: hull neighbour capacity exceeded", where);
+    if (e & ERR_BOX) return fail(ctx, GG_ERR_UNSUPPORTED, "%s: a box left the grid or exceeded the supported side", where);
+    return GG_OK;
+}
+
+template <typename T>
+Arena<T> arena(gg_ctx* c, int a) {
+    return Arena<T>{reinterpret_cast<T*>(c->d_arena[a]), c->d_box[a], c->d_off[a]};
+}
+
+int plan(gg_ctx* ctx, const int* box, int only_existing, long long* off, long long* spec_off, int* toff_n,
+         int* toff_slab, int* toff_one, long long* total_voxels = nullptr) {
+    PlanArgs a{};
+    a.G = ctx->G;
+    a.present = ctx->d_present;
+    a.exists = ctx->d_exists;
+    a.box = box;
+    a.only_existing = only_existing;
+    a.off = off;
+    a.capacity = ctx->pool_voxels;
+    a.spec_off = spec_off;
+    a.spec_capacity = ctx->spec_capacity;
+    a.toff_n = toff_n;
+    a.toff_slab = toff_slab;
+    a.slab = ctx->slab;
+    a.toff_one = toff_one;
+    a.total_voxels = total_voxels;
+    a.err = ctx->d_err;
+    launch_plan(a, ctx->stream);
+    return GG_OK;
+}
+
+int read_counts(gg_ctx* ctx, const int* box) {
+    launch_count(ctx->G, ctx->d_present, ctx->d_exists, box, ctx->d_count3, ctx->stream);
+    CK(cudaMemcpyAsync(ctx->h_count3, ctx->d_count3, 3 * sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
+    CK(cudaMemcpyAsync(ctx->h_total_vox, ctx->d_total_vox, sizeof(long long), cudaMemcpyDeviceToHost, ctx->stream));
+    CK(cudaStreamSynchronize(ctx->stream));
+    ctx->grain_count = ctx->h_count3[0];
+    ctx->live = ctx->h_count3[1];
+    return GG_OK;
+}
+
+int side_check(gg_ctx* ctx, int side) {
+    if (side > ctx->side_limit)
+        return fail(ctx, GG_ERR_UNSUPPORTED, "box side %d exceeds the supported maximum %d", side, ctx->side_limit);
+    return GG_OK;
+}
+
+template <typename T>
+int redistance(gg_ctx* ctx, int in_a, int out_a, const int* toff, int side) {
+    RedistArgs<T> r{};
+    r.G = ctx->G;
+    r.geo = ctx->geo;
+    r.toff = toff;
+    r.exists = ctx->d_exists;
+    r.in = arena<T>(ctx, in_a);
+    r.out = arena<T>(ctx, out_a);
+    r.err = ctx->d_err;
+    const size_t smem = redist_smem_bytes(side, sizeof(T) == 8);
+    launch_redistance<T>(r, ctx->grid, smem, smem, ctx->stream);
+    CK(cudaGetLastError());
+    return GG_OK;
+}
+
+template <typename T>
+int load_state_t(gg_ctx* ctx, const uint32_t* labels) {
+    const int G = ctx->G;
+    // initial layout in arena 0, mirrored to arena 1 and the first IDLocal arena
+    plan(ctx, ctx->d_box[0], 1, ctx->d_off[0], nullptr, ctx->d_toff_n, nullptr, nullptr);
+    launch_copy_layout(G, ctx->d_present, ctx->d_box[0], ctx->d_off[0], ctx->d_box[1], ctx->d_off[1], ctx->stream);
+    launch_copy_layout(G, ctx->d_present, ctx->d_box[0], ctx->d_off[0], ctx->d_idbox[0], ctx->d_idoff[0], ctx->stream);
+    CK(cudaMemsetAsync(ctx->d_idarena[0], 0, sizeof(uint32_t) * ctx->pool_voxels, ctx->stream));
+    int rc = check_err(ctx, "gg_load_state");
+    if (rc) return rc;
+    uint32_t* d_labels = nullptr;
+    const size_t nl = (size_t)ctx->N * ctx->N * ctx->N;
+    CK(dalloc(&d_labels, nl));
+    CK(cudaMemcpyAsync(d_labels, labels, nl * sizeof(uint32_t), cudaMemcpyHostToDevice, ctx->stream));
+    InitArgs<T> ia{};
+    ia.G = G;
+    ia.geo = ctx->geo;
+    ia.toff = ctx->d_toff_n;
+    ia.present = ctx->d_present;
+    ia.dst = arena<T>(ctx, 0);
+    ia.labels = d_labels;
+    launch_init_sdf<T>(ia, ctx->grid, ctx->stream);
+    CK(cudaGetLastError());
+    // calculateDistanceFunction ends with executeRedistancing (box.cpp:396): arena 0 -> arena 1
+    rc = redistance<T>(ctx, 0, 1, ctx->d_toff_n, ctx->side_max);
+    if (rc) return rc;
+    CK(cudaStreamSynchronize(ctx->stream));
+    CK(cudaFree(d_labels));
+    ctx->p = 0;   // m_inputDistance = +-h field, m_outputDistance = initial SDF
+    ctx->q = 0;
+    return check_err(ctx, "gg_load_state");
+}
+
+template <typename T>
+int stage_convolution_t(gg_ctx* ctx) {
+    ctx->p ^= 1;  // switchDistancebuffer (gridCoarsement off), grainhdl.cpp:1496
+    const int p = ctx->p;
+    plan(ctx, ctx->d_box[p], 1, nullptr, sizeof(T) == 8 ? ctx->d_spec_off : nullptr, ctx->d_toff_n,
+         ctx->d_toff_slab, ctx->d_toff_one, ctx->d_total_vox);
+    // IDLocal follows the output box (resizeIDLocalToDistanceBuffer, box.cpp:426)
+    launch_copy_layout(ctx->G, ctx->d_present, ctx->d_box[p], ctx->d_off[p], ctx->d_idbox[ctx->q ^ 1],
+                       ctx->d_idoff[ctx->q ^ 1], ctx->stream);
+    if (sizeof(T) == 8) {
+        ConvArgs a{};
+        a.G = ctx->G;
+        a.toff = ctx->d_toff_n;
+        a.in = reinterpret_cast<const double*>(ctx->d_arena[p]);
+        a.in_box = ctx->d_box[p];
+        a.in_off = ctx->d_off[p];
+        a.out = reinterpret_cast<double*>(ctx->d_arena[p ^ 1]);
+        a.out_off = ctx->d_off[p ^ 1];
+        a.spec = ctx->d_spec;
+        a.spec_off = ctx->d_spec_off;
+        a.tw = ctx->d_tw;
+        a.tw_off = ctx->d_tw_off;
+        a.gtab = ctx->d_gtab;
+        a.g_off = ctx->d_g_off;
+        launch_conv_f64(a, ctx->grid, conv_f64_smem_bytes(ctx->side_max), ctx->stream);
+    } else {
+        ConvTCArgs a{};
+        a.G = ctx->G;
+        a.toff = ctx->d_toff_n;
+        a.in = reinterpret_cast<const float*>(ctx->d_arena[p]);
+        a.box = ctx->d_box[p];
+        a.in_off = ctx->d_off[p];
+        a.out = reinterpret_cast<float*>(ctx->d_arena[p ^ 1]);
+        a.out_off = ctx->d_off[p ^ 1];
+        a.circ = ctx->d_circ;
+        a.circ_off = ctx->d_circ_off;
+        a.err = ctx->d_err;
+        launch_conv_tc(a, ctx->num_sms, ctx->side_max, ctx->stream);
+    }
+    CK(cudaGetLastError());
+    return GG_OK;
+}
+
+int stage_update_lists_t(gg_ctx* ctx) {
+    ctx->p ^= 1;  // switchDistancebuffer, grainhdl.cpp:852
+    ListArgs a{};
+    a.G = ctx->G;
+    a.toff = ctx->d_toff_one;
+    a.exists = ctx->d_exists;
+    a.box = ctx->d_box[ctx->p];
+    a.son = ctx->d_son;
+    a.n_son = ctx->d_nson;
+    a.cmp = ctx->d_cmp;
+    a.n_cmp = ctx->d_ncmp;
+    a.list_cap = ctx->list_cap;
+    a.hash_cap = ctx->hash_cap;
+    a.err = ctx->d_err;
+    launch_update_lists(a, ctx->grid, ctx->stream);
+    CK(cudaGetLastError());
+    return GG_OK;
+}
+
+template <typename T>
+int stage_comparison_t(gg_ctx* ctx) {
+    const int p = ctx->p, q = ctx->q;
+    launch_newbox_init(ctx->G, ctx->d_present, ctx->d_exists, ctx->d_box[p ^ 1], ctx->d_newbox, ctx->stream);
+    CompareArgs<T> a{};
+    a.G = ctx->G;
+    a.geo = ctx->geo;
+    a.toff = ctx->d_toff_slab;
+    a.slab = ctx->slab;
+    a.exists = ctx->d_exists;
+    a.in = arena<T>(ctx, p);
+    a.out = arena<T>(ctx, p ^ 1);
+    a.id_old = ctx->d_idarena[q];
+    a.idbox_old = ctx->d_idbox[q];
+    a.idoff_old = ctx->d_idoff[q];
+    a.id_new = ctx->d_idarena[q ^ 1];
+    a.idoff_new = ctx->d_idoff[q ^ 1];
+    a.cmp = ctx->d_cmp;
+    a.n_cmp = ctx->d_ncmp;
+    a.son = ctx->d_son;
+    a.n_son = ctx->d_nson;
+    a.list_cap = ctx->list_cap;
+    a.newbox = ctx->d_newbox;
+    a.err = ctx->d_err;
+    launch_compare<T>(a, ctx->grid, compare_smem_bytes(ctx->side_max, ctx->slab, sizeof(T) == 8), ctx->stream);
+    CK(cudaGetLastError());
+    ctx->q ^= 1;
+    ctx->p ^= 1;  // switchDistancebuffer, grainhdl.cpp:865
+    return GG_OK;
+}
+
+template <typename T>
+int stage_level_set_t(gg_ctx* ctx) {
+    const int p = ctx->p;
+    plan(ctx, ctx->d_box[p], 0, nullptr, nullptr, nullptr, nullptr, ctx->d_toff_mc);
+    MCArgs<T> a{};
+    a.G = ctx->G;
+    a.geo = ctx->geo;
+    a.toff = ctx->d_toff_mc;
+    a.present = ctx->d_present;
+    a.exists = ctx->d_exists;
+    a.in = arena<T>(ctx, p);
+    a.idl = ctx->d_idarena[ctx->q];
+    a.idoff = ctx->d_idoff[ctx->q];
+    a.newbox = ctx->d_newbox;
+    a.out_box = ctx->d_box[p ^ 1];
+    a.volume = ctx->d_volume;
+    a.surface = ctx->d_surface;
+    a.nb = ctx->d_nb;
+    a.n_nb = ctx->d_nnb;
+    a.nb_cap = kNbCap;
+    a.err = ctx->d_err;
+    launch_mc<T>(a, ctx->grid, ctx->stream);
+    CK(cudaGetLastError());
+    return GG_OK;
+}
+
+template <typename T>
+int stage_redistancing_t(gg_ctx* ctx) {
+    const int p = ctx->p;
+    // new packing of the resized output boxes
+    plan(ctx, ctx->d_box[p ^ 1], 1, ctx->d_off[p ^ 1], nullptr, ctx->d_toff_red, nullptr, nullptr);
+    int rc = read_counts(ctx, ctx->d_box[p ^ 1]);
+    if (rc) return rc;
+    const int side_new = ctx->h_count3[2];
+    rc = side_check(ctx, side_new);
+    if (rc) return rc;
+    rc = check_err(ctx, "redistancing plan");
+    if (rc) return rc;
+    rc = redistance<T>(ctx, p, p ^ 1, ctx->d_toff_red, std::max(side_new, ctx->side_max));
+    if (rc) return rc;
+    // in.resize(out dims), box.cpp:2581-2584
+    launch_copy_layout(ctx->G, ctx->d_present, ctx->d_box[p ^ 1], ctx->d_off[p ^ 1], ctx->d_box[p], ctx->d_off[p],
+                       ctx->stream);
+    ctx->side_max = side_new;
+    return GG_OK;
+}
+
+template <typename T>
+int step_t(gg_ctx* ctx, gg_step_stats* st) {
+    cudaEventRecord(ctx->ev[0], ctx->stream);
+    int rc = stage_convolution_t<T>(ctx);
+    if (rc) return rc;
+    cudaEventRecord(ctx->ev[1], ctx->stream);
+    if ((rc = stage_update_lists_t(ctx))) return rc;
+    cudaEventRecord(ctx->ev[2], ctx->stream);
+    if ((rc = stage_comparison_t<T>(ctx))) return rc;
+    cudaEventRecord(ctx->ev[3], ctx->stream);
+    if ((rc = stage_level_set_t<T>(ctx))) return rc;
+    cudaEventRecord(ctx->ev[4], ctx->stream);
+    if ((rc = stage_redistancing_t<T>(ctx))) return rc;
+    cudaEventRecord(ctx->ev[5], ctx->stream);
+    CK(cudaEventSynchronize(ctx->ev[5]));
+    rc = check_err(ctx, "gg_step");
+    if (rc) return rc;
+    if (st) {
+        st->loop = ctx->loop;
+        st->grain_count = ctx->grain_count;
+        st->live_grains = ctx->live;
+        st->voxel_updates = *ctx->h_total_vox;
+        float* f[5] = {&st->ms_convolution, &st->ms_lists, &st->ms_comparison, &st->ms_levelset, &st->ms_redistancing};
+        for (int i = 0; i < 5; i++) cudaEventElapsedTime(f[i], ctx->ev[i], ctx->ev[i + 1]);
+        cudaEventElapsedTime(&st->ms_total, ctx->ev[0], ctx->ev[5]);
+    }
+    ctx->loop++;
+    return GG_OK;
+}
+
+}  // namespace
+
+// ===================================================================================
+// C ABI
+// ===================================================================================
+namespace {
+
+// Box of the mode-4 LSbox constructor (box.cpp:239-304) followed by resizeToCube.
+Box initial_box(const int32_t* e, int gb, int M) {
+    int xmin = e[0], xmax = e[1], ymin = e[2], ymax = e[3], zmin = e[4], zmax = e[5];
+    xmax += 2 * gb;
+    ymax += 2 * gb;
+    zmax += 2 * gb;
+    if (ymax > M) ymax = M;
+    if (xmax > M) xmax = M;
+    if (zmax > M) zmax = M;
+    if (ymin < 0) ymin = 0;
+    if (xmin < 0) xmin = 0;
+    if (zmin < 0) zmin = 0;
+    Box b{xmin, xmax, ymin, ymax, zmin, zmax};
+    // DimensionalBuffer::resizeToCube, dimensionalBuffer.h:139-219
+    const int grid_size = M - 1;
+    const unsigned height = b.y1 - b.y0, width = b.x1 - b.x0, depth = b.z1 - b.z0;
+    if (width == height && width == depth) return b;
+    int ref = width > height ? (int)width : (int)height;
+    if (ref < (int)depth) ref = (int)depth;
+    if (ref > (int)width) { const int d = ref - (int)width; b.x0 -= d / 2; b.x1 += d / 2 + d % 2; }
+    if (ref > (int)height) { const int d = ref - (int)height; b.y0 -= d / 2; b.y1 += d / 2 + d % 2; }
+    if (ref > (int)depth) { const int d = ref - (int)depth; b.z0 -= d / 2; b.z1 += d / 2 + d % 2; }
+    if (b.x0 < 0) { const int d = -b.x0; b.x1 += d; b.x0 += d; }
+    else if (b.x1 > grid_size) { const int d = grid_size - b.x1; b.x1 += d; b.x0 += d; }
+    if (b.y0 < 0) { const int d = -b.y0; b.y1 += d; b.y0 += d; }
+    else if (b.y1 > grid_size) { const int d = grid_size - b.y1; b.y1 += d; b.y0 += d; }
+    if (b.z0 < 0) { const int d = -b.z0; b.z1 += d; b.z0 += d; }
+    else if (b.z1 > grid_size) { const int d = grid_size - b.z1; b.z1 += d; b.z0 += d; }
+    return b;
+}
+
+// Slab depth of the comparison tiles for the current largest box side.
+int pick_slab(int side, bool fp64) {
+    const size_t per = fp64 ? 12 : 8;
+    const size_t budget = 100 * 1024;
+    long long s = (long long)(budget / (per * (size_t)std::max(1, side * side)));
+    if (s < 1) s = 1;
+    if (s > 16) s = 16;
+    return (int)s;
+}
+
+int supported_side(bool fp64) {
+    const size_t lim = 227 * 1024;
+    int n = 8;
+    for (;;) {
+        const int m = n + 1;
+        bool ok = redist_smem_bytes(m, fp64) <= lim && compare_smem_bytes(m, 1, fp64) <= lim;
+        if (fp64) ok = ok && conv_f64_smem_bytes(m) <= lim;
+        else ok = ok && 3 * (size_t)m * (m | 1) * 4 <= lim;
+        if (!ok || m > 4096) return n;
+        n = m;
+    }
+}
+
+void free_all(gg_ctx* c) {
+    void* ptrs[] = {c->d_present, c->d_exists, c->d_newbox, c->d_nnb, c->d_volume, c->d_surface, c->d_nb, c->d_cmp,
+                    c->d_son, c->d_ncmp, c->d_nson, c->d_arena[0], c->d_arena[1], c->d_box[0], c->d_box[1],
+                    c->d_off[0], c->d_off[1], c->d_idarena[0], c->d_idarena[1], c->d_idbox[0], c->d_idbox[1],
+                    c->d_idoff[0], c->d_idoff[1], c->d_spec, c->d_spec_off, c->d_toff_n, c->d_toff_slab,
+                    c->d_toff_one, c->d_toff_mc, c->d_toff_red, c->d_tw, c->d_tw_off, c->d_gtab, c->d_g_off,
+                    c->d_circ, c->d_circ_off, c->d_err, c->d_total_vox, c->d_count3};
+    for (void* p : ptrs)
+        if (p) cudaFree(p);
+    if (c->h_count3) cudaFreeHost(c->h_count3);
+    if (c->h_total_vox) cudaFreeHost(c->h_total_vox);
+    for (auto& e : c->ev)
+        if (e) cudaEventDestroy(e);
+    if (c->stream) cudaStreamDestroy(c->stream);
+}
+
+}  // namespace
+
+extern "C" {
+
+int gg_create(const gg_params* params, gg_ctx** out) {
+    gg_ctx* ctx = nullptr;
+    if (!params || !out) return GG_ERR_INVALID;
+    *out = nullptr;
+    ctx = new gg_ctx();
+    ctx->P = *params;
+    const gg_params& P = ctx->P;
+    int rc = GG_OK;
+    if (P.domain_size < 2 || P.border < 0 || P.n_grains < 1 || !(P.time_step > 0))
+        rc = fail(ctx, GG_ERR_INVALID, "invalid geometry (domain_size=%d border=%d n_grains=%d)", P.domain_size,
+                  P.border, P.n_grains);
+    else if (P.precision != GG_PRECISION_FP64 && P.precision != GG_PRECISION_MIXED)
+        rc = fail(ctx, GG_ERR_INVALID, "unknown precision mode %d", P.precision);
+    else if (!P.disable_correction)
+        rc = fail(ctx, GG_ERR_UNSUPPORTED, "the convolution correction (DisableConvolutionCorrection=0) is not on this path");
+    if (rc) {
+        *out = ctx;  // keep the message readable through gg_last_error
+        return rc;
+    }
+    ctx->G = P.n_grains;
+    ctx->N = P.domain_size;
+    ctx->gb = P.border;
+    ctx->M = ctx->N + 2 * ctx->gb;
+    ctx->fp64 = P.precision == GG_PRECISION_FP64;
+    ctx->esz = ctx->fp64 ? 8 : 4;
+    ctx->geo = Geometry{ctx->N, ctx->gb, ctx->M, 1 / (double)ctx->N, ctx->gb / double(ctx->N), P.time_step};
+    ctx->list_cap = P.list_capacity > 0 ? P.list_capacity : 4096;
+    ctx->side_limit = supported_side(ctx->fp64);
+    *out = ctx;
+#undef CK_RET
+    cudaError_t e = cudaSetDevice(P.device);
+    if (e != cudaSuccess) return fail(ctx, GG_ERR_CUDA, "cudaSetDevice(%d): %s", P.device, cudaGetErrorString(e));
+    CK(cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking));
+    CK(cudaDeviceGetAttribute(&ctx->num_sms, cudaDevAttrMultiProcessorCount, P.device));
+    ctx->grid = ctx->num_sms * 8;
+    for (auto& ev : ctx->ev) CK(cudaEventCreate(&ev));
+    const size_t G1 = (size_t)ctx->G + 1;
+    CK(dalloc(&ctx->d_present, G1));
+    CK(dalloc(&ctx->d_exists, G1));
+    CK(dalloc(&ctx->d_newbox, 6 * G1));
+    CK(dalloc(&ctx->d_nnb, G1));
+    CK(dalloc(&ctx->d_volume, G1));
+    CK(dalloc(&ctx->d_surface, G1));
+    CK(dalloc(&ctx->d_nb, (size_t)kNbCap * G1));
+    CK(dalloc(&ctx->d_cmp, (size_t)ctx->list_cap * G1));
+    CK(dalloc(&ctx->d_son, (size_t)ctx->list_cap * G1));
+    CK(dalloc(&ctx->d_ncmp, G1));
+    CK(dalloc(&ctx->d_nson, G1));
+    for (int a = 0; a < 2; a++) {
+        CK(dalloc(&ctx->d_box[a], 6 * G1));
+        CK(dalloc(&ctx->d_off[a], G1));
+        CK(dalloc(&ctx->d_idbox[a], 6 * G1));
+        CK(dalloc(&ctx->d_idoff[a], G1));
+    }
+    CK(dalloc(&ctx->d_spec_off, G1));
+    CK(dalloc(&ctx->d_toff_n, G1 + 1));
+    CK(dalloc(&ctx->d_toff_slab, G1 + 1));
+    CK(dalloc(&ctx->d_toff_one, G1 + 1));
+    CK(dalloc(&ctx->d_toff_mc, G1 + 1));
+    CK(dalloc(&ctx->d_toff_red, G1 + 1));
+    CK(dalloc(&ctx->d_err, 1));
+    CK(dalloc(&ctx->d_total_vox, 1));
+    CK(dalloc(&ctx->d_count3, 3));
+    CK(cudaMallocHost((void**)&ctx->h_count3, 3 * sizeof(int)));
+    CK(cudaMallocHost((void**)&ctx->h_total_vox, sizeof(long long)));
+    CK(cudaMemset(ctx->d_err, 0, sizeof(int)));
+    CK(cudaMemset(ctx->d_total_vox, 0, sizeof(long long)));
+    CK(cudaMemset(ctx->d_present, 0, sizeof(int) * G1));
+    CK(cudaMemset(ctx->d_exists, 0, sizeof(int) * G1));
+    CK(cudaMemset(ctx->d_nnb, 0, sizeof(int) * G1));
+    CK(cudaMemset(ctx->d_ncmp, 0, sizeof(int) * G1));
+    CK(cudaMemset(ctx->d_nson, 0, sizeof(int) * G1));
+    CK(cudaMemset(ctx->d_volume, 0, sizeof(double) * G1));
+    CK(cudaMemset(ctx->d_surface, 0, sizeof(double) * G1));
+    for (int a = 0; a < 2; a++) {
+        CK(cudaMemset(ctx->d_box[a], 0, sizeof(int) * 6 * G1));
+        CK(cudaMemset(ctx->d_off[a], 0, sizeof(long long) * G1));
+        CK(cudaMemset(ctx->d_idbox[a], 0, sizeof(int) * 6 * G1));
+        CK(cudaMemset(ctx->d_idoff[a], 0, sizeof(long long) * G1));
+    }
+    return upload_tables(ctx);
+}
+
+int gg_destroy(gg_ctx* ctx) {
+    if (!ctx) return GG_OK;
+    free_all(ctx);
+    delete ctx;
+    return GG_OK;
+}
+
+const char* gg_last_error(const gg_ctx* ctx) { return ctx ? ctx->err.c_str() : "no context"; }
+
+int gg_load_state(gg_ctx* ctx, const uint32_t* labels, const int32_t* extents, const int64_t* counts) {
+    if (!ctx || !labels || !extents || !counts) return GG_ERR_INVALID;
+    if (ctx->loaded) return fail(ctx, GG_ERR_INVALID, "state already loaded");
+    const int G = ctx->G, gb = ctx->gb, M = ctx->M;
+    std::vector<int> present(G + 1, 0), box(6 * (G + 1), 0);
+    long long need = 0;
+    int side = 0;
+    for (int g = 1; g <= G; g++) {
+        if (counts[g - 1] <= 0) continue;  // the reference skips empty grains, grainhdl.cpp:492-497
+        const Box b = initial_box(extents + 6 * (g - 1), gb, M);
+        if (b.x0 < 0 || b.y0 < 0 || b.z0 < 0 || b.nx() <= 0 || b.nx() != b.ny() || b.nx() != b.nz())
+            return fail(ctx, GG_ERR_INVALID, "grain %d: invalid initial box", g);
+        present[g] = 1;
+        store_box(&box[6 * g], b);
+        need += (b.count() + 31) / 32 * 32;
+        side = std::max(side, b.nx());
+    }
+    int rc = side_check(ctx, side);
+    if (rc) return rc;
+    ctx->side_max = side;
+    ctx->pool_voxels = ctx->P.pool_voxels > 0 ? ctx->P.pool_voxels : 2 * need + 4096;
+    if (need > ctx->pool_voxels)
+        return fail(ctx, GG_ERR_POOL_EXHAUSTED, "initial boxes need %lld voxels, pool holds %lld", need,
+                    ctx->pool_voxels);
+    ctx->spec_capacity = ctx->fp64 ? (ctx->pool_voxels * 6) / 10 + 32LL * (G + 1) : 0;
+    for (int a = 0; a < 2; a++) {
+        CK(cudaMalloc(&ctx->d_arena[a], ctx->esz * ctx->pool_voxels));
+        CK(dalloc(&ctx->d_idarena[a], ctx->pool_voxels));
+    }
+    if (ctx->fp64) CK(dalloc(&ctx->d_spec, ctx->spec_capacity));
+    const size_t G1 = (size_t)G + 1;
+    CK(cudaMemcpy(ctx->d_present, present.data(), sizeof(int) * G1, cudaMemcpyHostToDevice));
+    CK(cudaMemcpy(ctx->d_exists, present.data(), sizeof(int) * G1, cudaMemcpyHostToDevice));
+    CK(cudaMemcpy(ctx->d_box[0], box.data(), sizeof(int) * 6 * G1, cudaMemcpyHostToDevice));
+    rc = ctx->fp64 ? load_state_t<double>(ctx, labels) : load_state_t<float>(ctx, labels);
+    if (rc) return rc;
+    rc = read_counts(ctx, ctx->d_box[1]);
+    if (rc) return rc;
+    ctx->loaded = true;
+    ctx->loop = 0;
+    return GG_OK;
+}
+
+int gg_set_lists(gg_ctx* ctx, const int64_t* offsets, const uint32_t* ids) {
+    if (!ctx || !offsets || (!ids && offsets[ctx->G + 1] > 0)) return GG_ERR_INVALID;
+    const int G = ctx->G, cap = ctx->list_cap;
+    std::vector<uint32_t> rows((size_t)cap * (G + 1), 0);
+    std::vector<int> n(G + 1, 0);
+    for (int g = 1; g <= G; g++) {
+        const int64_t len = offsets[g + 1] - offsets[g];
+        if (len < 0 || len > cap) return fail(ctx, GG_ERR_LIST_OVERFLOW, "list of grain %d has %lld entries", g, (long long)len);
+        for (int64_t k = 0; k < len; k++) {
+            const uint32_t v = ids[offsets[g] + k];
+            if (v < 1 || v > (uint32_t)G) return fail(ctx, GG_ERR_INVALID, "list of grain %d names grain %u", g, v);
+            rows[(size_t)g * cap + k] = v;
+        }
+        n[g] = (int)len;
+    }
+    CK(cudaMemcpy(ctx->d_son, rows.data(), rows.size() * sizeof(uint32_t), cudaMemcpyHostToDevice));
+    CK(cudaMemcpy(ctx->d_nson, n.data(), n.size() * sizeof(int), cudaMemcpyHostToDevice));
+    CK(cudaMemcpy(ctx->d_cmp, rows.data(), rows.size() * sizeof(uint32_t), cudaMemcpyHostToDevice));
+    CK(cudaMemcpy(ctx->d_ncmp, n.data(), n.size() * sizeof(int), cudaMemcpyHostToDevice));
+    return GG_OK;
+}
+
+int gg_default_lists(gg_ctx* ctx) {
+    if (!ctx || !ctx->loaded) return GG_ERR_INVALID;
+    const int G = ctx->G;
+    std::vector<int> box(6 * (G + 1)), present(G + 1);
+    CK(cudaMemcpy(box.data(), ctx->d_box[ctx->p ^ 1], sizeof(int) * box.size(), cudaMemcpyDeviceToHost));
+    CK(cudaMemcpy(present.data(), ctx->d_present, sizeof(int) * present.size(), cudaMemcpyDeviceToHost));
+    // uniform grid of cells no smaller than the largest box: each box meets at most 8 cells
+    const int cell = std::max(1, ctx->side_max + 1);
+    const int nc = ctx->M / cell + 2;
+    std::vector<std::vector<int>> cells((size_t)nc * nc * nc);
+    auto cid = [&](int x, int y, int z) { return ((size_t)z * nc + y) * nc + x; };
+    for (int g = 1; g <= G; g++) {
+        if (!present[g]) continue;
+        const int* b = &box[6 * g];
+        for (int z = b[4] / cell; z <= b[5] / cell; z++)
+            for (int y = b[2] / cell; y <= b[3] / cell; y++)
+                for (int x = b[0] / cell; x <= b[1] / cell; x++) cells[cid(x, y, z)].push_back(g);
+    }
+    std::vector<int64_t> off(G + 2, 0);
+    std::vector<uint32_t> ids;
+    std::vector<int> seen(G + 1, 0);
+    for (int g = 1; g <= G; g++) {
+        off[g] = (int64_t)ids.size();
+        if (!present[g]) continue;
+        const int* a = &box[6 * g];
+        std::vector<uint32_t> mine;
+        for (int z = a[4] / cell; z <= a[5] / cell; z++)
+            for (int y = a[2] / cell; y <= a[3] / cell; y++)
+                for (int x = a[0] / cell; x <= a[1] / cell; x++)
+                    for (int o : cells[cid(x, y, z)]) {
+                        if (o == g || seen[o] == g) continue;
+                        const int* b = &box[6 * o];
+                        // inclusive overlap, as the reference's R-tree search (RTree.h Overlap)
+                        if (a[0] > b[1] || a[1] < b[0] || a[2] > b[3] || a[3] < b[2] || a[4] > b[5] || a[5] < b[4])
+                            continue;
+                        seen[o] = g;
+                        mine.push_back((uint32_t)o);
+                    }
+        std::sort(mine.begin(), mine.end());
+        ids.insert(ids.end(), mine.begin(), mine.end());
+    }
+    off[G + 1] = (int64_t)ids.size();
+    return gg_set_lists(ctx, off.data(), ids.data());
+}
+
+int gg_stage_convolution(gg_ctx* ctx) {
+    if (!ctx || !ctx->loaded) return GG_ERR_INVALID;
+    ctx->slab = pick_slab(ctx->side_max, ctx->fp64);
+    int rc = ctx->fp64 ? stage_convolution_t<double>(ctx) : stage_convolution_t<float>(ctx);
+    return rc ? rc : check_err(ctx, "convolution");
+}
+int gg_stage_update_lists(gg_ctx* ctx) {
+    if (!ctx || !ctx->loaded) return GG_ERR_INVALID;
+    int rc = stage_update_lists_t(ctx);
+    return rc ? rc : check_err(ctx, "update lists");
+}
+int gg_stage_comparison(gg_ctx* ctx) {
+    if (!ctx || !ctx->loaded) return GG_ERR_INVALID;
+    int rc = ctx->fp64 ? stage_comparison_t<double>(ctx) : stage_comparison_t<float>(ctx);
+    return rc ? rc : check_err(ctx, "comparison");
+}
+int gg_stage_level_set(gg_ctx* ctx) {
+    if (!ctx || !ctx->loaded) return GG_ERR_INVALID;
+    int rc = ctx->fp64 ? stage_level_set_t<double>(ctx) : stage_level_set_t<float>(ctx);
+    return rc ? rc : check_err(ctx, "level set");
+}
+int gg_stage_redistancing(gg_ctx* ctx) {
+    if (!ctx || !ctx->loaded) return GG_ERR_INVALID;
+    int rc = ctx->fp64 ? stage_redistancing_t<double>(ctx) : stage_redistancing_t<float>(ctx);
+    if (rc) return rc;
+    rc = check_err(ctx, "redistancing");
+    if (rc) return rc;
+    ctx->loop++;
+    return GG_OK;
+}
+
+int gg_step(gg_ctx* ctx, gg_step_stats* stats) {
+    if (!ctx || !ctx->loaded) return GG_ERR_INVALID;
+    ctx->slab = pick_slab(ctx->side_max, ctx->fp64);
+    return ctx->fp64 ? step_t<double>(ctx, stats) : step_t<float>(ctx, stats);
+}
+
+int gg_get_grain_stats(gg_ctx* ctx, uint8_t* exists, double* volume, double* surface, int32_t* boxes,
+                       int32_t* n_neighbors) {
+    if (!ctx || !ctx->loaded) return GG_ERR_INVALID;
+    const size_t G1 = (size_t)ctx->G + 1;
+    CK(cudaStreamSynchronize(ctx->stream));
+    if (exists) {
+        std::vector<int> pr(G1), ex(G1);
+        CK(cudaMemcpy(pr.data(), ctx->d_present, sizeof(int) * G1, cudaMemcpyDeviceToHost));
+        CK(cudaMemcpy(ex.data(), ctx->d_exists, sizeof(int) * G1, cudaMemcpyDeviceToHost));
+        for (size_t g = 0; g < G1; g++) exists[g] = (uint8_t)(g > 0 && pr[g] && ex[g]);
+    }
+    if (volume) CK(cudaMemcpy(volume, ctx->d_volume, sizeof(double) * G1, cudaMemcpyDeviceToHost));
+    if (surface) CK(cudaMemcpy(surface, ctx->d_surface, sizeof(double) * G1, cudaMemcpyDeviceToHost));
+    if (boxes) CK(cudaMemcpy(boxes, ctx->d_box[ctx->p ^ 1], sizeof(int) * 6 * G1, cudaMemcpyDeviceToHost));
+    if (n_neighbors) CK(cudaMemcpy(n_neighbors, ctx->d_nnb, sizeof(int) * G1, cudaMemcpyDeviceToHost));
+    return GG_OK;
+}
+
+int gg_get_neighbors(gg_ctx* ctx, int32_t id, uint32_t* out, int32_t cap) {
+    if (!ctx || id < 1 || id > ctx->G) return GG_ERR_INVALID;
+    int n = 0;
+    CK(cudaMemcpy(&n, ctx->d_nnb + id, sizeof(int), cudaMemcpyDeviceToHost));
+    const int k = std::min(std::min(n, cap), kNbCap);
+    if (out && k > 0)
+        CK(cudaMemcpy(out, ctx->d_nb + (size_t)id * kNbCap, sizeof(uint32_t) * k, cudaMemcpyDeviceToHost));
+    return n;
+}
+
+int gg_get_list(gg_ctx* ctx, int32_t id, uint32_t* out, int32_t cap) {
+    if (!ctx || id < 1 || id > ctx->G) return GG_ERR_INVALID;
+    int n = 0;
+    CK(cudaMemcpy(&n, ctx->d_ncmp + id, sizeof(int), cudaMemcpyDeviceToHost));
+    const int k = std::min(n, cap);
+    if (out && k > 0)
+        CK(cudaMemcpy(out, ctx->d_cmp + (size_t)id * ctx->list_cap, sizeof(uint32_t) * k, cudaMemcpyDeviceToHost));
+    return n;
+}
+
+int64_t gg_get_sdf(gg_ctx* ctx, int32_t id, int32_t which, int32_t box[6], double* out, int64_t cap) {
+    if (!ctx || !ctx->loaded || id < 1 || id > ctx->G || !box) return GG_ERR_INVALID;
+    const int a = which == 0 ? ctx->p : ctx->p ^ 1;
+    long long off = 0;
+    CK(cudaMemcpy(box, ctx->d_box[a] + 6 * id, sizeof(int) * 6, cudaMemcpyDeviceToHost));
+    CK(cudaMemcpy(&off, ctx->d_off[a] + id, sizeof(long long), cudaMemcpyDeviceToHost));
+    const Box b = load_box(box);
+    const long long n = b.count();
+    if (out && n > 0) {
+        const long long k = std::min((long long)cap, n);
+        if (ctx->fp64) {
+            CK(cudaMemcpy(out, (double*)ctx->d_arena[a] + off, sizeof(double) * k, cudaMemcpyDeviceToHost));
+        } else {
+            std::vector<float> tmp(k);
+            CK(cudaMemcpy(tmp.data(), (float*)ctx->d_arena[a] + off, sizeof(float) * k, cudaMemcpyDeviceToHost));
+            for (long long i = 0; i < k; i++) out[i] = tmp[i];
+        }
+    }
+    return n;
+}
+
+int64_t gg_get_idlocal(gg_ctx* ctx, int32_t id, int32_t box[6], uint32_t* out, int64_t cap) {
+    if (!ctx || !ctx->loaded || id < 1 || id > ctx->G || !box) return GG_ERR_INVALID;
+    long long off = 0;
+    CK(cudaMemcpy(box, ctx->d_idbox[ctx->q] + 6 * id, sizeof(int) * 6, cudaMemcpyDeviceToHost));
+    CK(cudaMemcpy(&off, ctx->d_idoff[ctx->q] + id, sizeof(long long), cudaMemcpyDeviceToHost));
+    const long long n = load_box(box).count();
+    if (out && n > 0)
+        CK(cudaMemcpy(out, ctx->d_idarena[ctx->q] + off, sizeof(uint32_t) * std::min((long long)cap, n),
+                      cudaMemcpyDeviceToHost));
+    return n;
+}
+
+int gg_grain_count(gg_ctx* ctx) { return ctx ? ctx->grain_count : GG_ERR_INVALID; }
+int gg_loop(gg_ctx* ctx) { return ctx ? ctx->loop : GG_ERR_INVALID; }
+
+int gg_convolve_boxes_f64(const double* d_in, double* d_out, const int32_t* sides, const int64_t* offs,
+                          int32_t n_boxes, int32_t domain_size, double time_step) {
+    gg_ctx* ctx = nullptr;  // for CK: no context to carry a message
+    if (!d_in || !d_out || !sides || !offs || n_boxes < 1 || domain_size < 1) return GG_ERR_INVALID;
+    int nmax = 0;
+    for (int b = 0; b < n_boxes; b++) nmax = std::max(nmax, (int)sides[b]);
+    if (nmax < 1 || conv_f64_smem_bytes(nmax) > 227 * 1024) return GG_ERR_UNSUPPORTED;
+    std::vector<double2> tw;
+    std::vector<long long> tw_off(nmax + 2, 0), g_off(nmax + 2, 0);
+    std::vector<double> gt;
+    for (int n = 1; n <= nmax; n++) {
+        tw_off[n] = (long long)tw.size();
+        twiddle_table(n, tw);
+        g_off[n] = (long long)gt.size();
+        gaussian_table(n, domain_size, time_step, gt);
+    }
+    // grains 1..n_boxes, box b at (0, n, 0, n, 0, n)
+    std::vector<int> box(6 * (n_boxes + 1), 0);
+    std::vector<long long> off(n_boxes + 1, 0), spec_off(n_boxes + 1, 0);
+    std::vector<int> toff(n_boxes + 2, 0);
+    long long spec_total = 0;
+    for (int b = 0; b < n_boxes; b++) {
+        const int n = sides[b];
+        int* bb = &box[6 * (b + 1)];
+        bb[1] = bb[3] = bb[5] = n;
+        off[b + 1] = offs[b];
+        spec_off[b + 1] = spec_total;
+        spec_total += (long long)n * n * (n / 2 + 1);
+        toff[b + 2] = toff[b + 1] + n;
+    }
+    double2 *d_tw = nullptr, *d_spec = nullptr;
+    double* d_gt = nullptr;
+    long long *d_tw_off = nullptr, *d_g_off = nullptr, *d_off = nullptr, *d_spec_off = nullptr;
+    int *d_box = nullptr, *d_toff = nullptr;
+    CK(dalloc(&d_tw, tw.size()));
+    CK(dalloc(&d_gt, gt.size()));
+    CK(dalloc(&d_tw_off, tw_off.size()));
+    CK(dalloc(&d_g_off, g_off.size()));
+    CK(dalloc(&d_spec, spec_total));
+    CK(dalloc(&d_box, box.size()));
+    CK(dalloc(&d_off, off.size()));
+    CK(dalloc(&d_spec_off, spec_off.size()));
+    CK(dalloc(&d_toff, toff.size()));
+    CK(cudaMemcpy(d_tw, tw.data(), sizeof(double2) * tw.size(), cudaMemcpyHostToDevice));
+    CK(cudaMemcpy(d_gt, gt.data(), sizeof(double) * gt.size(), cudaMemcpyHostToDevice));
+    CK(cudaMemcpy(d_tw_off, tw_off.data(), sizeof(long long) * tw_off.size(), cudaMemcpyHostToDevice));
+    CK(cudaMemcpy(d_g_off, g_off.data(), sizeof(long long) * g_off.size(), cudaMemcpyHostToDevice));
+    CK(cudaMemcpy(d_box, box.data(), sizeof(int) * box.size(), cudaMemcpyHostToDevice));
+    CK(cudaMemcpy(d_off, off.data(), sizeof(long long) * off.size(), cudaMemcpyHostToDevice));
+    CK(cudaMemcpy(d_spec_off, spec_off.data(), sizeof(long long) * spec_off.size(), cudaMemcpyHostToDevice));
+    CK(cudaMemcpy(d_toff, toff.data(), sizeof(int) * toff.size(), cudaMemcpyHostToDevice));
+    ConvArgs a{};
+    a.G = n_boxes;
+    a.toff = d_toff;
+    a.in = d_in;
+    a.in_box = d_box;
+    a.in_off = d_off;
+    a.out = d_out;
+    a.out_off = d_off;
+    a.spec = d_spec;
+    a.spec_off = d_spec_off;
+    a.tw = d_tw;
+    a.tw_off = d_tw_off;
+    a.gtab = d_gt;
+    a.g_off = d_g_off;
+    int sms = 148;
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, 0);
+    launch_conv_f64(a, sms * 8, conv_f64_smem_bytes(nmax), 0);
+    CK(cudaGetLastError());
+    CK(cudaDeviceSynchronize());
+    void* ptrs[] = {d_tw, d_gt, d_tw_off, d_g_off, d_spec, d_box, d_off, d_spec_off, d_toff};
+    for (void* p : ptrs) cudaFree(p);
+    return GG_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,108 @@
+// gg_common.cuh -- device-side state shared by the level-set kernels.
+//
+// All grain boxes live in two SDF arenas in HBM.  Arena a holds the buffer that
+// the reference calls m_inputDistance or m_outputDistance depending on a parity
+// the host flips at every switchDistancebuffer (grainhdl.cpp:1166-1178), so a
+// swap costs nothing.  Each arena has its own per-grain box and element offset:
+// the two layouts agree except while redistancing writes the new (resized) boxes
+// (box.cpp:2322-2586).  IDLocal lives in two more arenas with the same scheme, so
+// the flat-prefix resize of the reference (dimensionalBuffer.h:120-131) becomes a
+// read from the previous layout.
+#pragma once
+
+#include <cstdint>
+#include <cuda_runtime.h>
+
+namespace gg {
+
+// Error bits set by kernels (atomicOr) and reported by the host.
+enum : int {
+    ERR_POOL = 1,        // arena or scratch capacity exceeded
+    ERR_LIST = 2,        // comparison list capacity exceeded
+    ERR_NEIGHBORS = 4,   // hull neighbour set capacity exceeded
+    ERR_HASH = 8,        // list-update hash table overflow
+    ERR_BOX = 16,        // a box outside the grid or larger than supported
+};
+
+struct Box {
+    int x0, x1, y0, y1, z0, z1;
+    __host__ __device__ int nx() const { return x1 - x0; }
+    __host__ __device__ int ny() const { return y1 - y0; }
+    __host__ __device__ int nz() const { return z1 - z0; }
+    __host__ __device__ long long count() const { return (long long)nx() * ny() * nz(); }
+    // getValueAt(row=i (y), column=j (x), depth=k (z)), dimensionalBuffer.h:71-76
+    __host__ __device__ long long at(int i, int j, int k) const {
+        return ((long long)(k - z0) * ny() + (i - y0)) * nx() + (j - x0);
+    }
+};
+
+__host__ __device__ inline Box load_box(const int* b6) { return Box{b6[0], b6[1], b6[2], b6[3], b6[4], b6[5]}; }
+__host__ __device__ inline void store_box(int* b6, const Box& b) {
+    b6[0] = b.x0; b6[1] = b.x1; b6[2] = b.y0; b6[3] = b.y1; b6[4] = b.z0; b6[5] = b.z1;
+}
+
+// One arena's view: data, per-grain boxes (6 ints) and element offsets.
+template <typename T>
+struct Arena {
+    T* data;
+    int* box;
+    long long* off;
+    __device__ Box grain_box(int g) const { return load_box(box + 6 * g); }
+    __device__ T* grain_ptr(int g) const { return data + off[g]; }
+};
+
+// Per-grain bookkeeping (entries 0..G, entry 0 = boundary grain, never processed).
+struct Grains {
+    int G;               // n_grains
+    int* present;        // grains[id] != NULL
+    int* exists;         // LSbox::m_exists
+    int* newbox;         // m_newXMin.. from executeSetComparison (6 per grain)
+    double* volume;      // m_volume
+    double* surface;     // m_surface
+    int* n_nb;           // distinct hull neighbours
+    uint32_t* nb;        // nb_cap per grain
+    int nb_cap;
+    uint32_t* cmp;       // m_comparisonList, list_cap per grain
+    int* n_cmp;
+    uint32_t* son;       // m_secondOrderNeighbours, list_cap per grain
+    int* n_son;
+    int list_cap;
+};
+
+struct Geometry {
+    int N;          // realDomainSize
+    int gb;         // grid_blowup = DomainBorderSize
+    int M;          // ngridpoints = N + 2 gb
+    double h;       // 1 / N
+    double delta;   // gb / N
+    double time_step;
+};
+
+// Map a flat tile index to (grain, local tile) through an exclusive scan of
+// per-grain tile counts (toff has G + 2 entries; toff[g] = first tile of g).
+__device__ __forceinline__ int tile_grain(const int* __restrict__ toff, int G, int t) {
+    int lo = 1, hi = G + 1;  // find the last g in [1, G] with toff[g] <= t
+    while (hi - lo > 1) {
+        int mid = (lo + hi) >> 1;
+        if (__ldg(toff + mid) <= t) lo = mid; else hi = mid;
+    }
+    return lo;
+}
+
+// Opt a kernel into the largest dynamic shared memory the device allows next to
+// its static shared memory.
+template <typename K>
+inline cudaError_t allow_max_dynamic_smem(K* kernel) {
+    int dev = 0, optin = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
+    cudaFuncAttributes fa{};
+    cudaError_t e = cudaFuncGetAttributes(&fa, kernel);
+    if (e != cudaSuccess) return e;
+    return cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, optin - (int)fa.sharedSizeBytes);
+}
+
+__device__ __forceinline__ int isgn(double v) { return (0.0 < v) - (v < 0.0); }  // utilities.h:27-30
+__device__ __forceinline__ int isgn(float v) { return (0.0f < v) - (v < 0.0f); }
+
+}  // namespace gg

@@ -1,0 +1,135 @@
+// gg_kernels.cuh -- launch interfaces of the level-set stage kernels.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <cstdint>
+
+#include "gg_common.cuh"
+
+namespace gg {
+
+// ---- planner (gg_plan.cu) ----
+struct PlanArgs {
+    int G;
+    const int* present;
+    const int* exists;
+    const int* box;           // boxes to plan from (6 per grain)
+    int only_existing;        // 1: grains with present && exists; 0: present
+    long long* off;           // out: element offsets (aligned), may be null
+    long long capacity;       // arena capacity in elements (off != null)
+    long long* spec_off;      // out: half-spectrum offsets (complex elements), may be null
+    long long spec_capacity;
+    int* toff_n;              // out: tile offsets with n tiles per grain, may be null
+    int* toff_slab;           // out: tile offsets with ceil(n / slab) tiles per grain, may be null
+    int slab;
+    int* toff_one;            // out: tile offsets with one tile per grain, may be null
+    int* box_copy;            // out: copy of box (6 per grain), may be null
+    long long* off_copy;      // out: copy of off, may be null
+    long long* total_voxels;  // out: sum of n^3 over planned grains (device scalar), may be null
+    int* err;
+};
+void launch_plan(const PlanArgs& a, cudaStream_t s);
+
+// Copy box + offsets of every present grain from one layout to another.
+void launch_copy_layout(int G, const int* present, const int* box_src, const long long* off_src, int* box_dst,
+                        long long* off_dst, cudaStream_t s);
+
+// ---- comparison (gg_compare.cu) ----
+template <typename T>
+struct CompareArgs {
+    int G;
+    Geometry geo;
+    const int* toff;          // slab tiles
+    int slab;
+    const int* exists;
+    Arena<T> in;              // convolved SDFs (self and neighbours)
+    Arena<T> out;             // comparison result written here (same boxes as in)
+    const uint32_t* id_old;   // IDLocal of the previous layout
+    const int* idbox_old;
+    const long long* idoff_old;
+    uint32_t* id_new;         // IDLocal on the current boxes
+    const long long* idoff_new;
+    const uint32_t* cmp;      // comparison lists
+    const int* n_cmp;
+    uint32_t* son;            // m_secondOrderNeighbours := m_comparisonList
+    int* n_son;
+    int list_cap;
+    int* newbox;              // per grain min/max (pre-initialised)
+    int* err;
+};
+template <typename T>
+void launch_compare(const CompareArgs<T>& a, int grid, size_t smem, cudaStream_t s);
+size_t compare_smem_bytes(int nmax, int slab, bool fp64);
+void launch_newbox_init(int G, const int* present, const int* exists, const int* box, int* newbox, cudaStream_t s);
+
+// ---- list update (gg_lists.cu) ----
+struct ListArgs {
+    int G;
+    const int* toff;          // one tile per existing grain
+    const int* exists;
+    const int* box;           // in-arena boxes (LSbox::checkIntersection uses m_inputDistance)
+    const uint32_t* son;
+    const int* n_son;
+    uint32_t* cmp;
+    int* n_cmp;
+    int list_cap;
+    int hash_cap;             // power of two
+    int* err;
+};
+void launch_update_lists(const ListArgs& a, int grid, cudaStream_t s);
+
+// ---- marching cubes + hull statistics (gg_mc.cu) ----
+template <typename T>
+struct MCArgs {
+    int G;
+    Geometry geo;
+    const int* toff;          // one tile per present grain
+    int* present;
+    int* exists;
+    Arena<T> in;              // compared SDF
+    const uint32_t* idl;      // IDLocal (same layout as in)
+    const long long* idoff;
+    const int* newbox;        // from the comparison
+    int* out_box;             // new box (resized to cube) written here for existing grains
+    double* volume;
+    double* surface;
+    uint32_t* nb;
+    int* n_nb;
+    int nb_cap;
+    int* err;
+};
+template <typename T>
+void launch_mc(const MCArgs<T>& a, int grid, cudaStream_t s);
+
+// ---- redistancing (gg_redist.cu) ----
+template <typename T>
+struct RedistArgs {
+    int G;
+    Geometry geo;
+    const int* toff;          // n tiles per grain (n of the output box)
+    const int* exists;
+    Arena<T> in;
+    Arena<T> out;
+    int* err;
+};
+template <typename T>
+void launch_redistance(const RedistArgs<T>& a, int grid, size_t smem_xy, size_t smem_z, cudaStream_t s);
+size_t redist_smem_bytes(int nmax, bool fp64);
+
+// ---- initial distance function (gg_init.cu) ----
+template <typename T>
+struct InitArgs {
+    int G;
+    Geometry geo;
+    const int* toff;          // n tiles per present grain
+    const int* present;
+    Arena<T> dst;
+    const uint32_t* labels;   // N^3 domain labels [z][y][x]
+};
+template <typename T>
+void launch_init_sdf(const InitArgs<T>& a, int grid, cudaStream_t s);
+
+// out3 = {present grains, present and existing grains, largest side of `box` among the latter}
+void launch_count(int G, const int* present, const int* exists, const int* box, int* out3, cudaStream_t s);
+
+}  // namespace gg

@@ -1,0 +1,149 @@
+// gg_lists.cu -- comparison-list maintenance of every grain.
+//
+// Stands in for LSbox::computeSecondOrderNeighbours (box.cpp:1090-1134), called
+// from grainhdl::updateSecondOrderNeighbors (grainhdl.cpp:1015-1027).  The new list
+// is: the members of the previous list that still exist, in order; then every
+// grain that appears in a member's own list, exists, is not the grain itself nor
+// the boundary grain, and whose box touches this grain's box (inclusive overlap,
+// box.cpp:880-889), in order of first appearance.
+//
+// The reference scans member lists pairwise with linear de-duplication.  Here one
+// CTA per grain hashes every (member i, entry j) of the neighbours' lists into
+// shared memory keeping the smallest enumeration position i * cap + j per ID.
+// Whether an ID qualifies depends on the ID alone, so its first position overall
+// is its first qualifying position; the qualifying new IDs are then ranked by
+// that position, which reproduces the reference's order exactly.
+#include "gg_kernels.cuh"
+
+namespace gg {
+
+namespace {
+
+constexpr int kThreads = 512;
+constexpr int kSel = 2048;
+constexpr unsigned kEmpty = 0xFFFFFFFFu;
+
+__device__ __forceinline__ int hash_slot(unsigned* hkey, unsigned id, int cap, int* err) {
+    unsigned h = (id * 2654435761u) & (unsigned)(cap - 1);
+    for (int probe = 0; probe < cap; probe++) {
+        const unsigned prev = atomicCAS(hkey + h, kEmpty, id);
+        if (prev == kEmpty || prev == id) return (int)h;
+        h = (h + 1) & (unsigned)(cap - 1);
+    }
+    atomicOr(err, ERR_HASH);
+    return -1;
+}
+
+__device__ __forceinline__ bool touch(const Box& a, const Box& b) {  // LSbox::checkIntersection
+    return !(a.x0 > b.x1 || a.x1 < b.x0 || a.y0 > b.y1 || a.y1 < b.y0 || a.z0 > b.z1 || a.z1 < b.z0);
+}
+
+__global__ void __launch_bounds__(kThreads) update_lists_kernel(ListArgs a) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    const int HC = a.hash_cap;
+    unsigned* hkey = reinterpret_cast<unsigned*>(smem_raw);
+    unsigned* hval = hkey + HC;
+    unsigned* hflag = hval + HC;
+    unsigned* sel_pos = hflag + HC;
+    unsigned* sel_id = sel_pos + kSel;
+    __shared__ int warp_sums[33];
+    __shared__ int n_sel;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+    const int total = a.toff[a.G + 1];
+    for (int t = blockIdx.x; t < total; t += gridDim.x) {
+        const int g = tile_grain(a.toff, a.G, t);
+        const int K = a.n_son[g];
+        const uint32_t* son = a.son + (long long)g * a.list_cap;
+        uint32_t* cmp = a.cmp + (long long)g * a.list_cap;
+        for (int q = threadIdx.x; q < HC; q += blockDim.x) { hkey[q] = kEmpty; hval[q] = kEmpty; hflag[q] = 0; }
+        if (threadIdx.x == 0) n_sel = 0;
+        __syncthreads();
+        // 1. existing members of the previous list, in order (block compaction)
+        int prefix = 0;
+        for (int base = 0; base < K; base += blockDim.x) {
+            const int i = base + threadIdx.x;
+            const unsigned id = i < K ? son[i] : 0u;
+            const int f = (i < K && a.exists[id]) ? 1 : 0;
+            int incl = f;
+#pragma unroll
+            for (int o = 1; o < 32; o <<= 1) {
+                const int u = __shfl_up_sync(0xffffffffu, incl, o);
+                if (lane >= o) incl += u;
+            }
+            if (lane == 31) warp_sums[warp] = incl;
+            __syncthreads();
+            if (warp == 0) {
+                const int w = lane < nw ? warp_sums[lane] : 0;
+                int wi = w;
+#pragma unroll
+                for (int o = 1; o < 32; o <<= 1) {
+                    const int u = __shfl_up_sync(0xffffffffu, wi, o);
+                    if (lane >= o) wi += u;
+                }
+                if (lane < nw) warp_sums[lane] = wi - w;
+                if (lane == 31) warp_sums[32] = wi;
+            }
+            __syncthreads();
+            if (f) {
+                const int pos = prefix + warp_sums[warp] + incl - f;
+                if (pos < a.list_cap) cmp[pos] = id;
+                const int slot = hash_slot(hkey, id, HC, a.err);
+                if (slot >= 0) hflag[slot] = 1;
+            }
+            prefix += warp_sums[32];
+            __syncthreads();
+        }
+        // 2. hash every entry of every member's list with its first position
+        for (int i = warp; i < K; i += nw) {
+            const unsigned c = son[i];
+            const int Kc = a.n_son[c];
+            const uint32_t* sc = a.son + (long long)c * a.list_cap;
+            for (int j = lane; j < Kc; j += 32) {
+                const unsigned id = sc[j];
+                const int slot = hash_slot(hkey, id, HC, a.err);
+                if (slot >= 0) atomicMin(hval + slot, (unsigned)i * (unsigned)a.list_cap + (unsigned)j);
+            }
+        }
+        __syncthreads();
+        // 3. keep the qualifying new IDs
+        const Box self = load_box(a.box + 6 * g);
+        for (int q = threadIdx.x; q < HC; q += blockDim.x) {
+            const unsigned id = hkey[q];
+            if (id == kEmpty || hflag[q] || hval[q] == kEmpty) continue;
+            if (id == (unsigned)g || id == 0u || id > (unsigned)a.G || !a.exists[id]) continue;
+            if (!touch(self, load_box(a.box + 6 * id))) continue;
+            const int s = atomicAdd(&n_sel, 1);
+            if (s < kSel) { sel_pos[s] = hval[q]; sel_id[s] = id; }
+        }
+        __syncthreads();
+        // 4. append them by first position
+        const int ns = min(n_sel, kSel);
+        for (int q = threadIdx.x; q < ns; q += blockDim.x) {
+            const unsigned pq = sel_pos[q];
+            int rank = 0;
+            for (int r = 0; r < ns; r++) rank += sel_pos[r] < pq;
+            const int pos = prefix + rank;
+            if (pos < a.list_cap) cmp[pos] = sel_id[q];
+        }
+        if (threadIdx.x == 0) {
+            const int n = prefix + n_sel;
+            if (n_sel > kSel || n > a.list_cap) atomicOr(a.err, ERR_LIST);
+            a.n_cmp[g] = min(n, a.list_cap);
+        }
+        __syncthreads();
+    }
+}
+
+}  // namespace
+
+void launch_update_lists(const ListArgs& a, int grid, cudaStream_t s) {
+    static bool configured = false;
+    if (!configured) {
+        allow_max_dynamic_smem(update_lists_kernel);
+        configured = true;
+    }
+    const size_t smem = (size_t)a.hash_cap * 12 + (size_t)kSel * 8;
+    update_lists_kernel<<<grid, kThreads, smem, s>>>(a);
+}
+
+}  // namespace gg

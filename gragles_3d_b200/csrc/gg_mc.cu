@@ -1,0 +1,296 @@
+// gg_mc.cu -- zero-isosurface extraction and hull statistics of every grain.
+//
+// Stands in for grainhdl::level_set's per-grain work (grainhdl.cpp:669-718):
+// deleting grains whose hull vanished in the previous step, then
+// LSbox::extractContour (box.cpp:1144-1161) = MarchingCubesAlgorithm::generateHull
+// (marchingCubes.cpp:364-478), GrainHull::generateHull (grainHull.cpp:146-155),
+// computeGrainVolume / computeSurfaceArea (grainHull.cpp:40-55, 120-131) and the
+// resize of the output box to the new bounding box (dimensionalBuffer.h:120-219).
+//
+// One CTA owns one grain and walks its cubes in the reference's z, y, x order in
+// chunks of blockDim cubes.  A block scan of per-cube triangle counts gives each
+// triangle its place in the reference's emission order; the FP64 volume and area
+// terms of a chunk are then added by one thread in that order, so the sums are
+// bit-identical to the reference's sequential loop.  The distinct neighbour IDs
+// keep the reference's first-seen order through a shared-memory hash holding, per
+// ID, the smallest (cube index, rank in the cube's sorted list) key.
+#include "gg_kernels.cuh"
+
+namespace gg {
+
+#include "gg_mc_tables.inc"
+
+namespace {
+
+constexpr int kThreads = 256;
+constexpr int kHash = 1024;  // distinct neighbour IDs per grain (power of two)
+
+// cubeindex bit b <-> corner offset (dx, dy, dz), marchingCubes.cpp:376-385
+__constant__ int c_corner[8][3] = {{0, 0, 1}, {1, 0, 1}, {1, 0, 0}, {0, 0, 0},
+                                   {0, 1, 1}, {1, 1, 1}, {1, 1, 0}, {0, 1, 0}};
+// edge e joins corners (a, b) in VertexInterp argument order, marchingCubes.cpp:392-469
+__constant__ int c_edge[12][2] = {{0, 1}, {1, 2}, {2, 3}, {3, 0}, {4, 5}, {5, 6},
+                                  {6, 7}, {7, 4}, {0, 4}, {1, 5}, {2, 6}, {3, 7}};
+// neighbour-list corner order, marchingCubes.cpp:505-553
+__constant__ int c_nbc[8][3] = {{0, 0, 0}, {1, 0, 0}, {1, 1, 0}, {0, 1, 0},
+                                {0, 0, 1}, {1, 0, 1}, {1, 1, 1}, {0, 1, 1}};
+
+struct V3 { double x, y, z; };
+
+// MarchingCubesAlgorithm::VertexInterp, marchingCubes.cpp:484-499
+__device__ __forceinline__ V3 vinterp(V3 p1, V3 p2, double v1, double v2) {
+    if (fabs(v1) < 0.00001) return p1;
+    if (fabs(v2) < 0.00001) return p2;
+    if (fabs(v1 - v2) < 0.00001) return p1;
+    const double mu = v1 / (v1 - v2);
+    return V3{p1.x + mu * (p2.x - p1.x), p1.y + mu * (p2.y - p1.y), p1.z + mu * (p2.z - p1.z)};
+}
+
+__device__ __forceinline__ int block_exclusive_scan(int v, int* warp_sums, int& total) {
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+    int incl = v;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const int u = __shfl_up_sync(0xffffffffu, incl, o);
+        if (lane >= o) incl += u;
+    }
+    if (lane == 31) warp_sums[warp] = incl;
+    __syncthreads();
+    if (warp == 0) {
+        int w = lane < nw ? warp_sums[lane] : 0;
+        int wi = w;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const int u = __shfl_up_sync(0xffffffffu, wi, o);
+            if (lane >= o) wi += u;
+        }
+        if (lane < nw) warp_sums[lane] = wi - w;
+        if (lane == nw - 1) warp_sums[32] = wi;
+    }
+    __syncthreads();
+    total = warp_sums[32];
+    const int r = warp_sums[warp] + incl - v;
+    return r;
+}
+
+__device__ __forceinline__ void hash_insert(unsigned* hkey, unsigned* hval, unsigned id, unsigned key, int* err) {
+    unsigned h = (id * 2654435761u) & (kHash - 1);
+    for (int probe = 0; probe < kHash; probe++) {
+        const unsigned prev = atomicCAS(hkey + h, 0xFFFFFFFFu, id);
+        if (prev == 0xFFFFFFFFu || prev == id) {
+            atomicMin(hval + h, key);
+            return;
+        }
+        h = (h + 1) & (kHash - 1);
+    }
+    atomicOr(err, ERR_NEIGHBORS);
+}
+
+// DimensionalBuffer::resizeToCube, dimensionalBuffer.h:139-219
+__device__ Box resize_to_cube(Box b, int maximumLength) {
+    const int grid_size = maximumLength - 1;
+    const unsigned height = b.y1 - b.y0, width = b.x1 - b.x0, depth = b.z1 - b.z0;
+    if (width == height && width == depth) return b;
+    int ref = width > height ? (int)width : (int)height;
+    if (ref < (int)depth) ref = (int)depth;
+    if (ref > (int)width) { const int d = ref - (int)width; b.x0 -= d / 2; b.x1 += d / 2 + d % 2; }
+    if (ref > (int)height) { const int d = ref - (int)height; b.y0 -= d / 2; b.y1 += d / 2 + d % 2; }
+    if (ref > (int)depth) { const int d = ref - (int)depth; b.z0 -= d / 2; b.z1 += d / 2 + d % 2; }
+    if (b.x0 < 0) { const int d = -b.x0; b.x1 += d; b.x0 += d; }
+    else if (b.x1 > grid_size) { const int d = grid_size - b.x1; b.x1 += d; b.x0 += d; }
+    if (b.y0 < 0) { const int d = -b.y0; b.y1 += d; b.y0 += d; }
+    else if (b.y1 > grid_size) { const int d = grid_size - b.y1; b.y1 += d; b.y0 += d; }
+    if (b.z0 < 0) { const int d = -b.z0; b.z1 += d; b.z0 += d; }
+    else if (b.z1 > grid_size) { const int d = grid_size - b.z1; b.z1 += d; b.z0 += d; }
+    return b;
+}
+
+template <typename T>
+__global__ void __launch_bounds__(kThreads) mc_kernel(MCArgs<T> a) {
+    __shared__ double vbuf[kThreads * 5];
+    __shared__ double abuf[kThreads * 5];
+    __shared__ int warp_sums[33];
+    __shared__ unsigned hkey[kHash];
+    __shared__ unsigned hval[kHash];
+    __shared__ unsigned nb_id[kHash];
+    __shared__ unsigned nb_key[kHash];
+    __shared__ int n_found;
+    const int total = a.toff[a.G + 1];
+    for (int t = blockIdx.x; t < total; t += gridDim.x) {
+        const int g = tile_grain(a.toff, a.G, t);
+        if (!a.exists[g]) {  // the hull vanished last step: delete, grainhdl.cpp:678-680
+            if (threadIdx.x == 0) a.present[g] = 0;
+            continue;
+        }
+        const Box b = a.in.grain_box(g);
+        const T* sdf = a.in.grain_ptr(g);
+        const uint32_t* idl = a.idl + a.idoff[g];
+        for (int q = threadIdx.x; q < kHash; q += blockDim.x) { hkey[q] = 0xFFFFFFFFu; hval[q] = 0xFFFFFFFFu; }
+        if (threadIdx.x == 0) n_found = 0;
+        const int ncx = b.nx() - 1, ncy = b.ny() - 1, ncz = b.nz() - 1;
+        const long long NC = (ncx > 0 && ncy > 0 && ncz > 0) ? (long long)ncx * ncy * ncz : 0;
+        double vol = 0.0, area = 0.0;
+        long long ntri = 0;
+        __syncthreads();
+        for (long long base = 0; base < NC; base += blockDim.x) {
+            const long long c = base + threadIdx.x;
+            int nt = 0, ci = 0;
+            int x = 0, y = 0, z = 0;
+            double val[8];
+            if (c < NC) {
+                x = b.x0 + (int)(c % ncx);
+                y = b.y0 + (int)((c / ncx) % ncy);
+                z = b.z0 + (int)(c / ((long long)ncx * ncy));
+#pragma unroll
+                for (int k = 0; k < 8; k++) {
+                    val[k] = (double)sdf[b.at(y + c_corner[k][1], x + c_corner[k][0], z + c_corner[k][2])];
+                    if (val[k] >= 0) ci |= 1 << k;
+                }
+                if (gg_mc_edge_table[ci] != 0)
+                    while (gg_mc_tri_table[ci][3 * nt] != -1) nt++;
+            }
+            int chunk_total;
+            const int off = block_exclusive_scan(nt, warp_sums, chunk_total);
+            if (nt > 0) {
+                const int et = gg_mc_edge_table[ci];
+                V3 vl[12];
+#pragma unroll
+                for (int e = 0; e < 12; e++) {
+                    if (!(et & (1 << e))) continue;
+                    const int ka = c_edge[e][0], kb = c_edge[e][1];
+                    const V3 p1{(double)(x + c_corner[ka][0]), (double)(y + c_corner[ka][1]), (double)(z + c_corner[ka][2])};
+                    const V3 p2{(double)(x + c_corner[kb][0]), (double)(y + c_corner[kb][1]), (double)(z + c_corner[kb][2])};
+                    vl[e] = vinterp(p1, p2, val[ka], val[kb]);
+                }
+                for (int q = 0; q < nt; q++) {
+                    const V3 p0 = vl[gg_mc_tri_table[ci][3 * q]];
+                    const V3 p1 = vl[gg_mc_tri_table[ci][3 * q + 1]];
+                    const V3 p2 = vl[gg_mc_tri_table[ci][3 * q + 2]];
+                    // GrainHull::computeGrainVolume, grainHull.cpp:42-51
+                    const double v321 = p2.x * p1.y * p0.z;
+                    const double v231 = p1.x * p2.y * p0.z;
+                    const double v312 = p2.x * p0.y * p1.z;
+                    const double v132 = p0.x * p2.y * p1.z;
+                    const double v213 = p1.x * p0.y * p2.z;
+                    const double v123 = p0.x * p1.y * p2.z;
+                    vbuf[off + q] = (double)(1.0f / 6.0f) * (-v321 + v231 + v312 - v132 - v213 + v123);
+                    // GrainHull::computeSurfaceArea, grainHull.cpp:122-127 (Eigen sums c0 + (c1 + c2))
+                    const double abx = p0.x - p1.x, aby = p0.y - p1.y, abz = p0.z - p1.z;
+                    const double bcx = p0.x - p2.x, bcy = p0.y - p2.y, bcz = p0.z - p2.z;
+                    const double cx = aby * bcz - abz * bcy, cy = abz * bcx - abx * bcz, cz = abx * bcy - aby * bcx;
+                    abuf[off + q] = sqrt(cx * cx + (cy * cy + cz * cz)) / 2.0;
+                }
+                // generateAdditionalInformation: sorted distinct corner IDs, marchingCubes.cpp:501-583
+                unsigned lst[8];
+                int cnt = 0;
+#pragma unroll
+                for (int k = 0; k < 8; k++) {
+                    const int xx = x + c_nbc[k][0], yy = y + c_nbc[k][1], zz = z + c_nbc[k][2];
+                    const long long at = b.at(yy, xx, zz);
+                    unsigned id = sdf[at] >= 0 ? (unsigned)g : idl[at];
+                    bool found = false;
+                    for (int q = 0; q < cnt; q++) found |= (lst[q] == id);
+                    if (!found) {
+                        for (int q = 0; q < cnt; q++)
+                            if (id < lst[q]) { const unsigned tmp = lst[q]; lst[q] = id; id = tmp; }
+                        lst[cnt++] = id;
+                    }
+                }
+                const unsigned ck = (unsigned)c << 3;
+                for (int q = 0; q < cnt; q++) hash_insert(hkey, hval, lst[q], ck | q, a.err);
+            }
+            __syncthreads();
+            if (threadIdx.x == 0) {
+                for (int q = 0; q < chunk_total; q++) {
+                    vol += vbuf[q];
+                    area += abuf[q];
+                }
+            }
+            ntri += chunk_total;
+            __syncthreads();
+        }
+        // collect the distinct IDs and order them by first appearance
+        for (int q = threadIdx.x; q < kHash; q += blockDim.x) {
+            if (hkey[q] != 0xFFFFFFFFu) {
+                const int slot = atomicAdd(&n_found, 1);
+                nb_id[slot] = hkey[q];
+                nb_key[slot] = hval[q];
+            }
+        }
+        __syncthreads();
+        const int nf = n_found;
+        uint32_t* nbo = a.nb + (long long)g * a.nb_cap;
+        for (int q = threadIdx.x; q < nf; q += blockDim.x) {
+            const unsigned kq = nb_key[q];
+            int rank = 0;
+            for (int r = 0; r < nf; r++) rank += nb_key[r] < kq;
+            if (rank < a.nb_cap) nbo[rank] = nb_id[q];
+        }
+        if (threadIdx.x == 0) {
+            if (nf > a.nb_cap) atomicOr(a.err, ERR_NEIGHBORS);
+            a.n_nb[g] = nf;
+            const double h = a.geo.h;
+            a.volume[g] = fabs(vol) * h * h * h;
+            a.surface[g] = area * h * h;
+            const bool ex = ntri > 0;
+            a.exists[g] = ex;
+            if (ex) {
+                // tail of executeSetComparison (box.cpp:858-877), then extractContour's resize
+                const int* nbx = a.newbox + 6 * g;
+                const int gb = a.geo.gb, M = a.geo.M;
+                int x0 = nbx[0] - gb, x1 = nbx[1] + gb, y0 = nbx[2] - gb, y1 = nbx[3] + gb;
+                int z0 = nbx[4] - gb, z1 = nbx[5] + gb;
+                if (x0 < 0) x0 = 0;
+                if (y0 < 0) y0 = 0;
+                if (z0 < 0) z0 = 0;
+                if (x1 >= M) x1 = M - 1;
+                if (y1 >= M) y1 = M - 1;
+                if (z1 >= M) z1 = M - 1;
+                const Box nb = resize_to_cube(Box{x0, x1, y0, y1, z0, z1}, M);
+                if (nb.x0 < 0 || nb.y0 < 0 || nb.z0 < 0 || nb.nx() <= 0) atomicOr(a.err, ERR_BOX);
+                store_box(a.out_box + 6 * g, nb);
+            }
+        }
+        __syncthreads();
+    }
+}
+
+// out3 = {present grains, present and existing grains, largest box side among those}
+__global__ void count_kernel(int G, const int* present, const int* exists, const int* box, int* out3) {
+    int np = 0, ne = 0, mx = 0;
+    for (int g = 1 + blockIdx.x * blockDim.x + threadIdx.x; g <= G; g += gridDim.x * blockDim.x) {
+        np += present[g] != 0;
+        if (present[g] && exists[g]) {
+            ne++;
+            mx = max(mx, box[6 * g + 1] - box[6 * g]);
+        }
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        np += __shfl_xor_sync(0xffffffffu, np, o);
+        ne += __shfl_xor_sync(0xffffffffu, ne, o);
+        mx = max(mx, __shfl_xor_sync(0xffffffffu, mx, o));
+    }
+    if ((threadIdx.x & 31) == 0) {
+        atomicAdd(out3, np);
+        atomicAdd(out3 + 1, ne);
+        atomicMax(out3 + 2, mx);
+    }
+}
+
+}  // namespace
+
+template <typename T>
+void launch_mc(const MCArgs<T>& a, int grid, cudaStream_t s) {
+    mc_kernel<T><<<grid, kThreads, 0, s>>>(a);
+}
+
+void launch_count(int G, const int* present, const int* exists, const int* box, int* out3, cudaStream_t s) {
+    cudaMemsetAsync(out3, 0, 3 * sizeof(int), s);
+    count_kernel<<<64, 256, 0, s>>>(G, present, exists, box, out3);
+}
+
+template void launch_mc<double>(const MCArgs<double>&, int, cudaStream_t);
+template void launch_mc<float>(const MCArgs<float>&, int, cudaStream_t);
+
+}  // namespace gg

@@ -1,0 +1,132 @@
+// gg_plan.cu -- device-side layout planner for the box pool.
+//
+// The reference allocates every box with std::vector and resizes it every step
+// (dimensionalBuffer.h:120-131, jemalloc underneath).  Here the boxes of all grains
+// are packed into one arena per buffer role; after every change of box sizes one
+// CTA re-plans the packing (exclusive scan of the aligned n^3 over grains), the
+// half-spectrum scratch, and the tile offsets that the batched stage kernels use
+// to map their CTAs to (grain, tile).  Nothing goes back to the host, so a whole
+// timestep can be launched without synchronisation.
+#include "gg_kernels.cuh"
+
+namespace gg {
+
+namespace {
+
+constexpr int kPlanThreads = 1024;
+constexpr long long kAlign = 32;  // elements; 256 B for FP64, 128 B for FP32
+
+struct Counts {
+    long long vox, spec, tot;
+    int tn, ts, t1;
+};
+
+__device__ __forceinline__ Counts add(const Counts& a, const Counts& b) {
+    return Counts{a.vox + b.vox, a.spec + b.spec, a.tot + b.tot, a.tn + b.tn, a.ts + b.ts, a.t1 + b.t1};
+}
+
+__device__ __forceinline__ Counts shfl_up(const Counts& c, int o) {
+    Counts r;
+    r.vox = __shfl_up_sync(0xffffffffu, c.vox, o);
+    r.spec = __shfl_up_sync(0xffffffffu, c.spec, o);
+    r.tot = __shfl_up_sync(0xffffffffu, c.tot, o);
+    r.tn = __shfl_up_sync(0xffffffffu, c.tn, o);
+    r.ts = __shfl_up_sync(0xffffffffu, c.ts, o);
+    r.t1 = __shfl_up_sync(0xffffffffu, c.t1, o);
+    return r;
+}
+
+__device__ __forceinline__ Counts grain_counts(const PlanArgs& a, int g) {
+    Counts c{0, 0, 0, 0, 0, 0};
+    if (g < 1 || g > a.G || !a.present[g] || (a.only_existing && !a.exists[g])) return c;
+    const Box b = load_box(a.box + 6 * g);
+    const long long n = b.nx();
+    const long long v = b.count();
+    c.vox = (v + kAlign - 1) / kAlign * kAlign;
+    const long long sp = n * n * (n / 2 + 1);
+    c.spec = (sp + kAlign - 1) / kAlign * kAlign;
+    c.tot = v;
+    c.tn = (int)n;
+    c.ts = a.slab > 0 ? (int)((n + a.slab - 1) / a.slab) : 0;
+    c.t1 = 1;
+    return c;
+}
+
+__global__ void __launch_bounds__(kPlanThreads) plan_kernel(PlanArgs a) {
+    __shared__ Counts warp_tot[32];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int per = (a.G + kPlanThreads) / kPlanThreads;  // grains 0..G
+    const int g0 = threadIdx.x * per, g1 = min(a.G + 1, g0 + per);
+    Counts mine{0, 0, 0, 0, 0, 0};
+    for (int g = g0; g < g1; g++) mine = add(mine, grain_counts(a, g));
+    // block exclusive scan of `mine`
+    Counts incl = mine;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const Counts u = shfl_up(incl, o);
+        if (lane >= o) incl = add(incl, u);
+    }
+    if (lane == 31) warp_tot[warp] = incl;
+    __syncthreads();
+    if (warp == 0) {
+        Counts w = warp_tot[lane];
+        Counts wi = w;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const Counts u = shfl_up(wi, o);
+            if (lane >= o) wi = add(wi, u);
+        }
+        warp_tot[lane] = wi;  // inclusive over warps
+    }
+    __syncthreads();
+    Counts run = warp > 0 ? warp_tot[warp - 1] : Counts{0, 0, 0, 0, 0, 0};
+    const Counts excl_in_warp = Counts{incl.vox - mine.vox, incl.spec - mine.spec, incl.tot - mine.tot,
+                                       incl.tn - mine.tn, incl.ts - mine.ts, incl.t1 - mine.t1};
+    run = add(run, excl_in_warp);
+    for (int g = g0; g < g1; g++) {
+        const Counts c = grain_counts(a, g);
+        if (a.off) a.off[g] = run.vox;
+        if (a.spec_off) a.spec_off[g] = run.spec;
+        if (a.toff_n) a.toff_n[g] = run.tn;
+        if (a.toff_slab) a.toff_slab[g] = run.ts;
+        if (a.toff_one) a.toff_one[g] = run.t1;
+        if (a.box_copy) {
+#pragma unroll
+            for (int q = 0; q < 6; q++) a.box_copy[6 * g + q] = a.box[6 * g + q];
+        }
+        if (a.off_copy && a.off) a.off_copy[g] = run.vox;
+        run = add(run, c);
+    }
+    if (threadIdx.x == kPlanThreads - 1) {
+        const Counts T = warp_tot[31];
+        // Over capacity: report, and give the stage kernels no tiles so that nothing
+        // is written past the end of an arena.
+        const bool over = (a.off && T.vox > a.capacity) || (a.spec_off && T.spec > a.spec_capacity);
+        if (over) atomicOr(a.err, ERR_POOL);
+        if (a.toff_n) a.toff_n[a.G + 1] = over ? 0 : T.tn;
+        if (a.toff_slab) a.toff_slab[a.G + 1] = over ? 0 : T.ts;
+        if (a.toff_one) a.toff_one[a.G + 1] = over ? 0 : T.t1;
+        if (a.total_voxels) *a.total_voxels = T.tot;
+    }
+}
+
+__global__ void copy_layout_kernel(int G, const int* present, const int* box_src, const long long* off_src,
+                                   int* box_dst, long long* off_dst) {
+    for (int g = blockIdx.x * blockDim.x + threadIdx.x; g <= G; g += gridDim.x * blockDim.x) {
+        if (!present[g]) continue;
+#pragma unroll
+        for (int q = 0; q < 6; q++) box_dst[6 * g + q] = box_src[6 * g + q];
+        off_dst[g] = off_src[g];
+    }
+}
+
+}  // namespace
+
+void launch_plan(const PlanArgs& a, cudaStream_t s) { plan_kernel<<<1, kPlanThreads, 0, s>>>(a); }
+
+void launch_copy_layout(int G, const int* present, const int* box_src, const long long* off_src, int* box_dst,
+                        long long* off_dst, cudaStream_t s) {
+    copy_layout_kernel<<<(G + 256) / 256, 256, 0, s>>>(G, present, box_src, off_src, box_dst, off_dst);
+}
+
+}  // namespace gg

@@ -1,0 +1,122 @@
+/*
+ * gg_b200.h -- C ABI of the B200-native GraGLeS_3D level-set timestep.
+ *
+ * The reference drives its per-timestep loop from grainhdl::run_sim
+ * (grainhdl.cpp:821-919) through OpenMP loops over LSbox methods (box.h:111-190).
+ * This library replaces that loop with device-resident state on one GPU: every
+ * grain box lives in a pool in HBM, every stage is a batched CUDA kernel over all
+ * boxes, and the host only sequences calls.  Each entry point below names the
+ * reference method (file:line) it stands in for.
+ *
+ * Conventions: every function returns GG_OK (0) or a negative GG_ERR_* code and
+ * never throws; gg_last_error() gives the message.  One context = one GPU, one
+ * CUDA stream, one host thread.  Boxes are int32[6] = {xmin, xmax, ymin, ymax,
+ * zmin, zmax} in absolute grid coordinates (border included), maxima exclusive,
+ * and box buffers are flat [z][y][x] with x fastest (dimensionalBuffer.h:71-76).
+ * Grain IDs run 1..n_grains; ID 0 is the domain-boundary grain.
+ */
+#ifndef GG_B200_H
+#define GG_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define GG_OK 0
+#define GG_ERR_INVALID (-1)          /* bad argument or call order */
+#define GG_ERR_CUDA (-2)             /* a CUDA call failed */
+#define GG_ERR_POOL_EXHAUSTED (-3)   /* box pool or scratch capacity exceeded */
+#define GG_ERR_LIST_OVERFLOW (-4)    /* a comparison or neighbour list exceeded its capacity */
+#define GG_ERR_UNSUPPORTED (-5)      /* option not implemented on this path */
+
+#define GG_PRECISION_FP64 0          /* FP64 storage and arithmetic, bit-exact with the oracle */
+#define GG_PRECISION_MIXED 1         /* FP32 storage, tensor-core convolution, FP64 tallies */
+
+typedef struct gg_ctx gg_ctx;
+
+/* The Settings fields the loop reads (Settings.h:63-119, grainhdl.cpp:1419-1442). */
+typedef struct {
+    int32_t domain_size;        /* realDomainSize N (NX of the mode-4 header) */
+    int32_t border;             /* DomainBorderSize (grid_blowup) */
+    double time_step;           /* TimeStepSize */
+    int32_t n_grains;           /* NumberOfParticles */
+    int32_t precision;          /* GG_PRECISION_* */
+    int32_t disable_correction; /* DisableConvolutionCorrection (must be 1 on this path) */
+    int32_t list_capacity;      /* comparison-list capacity per grain (0 = 4096) */
+    int64_t pool_voxels;        /* voxels per SDF arena (0 = 2x the initial total) */
+    int32_t device;             /* CUDA device ordinal */
+    int32_t reserved[7];
+} gg_params;
+
+/* Per-step report (the reference prints the same stage times, grainhdl.cpp:920-933). */
+typedef struct {
+    int32_t loop;               /* loop index of the step just run */
+    int32_t grain_count;        /* currentNrGrains after the step (countGrains) */
+    int32_t live_grains;        /* grains whose hull is non-empty after the step */
+    int32_t reserved0;
+    int64_t voxel_updates;      /* sum of n^3 over the boxes convolved this step */
+    float ms_convolution, ms_lists, ms_comparison, ms_levelset, ms_redistancing, ms_total;
+} gg_step_stats;
+
+/* grainhdl::grainhdl + initializeSimulation (grainhdl.cpp:50-128): allocate the
+ * context, the box pool and the per-size DFT / Gaussian tables on the device. */
+int gg_create(const gg_params* params, gg_ctx** out);
+int gg_destroy(gg_ctx* ctx);
+const char* gg_last_error(const gg_ctx* ctx);
+
+/* read_voxelized_microstructure + buildBoxVectors + distanceInitialisation
+ * (grainhdl.cpp:404-578, 1220-1254, 580-596; box.cpp:227-304, 374-397):
+ * labels = N^3 grain IDs [z][y][x] (host memory, IDs 1..n_grains), extents =
+ * n_grains x 6 inclusive domain extents {xmin,xmax,ymin,ymax,zmin,zmax}, counts =
+ * voxels per grain (0 = no such grain).  Builds the boxes and the initial SDFs on
+ * the device. */
+int gg_load_state(gg_ctx* ctx, const uint32_t* labels, const int32_t* extents, const int64_t* counts);
+
+/* find_neighbors (grainhdl.cpp:1029-1054, box.cpp:2871-2887): initial comparison
+ * lists as CSR (offsets[n_grains + 2], row = grain ID).  The reference fills them
+ * from an R-tree search; the order of each row sets the comparison tie-break. */
+int gg_set_lists(gg_ctx* ctx, const int64_t* offsets, const uint32_t* ids);
+/* The same membership (inclusive box overlap) in grain-ID order. */
+int gg_default_lists(gg_ctx* ctx);
+
+/* One loop iteration of grainhdl::run_sim (grainhdl.cpp:837-917). */
+int gg_step(gg_ctx* ctx, gg_step_stats* stats);
+
+/* The stages of one iteration, for stage-level testing, in the order gg_step runs
+ * them.  Each stands in for the grainhdl method named. */
+int gg_stage_convolution(gg_ctx* ctx);       /* switchDistancebuffer + convolution, :839-849 */
+int gg_stage_update_lists(gg_ctx* ctx);      /* switchDistancebuffer + updateSecondOrderNeighbors, :852-853 */
+int gg_stage_comparison(gg_ctx* ctx);        /* comparison_box + switchDistancebuffer, :858-868 */
+int gg_stage_level_set(gg_ctx* ctx);         /* level_set, :875 */
+int gg_stage_redistancing(gg_ctx* ctx);      /* redistancing + countGrains, :881-886 */
+
+/* Host mirror of per-grain state (LSbox getters, box.h:211-250): arrays of
+ * n_grains + 1 entries indexed by grain ID (entry 0 unused); any pointer may be NULL. */
+int gg_get_grain_stats(gg_ctx* ctx, uint8_t* exists, double* volume, double* surface, int32_t* boxes,
+                       int32_t* n_neighbors);
+/* Distinct grain IDs of the last hull in first-seen order (GrainHull::getAllNeighbors). */
+int gg_get_neighbors(gg_ctx* ctx, int32_t id, uint32_t* out, int32_t cap);
+/* Current comparison list (LSbox::m_comparisonList). */
+int gg_get_list(gg_ctx* ctx, int32_t id, uint32_t* out, int32_t cap);
+/* One of the grain's two SDF buffers as FP64: which = 0 -> m_inputDistance,
+ * 1 -> m_outputDistance (after a full step that is the redistanced field).
+ * Returns the voxel count; out may be NULL to query the box only. */
+int64_t gg_get_sdf(gg_ctx* ctx, int32_t id, int32_t which, int32_t box[6], double* out, int64_t cap);
+/* The grain's IDLocal buffer; returns voxels. */
+int64_t gg_get_idlocal(gg_ctx* ctx, int32_t id, int32_t box[6], uint32_t* out, int64_t cap);
+int gg_grain_count(gg_ctx* ctx);
+int gg_loop(gg_ctx* ctx);
+
+/* Single-box stage kernels on caller-owned device memory (stream 0 of the current
+ * device), for testing each kernel against the oracle on arbitrary inputs.
+ * n_boxes cubic boxes of sides sides[b] packed at element offsets offs[b]. */
+int gg_convolve_boxes_f64(const double* d_in, double* d_out, const int32_t* sides, const int64_t* offs,
+                          int32_t n_boxes, int32_t domain_size, double time_step);
+
+#ifdef __cplusplus
+}
+#endif
+#endif
