@@ -1,0 +1,349 @@
+#!/usr/bin/env python
+"""Throughput of the GraGLeS_3D level-set timestep on B200.
+
+Workload: a 128^3 voxel domain, 2,000 grains from a Voronoi tessellation of
+seeded uniform-random points, isotropic grain-boundary energy and mobility,
+10-voxel box border, TimeStepSize 0.2 (the reference's non-periodic domain with
+the boundary grain).  A *step* is one full timestep of the loop (convolution,
+list update, comparison, marching cubes, redistancing, box bookkeeping) over
+every live grain box.  The unit of work is a voxel-update: one box voxel carried
+through one timestep (the sum of n^3 over the boxes the step convolves).
+
+Headline: the mixed path (FP32 storage, per-axis circulant convolution, FP64
+volume tallies).  The FP64 path (bit-exact with the reference) runs beside it
+and the maximum per-grain relative volume difference between the two is reported.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl gg|reference]
+
+N > 1 runs one independent replica per GPU (the path shares nothing between
+grains of different simulations); launch it with torch.distributed.run.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "voxel-updates/s per timestep, mixed vs FP64 path on 1 B200, at vol err ≤1e-3"
+UNIT = "voxel-updates/s"
+WORKLOAD = dict(workload="voronoi-128^3-2000-grains-isotropic", domain=128, grains=2000, border=10,
+                time_step=0.2, seed=1002)
+
+
+# ----------------------------------------------------------------------------------
+# helpers
+# ----------------------------------------------------------------------------------
+def microstructure():
+    from gragles_3d_b200 import microstructure as msgen
+
+    ms = msgen.voronoi(WORKLOAD["domain"], WORKLOAD["grains"], seed=WORKLOAD["seed"])
+    ext, counts = ms.grain_extents()
+    return ms, ext, counts
+
+
+def read_peaks():
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(path):
+        with open(path) as f:
+            p = json.load(f)
+        return float(p["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons while the timed region runs."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device: int):
+        self.device = device
+        self.proc = None
+        self.lines = []
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits", "-lms", "200",
+                 "-i", str(self.device)], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.reader = threading.Thread(target=self._read, daemon=True)
+            self.reader.start()
+        except OSError:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def __exit__(self, *exc):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self) -> dict:
+        sm, mx, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in self.lines:
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                mx.append(float(parts[2]))
+            except ValueError:
+                continue
+            for n, v in zip(names, parts[5:9]):
+                if v.lower() == "active":
+                    reasons.add(n)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+# algorithmic (compulsory) bytes per voxel-update by stage and precision
+STAGE_BYTES = {
+    "mixed": {"ms_convolution": 8, "ms_comparison": 12, "ms_levelset": 4, "ms_redistancing": 8},
+    "fp64": {"ms_convolution": 16, "ms_comparison": 20, "ms_levelset": 8, "ms_redistancing": 16},
+}
+STAGE_KERNEL = {"ms_convolution": "convolution", "ms_comparison": "compare_kernel", "ms_levelset": "mc_kernel",
+                "ms_redistancing": "redist_xy/z", "ms_lists": "update_lists_kernel"}
+
+
+def run_device(gg, precision, ms, ext, counts, steps, warmup, device, dist):
+    """Device-resident run: state loaded before the timed region."""
+    import torch
+
+    gh = gg.GrainHandler(WORKLOAD["domain"], WORKLOAD["border"], WORKLOAD["time_step"], WORKLOAD["grains"],
+                         precision=precision, device=device)
+    gh.load(ms.labels, ext, counts)
+    gh.default_lists()
+    for _ in range(warmup):
+        gh.step()
+    reps = []
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with ClockSampler(device) as clk:
+        ev0.record()
+        for _ in range(steps):
+            reps.append(gh.step())
+        ev1.record()
+        torch.cuda.synchronize()
+    if dist:
+        dist.barrier()
+    ms_elapsed = ev0.elapsed_time(ev1)
+    st = gh.stats()
+    vol = st.volume.copy()
+    ex = st.exists.copy()
+    gh.close()
+    return reps, ms_elapsed, clk.summary(), vol, ex
+
+
+def run_e2e(gg, precision, ms, ext, counts, steps, device):
+    """Through the public API with host buffers: upload, steps, per-step read-back."""
+    import torch
+
+    gh = gg.GrainHandler(WORKLOAD["domain"], WORKLOAD["border"], WORKLOAD["time_step"], WORKLOAD["grains"],
+                         precision=precision, device=device)
+    labels = np.ascontiguousarray(ms.labels)
+    torch.cuda.synchronize()
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    ev0.record()
+    gh.load(labels, ext, counts)
+    gh.default_lists()
+    vox = 0
+    for _ in range(steps):
+        vox += gh.step()["voxel_updates"]
+        gh.stats()
+    ev1.record()
+    torch.cuda.synchronize()
+    ms_elapsed = ev0.elapsed_time(ev1)
+    G1 = WORKLOAD["grains"] + 1
+    h2d = labels.nbytes + ext.astype(np.int32).nbytes + counts.astype(np.int64).nbytes
+    d2h = G1 * (1 + 8 + 8 + 24 + 4)
+    gh.close()
+    return {"value": vox / (ms_elapsed / 1e3), "unit": UNIT, "h2d_bytes_per_step": int(h2d // steps),
+            "d2h_bytes_per_step": int(d2h), "ms": ms_elapsed}
+
+
+# ----------------------------------------------------------------------------------
+# reference CPU path (the reference's own solver, compiled from its sources)
+# ----------------------------------------------------------------------------------
+def run_reference_cpu(ms, steps: int, warmup: int, threads: int):
+    """Time `steps` loop iterations after `warmup` of the compiled reference on the
+    host cores.  Returns (voxel-updates/s, sample description, cores, kind)."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import refdump
+    from gragles_3d_b200 import microstructure as msgen
+
+    if os.path.exists(refdump.REF_BINARY):
+        with tempfile.TemporaryDirectory() as d:
+            msgen.write_mode4(ms, d)
+            msgen.write_parameters(os.path.join(d, "parameters.xml"), n_grains=ms.n_grains,
+                                   border=WORKLOAD["border"], steps=warmup + steps, threads=threads,
+                                   time_step=WORKLOAD["time_step"])
+            res, _ = refdump.run_case(d, threads=threads, timeout=3600)
+        lt = res["loop_time"]
+        # voxels convolved in loop t: boxes of the grains alive entering loop t
+        vox = {}
+        init = sum(int(np.prod([r.box[1] - r.box[0]] * 3)) for r in res["init_sdf"].values())
+        vox[0] = init
+        for loop, st in res["stats"].items():
+            vox[loop + 1] = sum((b[1] - b[0]) ** 3 for (d_, b) in st.values() if d_[0] == 1.0)
+        t = lt[warmup + steps] - lt[warmup]
+        v = sum(vox[l] for l in range(warmup, warmup + steps))
+        sample = (f"reference solver (g++ -O2, OpenMP, shim DFT) on the full workload: loops {warmup}.."
+                  f"{warmup + steps - 1} of {warmup + steps + 1}, {v} voxel-updates in {t:.2f} s")
+        return v / t, sample, threads, "reference"
+    # the C restatement (single thread) on a smaller slice of the loop
+    import pyoracle
+
+    ext, counts = ms.grain_extents()
+    sim = pyoracle.OracleSim(ms.n, WORKLOAD["border"], WORKLOAD["time_step"], ms.labels, ext, counts)
+    sim.step()
+    t0 = time.perf_counter()
+    sim.step()
+    t = time.perf_counter() - t0
+    v = sim.last_voxels()
+    return v / t, f"oracle restatement, 1 thread, 1 timestep of the full workload ({v} voxel-updates)", 1, "port"
+
+
+def reference_arm(args):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    ms, _, _ = microstructure()
+    threads = os.cpu_count() or 1
+    value, sample, cores, kind = run_reference_cpu(ms, args.steps, args.warmup, threads)
+    print(json.dumps({
+        "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
+        "steps": args.steps, "warmup": args.warmup, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64", "data": "synthetic", "config": dict(WORKLOAD),
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores, "kind": kind, "sample": sample},
+        "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }))
+
+
+def aggregate_replicas(elapsed_ms: float, voxels: float, dist, device: str = "cuda"):
+    """Whole-job figures over independent replicas: the slowest rank's time and the
+    sum of every rank's voxel-updates (every rank takes the same two collectives)."""
+    if dist is None:
+        return float(elapsed_ms), float(voxels)
+    import torch
+
+    t = torch.tensor([float(elapsed_ms)], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    v = torch.tensor([float(voxels)], dtype=torch.float64, device=device)
+    dist.all_reduce(v, op=dist.ReduceOp.SUM)
+    return float(t[0]), float(v[0])
+
+
+# ----------------------------------------------------------------------------------
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="gg", choices=["gg", "reference"])
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    args.warmup = max(args.warmup, 3)
+    if args.impl == "reference":
+        return reference_arm(args)
+
+    import torch
+    import gragles_3d_b200 as gg
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as tdist
+
+        torch.cuda.set_device(local)
+        tdist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600), device_id=torch.device("cuda", local))
+        dist = tdist
+    else:
+        torch.cuda.set_device(local)
+    ms, ext, counts = microstructure()
+
+    reps_m, ms_m, clk_m, vol_m, ex_m = run_device(gg, gg.PRECISION_MIXED, ms, ext, counts, args.steps, args.warmup,
+                                                  local, dist)
+    reps_d, ms_d, clk_d, vol_d, ex_d = run_device(gg, gg.PRECISION_FP64, ms, ext, counts, args.steps, args.warmup,
+                                                  local, dist)
+    vox_m = sum(r["voxel_updates"] for r in reps_m)
+    vox_d = sum(r["voxel_updates"] for r in reps_d)
+    elapsed_m, vox_m = aggregate_replicas(ms_m, vox_m, dist)
+    elapsed_d, vox_d = aggregate_replicas(ms_d, vox_d, dist)
+    value = vox_m / (elapsed_m / 1e3)
+    value_fp64 = vox_d / (elapsed_d / 1e3)
+
+    both = ex_m & ex_d
+    both[0] = False
+    rel = np.abs(vol_m[both] - vol_d[both]) / np.maximum(vol_d[both], 1e-300)
+    max_rel = float(rel.max()) if rel.size else None
+
+    def stage_means(reps):
+        keys = ["ms_convolution", "ms_lists", "ms_comparison", "ms_levelset", "ms_redistancing", "ms_total"]
+        return {k: float(np.mean([r[k] for r in reps])) for k in keys}
+
+    st_m, st_d = stage_means(reps_m), stage_means(reps_d)
+    dom = max((k for k in st_m if k not in ("ms_total",)), key=lambda k: st_m[k])
+    peak, peak_kind = read_peaks()
+    vox_per_step = np.mean([r["voxel_updates"] for r in reps_m])
+    bytes_per = STAGE_BYTES["mixed"].get(dom)
+    achieved = (bytes_per * vox_per_step / (st_m[dom] / 1e3) / 1e9) if bytes_per else None
+
+    e2e = None
+    out = None
+    if rank == 0:
+        e2e = run_e2e(gg, gg.PRECISION_MIXED, ms, ext, counts, args.steps, local)
+        cpu = None
+        if not args.no_cpu_baseline and world == 1:
+            cv, sample, cores, kind = run_reference_cpu(ms, 1, 1, os.cpu_count() or 1)
+            cpu = {"value": cv, "unit": UNIT, "cores": cores, "kind": kind, "sample": sample}
+        out = {
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": elapsed_m / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": dict(WORKLOAD, path="mixed", parallelism=f"replicas{world}",
+                           l2="inputs larger than L2 (box pool >= 0.3 GB per arena)"),
+            "fp64": {"value": value_fp64, "ms_per_step": elapsed_d / args.steps, "dtype": "f64",
+                     "stage_ms": st_d, "clocks": clk_d},
+            "mixed_over_fp64": value / value_fp64,
+            "max_rel_volume_err_mixed_vs_fp64": max_rel,
+            "stage_ms": st_m,
+            "roofline": {"bound": "hbm", "kernel": STAGE_KERNEL[dom], "achieved": achieved, "peak": peak,
+                         "unit": "GB/s", "frac": (achieved / peak) if achieved else None, "traffic": None,
+                         "peak_source": peak_kind, "bytes_per_voxel_update": bytes_per},
+            "cpu_baseline": cpu,
+            "e2e": {k: e2e[k] for k in ("value", "unit", "h2d_bytes_per_step", "d2h_bytes_per_step")},
+            "gpu_launches": int(sum(r["kernel_launches"] for r in reps_m)),
+            "clocks": clk_m,
+        }
+        print(json.dumps(out))
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

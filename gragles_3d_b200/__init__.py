@@ -51,7 +51,7 @@ class Params(C.Structure):
 
 class StepStats(C.Structure):
     _fields_ = [
-        ("loop", C.c_int32), ("grain_count", C.c_int32), ("live_grains", C.c_int32), ("reserved0", C.c_int32),
+        ("loop", C.c_int32), ("grain_count", C.c_int32), ("live_grains", C.c_int32), ("kernel_launches", C.c_int32),
         ("voxel_updates", C.c_int64), ("ms_convolution", C.c_float), ("ms_lists", C.c_float),
         ("ms_comparison", C.c_float), ("ms_levelset", C.c_float), ("ms_redistancing", C.c_float),
         ("ms_total", C.c_float),

@@ -84,6 +84,7 @@ struct gg_ctx {
     int side_max = 0;      // largest box side of the current layout
     int side_limit = 0;    // largest side the shared-memory kernels accept
     int list_cap = 4096, slab = kSlab64, hash_cap = 8192;
+    long long launches = 0;  // kernels launched by this context
     cudaEvent_t ev[7] = {};
 };
 
@@ -203,11 +204,13 @@ int plan(gg_ctx* ctx, const int* box, int only_existing, long long* off, long lo
     a.total_voxels = total_voxels;
     a.err = ctx->d_err;
     launch_plan(a, ctx->stream);
+    ctx->launches += 1;
     return GG_OK;
 }
 
 int read_counts(gg_ctx* ctx, const int* box) {
     launch_count(ctx->G, ctx->d_present, ctx->d_exists, box, ctx->d_count3, ctx->stream);
+    ctx->launches += 1;
     CK(cudaMemcpyAsync(ctx->h_count3, ctx->d_count3, 3 * sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
     CK(cudaMemcpyAsync(ctx->h_total_vox, ctx->d_total_vox, sizeof(long long), cudaMemcpyDeviceToHost, ctx->stream));
     CK(cudaStreamSynchronize(ctx->stream));
@@ -234,6 +237,7 @@ int redistance(gg_ctx* ctx, int in_a, int out_a, const int* toff, int side) {
     r.err = ctx->d_err;
     const size_t smem = redist_smem_bytes(side, sizeof(T) == 8);
     launch_redistance<T>(r, ctx->grid, smem, smem, ctx->stream);
+    ctx->launches += 2;
     CK(cudaGetLastError());
     return GG_OK;
 }
@@ -244,7 +248,9 @@ int load_state_t(gg_ctx* ctx, const uint32_t* labels) {
     // initial layout in arena 0, mirrored to arena 1 and the first IDLocal arena
     plan(ctx, ctx->d_box[0], 1, ctx->d_off[0], nullptr, ctx->d_toff_n, nullptr, nullptr);
     launch_copy_layout(G, ctx->d_present, ctx->d_box[0], ctx->d_off[0], ctx->d_box[1], ctx->d_off[1], ctx->stream);
+    ctx->launches += 1;
     launch_copy_layout(G, ctx->d_present, ctx->d_box[0], ctx->d_off[0], ctx->d_idbox[0], ctx->d_idoff[0], ctx->stream);
+    ctx->launches += 1;
     CK(cudaMemsetAsync(ctx->d_idarena[0], 0, sizeof(uint32_t) * ctx->pool_voxels, ctx->stream));
     int rc = check_err(ctx, "gg_load_state");
     if (rc) return rc;
@@ -280,6 +286,7 @@ int stage_convolution_t(gg_ctx* ctx) {
     // IDLocal follows the output box (resizeIDLocalToDistanceBuffer, box.cpp:426)
     launch_copy_layout(ctx->G, ctx->d_present, ctx->d_box[p], ctx->d_off[p], ctx->d_idbox[ctx->q ^ 1],
                        ctx->d_idoff[ctx->q ^ 1], ctx->stream);
+    ctx->launches += 1;
     if (sizeof(T) == 8) {
         ConvArgs a{};
         a.G = ctx->G;
@@ -296,6 +303,7 @@ int stage_convolution_t(gg_ctx* ctx) {
         a.gtab = ctx->d_gtab;
         a.g_off = ctx->d_g_off;
         launch_conv_f64(a, ctx->grid, conv_f64_smem_bytes(ctx->side_max), ctx->stream);
+        ctx->launches += 3;
     } else {
         ConvTCArgs a{};
         a.G = ctx->G;
@@ -309,6 +317,7 @@ int stage_convolution_t(gg_ctx* ctx) {
         a.circ_off = ctx->d_circ_off;
         a.err = ctx->d_err;
         launch_conv_tc(a, ctx->num_sms, ctx->side_max, ctx->stream);
+        ctx->launches += 2;
     }
     CK(cudaGetLastError());
     return GG_OK;
@@ -329,6 +338,7 @@ int stage_update_lists_t(gg_ctx* ctx) {
     a.hash_cap = ctx->hash_cap;
     a.err = ctx->d_err;
     launch_update_lists(a, ctx->grid, ctx->stream);
+    ctx->launches += 1;
     CK(cudaGetLastError());
     return GG_OK;
 }
@@ -337,6 +347,7 @@ template <typename T>
 int stage_comparison_t(gg_ctx* ctx) {
     const int p = ctx->p, q = ctx->q;
     launch_newbox_init(ctx->G, ctx->d_present, ctx->d_exists, ctx->d_box[p ^ 1], ctx->d_newbox, ctx->stream);
+    ctx->launches += 1;
     CompareArgs<T> a{};
     a.G = ctx->G;
     a.geo = ctx->geo;
@@ -358,6 +369,7 @@ int stage_comparison_t(gg_ctx* ctx) {
     a.newbox = ctx->d_newbox;
     a.err = ctx->d_err;
     launch_compare<T>(a, ctx->grid, compare_smem_bytes(ctx->side_max, ctx->slab, sizeof(T) == 8), ctx->stream);
+    ctx->launches += 1;
     CK(cudaGetLastError());
     ctx->q ^= 1;
     ctx->p ^= 1;  // switchDistancebuffer, grainhdl.cpp:865
@@ -386,6 +398,7 @@ int stage_level_set_t(gg_ctx* ctx) {
     a.nb_cap = kNbCap;
     a.err = ctx->d_err;
     launch_mc<T>(a, ctx->grid, ctx->stream);
+    ctx->launches += 1;
     CK(cudaGetLastError());
     return GG_OK;
 }
@@ -407,12 +420,14 @@ int stage_redistancing_t(gg_ctx* ctx) {
     // in.resize(out dims), box.cpp:2581-2584
     launch_copy_layout(ctx->G, ctx->d_present, ctx->d_box[p ^ 1], ctx->d_off[p ^ 1], ctx->d_box[p], ctx->d_off[p],
                        ctx->stream);
+    ctx->launches += 1;
     ctx->side_max = side_new;
     return GG_OK;
 }
 
 template <typename T>
 int step_t(gg_ctx* ctx, gg_step_stats* st) {
+    const long long launches0 = ctx->launches;
     cudaEventRecord(ctx->ev[0], ctx->stream);
     int rc = stage_convolution_t<T>(ctx);
     if (rc) return rc;
@@ -432,6 +447,7 @@ int step_t(gg_ctx* ctx, gg_step_stats* st) {
         st->loop = ctx->loop;
         st->grain_count = ctx->grain_count;
         st->live_grains = ctx->live;
+        st->kernel_launches = (int32_t)(ctx->launches - launches0);
         st->voxel_updates = *ctx->h_total_vox;
         float* f[5] = {&st->ms_convolution, &st->ms_lists, &st->ms_comparison, &st->ms_levelset, &st->ms_redistancing};
         for (int i = 0; i < 5; i++) cudaEventElapsedTime(f[i], ctx->ev[i], ctx->ev[i + 1]);

@@ -56,7 +56,7 @@ typedef struct {
     int32_t loop;               /* loop index of the step just run */
     int32_t grain_count;        /* currentNrGrains after the step (countGrains) */
     int32_t live_grains;        /* grains whose hull is non-empty after the step */
-    int32_t reserved0;
+    int32_t kernel_launches;    /* kernels this library launched for the step */
     int64_t voxel_updates;      /* sum of n^3 over the boxes convolved this step */
     float ms_convolution, ms_lists, ms_comparison, ms_levelset, ms_redistancing, ms_total;
 } gg_step_stats;

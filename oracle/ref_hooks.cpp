@@ -39,6 +39,8 @@
 #include <stdexcept>
 #include <string>
 #include <vector>
+#include <atomic>
+#include <sys/time.h>
 #include <omp.h>
 #include "Eigen/Dense"
 
@@ -55,7 +57,7 @@ namespace {
 enum Kind {
     K_INIT_SDF = 1, K_INIT_LIST = 2, K_STATS = 3, K_NEIGHBORS = 4, K_CONV_IN = 5, K_CONV_OUT = 6,
     K_LIST = 7, K_CMP_OUT = 8, K_CMP_ID = 9, K_SETCMP_OUT = 10, K_REDIST_IN = 11, K_REDIST_OUT = 12,
-    K_MC_ID = 13, K_MC_IN = 14
+    K_MC_ID = 13, K_MC_IN = 14, K_LOOP_TIME = 15
 };
 
 struct Dumper {
@@ -143,6 +145,24 @@ void dump_list(int kind, int loop, int grain, const std::vector<unsigned int>& l
 
 int loop_of(LSbox* b) { return b->m_grainHandler->loop; }
 
+// LOOP_TIME record: wall-clock seconds when the first grain of a loop iteration
+// enters its convolution, i.e. when the iteration's convolution stage starts.
+// Written whenever GG_REF_DUMP is set.
+void stamp_loop(int loop) {
+    static std::atomic<int> last(-1000);
+    int prev = last.load();
+    while (prev < loop) {
+        if (last.compare_exchange_weak(prev, loop)) {
+            timeval tv;
+            gettimeofday(&tv, nullptr);
+            double t = tv.tv_sec + tv.tv_usec * 1e-6;
+            int box[6] = {0, 0, 0, 0, 0, 0};
+            dumper().write(K_LOOP_TIME, loop, 0, box, 0, &t, 1);
+            return;
+        }
+    }
+}
+
 }  // namespace
 
 extern "C" {
@@ -169,6 +189,7 @@ void __wrap__ZN5LSbox23computeDirectNeighboursERK5RTreeIjiLi3EfLi8ELi4EE(LSbox* 
 }
 
 void __wrap__ZN5LSbox18executeConvolutionER15ExpandingVectorIcE(LSbox* self, void* pool) {
+    stamp_loop(loop_of(self));
     const bool w = self->m_exists && dumper().want_buffers((int)self->m_ID, loop_of(self));
     if (w) dump_sdf(K_CONV_IN, loop_of(self), (int)self->m_ID, self->m_inputDistance);
     __real__ZN5LSbox18executeConvolutionER15ExpandingVectorIcE(self, pool);

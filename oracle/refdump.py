@@ -16,7 +16,7 @@ import numpy as np
 KIND = {
     "INIT_SDF": 1, "INIT_LIST": 2, "STATS": 3, "NEIGHBORS": 4, "CONV_IN": 5, "CONV_OUT": 6,
     "LIST": 7, "CMP_OUT": 8, "CMP_ID": 9, "SETCMP_OUT": 10, "REDIST_IN": 11, "REDIST_OUT": 12,
-    "MC_ID": 13, "MC_IN": 14,
+    "MC_ID": 13, "MC_IN": 14, "LOOP_TIME": 15,
 }
 KIND_NAME = {v: k for k, v in KIND.items()}
 HERE = os.path.dirname(os.path.abspath(__file__))
@@ -94,9 +94,12 @@ def parse_timers(stdout: str) -> dict:
 
 def collect(records) -> dict:
     """Group records: init state, per-loop stats/neighbours/lists, stage buffers."""
-    res = {"init_sdf": {}, "init_list": {}, "stats": {}, "neighbors": {}, "lists": {}, "buffers": {}}
+    res = {"init_sdf": {}, "init_list": {}, "stats": {}, "neighbors": {}, "lists": {}, "buffers": {},
+           "loop_time": {}}
     for r in records:
-        if r.kind == "INIT_SDF":
+        if r.kind == "LOOP_TIME":
+            res["loop_time"][r.loop] = float(r.data[0])
+        elif r.kind == "INIT_SDF":
             res["init_sdf"][r.grain] = r
         elif r.kind == "INIT_LIST":
             res["init_list"][r.grain] = r.data

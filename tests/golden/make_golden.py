@@ -1,0 +1,84 @@
+"""Generate the golden fixtures in tests/golden/ from the reference solver itself.
+
+The reference (compiled from its own sources by `make -C oracle ref`, with the
+specified DFT standing in for MKL) runs on seeded voxelised microstructures; the
+observation hooks record the initial state and, every step, each grain's
+existence, volume, surface, box, hull neighbours (first-seen order) and
+comparison list, plus single-box buffers of one grain around every stage.
+
+    python tests/golden/make_golden.py
+"""
+from __future__ import annotations
+
+import os
+import sys
+import tempfile
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ROOT = os.path.dirname(os.path.dirname(HERE))
+sys.path.insert(0, ROOT)
+sys.path.insert(0, os.path.join(ROOT, "oracle"))
+
+from gragles_3d_b200 import microstructure as msgen  # noqa: E402
+import refdump  # noqa: E402
+
+CASES = {
+    # name: (N, grains, border, seed, steps, grain whose buffers are kept, loop of those buffers)
+    "tiny": (32, 20, 5, 1032, 6, 14, 2),
+    "vanish": (40, 150, 5, 1040, 40, 0, 0),
+}
+
+
+def ragged(d: dict, G: int):
+    off = np.zeros(G + 2, np.int64)
+    vals = []
+    for g in range(G + 1):
+        v = d.get(g, np.zeros(0, np.uint32))
+        vals.append(np.asarray(v, np.uint32))
+        off[g + 1] = off[g] + len(v)
+    return off, (np.concatenate(vals) if vals else np.zeros(0, np.uint32))
+
+
+def make(name, N, G, border, seed, steps, keep_grain, keep_loop):
+    ms = msgen.voronoi(N, G, seed=seed)
+    with tempfile.TemporaryDirectory() as d:
+        msgen.write_mode4(ms, d)
+        msgen.write_parameters(os.path.join(d, "parameters.xml"), n_grains=G, border=border, steps=steps)
+        res, _ = refdump.run_case(d, threads=4, grains=str(keep_grain) if keep_grain else None,
+                                  loops=str(keep_loop) if keep_grain else None)
+    out = {"N": N, "G": G, "border": border, "seed": seed, "steps": steps}
+    out["init_list_off"], out["init_list_ids"] = ragged(res["init_list"], G)
+    loops = sorted(res["stats"])
+    S = len(loops)
+    exists = np.zeros((S, G + 1), np.uint8)
+    vol = np.zeros((S, G + 1))
+    sur = np.zeros((S, G + 1))
+    box = np.zeros((S, G + 1, 6), np.int32)
+    nb_off, nb_ids, li_off, li_ids = [], [], [], []
+    for s, loop in enumerate(loops):
+        for g, (dat, b) in res["stats"][loop].items():
+            exists[s, g] = dat[0] == 1.0
+            vol[s, g], sur[s, g] = dat[1], dat[2]
+            box[s, g] = b
+        o, i = ragged(res["neighbors"].get(loop, {}), G)
+        nb_off.append(o); nb_ids.append(i)
+        o, i = ragged(res["lists"].get(loop, {}), G)
+        li_off.append(o); li_ids.append(i)
+    out.update(exists=exists, volume=vol, surface=sur, box=box,
+               nb_off=np.stack(nb_off), nb_ids=np.concatenate(nb_ids), nb_len=np.array([len(x) for x in nb_ids]),
+               list_off=np.stack(li_off), list_ids=np.concatenate(li_ids),
+               list_len=np.array([len(x) for x in li_ids]))
+    if keep_grain:
+        for (kind, loop, g), r in res["buffers"].items():
+            out[f"buf_{kind}"] = r.data
+            out[f"box_{kind}"] = np.array(r.box, np.int32)
+        out["buf_grain"], out["buf_loop"] = keep_grain, keep_loop
+    np.savez_compressed(os.path.join(HERE, f"{name}.npz"), **out)
+    print(name, "ok", {k: v.shape for k, v in out.items() if hasattr(v, "shape")})
+
+
+if __name__ == "__main__":
+    for name, args in CASES.items():
+        make(name, *args)

@@ -1,0 +1,128 @@
+"""CPU tests of the host side: the C ABI library loads and exports every symbol
+include/gg_b200.h declares (no compute calls without a GPU), the microstructure
+generator and its mode-4 files, and the replica aggregation of the multi-GPU
+bench path over a two-rank gloo group."""
+import os
+import re
+import socket
+import tempfile
+
+import numpy as np
+import pytest
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+
+def _declared():
+    src = open(os.path.join(ROOT, "include", "gg_b200.h")).read()
+    src = re.sub(r"/\*.*?\*/", "", src, flags=re.S)
+    return sorted(set(re.findall(r"\b(gg_[a-z0-9_]+)\s*\(", src)))
+
+
+def test_library_exports_every_declared_symbol():
+    import ctypes
+
+    import gragles_3d_b200 as gg
+
+    lib_path = gg.LIB_PATH
+    if not os.path.exists(lib_path):
+        from gragles_3d_b200 import build
+
+        build.build()
+    lib = ctypes.CDLL(lib_path)
+    names = _declared()
+    assert len(names) >= 20
+    missing = [n for n in names if not hasattr(lib, n)]
+    assert not missing, missing
+    assert sorted(gg.EXPORTED) == names
+
+
+def test_create_rejects_bad_parameters_without_touching_the_device():
+    import gragles_3d_b200 as gg
+
+    with pytest.raises(gg.GGError) as e:
+        gg.GrainHandler(1, 10, 0.2, 5)
+    assert e.value.code == gg.GG_ERR_INVALID
+    with pytest.raises(gg.GGError) as e:
+        gg.GrainHandler(64, 10, 0.2, 5, precision=7)
+    assert e.value.code == gg.GG_ERR_INVALID
+
+
+def test_generator_is_deterministic_and_consistent():
+    from gragles_3d_b200 import microstructure as msgen
+
+    a = msgen.voronoi(24, 30, seed=5)
+    b = msgen.voronoi(24, 30, seed=5)
+    assert np.array_equal(a.labels, b.labels) and np.array_equal(a.euler, b.euler)
+    assert a.labels.min() >= 1 and a.labels.max() <= 30
+    ext, counts = a.grain_extents()
+    assert counts.sum() == 24 ** 3
+    for g in range(30):
+        if counts[g] == 0:
+            continue
+        z, y, x = np.nonzero(a.labels == g + 1)
+        assert tuple(ext[g]) == (x.min(), x.max(), y.min(), y.max(), z.min(), z.max())
+    c = msgen.laguerre(24, 30, seed=5, sigma=0.3)
+    assert c.labels.min() >= 1
+
+
+def test_mode4_files_follow_the_reference_reader():
+    """The header/rows parse the way grainhdl.cpp:404-578 reads them (fscanf)."""
+    from gragles_3d_b200 import microstructure as msgen
+
+    ms = msgen.voronoi(16, 9, seed=3)
+    with tempfile.TemporaryDirectory() as d:
+        raw, uds = msgen.write_mode4(ms, d)
+        data = np.fromfile(raw, dtype="<u4").reshape(16, 16, 16)
+        assert np.array_equal(data, ms.labels)
+        lines = open(uds).read().split("\n")
+        assert lines[1].split() == ["ID_offset", "1"]
+        assert [l.split()[1] for l in lines[5:8]] == ["16", "16", "16"]
+        assert lines[8].split() == ["NumberOfGrains", "9"]
+        assert lines[9] == "" and lines[10] == ""
+        rows = [l.split() for l in lines[12:] if l.strip()]
+        assert len(rows) == 9 and all(len(r) == 15 for r in rows)
+        ext, counts = ms.grain_extents()
+        for g, r in enumerate(rows):
+            assert int(r[0]) == g + 1
+            assert [int(v) for v in r[7:13]] == list(ext[g]) and int(r[13]) == counts[g]
+
+
+def _free_port():
+    s = socket.socket()
+    s.bind(("127.0.0.1", 0))
+    p = s.getsockname()[1]
+    s.close()
+    return p
+
+
+def _replica_worker(rank, world, port, q):
+    import torch
+    import torch.distributed as dist
+
+    os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port))
+    dist.init_process_group("gloo", rank=rank, world_size=world)
+    import bench
+
+    elapsed = [10.0, 14.0][rank]
+    vox = [1000.0, 1200.0][rank]
+    q.put((rank, bench.aggregate_replicas(elapsed, vox, dist, device="cpu")))
+    dist.destroy_process_group()
+
+
+def test_replica_aggregation_two_ranks_gloo():
+    """N>1 bench path: throughput = all ranks' voxel-updates / slowest rank's time."""
+    import multiprocessing as mp
+
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    port = _free_port()
+    procs = [ctx.Process(target=_replica_worker, args=(r, 2, port, q)) for r in range(2)]
+    for p in procs:
+        p.start()
+    res = dict(q.get(timeout=120) for _ in procs)
+    for p in procs:
+        p.join(timeout=60)
+    for r in (0, 1):
+        elapsed, vox = res[r]
+        assert elapsed == 14.0 and vox == 2200.0
