@@ -262,8 +262,16 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="gg", choices=["gg", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--paths", default="both", choices=["both", "mixed", "fp64"],
+                    help="profiling aid: run only one precision path")
+    ap.add_argument("--domain", type=int, default=None, help="profiling aid: smaller domain of the same kind")
+    ap.add_argument("--grains", type=int, default=None, help="profiling aid: grain count for --domain")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
+    if args.domain:
+        WORKLOAD.update(workload=f"voronoi-{args.domain}^3-{args.grains}-grains-isotropic", domain=args.domain,
+                        grains=args.grains)
     if args.impl == "reference":
         return reference_arm(args)
 
@@ -284,6 +292,20 @@ def main():
     else:
         torch.cuda.set_device(local)
     ms, ext, counts = microstructure()
+
+    if args.paths != "both":  # profiling aid: one path, no comparison, no baselines
+        prec = gg.PRECISION_MIXED if args.paths == "mixed" else gg.PRECISION_FP64
+        reps, ms_e, clk, _, _ = run_device(gg, prec, ms, ext, counts, args.steps, args.warmup, local, dist)
+        if rank == 0:
+            vox = sum(r["voxel_updates"] for r in reps)
+            keys = ["ms_convolution", "ms_lists", "ms_comparison", "ms_levelset", "ms_redistancing", "ms_total"]
+            print(json.dumps({"profile_run": args.paths, "config": dict(WORKLOAD), "value": vox / (ms_e / 1e3),
+                              "unit": UNIT, "ms_per_step": ms_e / args.steps, "clocks": clk,
+                              "stage_ms": {k: float(np.mean([r[k] for r in reps])) for k in keys}}))
+        if dist:
+            dist.barrier()
+            dist.destroy_process_group()
+        return
 
     reps_m, ms_m, clk_m, vol_m, ex_m = run_device(gg, gg.PRECISION_MIXED, ms, ext, counts, args.steps, args.warmup,
                                                   local, dist)
@@ -315,7 +337,8 @@ def main():
     e2e = None
     out = None
     if rank == 0:
-        e2e = run_e2e(gg, gg.PRECISION_MIXED, ms, ext, counts, args.steps, local)
+        e2e = (run_e2e(gg, gg.PRECISION_MIXED, ms, ext, counts, args.steps, local) if not args.no_e2e else
+               {"value": None, "unit": UNIT, "h2d_bytes_per_step": None, "d2h_bytes_per_step": None})
         cpu = None
         if not args.no_cpu_baseline and world == 1:
             cv, sample, cores, kind = run_reference_cpu(ms, 1, 1, os.cpu_count() or 1)

@@ -25,8 +25,6 @@ namespace {
 
 constexpr double kPi = 3.14159265358979323846;  // ggLS.h:25
 constexpr int kNbCap = 256;
-constexpr int kSlab64 = 4;   // comparison slab (z-planes per tile), FP64 path
-constexpr int kSlab32 = 8;   // FP32 path
 
 struct Timer {
     cudaEvent_t e[6];
@@ -83,7 +81,7 @@ struct gg_ctx {
     int grain_count = 0, live = 0;
     int side_max = 0;      // largest box side of the current layout
     int side_limit = 0;    // largest side the shared-memory kernels accept
-    int list_cap = 4096, slab = kSlab64, hash_cap = 8192;
+    int list_cap = 4096, slab = 8, hash_cap = 8192;
     long long launches = 0;  // kernels launched by this context
     cudaEvent_t ev[7] = {};
 };
@@ -495,16 +493,6 @@ Box initial_box(const int32_t* e, int gb, int M) {
     return b;
 }
 
-// Slab depth of the comparison tiles for the current largest box side.
-int pick_slab(int side, bool fp64) {
-    const size_t per = fp64 ? 12 : 8;
-    const size_t budget = 100 * 1024;
-    long long s = (long long)(budget / (per * (size_t)std::max(1, side * side)));
-    if (s < 1) s = 1;
-    if (s > 16) s = 16;
-    return (int)s;
-}
-
 int supported_side(bool fp64) {
     const size_t lim = 227 * 1024;
     int n = 8;
@@ -742,7 +730,7 @@ int gg_default_lists(gg_ctx* ctx) {
 
 int gg_stage_convolution(gg_ctx* ctx) {
     if (!ctx || !ctx->loaded) return GG_ERR_INVALID;
-    ctx->slab = pick_slab(ctx->side_max, ctx->fp64);
+    ctx->slab = compare_slab(ctx->side_max, ctx->fp64);
     int rc = ctx->fp64 ? stage_convolution_t<double>(ctx) : stage_convolution_t<float>(ctx);
     return rc ? rc : check_err(ctx, "convolution");
 }
@@ -773,7 +761,7 @@ int gg_stage_redistancing(gg_ctx* ctx) {
 
 int gg_step(gg_ctx* ctx, gg_step_stats* stats) {
     if (!ctx || !ctx->loaded) return GG_ERR_INVALID;
-    ctx->slab = pick_slab(ctx->side_max, ctx->fp64);
+    ctx->slab = compare_slab(ctx->side_max, ctx->fp64);
     return ctx->fp64 ? step_t<double>(ctx, stats) : step_t<float>(ctx, stats);
 }
 

@@ -4,17 +4,17 @@
 // (box.cpp:997-1088) and executeSetComparison (box.cpp:814-878), fused in one
 // pass over each box.
 //
-// The reference walks the comparison list in order and keeps, per voxel, the
-// first neighbour whose SDF is strictly greater than everything before it
-// (starting from -1).  That is the maximum value with ties going to the earliest
-// list position, an order-free reduction, so the warps of a tile take
-// neighbours in any order: pass 1 folds each neighbour value into a per-voxel
-// shared-memory atomicMax, pass 2 (FP64) keeps the smallest list position that
-// attains it.  On the FP32 path value and position pack into one 64-bit key and
-// one pass suffices.  The winner's value is re-read for the output, so the result
-// is bit-identical to the sequential walk.  Voxels no neighbour covers keep their
-// IDLocal from the previous layout by the reference's flat-prefix resize
-// (dimensionalBuffer.h:120-131).
+// Work decomposition: a CTA takes one (grain, slab of z-planes) tile and keeps the
+// slab's running maximum and its grain ID in shared memory.  The neighbours whose
+// boxes reach the slab are staged in shared memory in list order.  Each warp owns
+// every nw-th row of the slab and walks the staged neighbours in list order,
+// updating only the voxels of its own rows inside the box intersection with the
+// reference's strict "greater than" rule -- so every voxel sees the neighbours in
+// the reference's order and the result is bit-identical, without atomics, and the
+// work is proportional to the voxels the neighbours cover (lanes along x, a
+// pointer-stepped loop along z).
+// Voxels no neighbour covers keep their IDLocal from the previous layout by the
+// reference's flat-prefix resize (dimensionalBuffer.h:120-131).
 #include "gg_kernels.cuh"
 
 #include <climits>
@@ -23,16 +23,16 @@ namespace gg {
 
 namespace {
 
+constexpr int kThreads = 256;
+constexpr int kStageCap = 512;   // staged neighbour boxes per round
 constexpr unsigned kNone = 0xFFFFFFFFu;
 
-__device__ __forceinline__ unsigned long long ord64(double v) {
-    const long long b = __double_as_longlong(v == 0.0 ? 0.0 : v);  // -0 and +0 compare equal
-    return b >= 0 ? ((unsigned long long)b ^ 0x8000000000000000ull) : ~(unsigned long long)b;
-}
-__device__ __forceinline__ unsigned ord32(float v) {
-    const int b = __float_as_int(v == 0.0f ? 0.0f : v);
-    return b >= 0 ? ((unsigned)b ^ 0x80000000u) : ~(unsigned)b;
-}
+struct Staged {
+    int x0, x1, y0, y1, z0, z1;
+    uint32_t id;
+    int pad;
+    long long off;
+};
 
 // One branch of the reference's boundary distance (box.cpp:1017-1082).  Returns
 // false where no branch assigns `dist`, in which case the reference keeps the value
@@ -91,28 +91,41 @@ __device__ double bc_dist(const Box& b, int i, int j, int k, int m, int gb) {
     }
 }
 
-// Iterate the voxels of intersection `I` with one warp: lanes cover x, several
-// rows per pass when the row is short.
-template <typename F>
-__device__ __forceinline__ void warp_foreach(int ix0, int ix1, int iy0, int iy1, int iz0, int iz1, F&& f) {
-    const int lane = threadIdx.x & 31;
-    const int wx = ix1 - ix0, wy = iy1 - iy0, rows = wy * (iz1 - iz0);
-    const int lpr = wx <= 1 ? 1 : wx <= 2 ? 2 : wx <= 4 ? 4 : wx <= 8 ? 8 : wx <= 16 ? 16 : 32;
-    const int rpi = 32 / lpr;
-    const int sub = lane & (lpr - 1), rsub = lane / lpr;
-    for (int r = rsub; r < rows; r += rpi) {
-        const int zz = r / wy;
-        const int y = iy0 + (r - zz * wy), z = iz0 + zz;
-        for (int x = ix0 + sub; x < ix1; x += lpr) f(x, y, z);
+__device__ __forceinline__ int block_excl_scan(int v, int* sums, int& total) {
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+    int incl = v;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const int u = __shfl_up_sync(0xffffffffu, incl, o);
+        if (lane >= o) incl += u;
     }
+    if (lane == 31) sums[warp] = incl;
+    __syncthreads();
+    if (warp == 0) {
+        const int w = lane < nw ? sums[lane] : 0;
+        int wi = w;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const int u = __shfl_up_sync(0xffffffffu, wi, o);
+            if (lane >= o) wi += u;
+        }
+        if (lane < nw) sums[lane] = wi - w;
+        if (lane == 31) sums[32] = wi;
+    }
+    __syncthreads();
+    total = sums[32];
+    const int r = sums[warp] + incl - v;
+    __syncthreads();
+    return r;
 }
 
 template <typename T>
-__global__ void __launch_bounds__(512) compare_kernel(CompareArgs<T> a) {
+__global__ void __launch_bounds__(kThreads) compare_kernel(CompareArgs<T> a) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
-    unsigned long long* key = reinterpret_cast<unsigned long long*>(smem_raw);
-    const bool fp64 = sizeof(T) == 8;
-    const int warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+    __shared__ int sums[33];
+    Staged* st = reinterpret_cast<Staged*>(smem_raw);
+    T* sval = reinterpret_cast<T*>(st + kStageCap);
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nw = blockDim.x >> 5;
     const int total = a.toff[a.G + 1];
     for (int t = blockIdx.x; t < total; t += gridDim.x) {
         const int g = tile_grain(a.toff, a.G, t);
@@ -120,12 +133,11 @@ __global__ void __launch_bounds__(512) compare_kernel(CompareArgs<T> a) {
         const Box A = a.in.grain_box(g);
         const int sz0 = A.z0 + s * a.slab, sz1 = min(A.z1, sz0 + a.slab);
         const int nx = A.nx(), ny = A.ny();
-        const int V = nx * ny * (sz1 - sz0);
-        unsigned* pos = reinterpret_cast<unsigned*>(key + V);
-        const unsigned long long init = fp64 ? ord64(-1.0) : ((unsigned long long)ord32(-1.0f) << 32);
+        const int P = nx * ny, V = P * (sz1 - sz0);
+        uint32_t* sid = reinterpret_cast<uint32_t*>(sval + V);
         for (int l = threadIdx.x; l < V; l += blockDim.x) {
-            key[l] = init;
-            if (fp64) pos[l] = kNone;
+            sval[l] = T(-1);  // clearValues(-1.0), box.cpp:894
+            sid[l] = kNone;
         }
         const uint32_t* list = a.cmp + (long long)g * a.list_cap;
         const int K = a.n_cmp[g];
@@ -134,31 +146,59 @@ __global__ void __launch_bounds__(512) compare_kernel(CompareArgs<T> a) {
             for (int q = threadIdx.x; q < K; q += blockDim.x) son[q] = list[q];
             if (threadIdx.x == 0) a.n_son[g] = K;
         }
-        __syncthreads();
-        const int passes = fp64 ? 2 : 1;
-        for (int pass = 0; pass < passes; pass++) {
-            for (int p = warp; p < K; p += nw) {
-                const int nbid = list[p];
-                const Box B = a.in.grain_box(nbid);
+        for (int c0 = 0; c0 < K; c0 += kStageCap) {
+            // stage the neighbours of this round that reach the slab, keeping list order
+            int n_staged = 0;
+            for (int r0 = c0; r0 < min(K, c0 + kStageCap); r0 += blockDim.x) {
+                const int p = r0 + threadIdx.x;
+                Staged e;
+                bool hit = false;
+                if (p < min(K, c0 + kStageCap)) {
+                    e.id = list[p];
+                    const int* bb = a.in.box + 6 * e.id;
+                    e.x0 = bb[0]; e.x1 = bb[1]; e.y0 = bb[2]; e.y1 = bb[3]; e.z0 = bb[4]; e.z1 = bb[5];
+                    e.pad = 0;
+                    hit = e.x0 < A.x1 && e.x1 > A.x0 && e.y0 < A.y1 && e.y1 > A.y0 && e.z0 < sz1 && e.z1 > sz0;
+                    e.off = hit ? a.in.off[e.id] : 0;
+                }
+                int cnt;
+                const int pos = block_excl_scan(hit ? 1 : 0, sums, cnt);
+                if (hit) st[n_staged + pos] = e;
+                n_staged += cnt;
+            }
+            __syncthreads();
+            // walk them in list order; warp w owns the slab rows y with (y - A.y0) % nw == w,
+            // and a short intersection row lets one warp take several owned rows at once
+            for (int e = 0; e < n_staged; e++) {
+                const Staged B = st[e];
+                const int ylo = max(A.y0, B.y0), yhi = min(A.y1, B.y1);
                 const int ix0 = max(A.x0, B.x0), ix1 = min(A.x1, B.x1);
-                const int iy0 = max(A.y0, B.y0), iy1 = min(A.y1, B.y1);
                 const int iz0 = max(sz0, B.z0), iz1 = min(sz1, B.z1);
-                if (ix0 >= ix1 || iy0 >= iy1 || iz0 >= iz1) continue;
-                const T* bin = a.in.grain_ptr(nbid);
-                warp_foreach(ix0, ix1, iy0, iy1, iz0, iz1, [&](int x, int y, int z) {
-                    const T v = bin[B.at(y, x, z)];
-                    if (!(v > T(-1))) return;
-                    const int l = ((z - sz0) * ny + (y - A.y0)) * nx + (x - A.x0);
-                    if (fp64) {
-                        const unsigned long long kv = ord64((double)v);
-                        if (pass == 0) atomicMax(key + l, kv);
-                        else if (kv == key[l]) atomicMin(pos + l, (unsigned)p);
-                    } else {
-                        const unsigned long long kv =
-                            ((unsigned long long)ord32((float)v) << 32) | (unsigned long long)(0xFFFFFFFFu - (unsigned)p);
-                        atomicMax(key + l, kv);
+                const int wx = ix1 - ix0;
+                const int lpr = wx <= 8 ? 8 : wx <= 16 ? 16 : 32;
+                const int rpi = 32 / lpr, xo = lane & (lpr - 1), rsub = lane / lpr;
+                // first row >= ylo owned by this warp, then this lane's row among the rpi taken together
+                int y = ylo + ((warp - (ylo - A.y0)) % nw + nw) % nw + rsub * nw;
+                if (ylo + ((warp - (ylo - A.y0)) % nw + nw) % nw >= yhi) continue;
+                const int bnx = B.x1 - B.x0;
+                const long long bplane = (long long)(B.y1 - B.y0) * bnx;
+                const long long bbase = B.off + (long long)(iz0 - B.z0) * bplane - B.x0 - (long long)B.y0 * bnx;
+                uint32_t* sidp = sid;
+                for (; y < yhi; y += rpi * nw) {
+                    for (int x = ix0 + xo; x < ix1; x += lpr) {
+                        const T* __restrict__ bp = a.in.data + (bbase + (long long)y * bnx + x);
+                        int sp = ((iz0 - sz0) * ny + (y - A.y0)) * nx + (x - A.x0);
+#pragma unroll 4
+                        for (int z = iz0; z < iz1; z++, bp += bplane, sp += P) {
+                            const T v = __ldg(bp);
+                            if (v > sval[sp]) {  // box.cpp:938: strict, the first in list order wins
+                                sval[sp] = v;
+                                sidp[sp] = B.id;
+                            }
+                        }
                     }
-                });
+                }
+                __syncwarp();
             }
             __syncthreads();
         }
@@ -172,44 +212,30 @@ __global__ void __launch_bounds__(512) compare_kernel(CompareArgs<T> a) {
         const T* self = a.in.grain_ptr(g);
         T* outp = a.out.grain_ptr(g);
         const double lim = 0.7 * a.geo.delta;
+        const long long base = (long long)(sz0 - A.z0) * P;
         int bx0 = INT_MAX, bx1 = INT_MIN, by0 = INT_MAX, by1 = INT_MIN, bz0 = INT_MAX, bz1 = INT_MIN;
-        const long long base = (long long)(sz0 - A.z0) * nx * ny;
         for (int l = threadIdx.x; l < V; l += blockDim.x) {
-            const int x = A.x0 + l % nx;
-            const int y = A.y0 + (l / nx) % ny;
-            const int z = sz0 + l / (nx * ny);
-            const long long f = base + l;
-            int p;
-            if (fp64) {
-                p = pos[l] == kNone ? -1 : (int)pos[l];
-            } else {
-                const unsigned low = (unsigned)(key[l] & 0xFFFFFFFFull);
-                p = low == 0 ? -1 : (int)(0xFFFFFFFFu - low);
-            }
-            T cmpv;
-            uint32_t id;
-            if (p >= 0) {
-                id = list[p];
-                const Box B = a.in.grain_box(id);
-                cmpv = a.in.grain_ptr(id)[B.at(y, x, z)];
-            } else {
-                cmpv = T(-1);
-                id = f < old_count ? idold[f] : 0u;
-            }
+            const int zl = l / P, rem = l - zl * P;
+            const int yl = rem / nx;
+            const int x = A.x0 + rem - yl * nx, y = A.y0 + yl, z = sz0 + zl;
+            const long long f3 = base + l;
+            T cmpv = sval[l];
+            uint32_t idv = sid[l];
+            if (idv == kNone) idv = f3 < old_count ? idold[f3] : 0u;
             if (boundary) {
                 const double d = bc_dist(A, y, x, z, a.geo.M, a.geo.gb);
                 if (d > -a.geo.gb)
                     if (d * a.geo.h > (double)cmpv) {
                         cmpv = (T)(d * a.geo.h);
-                        id = 0;
+                        idv = 0;
                     }
             }
-            const T in = self[f];
+            const T in = self[f3];
             T res;
             if ((double)fabs(in) < lim) res = T(0.5) * (in - cmpv);
             else res = in;
-            outp[f] = res;
-            idnew[f] = id;
+            outp[f3] = res;
+            idnew[f3] = idv;
             if (res >= 0) {
                 bx0 = min(bx0, x); bx1 = max(bx1, x);
                 by0 = min(by0, y); by1 = max(by1, y);
@@ -225,7 +251,7 @@ __global__ void __launch_bounds__(512) compare_kernel(CompareArgs<T> a) {
             bz0 = min(bz0, __shfl_xor_sync(0xffffffffu, bz0, o));
             bz1 = max(bz1, __shfl_xor_sync(0xffffffffu, bz1, o));
         }
-        if ((threadIdx.x & 31) == 0 && bx0 != INT_MAX) {
+        if (lane == 0 && bx0 != INT_MAX) {
             int* nb = a.newbox + 6 * g;
             atomicMin(nb + 0, bx0); atomicMax(nb + 1, bx1);
             atomicMin(nb + 2, by0); atomicMax(nb + 3, by1);
@@ -247,9 +273,15 @@ __global__ void newbox_init_kernel(int G, const int* present, const int* exists,
 
 }  // namespace
 
-size_t compare_smem_bytes(int nmax, int slab, bool fp64) {
-    const size_t V = (size_t)nmax * nmax * slab;
-    return V * 8 + (fp64 ? V * 4 : 0);
+int compare_slab(int side, bool fp64) {
+    const size_t per = fp64 ? 12 : 8;
+    const size_t budget = 80 * 1024;
+    long long s = (long long)(budget / (per * (size_t)(side > 0 ? side * side : 1)));
+    return (int)(s < 1 ? 1 : s > 16 ? 16 : s);
+}
+
+size_t compare_smem_bytes(int side, int slab, bool fp64) {
+    return sizeof(Staged) * kStageCap + (size_t)side * side * slab * (fp64 ? 12 : 8);
 }
 
 template <typename T>
@@ -259,7 +291,7 @@ void launch_compare(const CompareArgs<T>& a, int grid, size_t smem, cudaStream_t
         allow_max_dynamic_smem(compare_kernel<T>);
         configured = true;
     }
-    compare_kernel<T><<<grid, 512, smem, s>>>(a);
+    compare_kernel<T><<<grid, kThreads, smem, s>>>(a);
 }
 
 void launch_newbox_init(int G, const int* present, const int* exists, const int* box, int* newbox, cudaStream_t s) {

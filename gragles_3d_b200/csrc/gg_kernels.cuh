@@ -59,7 +59,8 @@ struct CompareArgs {
 };
 template <typename T>
 void launch_compare(const CompareArgs<T>& a, int grid, size_t smem, cudaStream_t s);
-size_t compare_smem_bytes(int nmax, int slab, bool fp64);
+int compare_slab(int side, bool fp64);                      // z-planes per comparison tile
+size_t compare_smem_bytes(int side, int slab, bool fp64);
 void launch_newbox_init(int G, const int* present, const int* exists, const int* box, int* newbox, cudaStream_t s);
 
 // ---- list update (gg_lists.cu) ----

@@ -24,6 +24,7 @@ namespace {
 
 constexpr int kThreads = 256;
 constexpr int kHash = 1024;  // distinct neighbour IDs per grain (power of two)
+constexpr int kChunk = 2048; // cubes classified per round
 
 // cubeindex bit b <-> corner offset (dx, dy, dz), marchingCubes.cpp:376-385
 __constant__ int c_corner[8][3] = {{0, 0, 1}, {1, 0, 1}, {1, 0, 0}, {0, 0, 0},
@@ -70,6 +71,7 @@ __device__ __forceinline__ int block_exclusive_scan(int v, int* warp_sums, int& 
     __syncthreads();
     total = warp_sums[32];
     const int r = warp_sums[warp] + incl - v;
+    __syncthreads();  // warp_sums is reused by the next scan
     return r;
 }
 
@@ -106,7 +108,7 @@ __device__ Box resize_to_cube(Box b, int maximumLength) {
 }
 
 template <typename T>
-__global__ void __launch_bounds__(kThreads) mc_kernel(MCArgs<T> a) {
+__global__ void __launch_bounds__(kThreads, 3) mc_kernel(MCArgs<T> a) {
     __shared__ double vbuf[kThreads * 5];
     __shared__ double abuf[kThreads * 5];
     __shared__ int warp_sums[33];
@@ -115,6 +117,8 @@ __global__ void __launch_bounds__(kThreads) mc_kernel(MCArgs<T> a) {
     __shared__ unsigned nb_id[kHash];
     __shared__ unsigned nb_key[kHash];
     __shared__ int n_found;
+    __shared__ unsigned char cidx[kChunk];
+    __shared__ unsigned short act[kChunk];
     const int total = a.toff[a.G + 1];
     for (int t = blockIdx.x; t < total; t += gridDim.x) {
         const int g = tile_grain(a.toff, a.G, t);
@@ -131,23 +135,53 @@ __global__ void __launch_bounds__(kThreads) mc_kernel(MCArgs<T> a) {
         const long long NC = (ncx > 0 && ncy > 0 && ncz > 0) ? (long long)ncx * ncy * ncz : 0;
         double vol = 0.0, area = 0.0;
         long long ntri = 0;
+        const long long plane = (long long)b.nx() * b.ny();
         __syncthreads();
-        for (long long base = 0; base < NC; base += blockDim.x) {
-            const long long c = base + threadIdx.x;
+        for (long long round = 0; round < NC; round += kChunk) {
+          // classify kChunk cubes with coalesced loads (inside = value >= 0, marchingCubes.cpp:12-15)
+          for (int k = 0; k < kChunk; k += kThreads) {
+              const long long c = round + k + threadIdx.x;
+              int ci = 0;
+              if (c < NC) {
+                  const int x = b.x0 + (int)(c % ncx);
+                  const int y = b.y0 + (int)((c / ncx) % ncy);
+                  const int z = b.z0 + (int)(c / ((long long)ncx * ncy));
+                  const T* p = sdf + b.at(y, x, z);
+#pragma unroll
+                  for (int q = 0; q < 8; q++)
+                      if (p[c_corner[q][2] * plane + c_corner[q][1] * b.nx() + c_corner[q][0]] >= 0) ci |= 1 << q;
+              }
+              cidx[k + threadIdx.x] = (unsigned char)ci;
+          }
+          __syncthreads();
+          // active cubes of the round, in cube order
+          int nloc = 0;
+#pragma unroll
+          for (int q = 0; q < kChunk / kThreads; q++) nloc += gg_mc_edge_table[cidx[threadIdx.x * (kChunk / kThreads) + q]] != 0;
+          int n_act;
+          int w = block_exclusive_scan(nloc, warp_sums, n_act);
+#pragma unroll
+          for (int q = 0; q < kChunk / kThreads; q++) {
+              const int lc = threadIdx.x * (kChunk / kThreads) + q;
+              if (gg_mc_edge_table[cidx[lc]] != 0) act[w++] = (unsigned short)lc;
+          }
+          __syncthreads();
+          for (int ab = 0; ab < n_act; ab += kThreads) {
+            const int ia = ab + threadIdx.x;
             int nt = 0, ci = 0;
             int x = 0, y = 0, z = 0;
+            long long c = 0;
             double val[8];
-            if (c < NC) {
+            if (ia < n_act) {
+                c = round + act[ia];
+                ci = cidx[act[ia]];
                 x = b.x0 + (int)(c % ncx);
                 y = b.y0 + (int)((c / ncx) % ncy);
                 z = b.z0 + (int)(c / ((long long)ncx * ncy));
 #pragma unroll
-                for (int k = 0; k < 8; k++) {
+                for (int k = 0; k < 8; k++)
                     val[k] = (double)sdf[b.at(y + c_corner[k][1], x + c_corner[k][0], z + c_corner[k][2])];
-                    if (val[k] >= 0) ci |= 1 << k;
-                }
-                if (gg_mc_edge_table[ci] != 0)
-                    while (gg_mc_tri_table[ci][3 * nt] != -1) nt++;
+                while (gg_mc_tri_table[ci][3 * nt] != -1) nt++;
             }
             int chunk_total;
             const int off = block_exclusive_scan(nt, warp_sums, chunk_total);
@@ -208,6 +242,7 @@ __global__ void __launch_bounds__(kThreads) mc_kernel(MCArgs<T> a) {
             }
             ntri += chunk_total;
             __syncthreads();
+          }
         }
         // collect the distinct IDs and order them by first appearance
         for (int q = threadIdx.x; q < kHash; q += blockDim.x) {
