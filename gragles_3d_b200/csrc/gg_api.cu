@@ -74,6 +74,10 @@ struct gg_ctx {
     int* d_count3 = nullptr;
     int* h_count3 = nullptr;  // pinned
     long long* h_total_vox = nullptr;
+    // comparison: grains per domain tile and sorted lists
+    TileBins bins{};
+    unsigned long long* d_sorted = nullptr;
+    int* h_maxcount = nullptr;  // pinned
     // host mirror
     int p = 0;        // SDF arena holding m_inputDistance
     int q = 0;        // ID arena holding m_IDLocal
@@ -336,22 +340,52 @@ int stage_update_lists_t(gg_ctx* ctx) {
     a.hash_cap = ctx->hash_cap;
     a.err = ctx->d_err;
     launch_update_lists(a, ctx->grid, ctx->stream);
-    ctx->launches += 1;
+    // sorted copies for the comparison's list look-ups; m_secondOrderNeighbours = list (box.cpp:895)
+    SortListArgs sl{};
+    sl.G = ctx->G;
+    sl.toff = ctx->d_toff_one;
+    sl.cmp = ctx->d_cmp;
+    sl.n_cmp = ctx->d_ncmp;
+    sl.son = ctx->d_son;
+    sl.n_son = ctx->d_nson;
+    sl.sorted = ctx->d_sorted;
+    sl.list_cap = ctx->list_cap;
+    launch_sort_lists(sl, ctx->grid, ctx->stream);
+    ctx->launches += 2;
     CK(cudaGetLastError());
+    return GG_OK;
+}
+
+// Make room for the tile-to-grain entries of the current layout.
+int ensure_bins(gg_ctx* ctx) {
+    const long long need = bin_capacity(ctx->G, ctx->side_max);
+    if (need <= ctx->bins.capacity) return GG_OK;
+    CK(cudaStreamSynchronize(ctx->stream));
+    if (ctx->bins.entries) CK(cudaFree(ctx->bins.entries));
+    ctx->bins.capacity = need + need / 4;
+    CK(dalloc(&ctx->bins.entries, ctx->bins.capacity));
     return GG_OK;
 }
 
 template <typename T>
 int stage_comparison_t(gg_ctx* ctx) {
     const int p = ctx->p, q = ctx->q;
+    int rc = ensure_bins(ctx);
+    if (rc) return rc;
     launch_newbox_init(ctx->G, ctx->d_present, ctx->d_exists, ctx->d_box[p ^ 1], ctx->d_newbox, ctx->stream);
-    ctx->launches += 1;
+    launch_bin(ctx->bins, ctx->G, ctx->d_exists, ctx->d_box[p], ctx->d_err, ctx->stream);
+    ctx->launches += 4;
+    CK(cudaMemcpyAsync(ctx->h_maxcount, ctx->bins.max_count, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
+    CK(cudaStreamSynchronize(ctx->stream));
+    rc = check_err(ctx, "comparison binning");  // nothing may read past the tile entries
+    if (rc) return rc;
+    const int mcap = std::max(1, *ctx->h_maxcount);
+    if (mcap > 254 || compare_smem_bytes(mcap, sizeof(T) == 8) > 227 * 1024)
+        return fail(ctx, GG_ERR_UNSUPPORTED, "%d grain boxes reach one comparison tile (at most 254 supported)", mcap);
     CompareArgs<T> a{};
-    a.G = ctx->G;
     a.geo = ctx->geo;
-    a.toff = ctx->d_toff_slab;
-    a.slab = ctx->slab;
-    a.exists = ctx->d_exists;
+    a.bins = ctx->bins;
+    a.mcap = mcap;
     a.in = arena<T>(ctx, p);
     a.out = arena<T>(ctx, p ^ 1);
     a.id_old = ctx->d_idarena[q];
@@ -359,14 +393,12 @@ int stage_comparison_t(gg_ctx* ctx) {
     a.idoff_old = ctx->d_idoff[q];
     a.id_new = ctx->d_idarena[q ^ 1];
     a.idoff_new = ctx->d_idoff[q ^ 1];
-    a.cmp = ctx->d_cmp;
+    a.sorted = ctx->d_sorted;
     a.n_cmp = ctx->d_ncmp;
-    a.son = ctx->d_son;
-    a.n_son = ctx->d_nson;
     a.list_cap = ctx->list_cap;
     a.newbox = ctx->d_newbox;
     a.err = ctx->d_err;
-    launch_compare<T>(a, ctx->grid, compare_smem_bytes(ctx->side_max, ctx->slab, sizeof(T) == 8), ctx->stream);
+    launch_compare<T>(a, ctx->num_sms * 4, ctx->stream);
     ctx->launches += 1;
     CK(cudaGetLastError());
     ctx->q ^= 1;
@@ -498,7 +530,7 @@ int supported_side(bool fp64) {
     int n = 8;
     for (;;) {
         const int m = n + 1;
-        bool ok = redist_smem_bytes(m, fp64) <= lim && compare_smem_bytes(m, 1, fp64) <= lim;
+        bool ok = redist_smem_bytes(m, fp64) <= lim;
         if (fp64) ok = ok && conv_f64_smem_bytes(m) <= lim;
         else ok = ok && 3 * (size_t)m * (m | 1) * 4 <= lim;
         if (!ok || m > 4096) return n;
@@ -512,9 +544,11 @@ void free_all(gg_ctx* c) {
                     c->d_off[0], c->d_off[1], c->d_idarena[0], c->d_idarena[1], c->d_idbox[0], c->d_idbox[1],
                     c->d_idoff[0], c->d_idoff[1], c->d_spec, c->d_spec_off, c->d_toff_n, c->d_toff_slab,
                     c->d_toff_one, c->d_toff_mc, c->d_toff_red, c->d_tw, c->d_tw_off, c->d_gtab, c->d_g_off,
-                    c->d_circ, c->d_circ_off, c->d_err, c->d_total_vox, c->d_count3};
+                    c->d_circ, c->d_circ_off, c->d_err, c->d_total_vox, c->d_count3, c->bins.count,
+                    c->bins.off, c->bins.cursor, c->bins.entries, c->bins.max_count, c->d_sorted};
     for (void* p : ptrs)
         if (p) cudaFree(p);
+    if (c->h_maxcount) cudaFreeHost(c->h_maxcount);
     if (c->h_count3) cudaFreeHost(c->h_count3);
     if (c->h_total_vox) cudaFreeHost(c->h_total_vox);
     for (auto& e : c->ev)
@@ -589,6 +623,16 @@ int gg_create(const gg_params* params, gg_ctx** out) {
     CK(dalloc(&ctx->d_err, 1));
     CK(dalloc(&ctx->d_total_vox, 1));
     CK(dalloc(&ctx->d_count3, 3));
+    ctx->bins.ntx = (ctx->M + kTX - 1) / kTX;
+    ctx->bins.nty = (ctx->M + kTY - 1) / kTY;
+    ctx->bins.ntz = (ctx->M + kTZ - 1) / kTZ;
+    const size_t n_tiles = (size_t)ctx->bins.ntx * ctx->bins.nty * ctx->bins.ntz;
+    CK(dalloc(&ctx->bins.count, n_tiles + 1));
+    CK(dalloc(&ctx->bins.off, n_tiles + 1));
+    CK(dalloc(&ctx->bins.cursor, n_tiles + 1));
+    CK(dalloc(&ctx->bins.max_count, 1));
+    CK(dalloc(&ctx->d_sorted, (size_t)ctx->list_cap * G1));
+    CK(cudaMallocHost((void**)&ctx->h_maxcount, sizeof(int)));
     CK(cudaMallocHost((void**)&ctx->h_count3, 3 * sizeof(int)));
     CK(cudaMallocHost((void**)&ctx->h_total_vox, sizeof(long long)));
     CK(cudaMemset(ctx->d_err, 0, sizeof(int)));
@@ -730,7 +774,6 @@ int gg_default_lists(gg_ctx* ctx) {
 
 int gg_stage_convolution(gg_ctx* ctx) {
     if (!ctx || !ctx->loaded) return GG_ERR_INVALID;
-    ctx->slab = compare_slab(ctx->side_max, ctx->fp64);
     int rc = ctx->fp64 ? stage_convolution_t<double>(ctx) : stage_convolution_t<float>(ctx);
     return rc ? rc : check_err(ctx, "convolution");
 }
@@ -761,7 +804,6 @@ int gg_stage_redistancing(gg_ctx* ctx) {
 
 int gg_step(gg_ctx* ctx, gg_step_stats* stats) {
     if (!ctx || !ctx->loaded) return GG_ERR_INVALID;
-    ctx->slab = compare_slab(ctx->side_max, ctx->fp64);
     return ctx->fp64 ? step_t<double>(ctx, stats) : step_t<float>(ctx, stats);
 }
 

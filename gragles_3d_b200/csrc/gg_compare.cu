@@ -1,21 +1,34 @@
 // gg_compare.cu -- comparison, boundary condition and set-comparison of every grain.
 //
 // Stands in for LSbox::executeComparison (box.cpp:891-966), boundaryCondition
-// (box.cpp:997-1088) and executeSetComparison (box.cpp:814-878), fused in one
-// pass over each box.
+// (box.cpp:997-1088) and executeSetComparison (box.cpp:814-878).
 //
-// Work decomposition: a CTA takes one (grain, slab of z-planes) tile and keeps the
-// slab's running maximum and its grain ID in shared memory.  The neighbours whose
-// boxes reach the slab are staged in shared memory in list order.  Each warp owns
-// every nw-th row of the slab and walks the staged neighbours in list order,
-// updating only the voxels of its own rows inside the box intersection with the
-// reference's strict "greater than" rule -- so every voxel sees the neighbours in
-// the reference's order and the result is bit-identical, without atomics, and the
-// work is proportional to the voxels the neighbours cover (lanes along x, a
-// pointer-stepped loop along z).
-// Voxels no neighbour covers keep their IDLocal from the previous layout by the
-// reference's flat-prefix resize (dimensionalBuffer.h:120-131).
+// The reference, per grain A and voxel v of A's box, walks A's comparison list in
+// order and keeps the first neighbour whose value at v is strictly greater than
+// everything before it (starting from -1).  That is: the largest value among the
+// listed neighbours whose box contains v, ties going to the earliest list
+// position.  Each box voxel is read about thirty times that way.  Here the work is
+// turned around and done per domain tile instead of per grain:
+//
+//   1. sort_lists: per grain, (ID, position) of its list sorted by ID, so that
+//      "is B in A's list, and where" is a binary search;
+//   2. bin: every tile of kTX x kTY x kTZ domain voxels gets the IDs of the
+//      grains whose boxes reach it (count, scan, fill);
+//   3. compare: one CTA per tile loads every covering box's values over the tile
+//      into shared memory once, keeps per voxel the kTop largest values, and for
+//      every (grain, voxel) pair picks the first candidate that is in that grain's
+//      list, resolving equal values by list position -- falling back to a full
+//      scan of the tile's boxes whenever the kTop candidates cannot decide.  The
+//      boundary condition, the set comparison, the outputs and the new bounding
+//      box follow in the same pass.
+//
+// Every value is read once and written once (12 B per voxel on the FP32 path),
+// and the result is bit-identical to the sequential walk.  Voxels no listed
+// neighbour covers keep their IDLocal from the previous layout by the reference's
+// flat-prefix resize (dimensionalBuffer.h:120-131).
 #include "gg_kernels.cuh"
+
+#include <math_constants.h>
 
 #include <climits>
 
@@ -24,15 +37,11 @@ namespace gg {
 namespace {
 
 constexpr int kThreads = 256;
-constexpr int kStageCap = 512;   // staged neighbour boxes per round
+constexpr int kTV = kTX * kTY * kTZ;   // voxels per tile (64)
+constexpr int kTop = 4;                // candidates kept per voxel
+constexpr int kParts = kThreads / kTV; // threads scanning the boxes of one voxel
 constexpr unsigned kNone = 0xFFFFFFFFu;
-
-struct Staged {
-    int x0, x1, y0, y1, z0, z1;
-    uint32_t id;
-    int pad;
-    long long off;
-};
+constexpr unsigned short kNotListed = 0xFFFF, kUnknown = 0xFFFE;
 
 // One branch of the reference's boundary distance (box.cpp:1017-1082).  Returns
 // false where no branch assigns `dist`, in which case the reference keeps the value
@@ -91,137 +100,350 @@ __device__ double bc_dist(const Box& b, int i, int j, int k, int m, int gb) {
     }
 }
 
-__device__ __forceinline__ int block_excl_scan(int v, int* sums, int& total) {
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
-    int incl = v;
+// ---------------------------------------------------------------------------------
+// 1. sorted copies of the comparison lists (and m_secondOrderNeighbours = list)
+// ---------------------------------------------------------------------------------
+__global__ void __launch_bounds__(512) sort_lists_kernel(SortListArgs a) {
+    extern __shared__ __align__(16) unsigned long long keys[];
+    const int total = a.toff[a.G + 1];
+    for (int t = blockIdx.x; t < total; t += gridDim.x) {
+        const int g = tile_grain(a.toff, a.G, t);
+        const int K = a.n_cmp[g];
+        const uint32_t* list = a.cmp + (long long)g * a.list_cap;
+        uint32_t* son = a.son + (long long)g * a.list_cap;  // box.cpp:895
+        int P2 = 1;
+        while (P2 < K) P2 <<= 1;
+        for (int i = threadIdx.x; i < P2; i += blockDim.x) {
+            if (i < K) {
+                const uint32_t id = list[i];
+                son[i] = id;
+                keys[i] = ((unsigned long long)id << 32) | (unsigned)i;
+            } else {
+                keys[i] = ~0ull;
+            }
+        }
+        if (threadIdx.x == 0) a.n_son[g] = K;
+        __syncthreads();
+        for (int k = 2; k <= P2; k <<= 1) {  // bitonic sort, ascending
+            for (int j = k >> 1; j > 0; j >>= 1) {
+                for (int i = threadIdx.x; i < P2; i += blockDim.x) {
+                    const int l = i ^ j;
+                    if (l > i) {
+                        const unsigned long long x = keys[i], y = keys[l];
+                        const bool up = (i & k) == 0;
+                        if ((x > y) == up) { keys[i] = y; keys[l] = x; }
+                    }
+                }
+                __syncthreads();
+            }
+        }
+        unsigned long long* dst = a.sorted + (long long)g * a.list_cap;
+        for (int i = threadIdx.x; i < K; i += blockDim.x) dst[i] = keys[i];
+        __syncthreads();
+    }
+}
+
+// ---------------------------------------------------------------------------------
+// 2. binning of grain boxes to domain tiles
+// ---------------------------------------------------------------------------------
+template <bool FILL>
+__global__ void bin_kernel(TileBins tb, int G, const int* exists, const int* box, int* err) {
+    for (int g = 1 + blockIdx.x * blockDim.x + threadIdx.x; g <= G; g += gridDim.x * blockDim.x) {
+        if (!exists[g]) continue;
+        const Box b = load_box(box + 6 * g);
+        if (b.nx() <= 0) continue;
+        const int tx0 = b.x0 / kTX, tx1 = (b.x1 - 1) / kTX;
+        const int ty0 = b.y0 / kTY, ty1 = (b.y1 - 1) / kTY;
+        const int tz0 = b.z0 / kTZ, tz1 = (b.z1 - 1) / kTZ;
+        for (int tz = tz0; tz <= tz1; tz++)
+            for (int ty = ty0; ty <= ty1; ty++)
+                for (int tx = tx0; tx <= tx1; tx++) {
+                    const int t = (tz * tb.nty + ty) * tb.ntx + tx;
+                    if (!FILL) {
+                        atomicAdd(tb.count + t, 1);
+                    } else {
+                        const long long slot = tb.off[t] + atomicAdd(tb.cursor + t, 1);
+                        if (slot < tb.capacity) tb.entries[slot] = (uint32_t)g;
+                        else atomicOr(err, ERR_POOL);
+                    }
+                }
+    }
+}
+
+// Exclusive scan of the tile counts (one CTA), largest count, capacity check.
+__global__ void __launch_bounds__(1024) bin_scan_kernel(TileBins tb, int n_tiles, int* err) {
+    __shared__ long long sums[33];
+    __shared__ int mx[32];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int per = (n_tiles + blockDim.x - 1) / blockDim.x;
+    const int t0 = threadIdx.x * per, t1 = min(n_tiles, t0 + per);
+    long long mine = 0;
+    int m = 0;
+    for (int t = t0; t < t1; t++) {
+        mine += tb.count[t];
+        m = max(m, tb.count[t]);
+    }
+    long long incl = mine;
 #pragma unroll
     for (int o = 1; o < 32; o <<= 1) {
-        const int u = __shfl_up_sync(0xffffffffu, incl, o);
+        const long long u = __shfl_up_sync(0xffffffffu, incl, o);
         if (lane >= o) incl += u;
     }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) m = max(m, __shfl_xor_sync(0xffffffffu, m, o));
     if (lane == 31) sums[warp] = incl;
+    if (lane == 0) mx[warp] = m;
     __syncthreads();
     if (warp == 0) {
-        const int w = lane < nw ? sums[lane] : 0;
-        int wi = w;
+        const long long w = sums[lane];
+        long long wi = w;
 #pragma unroll
         for (int o = 1; o < 32; o <<= 1) {
-            const int u = __shfl_up_sync(0xffffffffu, wi, o);
+            const long long u = __shfl_up_sync(0xffffffffu, wi, o);
             if (lane >= o) wi += u;
         }
-        if (lane < nw) sums[lane] = wi - w;
+        sums[lane] = wi - w;
         if (lane == 31) sums[32] = wi;
+        int mm = mx[lane];
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) mm = max(mm, __shfl_xor_sync(0xffffffffu, mm, o));
+        if (lane == 0) mx[0] = mm;
     }
     __syncthreads();
-    total = sums[32];
-    const int r = sums[warp] + incl - v;
-    __syncthreads();
-    return r;
+    long long run = sums[warp] + incl - mine;
+    for (int t = t0; t < t1; t++) {
+        tb.off[t] = (int)run;
+        run += tb.count[t];
+    }
+    if (threadIdx.x == 0) {
+        tb.off[n_tiles] = (int)sums[32];
+        *tb.max_count = mx[0];
+        if (sums[32] > tb.capacity) atomicOr(err, ERR_POOL);
+    }
+}
+
+// ---------------------------------------------------------------------------------
+// 3. the per-tile comparison
+// ---------------------------------------------------------------------------------
+__device__ __forceinline__ unsigned short list_pos(const unsigned long long* sorted, int n, uint32_t id) {
+    int lo = 0, hi = n;  // first key >= (id << 32)
+    const unsigned long long key = (unsigned long long)id << 32;
+    while (lo < hi) {
+        const int mid = (lo + hi) >> 1;
+        if (__ldg(sorted + mid) < key) lo = mid + 1; else hi = mid;
+    }
+    if (lo < n) {
+        const unsigned long long k = __ldg(sorted + lo);
+        if ((uint32_t)(k >> 32) == id) return (unsigned short)(k & 0xFFFFu);
+    }
+    return kNotListed;
+}
+
+template <typename T>
+struct TileSmem {
+    // entries (boxes reaching the tile)
+    uint32_t* id;
+    int* box;           // 6 per entry
+    long long* off;
+    int* bbox;          // 6 per entry: new bounding box contributions
+    T* val;             // [entry][voxel]
+    unsigned short* pos;// [entry a][entry b]: position of b in a's list, kNotListed, or kUnknown
+    T* topv;            // [voxel][kTop]
+    unsigned char* topi;
+    int* ncand;         // covering entries with value > -1, per voxel
+};
+
+template <typename T>
+__device__ TileSmem<T> carve(unsigned char* base, int mcap) {
+    TileSmem<T> s;
+    unsigned char* p = base;
+    s.off = reinterpret_cast<long long*>(p); p += 8 * mcap;
+    s.val = reinterpret_cast<T*>(p); p += sizeof(T) * (size_t)mcap * kTV;
+    s.topv = reinterpret_cast<T*>(p); p += sizeof(T) * kTV * kTop * kParts;
+    s.id = reinterpret_cast<uint32_t*>(p); p += 4 * mcap;
+    s.box = reinterpret_cast<int*>(p); p += 24 * mcap;
+    s.bbox = reinterpret_cast<int*>(p); p += 24 * mcap;
+    s.ncand = reinterpret_cast<int*>(p); p += 4 * kTV * kParts;
+    s.pos = reinterpret_cast<unsigned short*>(p); p += 2 * (size_t)mcap * mcap;
+    s.topi = p;
+    return s;
+}
+
+template <typename T>
+__device__ __forceinline__ T neg_inf();
+template <>
+__device__ __forceinline__ double neg_inf<double>() { return -CUDART_INF; }
+template <>
+__device__ __forceinline__ float neg_inf<float>() { return -CUDART_INF_F; }
+
+template <typename T>
+__device__ __forceinline__ unsigned short lazy_pos(TileSmem<T>& s, const CompareArgs<T>& a, int m, int ea, int eb) {
+    unsigned short p = s.pos[ea * m + eb];
+    if (p == kUnknown) {
+        const uint32_t ga = s.id[ea];
+        p = list_pos(a.sorted + (long long)ga * a.list_cap, a.n_cmp[ga], s.id[eb]);
+        s.pos[ea * m + eb] = p;  // every thread that computes it writes the same value
+    }
+    return p;
 }
 
 template <typename T>
 __global__ void __launch_bounds__(kThreads) compare_kernel(CompareArgs<T> a) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
-    __shared__ int sums[33];
-    Staged* st = reinterpret_cast<Staged*>(smem_raw);
-    T* sval = reinterpret_cast<T*>(st + kStageCap);
-    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nw = blockDim.x >> 5;
-    const int total = a.toff[a.G + 1];
-    for (int t = blockIdx.x; t < total; t += gridDim.x) {
-        const int g = tile_grain(a.toff, a.G, t);
-        const int s = t - a.toff[g];
-        const Box A = a.in.grain_box(g);
-        const int sz0 = A.z0 + s * a.slab, sz1 = min(A.z1, sz0 + a.slab);
-        const int nx = A.nx(), ny = A.ny();
-        const int P = nx * ny, V = P * (sz1 - sz0);
-        uint32_t* sid = reinterpret_cast<uint32_t*>(sval + V);
-        for (int l = threadIdx.x; l < V; l += blockDim.x) {
-            sval[l] = T(-1);  // clearValues(-1.0), box.cpp:894
-            sid[l] = kNone;
+    TileSmem<T> s = carve<T>(smem_raw, a.mcap);
+    const TileBins& tb = a.bins;
+    const int n_tiles = tb.ntx * tb.nty * tb.ntz;
+    const T NEG = neg_inf<T>();
+    for (int t = blockIdx.x; t < n_tiles; t += gridDim.x) {
+        const int e0 = tb.off[t], m = tb.off[t + 1] - e0;
+        if (m == 0) continue;
+        if (m > a.mcap) {
+            if (threadIdx.x == 0) atomicOr(a.err, ERR_BOX);
+            continue;
         }
-        const uint32_t* list = a.cmp + (long long)g * a.list_cap;
-        const int K = a.n_cmp[g];
-        if (s == 0) {  // m_secondOrderNeighbours = m_comparisonList, box.cpp:895
-            uint32_t* son = a.son + (long long)g * a.list_cap;
-            for (int q = threadIdx.x; q < K; q += blockDim.x) son[q] = list[q];
-            if (threadIdx.x == 0) a.n_son[g] = K;
+        const int tx = t % tb.ntx, ty = (t / tb.ntx) % tb.nty, tz = t / (tb.ntx * tb.nty);
+        const int X0 = tx * kTX, Y0 = ty * kTY, Z0 = tz * kTZ;
+        // entries
+        for (int e = threadIdx.x; e < m; e += blockDim.x) {
+            const uint32_t g = tb.entries[e0 + e];
+            s.id[e] = g;
+            const int* bb = a.in.box + 6 * g;
+#pragma unroll
+            for (int q = 0; q < 6; q++) s.box[6 * e + q] = bb[q];
+            s.off[e] = a.in.off[g];
+            s.bbox[6 * e + 0] = INT_MAX; s.bbox[6 * e + 1] = INT_MIN;
+            s.bbox[6 * e + 2] = INT_MAX; s.bbox[6 * e + 3] = INT_MIN;
+            s.bbox[6 * e + 4] = INT_MAX; s.bbox[6 * e + 5] = INT_MIN;
         }
-        for (int c0 = 0; c0 < K; c0 += kStageCap) {
-            // stage the neighbours of this round that reach the slab, keeping list order
-            int n_staged = 0;
-            for (int r0 = c0; r0 < min(K, c0 + kStageCap); r0 += blockDim.x) {
-                const int p = r0 + threadIdx.x;
-                Staged e;
-                bool hit = false;
-                if (p < min(K, c0 + kStageCap)) {
-                    e.id = list[p];
-                    const int* bb = a.in.box + 6 * e.id;
-                    e.x0 = bb[0]; e.x1 = bb[1]; e.y0 = bb[2]; e.y1 = bb[3]; e.z0 = bb[4]; e.z1 = bb[5];
-                    e.pad = 0;
-                    hit = e.x0 < A.x1 && e.x1 > A.x0 && e.y0 < A.y1 && e.y1 > A.y0 && e.z0 < sz1 && e.z1 > sz0;
-                    e.off = hit ? a.in.off[e.id] : 0;
+        for (int q = threadIdx.x; q < m * m; q += blockDim.x) s.pos[q] = kUnknown;
+        __syncthreads();
+        // values of every covering box over the tile (-inf outside the box)
+        for (int q = threadIdx.x; q < m * kTV; q += blockDim.x) {
+            const int e = q / kTV, v = q % kTV;
+            const int x = X0 + v % kTX, y = Y0 + (v / kTX) % kTY, z = Z0 + v / (kTX * kTY);
+            const Box B = load_box(s.box + 6 * e);
+            T w = NEG;
+            if (x >= B.x0 && x < B.x1 && y >= B.y0 && y < B.y1 && z >= B.z0 && z < B.z1)
+                w = a.in.data[s.off[e] + B.at(y, x, z)];
+            s.val[q] = w;
+        }
+        __syncthreads();
+        // per voxel: the kTop largest values > -1 (kParts threads share a voxel)
+        {
+            const int v = threadIdx.x % kTV, part = threadIdx.x / kTV;
+            T tv[kTop];
+            int ti[kTop];
+            int cnt = 0, nc = 0;
+            for (int e = part; e < m; e += kParts) {
+                const T w = s.val[e * kTV + v];
+                if (!(w > T(-1))) continue;
+                nc++;
+                // insert keeping descending order (equal values keep arrival order)
+                int k = cnt < kTop ? cnt : kTop;
+                if (k == kTop && !(w > tv[kTop - 1])) continue;
+                if (k == kTop) k = kTop - 1;
+                while (k > 0 && w > tv[k - 1]) {
+                    if (k < kTop) { tv[k] = tv[k - 1]; ti[k] = ti[k - 1]; }
+                    k--;
                 }
-                int cnt;
-                const int pos = block_excl_scan(hit ? 1 : 0, sums, cnt);
-                if (hit) st[n_staged + pos] = e;
-                n_staged += cnt;
+                tv[k] = w;
+                ti[k] = e;
+                if (cnt < kTop) cnt++;
             }
-            __syncthreads();
-            // walk them in list order; warp w owns the slab rows y with (y - A.y0) % nw == w,
-            // and a short intersection row lets one warp take several owned rows at once
-            for (int e = 0; e < n_staged; e++) {
-                const Staged B = st[e];
-                const int ylo = max(A.y0, B.y0), yhi = min(A.y1, B.y1);
-                const int ix0 = max(A.x0, B.x0), ix1 = min(A.x1, B.x1);
-                const int iz0 = max(sz0, B.z0), iz1 = min(sz1, B.z1);
-                const int wx = ix1 - ix0;
-                const int lpr = wx <= 8 ? 8 : wx <= 16 ? 16 : 32;
-                const int rpi = 32 / lpr, xo = lane & (lpr - 1), rsub = lane / lpr;
-                // first row >= ylo owned by this warp, then this lane's row among the rpi taken together
-                int y = ylo + ((warp - (ylo - A.y0)) % nw + nw) % nw + rsub * nw;
-                if (ylo + ((warp - (ylo - A.y0)) % nw + nw) % nw >= yhi) continue;
-                const int bnx = B.x1 - B.x0;
-                const long long bplane = (long long)(B.y1 - B.y0) * bnx;
-                const long long bbase = B.off + (long long)(iz0 - B.z0) * bplane - B.x0 - (long long)B.y0 * bnx;
-                uint32_t* sidp = sid;
-                for (; y < yhi; y += rpi * nw) {
-                    for (int x = ix0 + xo; x < ix1; x += lpr) {
-                        const T* __restrict__ bp = a.in.data + (bbase + (long long)y * bnx + x);
-                        int sp = ((iz0 - sz0) * ny + (y - A.y0)) * nx + (x - A.x0);
-#pragma unroll 4
-                        for (int z = iz0; z < iz1; z++, bp += bplane, sp += P) {
-                            const T v = __ldg(bp);
-                            if (v > sval[sp]) {  // box.cpp:938: strict, the first in list order wins
-                                sval[sp] = v;
-                                sidp[sp] = B.id;
-                            }
-                        }
+            for (int k = 0; k < kTop; k++) {
+                s.topv[(part * kTV + v) * kTop + k] = k < cnt ? tv[k] : NEG;
+                s.topi[(part * kTV + v) * kTop + k] = k < cnt ? (unsigned char)ti[k] : 0xFF;
+            }
+            s.ncand[part * kTV + v] = nc;
+        }
+        __syncthreads();
+        if (threadIdx.x < kTV) {  // merge the kParts partial lists
+            const int v = threadIdx.x;
+            T tv[kTop];
+            int ti[kTop];
+            int cnt = 0, nc = 0;
+            for (int part = 0; part < kParts; part++) {
+                nc += s.ncand[part * kTV + v];
+                for (int k = 0; k < kTop; k++) {
+                    const int e = s.topi[(part * kTV + v) * kTop + k];
+                    if (e == 0xFF) break;
+                    const T w = s.topv[(part * kTV + v) * kTop + k];
+                    int j = cnt < kTop ? cnt : kTop;
+                    if (j == kTop && !(w > tv[kTop - 1])) continue;
+                    if (j == kTop) j = kTop - 1;
+                    while (j > 0 && w > tv[j - 1]) {
+                        if (j < kTop) { tv[j] = tv[j - 1]; ti[j] = ti[j - 1]; }
+                        j--;
                     }
+                    tv[j] = w;
+                    ti[j] = e;
+                    if (cnt < kTop) cnt++;
                 }
-                __syncwarp();
             }
-            __syncthreads();
+            for (int k = 0; k < kTop; k++) {
+                s.topv[v * kTop + k] = k < cnt ? tv[k] : NEG;
+                s.topi[v * kTop + k] = k < cnt ? (unsigned char)ti[k] : 0xFF;
+            }
+            s.ncand[v] = nc;
         }
-        // epilogue: boundary condition, set comparison, outputs, new bbox
-        const bool boundary = !(A.x0 > a.geo.gb && A.x1 < a.geo.M - a.geo.gb && A.y0 > a.geo.gb &&
-                                A.y1 < a.geo.M - a.geo.gb && A.z0 > a.geo.gb && A.z1 < a.geo.M - a.geo.gb);
-        const Box Bold = load_box(a.idbox_old + 6 * g);
-        const long long old_count = Bold.count();
-        const uint32_t* idold = a.id_old + a.idoff_old[g];
-        uint32_t* idnew = a.id_new + a.idoff_new[g];
-        const T* self = a.in.grain_ptr(g);
-        T* outp = a.out.grain_ptr(g);
+        __syncthreads();
+        // every (grain, voxel) pair of the tile
         const double lim = 0.7 * a.geo.delta;
-        const long long base = (long long)(sz0 - A.z0) * P;
-        int bx0 = INT_MAX, bx1 = INT_MIN, by0 = INT_MAX, by1 = INT_MIN, bz0 = INT_MAX, bz1 = INT_MIN;
-        for (int l = threadIdx.x; l < V; l += blockDim.x) {
-            const int zl = l / P, rem = l - zl * P;
-            const int yl = rem / nx;
-            const int x = A.x0 + rem - yl * nx, y = A.y0 + yl, z = sz0 + zl;
-            const long long f3 = base + l;
-            T cmpv = sval[l];
-            uint32_t idv = sid[l];
-            if (idv == kNone) idv = f3 < old_count ? idold[f3] : 0u;
+        for (int q = threadIdx.x; q < m * kTV; q += blockDim.x) {
+            const int ea = q / kTV, v = q % kTV;
+            const T in = s.val[q];
+            if (in == NEG) continue;  // voxel outside this grain's box
+            const int x = X0 + v % kTX, y = Y0 + (v / kTX) % kTY, z = Z0 + v / (kTX * kTY);
+            // the first listed neighbour among the largest values, ties to the earliest position
+            int best = -1;
+            unsigned short bpos = kNotListed;
+            T level = NEG;
+            bool decided = false;
+            int k = 0;
+            for (; k < kTop; k++) {
+                const int eb = s.topi[v * kTop + k];
+                if (eb == 0xFF) break;
+                const T w = s.topv[v * kTop + k];
+                if (best >= 0 && !(w == level)) { decided = true; break; }
+                if (eb == ea) continue;
+                const unsigned short p = lazy_pos(s, a, m, ea, eb);
+                if (p == kNotListed) continue;
+                if (best < 0 || p < bpos) { best = eb; bpos = p; level = w; }
+            }
+            const int listed = k;  // candidates examined
+            if (!decided) {
+                // decided anyway when every covering candidate was among the kTop examined
+                if (s.ncand[v] <= listed && k < kTop + 1) decided = true;
+            }
+            if (!decided) {  // full scan of the tile's boxes at this voxel
+                best = -1;
+                bpos = kNotListed;
+                level = NEG;
+                for (int eb = 0; eb < m; eb++) {
+                    if (eb == ea) continue;
+                    const T w = s.val[eb * kTV + v];
+                    if (!(w > T(-1))) continue;
+                    if (best >= 0 && w < level) continue;
+                    const unsigned short p = lazy_pos(s, a, m, ea, eb);
+                    if (p == kNotListed) continue;
+                    if (best < 0 || w > level || (w == level && p < bpos)) { best = eb; bpos = p; level = w; }
+                }
+            }
+            const uint32_t ga = s.id[ea];
+            const Box A = load_box(s.box + 6 * ea);
+            const long long f = A.at(y, x, z);
+            T cmpv;
+            uint32_t idv;
+            if (best >= 0) {
+                cmpv = s.val[best * kTV + v];
+                idv = s.id[best];
+            } else {  // no listed neighbour covers the voxel: value -1, IDLocal kept
+                cmpv = T(-1);
+                const Box Bold = load_box(a.idbox_old + 6 * ga);
+                idv = f < Bold.count() ? a.id_old[a.idoff_old[ga] + f] : 0u;
+            }
+            const bool boundary = !(A.x0 > a.geo.gb && A.x1 < a.geo.M - a.geo.gb && A.y0 > a.geo.gb &&
+                                    A.y1 < a.geo.M - a.geo.gb && A.z0 > a.geo.gb && A.z1 < a.geo.M - a.geo.gb);
             if (boundary) {
                 const double d = bc_dist(A, y, x, z, a.geo.M, a.geo.gb);
                 if (d > -a.geo.gb)
@@ -230,32 +452,26 @@ __global__ void __launch_bounds__(kThreads) compare_kernel(CompareArgs<T> a) {
                         idv = 0;
                     }
             }
-            const T in = self[f3];
             T res;
             if ((double)fabs(in) < lim) res = T(0.5) * (in - cmpv);
             else res = in;
-            outp[f3] = res;
-            idnew[f3] = idv;
+            a.out.data[a.out.off[ga] + f] = res;
+            a.id_new[a.idoff_new[ga] + f] = idv;
             if (res >= 0) {
-                bx0 = min(bx0, x); bx1 = max(bx1, x);
-                by0 = min(by0, y); by1 = max(by1, y);
-                bz0 = min(bz0, z); bz1 = max(bz1, z);
+                int* bb = s.bbox + 6 * ea;
+                atomicMin(bb + 0, x); atomicMax(bb + 1, x);
+                atomicMin(bb + 2, y); atomicMax(bb + 3, y);
+                atomicMin(bb + 4, z); atomicMax(bb + 5, z);
             }
         }
-#pragma unroll
-        for (int o = 16; o > 0; o >>= 1) {
-            bx0 = min(bx0, __shfl_xor_sync(0xffffffffu, bx0, o));
-            bx1 = max(bx1, __shfl_xor_sync(0xffffffffu, bx1, o));
-            by0 = min(by0, __shfl_xor_sync(0xffffffffu, by0, o));
-            by1 = max(by1, __shfl_xor_sync(0xffffffffu, by1, o));
-            bz0 = min(bz0, __shfl_xor_sync(0xffffffffu, bz0, o));
-            bz1 = max(bz1, __shfl_xor_sync(0xffffffffu, bz1, o));
-        }
-        if (lane == 0 && bx0 != INT_MAX) {
-            int* nb = a.newbox + 6 * g;
-            atomicMin(nb + 0, bx0); atomicMax(nb + 1, bx1);
-            atomicMin(nb + 2, by0); atomicMax(nb + 3, by1);
-            atomicMin(nb + 4, bz0); atomicMax(nb + 5, bz1);
+        __syncthreads();
+        for (int e = threadIdx.x; e < m; e += blockDim.x) {
+            const int* bb = s.bbox + 6 * e;
+            if (bb[0] == INT_MAX) continue;
+            int* nb = a.newbox + 6 * s.id[e];
+            atomicMin(nb + 0, bb[0]); atomicMax(nb + 1, bb[1]);
+            atomicMin(nb + 2, bb[2]); atomicMax(nb + 3, bb[3]);
+            atomicMin(nb + 4, bb[4]); atomicMax(nb + 5, bb[5]);
         }
         __syncthreads();
     }
@@ -273,32 +489,53 @@ __global__ void newbox_init_kernel(int G, const int* present, const int* exists,
 
 }  // namespace
 
-int compare_slab(int side, bool fp64) {
-    const size_t per = fp64 ? 12 : 8;
-    const size_t budget = 80 * 1024;
-    long long s = (long long)(budget / (per * (size_t)(side > 0 ? side * side : 1)));
-    return (int)(s < 1 ? 1 : s > 16 ? 16 : s);
+size_t compare_smem_bytes(int mcap, bool fp64) {
+    const size_t e = fp64 ? 8 : 4;
+    return 8 * (size_t)mcap + e * (size_t)mcap * kTV + e * kTV * kTop * kParts + 4 * (size_t)mcap +
+           48 * (size_t)mcap + 4 * kTV * kParts + 2 * (size_t)mcap * mcap + kTV * kTop * kParts + 64;
 }
 
-size_t compare_smem_bytes(int side, int slab, bool fp64) {
-    return sizeof(Staged) * kStageCap + (size_t)side * side * slab * (fp64 ? 12 : 8);
+long long bin_capacity(int G, int side) {
+    const long long tx = side / kTX + 2, ty = side / kTY + 2, tz = side / kTZ + 2;
+    return (long long)G * tx * ty * tz;
+}
+
+void launch_sort_lists(const SortListArgs& a, int grid, cudaStream_t s) {
+    static bool configured = false;
+    if (!configured) {
+        allow_max_dynamic_smem(sort_lists_kernel);
+        configured = true;
+    }
+    int p2 = 1;
+    while (p2 < a.list_cap) p2 <<= 1;
+    sort_lists_kernel<<<grid, 512, sizeof(unsigned long long) * p2, s>>>(a);
+}
+
+void launch_bin(const TileBins& tb, int G, const int* exists, const int* box, int* err, cudaStream_t s) {
+    const int n_tiles = tb.ntx * tb.nty * tb.ntz;
+    cudaMemsetAsync(tb.count, 0, sizeof(int) * (n_tiles + 1), s);
+    cudaMemsetAsync(tb.cursor, 0, sizeof(int) * (n_tiles + 1), s);
+    const int grid = (G + 127) / 128;
+    bin_kernel<false><<<grid, 128, 0, s>>>(tb, G, exists, box, err);
+    bin_scan_kernel<<<1, 1024, 0, s>>>(tb, n_tiles, err);
+    bin_kernel<true><<<grid, 128, 0, s>>>(tb, G, exists, box, err);
 }
 
 template <typename T>
-void launch_compare(const CompareArgs<T>& a, int grid, size_t smem, cudaStream_t s) {
+void launch_compare(const CompareArgs<T>& a, int grid, cudaStream_t s) {
     static bool configured = false;
     if (!configured) {
         allow_max_dynamic_smem(compare_kernel<T>);
         configured = true;
     }
-    compare_kernel<T><<<grid, kThreads, smem, s>>>(a);
+    compare_kernel<T><<<grid, kThreads, compare_smem_bytes(a.mcap, sizeof(T) == 8), s>>>(a);
 }
 
 void launch_newbox_init(int G, const int* present, const int* exists, const int* box, int* newbox, cudaStream_t s) {
     newbox_init_kernel<<<(G + 256) / 256, 256, 0, s>>>(G, present, exists, box, newbox);
 }
 
-template void launch_compare<double>(const CompareArgs<double>&, int, size_t, cudaStream_t);
-template void launch_compare<float>(const CompareArgs<float>&, int, size_t, cudaStream_t);
+template void launch_compare<double>(const CompareArgs<double>&, int, cudaStream_t);
+template void launch_compare<float>(const CompareArgs<float>&, int, cudaStream_t);
 
 }  // namespace gg

@@ -35,13 +35,39 @@ void launch_copy_layout(int G, const int* present, const int* box_src, const lon
                         long long* off_dst, cudaStream_t s);
 
 // ---- comparison (gg_compare.cu) ----
+constexpr int kTX = 8, kTY = 4, kTZ = 2;  // domain tile of the comparison
+
+// Grains whose (input) boxes reach each domain tile, as CSR over tiles.
+struct TileBins {
+    int ntx, nty, ntz;
+    int* count;               // n_tiles + 1
+    int* off;                 // n_tiles + 1 (exclusive scan of count)
+    int* cursor;              // n_tiles + 1
+    uint32_t* entries;        // grain IDs
+    long long capacity;
+    int* max_count;           // device scalar: most grains reaching one tile
+};
+void launch_bin(const TileBins& tb, int G, const int* exists, const int* box, int* err, cudaStream_t s);
+long long bin_capacity(int G, int side);
+
+// Sorted (ID << 32 | position) copy of every comparison list, and son := cmp.
+struct SortListArgs {
+    int G;
+    const int* toff;          // one tile per existing grain
+    const uint32_t* cmp;
+    const int* n_cmp;
+    uint32_t* son;
+    int* n_son;
+    unsigned long long* sorted;
+    int list_cap;
+};
+void launch_sort_lists(const SortListArgs& a, int grid, cudaStream_t s);
+
 template <typename T>
 struct CompareArgs {
-    int G;
     Geometry geo;
-    const int* toff;          // slab tiles
-    int slab;
-    const int* exists;
+    TileBins bins;
+    int mcap;                 // most grains one tile holds (shared-memory sizing)
     Arena<T> in;              // convolved SDFs (self and neighbours)
     Arena<T> out;             // comparison result written here (same boxes as in)
     const uint32_t* id_old;   // IDLocal of the previous layout
@@ -49,18 +75,15 @@ struct CompareArgs {
     const long long* idoff_old;
     uint32_t* id_new;         // IDLocal on the current boxes
     const long long* idoff_new;
-    const uint32_t* cmp;      // comparison lists
+    const unsigned long long* sorted;  // sorted comparison lists
     const int* n_cmp;
-    uint32_t* son;            // m_secondOrderNeighbours := m_comparisonList
-    int* n_son;
     int list_cap;
     int* newbox;              // per grain min/max (pre-initialised)
     int* err;
 };
 template <typename T>
-void launch_compare(const CompareArgs<T>& a, int grid, size_t smem, cudaStream_t s);
-int compare_slab(int side, bool fp64);                      // z-planes per comparison tile
-size_t compare_smem_bytes(int side, int slab, bool fp64);
+void launch_compare(const CompareArgs<T>& a, int grid, cudaStream_t s);
+size_t compare_smem_bytes(int mcap, bool fp64);
 void launch_newbox_init(int G, const int* present, const int* exists, const int* box, int* newbox, cudaStream_t s);
 
 // ---- list update (gg_lists.cu) ----
