@@ -74,9 +74,8 @@ struct gg_ctx {
     int* d_count3 = nullptr;
     int* h_count3 = nullptr;  // pinned
     long long* h_total_vox = nullptr;
-    // comparison: grains per domain tile and sorted lists
+    // comparison: grains per domain tile
     TileBins bins{};
-    unsigned long long* d_sorted = nullptr;
     int* h_maxcount = nullptr;  // pinned
     // host mirror
     int p = 0;        // SDF arena holding m_inputDistance
@@ -340,17 +339,16 @@ int stage_update_lists_t(gg_ctx* ctx) {
     a.hash_cap = ctx->hash_cap;
     a.err = ctx->d_err;
     launch_update_lists(a, ctx->grid, ctx->stream);
-    // sorted copies for the comparison's list look-ups; m_secondOrderNeighbours = list (box.cpp:895)
-    SortListArgs sl{};
+    // m_secondOrderNeighbours = m_comparisonList (box.cpp:895), once every list is rebuilt
+    ListCopyArgs sl{};
     sl.G = ctx->G;
     sl.toff = ctx->d_toff_one;
     sl.cmp = ctx->d_cmp;
     sl.n_cmp = ctx->d_ncmp;
     sl.son = ctx->d_son;
     sl.n_son = ctx->d_nson;
-    sl.sorted = ctx->d_sorted;
     sl.list_cap = ctx->list_cap;
-    launch_sort_lists(sl, ctx->grid, ctx->stream);
+    launch_copy_lists(sl, ctx->grid, ctx->stream);
     ctx->launches += 2;
     CK(cudaGetLastError());
     return GG_OK;
@@ -393,7 +391,7 @@ int stage_comparison_t(gg_ctx* ctx) {
     a.idoff_old = ctx->d_idoff[q];
     a.id_new = ctx->d_idarena[q ^ 1];
     a.idoff_new = ctx->d_idoff[q ^ 1];
-    a.sorted = ctx->d_sorted;
+    a.cmp = ctx->d_cmp;
     a.n_cmp = ctx->d_ncmp;
     a.list_cap = ctx->list_cap;
     a.newbox = ctx->d_newbox;
@@ -545,7 +543,7 @@ void free_all(gg_ctx* c) {
                     c->d_idoff[0], c->d_idoff[1], c->d_spec, c->d_spec_off, c->d_toff_n, c->d_toff_slab,
                     c->d_toff_one, c->d_toff_mc, c->d_toff_red, c->d_tw, c->d_tw_off, c->d_gtab, c->d_g_off,
                     c->d_circ, c->d_circ_off, c->d_err, c->d_total_vox, c->d_count3, c->bins.count,
-                    c->bins.off, c->bins.cursor, c->bins.entries, c->bins.max_count, c->d_sorted};
+                    c->bins.off, c->bins.cursor, c->bins.entries, c->bins.max_count};
     for (void* p : ptrs)
         if (p) cudaFree(p);
     if (c->h_maxcount) cudaFreeHost(c->h_maxcount);
@@ -631,7 +629,6 @@ int gg_create(const gg_params* params, gg_ctx** out) {
     CK(dalloc(&ctx->bins.off, n_tiles + 1));
     CK(dalloc(&ctx->bins.cursor, n_tiles + 1));
     CK(dalloc(&ctx->bins.max_count, 1));
-    CK(dalloc(&ctx->d_sorted, (size_t)ctx->list_cap * G1));
     CK(cudaMallocHost((void**)&ctx->h_maxcount, sizeof(int)));
     CK(cudaMallocHost((void**)&ctx->h_count3, 3 * sizeof(int)));
     CK(cudaMallocHost((void**)&ctx->h_total_vox, sizeof(long long)));

@@ -10,17 +10,18 @@
 // position.  Each box voxel is read about thirty times that way.  Here the work is
 // turned around and done per domain tile instead of per grain:
 //
-//   1. sort_lists: per grain, (ID, position) of its list sorted by ID, so that
-//      "is B in A's list, and where" is a binary search;
-//   2. bin: every tile of kTX x kTY x kTZ domain voxels gets the IDs of the
+//   1. bin: every tile of kTX x kTY x kTZ domain voxels gets the IDs of the
 //      grains whose boxes reach it (count, scan, fill);
-//   3. compare: one CTA per tile loads every covering box's values over the tile
-//      into shared memory once, keeps per voxel the kTop largest values, and for
-//      every (grain, voxel) pair picks the first candidate that is in that grain's
-//      list, resolving equal values by list position -- falling back to a full
-//      scan of the tile's boxes whenever the kTop candidates cannot decide.  The
-//      boundary condition, the set comparison, the outputs and the new bounding
-//      box follow in the same pass.
+//   2. compare: one CTA per tile loads every covering box's values over the tile
+//      into shared memory once and builds, by streaming each covering grain's
+//      comparison list against a small hash of the tile's grains, the position of
+//      every covering grain in every other's list.  Per voxel it keeps the kTop
+//      largest values; every (grain, voxel) pair then picks the first candidate
+//      that is in that grain's list, resolving equal values by list position --
+//      falling back to a full scan of the tile's boxes whenever the kTop
+//      candidates cannot decide.  The boundary condition, the set comparison, the
+//      outputs and the new bounding box follow in the same pass.
+//   3. copy_lists: m_secondOrderNeighbours = m_comparisonList for the next step.
 //
 // Every value is read once and written once (12 B per voxel on the FP32 path),
 // and the result is bit-identical to the sequential walk.  Voxels no listed
@@ -41,7 +42,8 @@ constexpr int kTV = kTX * kTY * kTZ;   // voxels per tile (64)
 constexpr int kTop = 4;                // candidates kept per voxel
 constexpr int kParts = kThreads / kTV; // threads scanning the boxes of one voxel
 constexpr unsigned kNone = 0xFFFFFFFFu;
-constexpr unsigned short kNotListed = 0xFFFF, kUnknown = 0xFFFE;
+constexpr unsigned short kNotListed = 0xFFFF;
+constexpr int kHashT = 512;            // grain ID -> tile entry (power of two, > 2 x most entries)
 
 // One branch of the reference's boundary distance (box.cpp:1017-1082).  Returns
 // false where no branch assigns `dist`, in which case the reference keeps the value
@@ -101,72 +103,46 @@ __device__ double bc_dist(const Box& b, int i, int j, int k, int m, int gb) {
 }
 
 // ---------------------------------------------------------------------------------
-// 1. sorted copies of the comparison lists (and m_secondOrderNeighbours = list)
+// 1. m_secondOrderNeighbours = m_comparisonList (box.cpp:895), for the next list update
 // ---------------------------------------------------------------------------------
-__global__ void __launch_bounds__(512) sort_lists_kernel(SortListArgs a) {
-    extern __shared__ __align__(16) unsigned long long keys[];
+__global__ void copy_lists_kernel(ListCopyArgs a) {
     const int total = a.toff[a.G + 1];
     for (int t = blockIdx.x; t < total; t += gridDim.x) {
         const int g = tile_grain(a.toff, a.G, t);
         const int K = a.n_cmp[g];
         const uint32_t* list = a.cmp + (long long)g * a.list_cap;
-        uint32_t* son = a.son + (long long)g * a.list_cap;  // box.cpp:895
-        int P2 = 1;
-        while (P2 < K) P2 <<= 1;
-        for (int i = threadIdx.x; i < P2; i += blockDim.x) {
-            if (i < K) {
-                const uint32_t id = list[i];
-                son[i] = id;
-                keys[i] = ((unsigned long long)id << 32) | (unsigned)i;
-            } else {
-                keys[i] = ~0ull;
-            }
-        }
+        uint32_t* son = a.son + (long long)g * a.list_cap;
+        for (int i = threadIdx.x; i < K; i += blockDim.x) son[i] = list[i];
         if (threadIdx.x == 0) a.n_son[g] = K;
-        __syncthreads();
-        for (int k = 2; k <= P2; k <<= 1) {  // bitonic sort, ascending
-            for (int j = k >> 1; j > 0; j >>= 1) {
-                for (int i = threadIdx.x; i < P2; i += blockDim.x) {
-                    const int l = i ^ j;
-                    if (l > i) {
-                        const unsigned long long x = keys[i], y = keys[l];
-                        const bool up = (i & k) == 0;
-                        if ((x > y) == up) { keys[i] = y; keys[l] = x; }
-                    }
-                }
-                __syncthreads();
-            }
-        }
-        unsigned long long* dst = a.sorted + (long long)g * a.list_cap;
-        for (int i = threadIdx.x; i < K; i += blockDim.x) dst[i] = keys[i];
-        __syncthreads();
     }
 }
 
 // ---------------------------------------------------------------------------------
-// 2. binning of grain boxes to domain tiles
+// 2. binning of grain boxes to domain tiles: one warp per grain, lanes over its tiles
 // ---------------------------------------------------------------------------------
 template <bool FILL>
 __global__ void bin_kernel(TileBins tb, int G, const int* exists, const int* box, int* err) {
-    for (int g = 1 + blockIdx.x * blockDim.x + threadIdx.x; g <= G; g += gridDim.x * blockDim.x) {
+    const int lane = threadIdx.x & 31;
+    const int warps = (gridDim.x * blockDim.x) >> 5;
+    for (int g = 1 + ((blockIdx.x * blockDim.x + threadIdx.x) >> 5); g <= G; g += warps) {
         if (!exists[g]) continue;
         const Box b = load_box(box + 6 * g);
         if (b.nx() <= 0) continue;
-        const int tx0 = b.x0 / kTX, tx1 = (b.x1 - 1) / kTX;
-        const int ty0 = b.y0 / kTY, ty1 = (b.y1 - 1) / kTY;
-        const int tz0 = b.z0 / kTZ, tz1 = (b.z1 - 1) / kTZ;
-        for (int tz = tz0; tz <= tz1; tz++)
-            for (int ty = ty0; ty <= ty1; ty++)
-                for (int tx = tx0; tx <= tx1; tx++) {
-                    const int t = (tz * tb.nty + ty) * tb.ntx + tx;
-                    if (!FILL) {
-                        atomicAdd(tb.count + t, 1);
-                    } else {
-                        const long long slot = tb.off[t] + atomicAdd(tb.cursor + t, 1);
-                        if (slot < tb.capacity) tb.entries[slot] = (uint32_t)g;
-                        else atomicOr(err, ERR_POOL);
-                    }
-                }
+        const int tx0 = b.x0 / kTX, nbx = (b.x1 - 1) / kTX - tx0 + 1;
+        const int ty0 = b.y0 / kTY, nby = (b.y1 - 1) / kTY - ty0 + 1;
+        const int tz0 = b.z0 / kTZ, nbz = (b.z1 - 1) / kTZ - tz0 + 1;
+        const int n = nbx * nby * nbz;
+        for (int i = lane; i < n; i += 32) {
+            const int tx = tx0 + i % nbx, ty = ty0 + (i / nbx) % nby, tz = tz0 + i / (nbx * nby);
+            const int t = (tz * tb.nty + ty) * tb.ntx + tx;
+            if (!FILL) {
+                atomicAdd(tb.count + t, 1);
+            } else {
+                const long long slot = tb.off[t] + atomicAdd(tb.cursor + t, 1);
+                if (slot < tb.capacity) tb.entries[slot] = (uint32_t)g;
+                else atomicOr(err, ERR_POOL);
+            }
+        }
     }
 }
 
@@ -225,20 +201,6 @@ __global__ void __launch_bounds__(1024) bin_scan_kernel(TileBins tb, int n_tiles
 // ---------------------------------------------------------------------------------
 // 3. the per-tile comparison
 // ---------------------------------------------------------------------------------
-__device__ __forceinline__ unsigned short list_pos(const unsigned long long* sorted, int n, uint32_t id) {
-    int lo = 0, hi = n;  // first key >= (id << 32)
-    const unsigned long long key = (unsigned long long)id << 32;
-    while (lo < hi) {
-        const int mid = (lo + hi) >> 1;
-        if (__ldg(sorted + mid) < key) lo = mid + 1; else hi = mid;
-    }
-    if (lo < n) {
-        const unsigned long long k = __ldg(sorted + lo);
-        if ((uint32_t)(k >> 32) == id) return (unsigned short)(k & 0xFFFFu);
-    }
-    return kNotListed;
-}
-
 template <typename T>
 struct TileSmem {
     // entries (boxes reaching the tile)
@@ -248,9 +210,11 @@ struct TileSmem {
     int* bbox;          // 6 per entry: new bounding box contributions
     T* val;             // [entry][voxel]
     unsigned short* pos;// [entry a][entry b]: position of b in a's list, kNotListed, or kUnknown
-    T* topv;            // [voxel][kTop]
+    T* topv;            // [part][voxel][kTop], the merged list in part 0
     unsigned char* topi;
     int* ncand;         // covering entries with value > -1, per voxel
+    uint32_t* hkey;     // grain ID -> entry, open addressing
+    unsigned char* hval;
 };
 
 template <typename T>
@@ -264,8 +228,10 @@ __device__ TileSmem<T> carve(unsigned char* base, int mcap) {
     s.box = reinterpret_cast<int*>(p); p += 24 * mcap;
     s.bbox = reinterpret_cast<int*>(p); p += 24 * mcap;
     s.ncand = reinterpret_cast<int*>(p); p += 4 * kTV * kParts;
+    s.hkey = reinterpret_cast<uint32_t*>(p); p += 4 * kHashT;
     s.pos = reinterpret_cast<unsigned short*>(p); p += 2 * (size_t)mcap * mcap;
-    s.topi = p;
+    s.topi = p; p += kTV * kTop * kParts;
+    s.hval = p;
     return s;
 }
 
@@ -276,15 +242,30 @@ __device__ __forceinline__ double neg_inf<double>() { return -CUDART_INF; }
 template <>
 __device__ __forceinline__ float neg_inf<float>() { return -CUDART_INF_F; }
 
+// Keep the kTop largest values seen so far in descending order (registers only).
 template <typename T>
-__device__ __forceinline__ unsigned short lazy_pos(TileSmem<T>& s, const CompareArgs<T>& a, int m, int ea, int eb) {
-    unsigned short p = s.pos[ea * m + eb];
-    if (p == kUnknown) {
-        const uint32_t ga = s.id[ea];
-        p = list_pos(a.sorted + (long long)ga * a.list_cap, a.n_cmp[ga], s.id[eb]);
-        s.pos[ea * m + eb] = p;  // every thread that computes it writes the same value
+__device__ __forceinline__ void top_insert(T (&tv)[kTop], int (&ti)[kTop], T w, int e) {
+    if (!(w > tv[kTop - 1])) return;
+    tv[kTop - 1] = w;
+    ti[kTop - 1] = e;
+#pragma unroll
+    for (int k = kTop - 1; k > 0; k--) {
+        if (tv[k] > tv[k - 1]) {
+            const T t = tv[k]; tv[k] = tv[k - 1]; tv[k - 1] = t;
+            const int u = ti[k]; ti[k] = ti[k - 1]; ti[k - 1] = u;
+        }
     }
-    return p;
+}
+
+__device__ __forceinline__ int tile_lookup(const uint32_t* hkey, const unsigned char* hval, uint32_t id) {
+    unsigned h = (id * 2654435761u) & (kHashT - 1);
+    for (int probe = 0; probe < kHashT; probe++) {
+        const uint32_t k = hkey[h];
+        if (k == id) return hval[h];
+        if (k == kNone) return -1;
+        h = (h + 1) & (kHashT - 1);
+    }
+    return -1;
 }
 
 template <typename T>
@@ -315,7 +296,28 @@ __global__ void __launch_bounds__(kThreads) compare_kernel(CompareArgs<T> a) {
             s.bbox[6 * e + 2] = INT_MAX; s.bbox[6 * e + 3] = INT_MIN;
             s.bbox[6 * e + 4] = INT_MAX; s.bbox[6 * e + 5] = INT_MIN;
         }
-        for (int q = threadIdx.x; q < m * m; q += blockDim.x) s.pos[q] = kUnknown;
+        for (int q = threadIdx.x; q < m * m; q += blockDim.x) s.pos[q] = kNotListed;
+        for (int q = threadIdx.x; q < kHashT; q += blockDim.x) s.hkey[q] = kNone;
+        __syncthreads();
+        for (int e = threadIdx.x; e < m; e += blockDim.x) {  // grain ID -> entry
+            const uint32_t id = s.id[e];
+            unsigned h = (id * 2654435761u) & (kHashT - 1);
+            while (atomicCAS(s.hkey + h, kNone, id) != kNone) h = (h + 1) & (kHashT - 1);
+            s.hval[h] = (unsigned char)e;
+        }
+        __syncthreads();
+        {  // pos[a][b] = position of b in a's list: a warp streams a's list, looks each ID up in the tile
+            const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nw = blockDim.x >> 5;
+            for (int ea = warp; ea < m; ea += nw) {
+                const uint32_t ga = s.id[ea];
+                const uint32_t* list = a.cmp + (long long)ga * a.list_cap;
+                const int K = a.n_cmp[ga];
+                for (int i = lane; i < K; i += 32) {
+                    const int eb = tile_lookup(s.hkey, s.hval, __ldg(list + i));
+                    if (eb >= 0) s.pos[ea * m + eb] = (unsigned short)i;
+                }
+            }
+        }
         __syncthreads();
         // values of every covering box over the tile (-inf outside the box)
         for (int q = threadIdx.x; q < m * kTV; q += blockDim.x) {
@@ -333,26 +335,19 @@ __global__ void __launch_bounds__(kThreads) compare_kernel(CompareArgs<T> a) {
             const int v = threadIdx.x % kTV, part = threadIdx.x / kTV;
             T tv[kTop];
             int ti[kTop];
-            int cnt = 0, nc = 0;
+#pragma unroll
+            for (int k = 0; k < kTop; k++) { tv[k] = NEG; ti[k] = 0xFF; }
+            int nc = 0;
             for (int e = part; e < m; e += kParts) {
                 const T w = s.val[e * kTV + v];
                 if (!(w > T(-1))) continue;
                 nc++;
-                // insert keeping descending order (equal values keep arrival order)
-                int k = cnt < kTop ? cnt : kTop;
-                if (k == kTop && !(w > tv[kTop - 1])) continue;
-                if (k == kTop) k = kTop - 1;
-                while (k > 0 && w > tv[k - 1]) {
-                    if (k < kTop) { tv[k] = tv[k - 1]; ti[k] = ti[k - 1]; }
-                    k--;
-                }
-                tv[k] = w;
-                ti[k] = e;
-                if (cnt < kTop) cnt++;
+                top_insert(tv, ti, w, e);
             }
+#pragma unroll
             for (int k = 0; k < kTop; k++) {
-                s.topv[(part * kTV + v) * kTop + k] = k < cnt ? tv[k] : NEG;
-                s.topi[(part * kTV + v) * kTop + k] = k < cnt ? (unsigned char)ti[k] : 0xFF;
+                s.topv[(part * kTV + v) * kTop + k] = tv[k];
+                s.topi[(part * kTV + v) * kTop + k] = (unsigned char)ti[k];
             }
             s.ncand[part * kTV + v] = nc;
         }
@@ -361,28 +356,21 @@ __global__ void __launch_bounds__(kThreads) compare_kernel(CompareArgs<T> a) {
             const int v = threadIdx.x;
             T tv[kTop];
             int ti[kTop];
-            int cnt = 0, nc = 0;
+#pragma unroll
+            for (int k = 0; k < kTop; k++) { tv[k] = NEG; ti[k] = 0xFF; }
+            int nc = 0;
             for (int part = 0; part < kParts; part++) {
                 nc += s.ncand[part * kTV + v];
+#pragma unroll
                 for (int k = 0; k < kTop; k++) {
                     const int e = s.topi[(part * kTV + v) * kTop + k];
-                    if (e == 0xFF) break;
-                    const T w = s.topv[(part * kTV + v) * kTop + k];
-                    int j = cnt < kTop ? cnt : kTop;
-                    if (j == kTop && !(w > tv[kTop - 1])) continue;
-                    if (j == kTop) j = kTop - 1;
-                    while (j > 0 && w > tv[j - 1]) {
-                        if (j < kTop) { tv[j] = tv[j - 1]; ti[j] = ti[j - 1]; }
-                        j--;
-                    }
-                    tv[j] = w;
-                    ti[j] = e;
-                    if (cnt < kTop) cnt++;
+                    if (e != 0xFF) top_insert(tv, ti, s.topv[(part * kTV + v) * kTop + k], e);
                 }
             }
+#pragma unroll
             for (int k = 0; k < kTop; k++) {
-                s.topv[v * kTop + k] = k < cnt ? tv[k] : NEG;
-                s.topi[v * kTop + k] = k < cnt ? (unsigned char)ti[k] : 0xFF;
+                s.topv[v * kTop + k] = tv[k];
+                s.topi[v * kTop + k] = (unsigned char)ti[k];
             }
             s.ncand[v] = nc;
         }
@@ -406,15 +394,12 @@ __global__ void __launch_bounds__(kThreads) compare_kernel(CompareArgs<T> a) {
                 const T w = s.topv[v * kTop + k];
                 if (best >= 0 && !(w == level)) { decided = true; break; }
                 if (eb == ea) continue;
-                const unsigned short p = lazy_pos(s, a, m, ea, eb);
+                const unsigned short p = s.pos[ea * m + eb];
                 if (p == kNotListed) continue;
                 if (best < 0 || p < bpos) { best = eb; bpos = p; level = w; }
             }
-            const int listed = k;  // candidates examined
-            if (!decided) {
-                // decided anyway when every covering candidate was among the kTop examined
-                if (s.ncand[v] <= listed && k < kTop + 1) decided = true;
-            }
+            // decided anyway when every covering candidate was among those examined
+            if (!decided && s.ncand[v] <= k) decided = true;
             if (!decided) {  // full scan of the tile's boxes at this voxel
                 best = -1;
                 bpos = kNotListed;
@@ -424,7 +409,7 @@ __global__ void __launch_bounds__(kThreads) compare_kernel(CompareArgs<T> a) {
                     const T w = s.val[eb * kTV + v];
                     if (!(w > T(-1))) continue;
                     if (best >= 0 && w < level) continue;
-                    const unsigned short p = lazy_pos(s, a, m, ea, eb);
+                    const unsigned short p = s.pos[ea * m + eb];
                     if (p == kNotListed) continue;
                     if (best < 0 || w > level || (w == level && p < bpos)) { best = eb; bpos = p; level = w; }
                 }
@@ -492,7 +477,8 @@ __global__ void newbox_init_kernel(int G, const int* present, const int* exists,
 size_t compare_smem_bytes(int mcap, bool fp64) {
     const size_t e = fp64 ? 8 : 4;
     return 8 * (size_t)mcap + e * (size_t)mcap * kTV + e * kTV * kTop * kParts + 4 * (size_t)mcap +
-           48 * (size_t)mcap + 4 * kTV * kParts + 2 * (size_t)mcap * mcap + kTV * kTop * kParts + 64;
+           48 * (size_t)mcap + 4 * kTV * kParts + 4 * kHashT + 2 * (size_t)mcap * mcap + kTV * kTop * kParts +
+           kHashT + 64;
 }
 
 long long bin_capacity(int G, int side) {
@@ -500,22 +486,15 @@ long long bin_capacity(int G, int side) {
     return (long long)G * tx * ty * tz;
 }
 
-void launch_sort_lists(const SortListArgs& a, int grid, cudaStream_t s) {
-    static bool configured = false;
-    if (!configured) {
-        allow_max_dynamic_smem(sort_lists_kernel);
-        configured = true;
-    }
-    int p2 = 1;
-    while (p2 < a.list_cap) p2 <<= 1;
-    sort_lists_kernel<<<grid, 512, sizeof(unsigned long long) * p2, s>>>(a);
+void launch_copy_lists(const ListCopyArgs& a, int grid, cudaStream_t s) {
+    copy_lists_kernel<<<grid, 256, 0, s>>>(a);
 }
 
 void launch_bin(const TileBins& tb, int G, const int* exists, const int* box, int* err, cudaStream_t s) {
     const int n_tiles = tb.ntx * tb.nty * tb.ntz;
     cudaMemsetAsync(tb.count, 0, sizeof(int) * (n_tiles + 1), s);
     cudaMemsetAsync(tb.cursor, 0, sizeof(int) * (n_tiles + 1), s);
-    const int grid = (G + 127) / 128;
+    const int grid = (G + 4) / 4;  // one warp per grain, 4 warps per block
     bin_kernel<false><<<grid, 128, 0, s>>>(tb, G, exists, box, err);
     bin_scan_kernel<<<1, 1024, 0, s>>>(tb, n_tiles, err);
     bin_kernel<true><<<grid, 128, 0, s>>>(tb, G, exists, box, err);

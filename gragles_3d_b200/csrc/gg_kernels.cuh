@@ -50,18 +50,17 @@ struct TileBins {
 void launch_bin(const TileBins& tb, int G, const int* exists, const int* box, int* err, cudaStream_t s);
 long long bin_capacity(int G, int side);
 
-// Sorted (ID << 32 | position) copy of every comparison list, and son := cmp.
-struct SortListArgs {
+// son := cmp for every existing grain (m_secondOrderNeighbours = m_comparisonList).
+struct ListCopyArgs {
     int G;
     const int* toff;          // one tile per existing grain
     const uint32_t* cmp;
     const int* n_cmp;
     uint32_t* son;
     int* n_son;
-    unsigned long long* sorted;
     int list_cap;
 };
-void launch_sort_lists(const SortListArgs& a, int grid, cudaStream_t s);
+void launch_copy_lists(const ListCopyArgs& a, int grid, cudaStream_t s);
 
 template <typename T>
 struct CompareArgs {
@@ -75,7 +74,7 @@ struct CompareArgs {
     const long long* idoff_old;
     uint32_t* id_new;         // IDLocal on the current boxes
     const long long* idoff_new;
-    const unsigned long long* sorted;  // sorted comparison lists
+    const uint32_t* cmp;      // comparison lists (position = list order)
     const int* n_cmp;
     int list_cap;
     int* newbox;              // per grain min/max (pre-initialised)
