@@ -30,7 +30,7 @@ EXPORTED = [
     "gg_create", "gg_destroy", "gg_last_error", "gg_load_state", "gg_set_lists", "gg_default_lists", "gg_step",
     "gg_stage_convolution", "gg_stage_update_lists", "gg_stage_comparison", "gg_stage_level_set",
     "gg_stage_redistancing", "gg_get_grain_stats", "gg_get_neighbors", "gg_get_list", "gg_get_sdf",
-    "gg_get_idlocal", "gg_grain_count", "gg_loop", "gg_convolve_boxes_f64",
+    "gg_get_idlocal", "gg_grain_count", "gg_loop", "gg_convolve_boxes_f64", "gg_convolve_boxes_f64_noalloc",
 ]
 
 
