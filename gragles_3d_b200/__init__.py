@@ -30,7 +30,8 @@ EXPORTED = [
     "gg_create", "gg_destroy", "gg_last_error", "gg_load_state", "gg_set_lists", "gg_default_lists", "gg_step",
     "gg_stage_convolution", "gg_stage_update_lists", "gg_stage_comparison", "gg_stage_level_set",
     "gg_stage_redistancing", "gg_get_grain_stats", "gg_get_neighbors", "gg_get_list", "gg_get_sdf",
-    "gg_get_idlocal", "gg_grain_count", "gg_loop", "gg_convolve_boxes_f64", "gg_convolve_boxes_f64_noalloc",
+    "gg_get_idlocal", "gg_grain_count", "gg_loop", "gg_convolve_boxes_f64", "gg_convolve_boxes_mixed",
+    "gg_convolve_boxes_f64_noalloc",
 ]
 
 
@@ -92,6 +93,7 @@ def load_library(path: str = LIB_PATH):
     L.gg_get_idlocal.argtypes = [vp, i32, vp, vp, i64]
     L.gg_get_idlocal.restype = i64
     L.gg_convolve_boxes_f64.argtypes = [vp, vp, vp, vp, i32, i32, C.c_double]
+    L.gg_convolve_boxes_mixed.argtypes = [vp, vp, vp, vp, i32, i32, C.c_double]
     _lib = L
     return L
 
@@ -238,6 +240,15 @@ def from_microstructure(ms, border: int = 10, time_step: float = 0.2, precision:
 
 def convolve_boxes_f64(boxes: list, domain_size: int, time_step: float) -> list:
     """FP64 Gaussian convolution of cubic boxes on the GPU (torch manages the device memory)."""
+    return _convolve_boxes(boxes, domain_size, time_step, np.float64, "gg_convolve_boxes_f64")
+
+
+def convolve_boxes_mixed(boxes: list, domain_size: int, time_step: float) -> list:
+    """The mixed path's FP32 convolution (tensor cores when all sides are <= 64) of cubic boxes."""
+    return _convolve_boxes(boxes, domain_size, time_step, np.float32, "gg_convolve_boxes_mixed")
+
+
+def _convolve_boxes(boxes: list, domain_size: int, time_step: float, dtype, fn: str) -> list:
     import torch
 
     L = load_library()
@@ -247,14 +258,14 @@ def convolve_boxes_f64(boxes: list, domain_size: int, time_step: float) -> list:
     for i, b in enumerate(boxes):
         offs[i] = total
         total += (b.size + 31) // 32 * 32
-    host = np.zeros(max(total, 1), np.float64)
+    host = np.zeros(max(total, 1), dtype)
     for i, b in enumerate(boxes):
         host[offs[i]:offs[i] + b.size] = b.ravel()
     d_in = torch.from_numpy(host).cuda()
     d_out = torch.zeros_like(d_in)
-    rc = L.gg_convolve_boxes_f64(C.c_void_p(d_in.data_ptr()), C.c_void_p(d_out.data_ptr()), _p(sides), _p(offs),
-                                 len(boxes), domain_size, float(time_step))
+    rc = getattr(L, fn)(C.c_void_p(d_in.data_ptr()), C.c_void_p(d_out.data_ptr()), _p(sides), _p(offs),
+                        len(boxes), domain_size, float(time_step))
     if rc < 0:
-        raise GGError(rc, "gg_convolve_boxes_f64 failed")
+        raise GGError(rc, f"{fn} failed")
     out = d_out.cpu().numpy()
     return [out[offs[i]:offs[i] + b.size].reshape(b.shape).copy() for i, b in enumerate(boxes)]

@@ -68,6 +68,9 @@ struct gg_ctx {
     long long* d_g_off = nullptr;
     float* d_circ = nullptr;          // FP32 circulant matrices (mixed path)
     long long* d_circ_off = nullptr;
+    float* d_bmat = nullptr;          // the same, split hi/lo in the tensor-core operand layout
+    long long* d_boff = nullptr;
+    float* d_cscr = nullptr;          // mixed-path convolution scratch (out's layout)
     // scalars
     int* d_err = nullptr;
     long long* d_total_vox = nullptr;
@@ -166,6 +169,13 @@ int upload_tables(gg_ctx* ctx) {
         CK(dalloc(&ctx->d_circ_off, c_off.size()));
         CK(cudaMemcpy(ctx->d_circ, circ.data(), circ.size() * sizeof(float), cudaMemcpyHostToDevice));
         CK(cudaMemcpy(ctx->d_circ_off, c_off.data(), c_off.size() * sizeof(long long), cudaMemcpyHostToDevice));
+        std::vector<float> bmat;
+        std::vector<long long> boff;
+        umma_tables(ctx->N, ctx->P.time_step, std::min(M, kUmmaMaxSide), bmat, boff);
+        CK(dalloc(&ctx->d_bmat, bmat.size()));
+        CK(dalloc(&ctx->d_boff, boff.size()));
+        CK(cudaMemcpy(ctx->d_bmat, bmat.data(), bmat.size() * sizeof(float), cudaMemcpyHostToDevice));
+        CK(cudaMemcpy(ctx->d_boff, boff.data(), boff.size() * sizeof(long long), cudaMemcpyHostToDevice));
     }
     return GG_OK;
 }
@@ -178,6 +188,7 @@ int check_err(gg_ctx* ctx, const char* where) {
     if (e & (ERR_LIST | ERR_HASH)) return fail(ctx, GG_ERR_LIST_OVERFLOW, "%s: comparison list capacity exceeded", where);
     if (e & ERR_NEIGHBORS) return fail(ctx, GG_ERR_LIST_OVERFLOW, "%s: hull neighbour capacity exceeded", where);
     if (e & ERR_BOX) return fail(ctx, GG_ERR_UNSUPPORTED, "%s: a box left the grid or exceeded the supported side", where);
+    if (e & ERR_TIMEOUT) return fail(ctx, GG_ERR_CUDA, "%s: a bounded tensor-core pipeline wait timed out", where);
     return GG_OK;
 }
 
@@ -201,6 +212,7 @@ int plan(gg_ctx* ctx, const int* box, int only_existing, long long* off, long lo
     a.toff_n = toff_n;
     a.toff_slab = toff_slab;
     a.slab = ctx->slab;
+    a.row_tile = ctx->fp64 ? 0 : kUmmaRows;
     a.toff_one = toff_one;
     a.total_voxels = total_voxels;
     a.err = ctx->d_err;
@@ -306,6 +318,24 @@ int stage_convolution_t(gg_ctx* ctx) {
         launch_conv_f64(a, ctx->grid, conv_f64_smem_bytes(ctx->side_max), ctx->stream);
         ctx->launches += 3;
     } else {
+        if (umma_supported(ctx->side_max)) {
+            UmmaConvArgs u{};
+            u.G = ctx->G;
+            u.toff = ctx->d_toff_slab;
+            u.box = ctx->d_box[p];
+            u.in = reinterpret_cast<const float*>(ctx->d_arena[p]);
+            u.in_off = ctx->d_off[p];
+            u.out = reinterpret_cast<float*>(ctx->d_arena[p ^ 1]);
+            u.out_off = ctx->d_off[p ^ 1];
+            u.scratch = ctx->d_cscr;
+            u.bmat = ctx->d_bmat;
+            u.boff = ctx->d_boff;
+            u.err = ctx->d_err;
+            launch_conv_umma(u, ctx->num_sms, ctx->side_max, ctx->stream);
+            ctx->launches += 3;
+            CK(cudaGetLastError());
+            return GG_OK;
+        }
         ConvTCArgs a{};
         a.G = ctx->G;
         a.toff = ctx->d_toff_n;
@@ -542,7 +572,7 @@ void free_all(gg_ctx* c) {
                     c->d_off[0], c->d_off[1], c->d_idarena[0], c->d_idarena[1], c->d_idbox[0], c->d_idbox[1],
                     c->d_idoff[0], c->d_idoff[1], c->d_spec, c->d_spec_off, c->d_toff_n, c->d_toff_slab,
                     c->d_toff_one, c->d_toff_mc, c->d_toff_red, c->d_tw, c->d_tw_off, c->d_gtab, c->d_g_off,
-                    c->d_circ, c->d_circ_off, c->d_err, c->d_total_vox, c->d_count3, c->bins.count,
+                    c->d_circ, c->d_circ_off, c->d_bmat, c->d_boff, c->d_cscr, c->d_err, c->d_total_vox, c->d_count3, c->bins.count,
                     c->bins.off, c->bins.cursor, c->bins.entries, c->bins.max_count};
     for (void* p : ptrs)
         if (p) cudaFree(p);
@@ -689,6 +719,7 @@ int gg_load_state(gg_ctx* ctx, const uint32_t* labels, const int32_t* extents, c
         CK(dalloc(&ctx->d_idarena[a], ctx->pool_voxels));
     }
     if (ctx->fp64) CK(dalloc(&ctx->d_spec, ctx->spec_capacity));
+    else CK(dalloc(&ctx->d_cscr, ctx->pool_voxels));
     const size_t G1 = (size_t)G + 1;
     CK(cudaMemcpy(ctx->d_present, present.data(), sizeof(int) * G1, cudaMemcpyHostToDevice));
     CK(cudaMemcpy(ctx->d_exists, present.data(), sizeof(int) * G1, cudaMemcpyHostToDevice));
@@ -950,6 +981,99 @@ int gg_convolve_boxes_f64(const double* d_in, double* d_out, const int32_t* side
     CK(cudaDeviceSynchronize());
     void* ptrs[] = {d_tw, d_gt, d_tw_off, d_g_off, d_spec, d_box, d_off, d_spec_off, d_toff};
     for (void* p : ptrs) cudaFree(p);
+    return GG_OK;
+}
+
+int gg_convolve_boxes_mixed(const float* d_in, float* d_out, const int32_t* sides, const int64_t* offs,
+                            int32_t n_boxes, int32_t domain_size, double time_step) {
+    gg_ctx* ctx = nullptr;  // for CK: no context to carry a message
+    if (!d_in || !d_out || !sides || !offs || n_boxes < 1 || domain_size < 1) return GG_ERR_INVALID;
+    int nmax = 0;
+    long long span = 0;
+    for (int b = 0; b < n_boxes; b++) {
+        if (sides[b] < 1 || offs[b] < 0 || offs[b] % 4) return GG_ERR_INVALID;
+        nmax = std::max(nmax, (int)sides[b]);
+        span = std::max(span, (long long)offs[b] + (long long)sides[b] * sides[b] * sides[b]);
+    }
+    const bool tc = umma_supported(nmax);
+    if (!tc && 3 * (size_t)nmax * (nmax | 1) * sizeof(float) > 227 * 1024) return GG_ERR_UNSUPPORTED;
+    std::vector<int> box(6 * (n_boxes + 1), 0);
+    std::vector<long long> off(n_boxes + 1, 0);
+    std::vector<int> toff(n_boxes + 2, 0);
+    for (int b = 0; b < n_boxes; b++) {
+        const int n = sides[b];
+        int* bb = &box[6 * (b + 1)];
+        bb[1] = bb[3] = bb[5] = n;
+        off[b + 1] = offs[b];
+        toff[b + 2] = toff[b + 1] + (tc ? (n * n + kUmmaRows - 1) / kUmmaRows : n);
+    }
+    std::vector<float> tab;
+    std::vector<long long> tab_off;
+    if (tc) {
+        umma_tables(domain_size, time_step, nmax, tab, tab_off);
+    } else {
+        tab_off.assign(nmax + 2, 0);
+        for (int n = 1; n <= nmax; n++) {
+            tab_off[n] = (long long)tab.size();
+            circulant_matrix(n, domain_size, time_step, tab);
+        }
+    }
+    float *d_tab = nullptr, *d_scr = nullptr;
+    long long *d_tab_off = nullptr, *d_off = nullptr;
+    int *d_box = nullptr, *d_toff = nullptr, *d_err = nullptr;
+    CK(dalloc(&d_tab, tab.size()));
+    CK(dalloc(&d_tab_off, tab_off.size()));
+    CK(dalloc(&d_box, box.size()));
+    CK(dalloc(&d_off, off.size()));
+    CK(dalloc(&d_toff, toff.size()));
+    CK(dalloc(&d_err, 1));
+    if (tc) CK(dalloc(&d_scr, (size_t)(span + 4) / 4 * 4));
+    CK(cudaMemcpy(d_tab, tab.data(), sizeof(float) * tab.size(), cudaMemcpyHostToDevice));
+    CK(cudaMemcpy(d_tab_off, tab_off.data(), sizeof(long long) * tab_off.size(), cudaMemcpyHostToDevice));
+    CK(cudaMemcpy(d_box, box.data(), sizeof(int) * box.size(), cudaMemcpyHostToDevice));
+    CK(cudaMemcpy(d_off, off.data(), sizeof(long long) * off.size(), cudaMemcpyHostToDevice));
+    CK(cudaMemcpy(d_toff, toff.data(), sizeof(int) * toff.size(), cudaMemcpyHostToDevice));
+    CK(cudaMemset(d_err, 0, sizeof(int)));
+    int sms = 148, dev = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    if (tc) {
+        UmmaConvArgs u{};
+        u.G = n_boxes;
+        u.toff = d_toff;
+        u.box = d_box;
+        u.in = d_in;
+        u.in_off = d_off;
+        u.out = d_out;
+        u.out_off = d_off;
+        u.scratch = d_scr;
+        u.bmat = d_tab;
+        u.boff = d_tab_off;
+        u.err = d_err;
+        launch_conv_umma(u, sms, nmax, 0);
+    } else {
+        ConvTCArgs a{};
+        a.G = n_boxes;
+        a.toff = d_toff;
+        a.in = d_in;
+        a.box = d_box;
+        a.in_off = d_off;
+        a.out = d_out;
+        a.out_off = d_off;
+        a.circ = d_tab;
+        a.circ_off = d_tab_off;
+        a.err = d_err;
+        launch_conv_tc(a, sms, nmax, 0);
+    }
+    CK(cudaGetLastError());
+    CK(cudaDeviceSynchronize());
+    int e = 0;
+    CK(cudaMemcpy(&e, d_err, sizeof(int), cudaMemcpyDeviceToHost));
+    void* ptrs[] = {d_tab, d_tab_off, d_box, d_off, d_toff, d_err, d_scr};
+    for (void* p : ptrs)
+        if (p) cudaFree(p);
+    if (e & ERR_TIMEOUT) return GG_ERR_CUDA;
+    if (e) return GG_ERR_UNSUPPORTED;
     return GG_OK;
 }
 

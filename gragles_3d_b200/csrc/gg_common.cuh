@@ -22,6 +22,7 @@ enum : int {
     ERR_NEIGHBORS = 4,   // hull neighbour set capacity exceeded
     ERR_HASH = 8,        // list-update hash table overflow
     ERR_BOX = 16,        // a box outside the grid or larger than supported
+    ERR_TIMEOUT = 32,    // a bounded wait on the tensor-core pipeline gave up
 };
 
 struct Box {

@@ -20,8 +20,10 @@ struct PlanArgs {
     long long* spec_off;      // out: half-spectrum offsets (complex elements), may be null
     long long spec_capacity;
     int* toff_n;              // out: tile offsets with n tiles per grain, may be null
-    int* toff_slab;           // out: tile offsets with ceil(n / slab) tiles per grain, may be null
+    int* toff_slab;           // out: tile offsets with ceil(n / slab) tiles per grain, or with
+                              // ceil(n^2 / row_tile) when row_tile > 0; may be null
     int slab;
+    int row_tile;
     int* toff_one;            // out: tile offsets with one tile per grain, may be null
     int* box_copy;            // out: copy of box (6 per grain), may be null
     long long* off_copy;      // out: copy of off, may be null

@@ -47,7 +47,8 @@ __device__ __forceinline__ Counts grain_counts(const PlanArgs& a, int g) {
     c.spec = (sp + kAlign - 1) / kAlign * kAlign;
     c.tot = v;
     c.tn = (int)n;
-    c.ts = a.slab > 0 ? (int)((n + a.slab - 1) / a.slab) : 0;
+    c.ts = a.row_tile > 0 ? (int)((n * n + a.row_tile - 1) / a.row_tile)
+                          : (a.slab > 0 ? (int)((n + a.slab - 1) / a.slab) : 0);
     c.t1 = 1;
     return c;
 }

@@ -116,6 +116,16 @@ int gg_loop(gg_ctx* ctx);
 int gg_convolve_boxes_f64(const double* d_in, double* d_out, const int32_t* sides, const int64_t* offs,
                           int32_t n_boxes, int32_t domain_size, double time_step);
 
+/* The mixed-precision convolution of GG_PRECISION_MIXED on FP32 boxes: three per-axis
+ * contractions with the circulant C_n on the tcgen05 tensor cores (3xTF32, FP32
+ * accumulation) when every side is <= 64, on the FP32 SIMT kernels otherwise.  Same packing
+ * and stream as gg_convolve_boxes_f64, except that the offsets must be multiples of 4
+ * elements and the buffers must extend to a multiple of 4 elements past the last box
+ * (boxes are read as 16-byte aligned spans); allocates its scratch.  Replaces the same
+ * call site (LSbox::convolutionGeneratorMKL, box.cpp:685-795) as the FP64 entry. */
+int gg_convolve_boxes_mixed(const float* d_in, float* d_out, const int32_t* sides, const int64_t* offs,
+                            int32_t n_boxes, int32_t domain_size, double time_step);
+
 /* The same FP64 convolution, bit for bit, without allocating any device memory.
  * No counterpart in the reference: it exists for callers that cannot call
  * cudaMalloc -- programs that give all device memory to their own pool at start-up,

@@ -59,6 +59,21 @@ def test_convolution_kernel_bitexact(gpu, oracle):
         assert np.array_equal(g, want), f"side {b.shape[0]}: max diff {np.abs(g - want).max()}"
 
 
+def test_mixed_convolution_kernel_accuracy(gpu, oracle):
+    """The mixed path's convolution (tcgen05 3xTF32 when all sides are <= 64, FP32 SIMT
+    otherwise) against the FP64 specified DFT: FP32-level error, far below plain TF32's
+    ~5e-4.  Side sets with repeated and alternating sides exercise the kernel's switch
+    between its two C_n buffers."""
+    rng = np.random.default_rng(8)
+    for sides in ([5, 8, 13, 20, 33, 47, 64], [40, 40, 17, 40, 17, 17, 64, 1, 2, 64, 33] * 3, [96, 100]):
+        boxes = [rng.uniform(-0.1, 0.1, (n, n, n)).astype(np.float32) for n in sides]
+        got = gpu.convolve_boxes_mixed(boxes, 128, 0.2)
+        for b, g in zip(boxes, got):
+            want = oracle.convolve_box(b.astype(np.float64), 128, 0.2)
+            err = np.abs(g.astype(np.float64) - want).max() / np.abs(b).max()
+            assert err <= 4e-6, f"side {b.shape[0]}: relative max error {err:.3g}"
+
+
 def test_initial_sdf_bitexact(gpu, oracle):
     c, gh, osim = _pair(gpu, oracle, "tiny")
     for g in range(1, c["G"] + 1):
