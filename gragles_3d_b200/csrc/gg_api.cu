@@ -68,7 +68,7 @@ struct gg_ctx {
     long long* d_g_off = nullptr;
     float* d_circ = nullptr;          // FP32 circulant matrices (mixed path)
     long long* d_circ_off = nullptr;
-    float* d_bmat = nullptr;          // the same, split hi/lo in the tensor-core operand layout
+    uint16_t* d_bmat = nullptr;       // the same, split FP16 hi/lo in the tensor-core operand layout
     long long* d_boff = nullptr;
     float* d_cscr = nullptr;          // mixed-path convolution scratch (out's layout)
     // scalars
@@ -169,12 +169,12 @@ int upload_tables(gg_ctx* ctx) {
         CK(dalloc(&ctx->d_circ_off, c_off.size()));
         CK(cudaMemcpy(ctx->d_circ, circ.data(), circ.size() * sizeof(float), cudaMemcpyHostToDevice));
         CK(cudaMemcpy(ctx->d_circ_off, c_off.data(), c_off.size() * sizeof(long long), cudaMemcpyHostToDevice));
-        std::vector<float> bmat;
+        std::vector<uint16_t> bmat;
         std::vector<long long> boff;
         umma_tables(ctx->N, ctx->P.time_step, std::min(M, kUmmaMaxSide), bmat, boff);
         CK(dalloc(&ctx->d_bmat, bmat.size()));
         CK(dalloc(&ctx->d_boff, boff.size()));
-        CK(cudaMemcpy(ctx->d_bmat, bmat.data(), bmat.size() * sizeof(float), cudaMemcpyHostToDevice));
+        CK(cudaMemcpy(ctx->d_bmat, bmat.data(), bmat.size() * sizeof(uint16_t), cudaMemcpyHostToDevice));
         CK(cudaMemcpy(ctx->d_boff, boff.data(), boff.size() * sizeof(long long), cudaMemcpyHostToDevice));
     }
     return GG_OK;
@@ -1008,9 +1008,10 @@ int gg_convolve_boxes_mixed(const float* d_in, float* d_out, const int32_t* side
         toff[b + 2] = toff[b + 1] + (tc ? (n * n + kUmmaRows - 1) / kUmmaRows : n);
     }
     std::vector<float> tab;
+    std::vector<uint16_t> tab16;
     std::vector<long long> tab_off;
     if (tc) {
-        umma_tables(domain_size, time_step, nmax, tab, tab_off);
+        umma_tables(domain_size, time_step, nmax, tab16, tab_off);
     } else {
         tab_off.assign(nmax + 2, 0);
         for (int n = 1; n <= nmax; n++) {
@@ -1019,16 +1020,20 @@ int gg_convolve_boxes_mixed(const float* d_in, float* d_out, const int32_t* side
         }
     }
     float *d_tab = nullptr, *d_scr = nullptr;
+    uint16_t* d_tab16 = nullptr;
     long long *d_tab_off = nullptr, *d_off = nullptr;
     int *d_box = nullptr, *d_toff = nullptr, *d_err = nullptr;
     CK(dalloc(&d_tab, tab.size()));
+    CK(dalloc(&d_tab16, tab16.size()));
     CK(dalloc(&d_tab_off, tab_off.size()));
     CK(dalloc(&d_box, box.size()));
     CK(dalloc(&d_off, off.size()));
     CK(dalloc(&d_toff, toff.size()));
     CK(dalloc(&d_err, 1));
     if (tc) CK(dalloc(&d_scr, (size_t)(span + 4) / 4 * 4));
-    CK(cudaMemcpy(d_tab, tab.data(), sizeof(float) * tab.size(), cudaMemcpyHostToDevice));
+    if (!tab.empty()) CK(cudaMemcpy(d_tab, tab.data(), sizeof(float) * tab.size(), cudaMemcpyHostToDevice));
+    if (!tab16.empty())
+        CK(cudaMemcpy(d_tab16, tab16.data(), sizeof(uint16_t) * tab16.size(), cudaMemcpyHostToDevice));
     CK(cudaMemcpy(d_tab_off, tab_off.data(), sizeof(long long) * tab_off.size(), cudaMemcpyHostToDevice));
     CK(cudaMemcpy(d_box, box.data(), sizeof(int) * box.size(), cudaMemcpyHostToDevice));
     CK(cudaMemcpy(d_off, off.data(), sizeof(long long) * off.size(), cudaMemcpyHostToDevice));
@@ -1047,7 +1052,7 @@ int gg_convolve_boxes_mixed(const float* d_in, float* d_out, const int32_t* side
         u.out = d_out;
         u.out_off = d_off;
         u.scratch = d_scr;
-        u.bmat = d_tab;
+        u.bmat = d_tab16;
         u.boff = d_tab_off;
         u.err = d_err;
         launch_conv_umma(u, sms, nmax, 0);
@@ -1069,7 +1074,7 @@ int gg_convolve_boxes_mixed(const float* d_in, float* d_out, const int32_t* side
     CK(cudaDeviceSynchronize());
     int e = 0;
     CK(cudaMemcpy(&e, d_err, sizeof(int), cudaMemcpyDeviceToHost));
-    void* ptrs[] = {d_tab, d_tab_off, d_box, d_off, d_toff, d_err, d_scr};
+    void* ptrs[] = {d_tab, d_tab16, d_tab_off, d_box, d_off, d_toff, d_err, d_scr};
     for (void* p : ptrs)
         if (p) cudaFree(p);
     if (e & ERR_TIMEOUT) return GG_ERR_CUDA;

@@ -7,6 +7,7 @@
 #pragma once
 
 #include <cuda_runtime.h>
+#include <cstdint>
 #include <vector>
 
 namespace gg {
@@ -43,7 +44,7 @@ struct UmmaPassArgs {
     const long long* src_off;
     float* dst;
     const long long* dst_off;
-    const float* bmat;        // C_n split into TF32 hi and lo, MMA operand layout, per side
+    const uint16_t* bmat;     // 2^8 C_n split into FP16 hi and lo, MMA operand layout, per side
     const long long* boff;
     int side_max;             // largest side in the launch (sizes the shared memory)
     int* err;
@@ -59,7 +60,7 @@ struct UmmaConvArgs {
     float* out;
     const long long* out_off;
     float* scratch;
-    const float* bmat;
+    const uint16_t* bmat;
     const long long* boff;
     int* err;
 };
@@ -68,7 +69,7 @@ int umma_side_limit();
 // True when the tensor-core kernel takes boxes up to side_max (else the SIMT kernels).
 bool umma_supported(int side_max);
 // C_n of every side 1..nmax as the MMA's B operand (hi block, then lo block).
-void umma_tables(int N, double time_step, int nmax, std::vector<float>& bmat, std::vector<long long>& boff);
+void umma_tables(int N, double time_step, int nmax, std::vector<uint16_t>& bmat, std::vector<long long>& boff);
 void launch_conv_umma(const UmmaConvArgs& a, int num_sms, int side_max, cudaStream_t s);
 
 }  // namespace gg

@@ -13,15 +13,17 @@
 //     and of C_n (pre-split hi/lo in HBM) when the side changes;
 //   split (8 warps): re-layout of a staged tile into the no-swizzle K-major
 //     core-matrix layout of the MMA operand (8 rows x 16 B per core matrix, K padding
-//     and rows past n^2 zero), split into TF32 hi and lo (3xTF32: a*b ~ ah*bh + al*bh
-//     + ah*bl, about FP32 accuracy);
-//   MMA (1 thread): 3 * K/8 tcgen05.mma kind::tf32 per tile into one of two FP32 TMEM
+//     and rows past n^2 zero), scaled by 2^8 and split into FP16 hi + lo (22
+//     significant bits; a*c ~ ah*ch + al*ch + ah*cl, about FP32 accuracy; C_n is
+//     scaled by 2^8 as well and the product by 2^-16 in the epilogue, all exact);
+//   MMA (1 thread): 3 * K/16 tcgen05.mma kind::f16 per tile into one of four FP32 TMEM
 //     accumulators; tcgen05.commit frees the operand stage and hands the accumulator on;
-//   epilogue (4 warps): tcgen05.ld of one tile row per thread, column c' stored to
+//   epilogue (8 warps, two tiles at a time): tcgen05.ld of one tile row per thread, column c' stored to
 //     U[c'][row]; lanes hold consecutive rows, so each store writes 128 contiguous bytes.
 // Every wait is bounded: a timeout flags ERR_TIMEOUT and raises a CTA abort flag that
 // ends the other roles' waits too; TMEM is freed on every exit path.
 #include <cstring>
+#include <cuda_fp16.h>
 
 #include "gg_common.cuh"
 #include "gg_conv_tc.cuh"
@@ -32,13 +34,19 @@ namespace {
 
 constexpr int kRows = kUmmaRows;     // MMA M and TMEM lanes
 constexpr int kSplitWarps = 8;
-constexpr int kThreadsU = (kSplitWarps + 6) * 32;  // split, 4 epilogue, MMA, TMA warps
-constexpr int kBars = 20;
+constexpr int kEpiWarps = 8;                         // two groups of four (one per TMEM lane quarter)
+constexpr int kAcc = 4;                              // TMEM accumulators
+constexpr int kThreadsU = (kSplitWarps + kEpiWarps + 2) * 32;  // split, epilogue, MMA, TMA warps
+constexpr int kMaxR = 4, kMaxS = 4;                  // staged tiles, operand stages
+constexpr int kBars = 2 * kMaxR + 2 * kMaxS + 2 * kAcc + 2 + 2;
 constexpr uint32_t kAccCols = 64;   // one accumulator: N <= round16(kUmmaMaxSide) columns
-constexpr uint32_t kTmemCols = 128; // two accumulators
+constexpr uint32_t kTmemCols = kAcc * kAccCols;
 constexpr long long kWaitCycles = 1LL << 31;  // ~1 s at the B200 clock
+constexpr int kSuspendNs = 1000;              // suspend-time hint of one mbarrier try_wait
+constexpr float kScale = 256.f;               // operands are scaled by 2^8 before the FP16 split
+constexpr float kUnscale = 1.f / 65536.f;     // the product by 2^-16
 
-__host__ __device__ constexpr int round_k(int n) { return (n + 7) & ~7; }   // K per MMA = 8 (tf32)
+__host__ __device__ constexpr int round_k(int n) { return (n + 15) & ~15; } // K per MMA = 16 (f16)
 __host__ __device__ constexpr int round_n(int n) { return (n + 15) & ~15; } // N multiple of 16 at M = 128
 
 __device__ __forceinline__ uint32_t smem_u32(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
@@ -47,15 +55,17 @@ __device__ __forceinline__ void mbar_init(uint32_t bar, uint32_t count) {
     asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;\n" ::"r"(bar), "r"(count) : "memory");
     asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
 }
+// The waiting thread sleeps until the phase completes or ~kSuspendNs elapse.
 __device__ __forceinline__ bool mbar_try_wait(uint32_t bar, uint32_t parity) {
     uint32_t ok;
     asm volatile(
-        "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}\n"
+        "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2, %3;\n selp.u32 %0, 1, 0, p;\n}\n"
         : "=r"(ok)
-        : "r"(bar), "r"(parity)
+        : "r"(bar), "r"(parity), "n"(kSuspendNs)
         : "memory");
     return ok != 0;
 }
+
 __device__ __forceinline__ void fence_proxy_async() { asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory"); }
 __device__ __forceinline__ void tc_fence_before() { asm volatile("tcgen05.fence::before_thread_sync;\n" ::: "memory"); }
 __device__ __forceinline__ void tc_fence_after() { asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory"); }
@@ -75,14 +85,14 @@ __device__ __forceinline__ uint64_t smem_desc(uint32_t addr, uint32_t sbo) {
     return (uint64_t)((addr >> 4) & 0x3FFFu) | ((uint64_t)(128u >> 4) << 16) | ((uint64_t)((sbo >> 4) & 0x3FFFu) << 32) |
            ((uint64_t)1 << 46);
 }
-// Instruction descriptor, kind::tf32: D f32, A/B tf32, both K-major, M = 128, N = np.
+// Instruction descriptor, kind::f16: D f32, A/B f16, both K-major, M = 128, N = np.
 __device__ __forceinline__ uint32_t instr_desc(int np) {
-    return (1u << 4) | (2u << 7) | (2u << 10) | ((uint32_t)(np >> 3) << 17) | ((uint32_t)(kRows >> 4) << 24);
+    return (1u << 4) | (0u << 7) | (0u << 10) | ((uint32_t)(np >> 3) << 17) | ((uint32_t)(kRows >> 4) << 24);
 }
-__device__ __forceinline__ void mma_tf32(uint32_t d_tmem, uint64_t a, uint64_t b, uint32_t idesc, uint32_t acc) {
+__device__ __forceinline__ void mma_f16(uint32_t d_tmem, uint64_t a, uint64_t b, uint32_t idesc, uint32_t acc) {
     asm volatile(
         "{\n .reg .pred p;\n setp.ne.b32 p, %4, 0;\n"
-        " tcgen05.mma.cta_group::1.kind::tf32 [%0], %1, %2, %3, p;\n}\n" ::"r"(d_tmem),
+        " tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n}\n" ::"r"(d_tmem),
         "l"(a), "l"(b), "r"(idesc), "r"(acc)
         : "memory");
 }
@@ -90,34 +100,36 @@ __device__ __forceinline__ void mma_commit(uint32_t bar) {
     asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];\n" ::"r"(bar)
                  : "memory");
 }
-__device__ __forceinline__ void tmem_ld16(uint32_t taddr, float (&v)[16]) {
+// 16 consecutive 32-bit TMEM columns of this thread's lane; complete after tmem_wait().
+__device__ __forceinline__ void tmem_ld16(uint32_t taddr, float* v) {
     uint32_t r[16];
     asm volatile(
         "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%16];\n"
         : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
           "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
         : "r"(taddr));
-    asm volatile("tcgen05.wait::ld.sync.aligned;\n" ::: "memory");
 #pragma unroll
     for (int i = 0; i < 16; i++) v[i] = __uint_as_float(r[i]);
 }
+__device__ __forceinline__ void tmem_wait() { asm volatile("tcgen05.wait::ld.sync.aligned;\n" ::: "memory"); }
 
-// TF32 part of v: round to nearest (ties away) at 10 explicit mantissa bits.
-__host__ __device__ __forceinline__ float tf32_hi(float v) {
-    uint32_t u;
-#ifdef __CUDA_ARCH__
-    u = __float_as_uint(v);
-#else
-    std::memcpy(&u, &v, 4);
-#endif
-    u = (u + 0x1000u) & 0xFFFFE000u;
-#ifdef __CUDA_ARCH__
-    return __uint_as_float(u);
-#else
-    float r;
-    std::memcpy(&r, &u, 4);
-    return r;
-#endif
+// FP16 hi + lo of v * 2^8 (round to nearest even, both parts).
+__host__ __device__ __forceinline__ void split_f16(float v, __half& h, __half& l) {
+    const float x = v * kScale;
+    h = __float2half_rn(x);
+    l = __float2half_rn(x - __half2float(h));
+}
+
+// The same split for a pair, with the hi part rounded in FP32 arithmetic (Veltkamp's
+// splitting of x at 11 significant bits: c = (2^13 + 1) x, hi = c - (c - x)), so that
+// only the two packed conversions touch the conversion unit.  hi is exact in FP16
+// above the FP16 subnormal range and x - hi is exact in FP32.
+__device__ __forceinline__ void split_f16x2(float v0, float v1, __half2& h, __half2& l) {
+    const float x0 = __fmul_rn(v0, kScale), x1 = __fmul_rn(v1, kScale);
+    const float c0 = __fmul_rn(x0, 8193.f), c1 = __fmul_rn(x1, 8193.f);
+    const float h0 = __fsub_rn(c0, __fsub_rn(c0, x0)), h1 = __fsub_rn(c1, __fsub_rn(c1, x1));
+    h = __floats2half2_rn(h0, h1);
+    l = __floats2half2_rn(__fsub_rn(x0, h0), __fsub_rn(x1, h1));
 }
 
 // Walks the tile range of a CTA in order: grain, tile within the grain, side.
@@ -167,12 +179,10 @@ __device__ __forceinline__ void bulk_load(uint32_t dst, const void* src, uint32_
 // that no role of the CTA waits for one that has stopped.
 __device__ __forceinline__ bool wait_bar(uint32_t bar, uint32_t parity, volatile int* abort_flag, int* err) {
     const long long t0 = clock64();
-    for (int it = 0; it < (1 << 30); it++) {
+    for (int it = 0; it < (1 << 24); it++) {
         if (mbar_try_wait(bar, parity)) return true;
-        if ((it & 15) == 15) {
-            if (*abort_flag) return false;
-            if (clock64() - t0 > kWaitCycles) break;
-        }
+        if (*abort_flag) return false;
+        if (clock64() - t0 > kWaitCycles) break;
     }
     *abort_flag = 1;
     atomicOr(err, ERR_TIMEOUT);
@@ -180,33 +190,42 @@ __device__ __forceinline__ bool wait_bar(uint32_t bar, uint32_t parity, volatile
 }
 
 // Re-layout one staged tile (rows x n floats, row-major) into the MMA's K-major
-// core-matrix layout, split into TF32 hi and lo.  Canonical element p = tid + 256 j is
-// core matrix cm = p / 32 (8-row group mg = cm / KC, K chunk kc = cm % KC), row
-// 8 mg + lane / 4, column 4 kc + lane % 4; padding rows and columns become zero.
-__device__ __forceinline__ void split_tile(const float* raw, float* hi, float* lo, int n, int rows, int stid) {
-    const int kp = round_k(n), KC = kp >> 2;
+// core-matrix layout, split into FP16 hi and lo.  Core matrix q = mg KC + kc holds
+// rows 8 mg .. 8 mg + 7, columns 8 kc .. 8 kc + 7 as 8 rows of 16 B at byte 128 q;
+// a thread writes one such row (lane % 8 = row, lane / 8 picks one of four
+// consecutive core matrices), so each 8-lane phase stores one whole core matrix.
+// Padding rows and columns become zero.
+__device__ __forceinline__ void split_tile(const float* raw, __half* hi, __half* lo, int n, int rows, int stid) {
+    const int KC = round_k(n) >> 3;
     const int w = stid >> 5, lane = stid & 31;
-    const int mlo = lane >> 2, klo = lane & 3;
-    int mg = w / KC, kc = w - (w / KC) * KC;
-    for (int cm = w; cm < 16 * KC; cm += kSplitWarps) {
-        const int m = 8 * mg + mlo, k = 4 * kc + klo;
-        const float v = (m < rows && k < n) ? raw[m * n + k] : 0.f;
-        const float h = tf32_hi(v);
-        const int p = 32 * cm + lane;
-        hi[p] = h;
-        lo[p] = tf32_hi(v - h);
-        kc += kSplitWarps;
-        while (kc >= KC) {
-            kc -= KC;
-            mg++;
+    const int r = lane & 7, j = lane >> 3;
+    const bool vec = (n & 3) == 0;  // rows start on 16-byte boundaries
+    for (int q = 4 * w + j; q < 16 * KC; q += 4 * kSplitWarps) {
+        const int mg = q / KC, kc = q - mg * KC;
+        const int m = 8 * mg + r, k0 = 8 * kc;
+        float v[8];
+        if (m < rows && vec && k0 + 8 <= n) {
+            const float4 a = *reinterpret_cast<const float4*>(raw + m * n + k0);
+            const float4 b = *reinterpret_cast<const float4*>(raw + m * n + k0 + 4);
+            v[0] = a.x; v[1] = a.y; v[2] = a.z; v[3] = a.w;
+            v[4] = b.x; v[5] = b.y; v[6] = b.z; v[7] = b.w;
+        } else {
+#pragma unroll
+            for (int e = 0; e < 8; e++) v[e] = (m < rows && k0 + e < n) ? raw[m * n + k0 + e] : 0.f;
         }
+        __align__(16) __half2 hv[4], lv[4];
+#pragma unroll
+        for (int e = 0; e < 4; e++) split_f16x2(v[2 * e], v[2 * e + 1], hv[e], lv[e]);
+        const int off = q * 64 + r * 8;  // halves
+        *reinterpret_cast<uint4*>(hi + off) = *reinterpret_cast<const uint4*>(hv);
+        *reinterpret_cast<uint4*>(lo + off) = *reinterpret_cast<const uint4*>(lv);
     }
 }
 
-// Warp roles: 0-7 split (staged tile -> hi/lo operands), 8-11 epilogue (TMEM -> HBM),
-// 12 MMA issue, 13 TMA loads (one thread each).  Rings: R staged tiles, S hi/lo
-// operand stages, two TMEM accumulators, two C_n buffers switched when the side
-// changes along the CTA's tile range.
+// Warp roles: 0-7 split (staged tile -> hi/lo operands), 8-15 epilogue (TMEM -> HBM,
+// two groups taking alternate tiles), 16 MMA issue, 17 TMA loads (one thread each).
+// Rings: R staged tiles, S hi/lo operand stages, four TMEM accumulators, two C_n
+// buffers switched when the side changes along the CTA's tile range.
 __global__ void __launch_bounds__(kThreadsU, 1)
     conv_umma_kernel(UmmaPassArgs a, int kp_max, int np_max, int R, int S) {
     extern __shared__ __align__(1024) unsigned char smem_raw[];
@@ -214,13 +233,15 @@ __global__ void __launch_bounds__(kThreadsU, 1)
     __shared__ uint32_t tmem_slot;
     __shared__ int abort_flag;
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
-    const int tile_floats = kRows * kp_max;
+    const int tile_floats = kRows * kp_max;                  // one staged tile (fp32)
+    const int tile_halves = kRows * kp_max;                  // one operand part (fp16)
     float* raw_base = reinterpret_cast<float*>(smem_raw);
-    float* op_base = raw_base + R * tile_floats;            // S x (hi, lo)
-    float* b_base = op_base + S * 2 * tile_floats;           // 2 x (hi, lo) C_n
-    const int b_floats = 2 * np_max * kp_max;
+    __half* op_base = reinterpret_cast<__half*>(raw_base + R * tile_floats);  // S x (hi, lo)
+    __half* b_base = op_base + S * 2 * tile_halves;                          // 2 x (hi, lo) C_n
+    const int b_halves = 2 * np_max * kp_max;
     auto bar = [&](int i) { return smem_u32(&bars[i]); };
-    constexpr int RFULL = 0, REMPTY = 4, FULL = 8, EMPTY = 10, TFULL = 12, TEMPTY = 14, BFULL = 16, BFREE = 18;
+    constexpr int RFULL = 0, REMPTY = kMaxR, FULL = 2 * kMaxR, EMPTY = FULL + kMaxS, TFULL = EMPTY + kMaxS,
+                  TEMPTY = TFULL + kAcc, BFULL = TEMPTY + kAcc, BFREE = BFULL + 2;
 
     const int total = a.toff[a.G + 1];
     const int t_begin = (int)((long long)total * blockIdx.x / gridDim.x);
@@ -232,15 +253,17 @@ __global__ void __launch_bounds__(kThreadsU, 1)
     if (tid == 0) {
         for (int r = 0; r < R; r++) {
             mbar_init(bar(RFULL + r), 1);
-            mbar_init(bar(REMPTY + r), kSplitWarps * 32);
+            mbar_init(bar(REMPTY + r), kSplitWarps);  // one arrive per warp
         }
         for (int s = 0; s < S; s++) {
-            mbar_init(bar(FULL + s), kSplitWarps * 32);
+            mbar_init(bar(FULL + s), kSplitWarps);
             mbar_init(bar(EMPTY + s), 1);
         }
-        for (int b = 0; b < 2; b++) {
+        for (int b = 0; b < kAcc; b++) {
             mbar_init(bar(TFULL + b), 1);
-            mbar_init(bar(TEMPTY + b), 128);
+            mbar_init(bar(TEMPTY + b), 4);
+        }
+        for (int b = 0; b < 2; b++) {
             mbar_init(bar(BFULL + b), 1);
             mbar_init(bar(BFREE + b), 1);
         }
@@ -248,12 +271,12 @@ __global__ void __launch_bounds__(kThreadsU, 1)
     }
     // a side beyond the launch's shared-memory sizing would overrun the buffers
     bool sized = true;
-    {
-        Cursor c;
-        c.init(&a, t_begin);
-        for (int i = 0; i < count; i++, c.advance())
-            if (c.n < 1 || round_k(c.n) > kp_max || round_n(c.n) > np_max || c.n > kUmmaMaxSide) sized = false;
-    }
+    if (warp == 0)
+        for (int t = t_begin + lane; t < t_end; t += 32) {
+            const int* bx = a.box + 6 * tile_grain(a.toff, a.G, t);
+            const int n = bx[1] - bx[0];
+            if (n < 1 || round_k(n) > kp_max || round_n(n) > np_max || n > kUmmaMaxSide) sized = false;
+        }
     tc_fence_before();
     sized = __syncthreads_and(sized);
     tc_fence_after();
@@ -270,20 +293,27 @@ __global__ void __launch_bounds__(kThreadsU, 1)
             const int r = i % R, s = i % S;
             if (!wait_bar(bar(RFULL + r), (i / R) & 1, ab, a.err)) break;
             if (i >= S && !wait_bar(bar(EMPTY + s), (i / S - 1) & 1, ab, a.err)) break;
-            float* hi = op_base + s * 2 * tile_floats;
-            split_tile(raw_base + r * tile_floats, hi, hi + tile_floats, c.n, c.rows(), tid);
+            __half* hi = op_base + s * 2 * tile_halves;
+            split_tile(raw_base + r * tile_floats, hi, hi + tile_halves, c.n, c.rows(), tid);
+            // every lane's stores visible to the tensor core, then one arrive per warp
+            // (arrives on one barrier serialise, so 256 of them would cost microseconds)
             fence_proxy_async();
-            mbar_arrive(bar(REMPTY + r));
-            mbar_arrive(bar(FULL + s));
+            __syncwarp();
+            if (lane == 0) {
+                mbar_arrive(bar(REMPTY + r));
+                mbar_arrive(bar(FULL + s));
+            }
         }
-    } else if (warp < kSplitWarps + 4) {
-        // ---------------- epilogue ----------------
+    } else if (warp < kSplitWarps + kEpiWarps) {
+        // ---------------- epilogue: group e drains tiles i = e mod 2 ----------------
         const int q = warp & 3;  // TMEM lane quarter of this warp
+        const int e = (warp - kSplitWarps) >> 2;
         Cursor c;
         c.init(&a, t_begin);
-        for (int i = 0; i < count; i++, c.advance()) {
-            const int b = i & 1;
-            if (!wait_bar(bar(TFULL + b), (i >> 1) & 1, ab, a.err)) break;
+        if (e) c.advance();
+        for (int i = e; i < count; i += 2, c.advance(), c.advance()) {
+            const int b = i % kAcc;
+            if (!wait_bar(bar(TFULL + b), (i / kAcc) & 1, ab, a.err)) break;
             tc_fence_after();
             const int n = c.n, np = round_n(n);
             const int row = q * 32 + lane;
@@ -291,25 +321,30 @@ __global__ void __launch_bounds__(kThreadsU, 1)
             float* dst = a.dst + a.dst_off[c.g] + c.r0() + row;
             const bool live = row < c.rows();
             const uint32_t trow = tmem + ((uint32_t)(q * 32) << 16) + (uint32_t)(b * kAccCols);
-            for (int c0 = 0; c0 < np; c0 += 16) {
-                float v[16];
-                tmem_ld16(trow + (uint32_t)c0, v);
-                if (live) {
+            float v[kAccCols];
 #pragma unroll
-                    for (int cc = 0; cc < 16; cc++)
-                        if (c0 + cc < n) dst[(long long)(c0 + cc) * n2] = v[cc];
-                }
-            }
+            for (int c0 = 0; c0 < (int)kAccCols; c0 += 16)
+                if (c0 < np) tmem_ld16(trow + (uint32_t)c0, v + c0);
+            tmem_wait();
+            // the accumulator is in registers: hand it back before the stores, so that the
+            // arrive's release does not wait for them
             tc_fence_before();
-            mbar_arrive(bar(TEMPTY + b));
+            __syncwarp();
+            if (lane == 0) mbar_arrive(bar(TEMPTY + b));
+            if (live) {
+                float* p = dst;
+#pragma unroll
+                for (int cc = 0; cc < (int)kAccCols; cc++, p += n2)
+                    if (cc < n) *p = v[cc] * kUnscale;
+            }
         }
-    } else if (warp == kSplitWarps + 4 && lane == 0) {
+    } else if (warp == kSplitWarps + kEpiWarps && lane == 0) {
         // ---------------- MMA issue ----------------
         Cursor c;
         c.init(&a, t_begin);
         int cur_n = -1, nsw = 0, kb = 0;
         for (int i = 0; i < count; i++, c.advance()) {
-            const int s = i % S, b = i & 1;
+            const int s = i % S, b = i % kAcc;
             if (!wait_bar(bar(FULL + s), (i / S) & 1, ab, a.err)) break;
             if (c.n != cur_n) {
                 kb = nsw & 1;
@@ -318,26 +353,26 @@ __global__ void __launch_bounds__(kThreadsU, 1)
                 cur_n = c.n;
                 nsw++;
             }
-            if (i >= 2 && !wait_bar(bar(TEMPTY + b), ((i >> 1) - 1) & 1, ab, a.err)) break;
+            if (i >= kAcc && !wait_bar(bar(TEMPTY + b), (i / kAcc - 1) & 1, ab, a.err)) break;
             tc_fence_after();
             const int kp = round_k(c.n), np = round_n(c.n);
-            const uint32_t sbo = 32u * kp;  // 8 rows x kp floats
-            const float* hi = op_base + s * 2 * tile_floats;
-            const uint32_t a_hi = smem_u32(hi), a_lo = smem_u32(hi + tile_floats);
-            const float* bk = b_base + kb * b_floats;
+            const uint32_t sbo = 16u * kp;  // 8 rows x kp halves
+            const __half* hi = op_base + s * 2 * tile_halves;
+            const uint32_t a_hi = smem_u32(hi), a_lo = smem_u32(hi + tile_halves);
+            const __half* bk = b_base + kb * b_halves;
             const uint32_t b_hi = smem_u32(bk), b_lo = smem_u32(bk + np * kp);
             const uint32_t idesc = instr_desc(np);
             const uint32_t d = tmem + (uint32_t)(b * kAccCols);
-            for (int j = 0; j < kp / 8; j++) {
+            for (int j = 0; j < kp / 16; j++) {
                 const uint32_t o = 256u * j;  // two 128-B core matrices along K
-                mma_tf32(d, smem_desc(a_lo + o, sbo), smem_desc(b_hi + o, sbo), idesc, j > 0);
-                mma_tf32(d, smem_desc(a_hi + o, sbo), smem_desc(b_lo + o, sbo), idesc, 1);
-                mma_tf32(d, smem_desc(a_hi + o, sbo), smem_desc(b_hi + o, sbo), idesc, 1);
+                mma_f16(d, smem_desc(a_lo + o, sbo), smem_desc(b_hi + o, sbo), idesc, j > 0);
+                mma_f16(d, smem_desc(a_hi + o, sbo), smem_desc(b_lo + o, sbo), idesc, 1);
+                mma_f16(d, smem_desc(a_hi + o, sbo), smem_desc(b_hi + o, sbo), idesc, 1);
             }
             mma_commit(bar(EMPTY + s));
             mma_commit(bar(TFULL + b));
         }
-    } else if (warp == kSplitWarps + 5 && lane == 0) {
+    } else if (warp == kSplitWarps + kEpiWarps + 1 && lane == 0) {
         // ---------------- TMA loads ----------------
         Cursor c;
         c.init(&a, t_begin);
@@ -348,9 +383,9 @@ __global__ void __launch_bounds__(kThreadsU, 1)
             if (c.n != cur_n) {
                 const int kb = nsw & 1;
                 if (nsw >= 2 && !wait_bar(bar(BFREE + kb), ((nsw - 2) >> 1) & 1, ab, a.err)) break;
-                const uint32_t bytes = 2u * round_n(c.n) * round_k(c.n) * 4u;
+                const uint32_t bytes = 2u * round_n(c.n) * round_k(c.n) * 2u;
                 mbar_expect_tx(bar(BFULL + kb), bytes);
-                bulk_load(smem_u32(b_base + kb * b_floats), a.bmat + a.boff[c.n], bytes, bar(BFULL + kb));
+                bulk_load(smem_u32(b_base + kb * b_halves), a.bmat + a.boff[c.n], bytes, bar(BFULL + kb));
                 cur_n = c.n;
                 nsw++;
             }
@@ -381,18 +416,20 @@ UmmaShape umma_shape(int side_max) {
     cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
     if (optin <= 0) optin = 227 * 1024;
     const size_t room = (size_t)optin - 2048;
-    const size_t tile = (size_t)kRows * sh.kp * sizeof(float);
-    const size_t bbytes = 2 * 2 * (size_t)sh.np * sh.kp * sizeof(float);
-    for (int S = 2; S >= 1; S--)
-        for (int R = 4; R >= 2; R--) {
-            const size_t need = R * tile + 2 * S * tile + bbytes;
-            if (need <= room) {
-                sh.R = R;
-                sh.S = S;
-                sh.smem = need;
-                return sh;
-            }
+    const size_t tile = (size_t)kRows * sh.kp * sizeof(float);    // staged fp32 tile
+    const size_t part = (size_t)kRows * sh.kp * sizeof(__half);   // one fp16 operand part
+    const size_t bbytes = 2 * 2 * (size_t)sh.np * sh.kp * sizeof(__half);
+    // deepest rings that fit, staged tiles at least as deep as operand stages
+    const int order[][2] = {{4, 4}, {4, 3}, {3, 3}, {3, 2}, {2, 2}, {2, 1}};
+    for (const auto& rs : order) {
+        const size_t need = rs[0] * tile + 2 * rs[1] * part + bbytes;
+        if (need <= room) {
+            sh.R = rs[0];
+            sh.S = rs[1];
+            sh.smem = need;
+            return sh;
         }
+    }
     return sh;
 }
 
@@ -402,23 +439,23 @@ int umma_side_limit() { return kUmmaMaxSide; }
 
 bool umma_supported(int side_max) { return side_max >= 1 && side_max <= kUmmaMaxSide && umma_shape(side_max).R >= 2; }
 
-void umma_tables(int N, double time_step, int nmax, std::vector<float>& bmat, std::vector<long long>& boff) {
+void umma_tables(int N, double time_step, int nmax, std::vector<uint16_t>& bmat, std::vector<long long>& boff) {
     boff.assign(nmax + 2, 0);
     for (int n = 1; n <= nmax; n++) {
         std::vector<float> C;
         circulant_matrix(n, N, time_step, C);
-        const int kp = round_k(n), np = round_n(n);
+        const int kp = round_k(n), np = round_n(n), KC = kp / 8;
         const size_t base = bmat.size();
         boff[n] = (long long)base;
-        bmat.resize(base + 2 * (size_t)np * kp, 0.f);
+        bmat.resize(base + 2 * (size_t)np * kp, 0);
         for (int r = 0; r < n; r++)
             for (int k = 0; k < n; k++) {
                 // B[k][r] = C[r][k] as the N x K K-major operand (row r = output column)
-                const float v = C[(size_t)r * n + k];
-                const float hi = tf32_hi(v);
-                const size_t pos = (size_t)(r / 8) * 8 * kp + (size_t)(k / 4) * 32 + (r % 8) * 4 + (k % 4);
-                bmat[base + pos] = hi;
-                bmat[base + (size_t)np * kp + pos] = tf32_hi(v - hi);
+                __half h, l;
+                split_f16(C[(size_t)r * n + k], h, l);
+                const size_t pos = ((size_t)(r / 8) * KC + k / 8) * 64 + (r % 8) * 8 + (k % 8);
+                bmat[base + pos] = __half_as_ushort(h);
+                bmat[base + (size_t)np * kp + pos] = __half_as_ushort(l);
             }
     }
 }
