@@ -248,8 +248,7 @@ int redistance(gg_ctx* ctx, int in_a, int out_a, const int* toff, int side) {
     r.in = arena<T>(ctx, in_a);
     r.out = arena<T>(ctx, out_a);
     r.err = ctx->d_err;
-    const size_t smem = redist_smem_bytes(side, sizeof(T) == 8);
-    launch_redistance<T>(r, ctx->grid, smem, smem, ctx->stream);
+    launch_redistance<T>(r, ctx->grid, side, ctx->stream);
     ctx->launches += 2;
     CK(cudaGetLastError());
     return GG_OK;

@@ -90,6 +90,48 @@ __device__ __forceinline__ int tile_grain(const int* __restrict__ toff, int G, i
     return lo;
 }
 
+// This CTA's share of the tiles, a contiguous range walked in order: one binary
+// search at the start, then (grain, tile within the grain) advance incrementally.
+// A binary search per tile would put ~log2(G) dependent loads in front of every tile.
+struct TileWalk {
+    const int* toff;
+    int G, t, end;
+    int g, local, count;  // grain, its tile index, its tile count
+    __device__ TileWalk(const int* toff_, int G_, int part, int parts) : toff(toff_), G(G_) {
+        const int total = toff[G + 1];
+        t = (int)((long long)total * part / parts);
+        end = (int)((long long)total * (part + 1) / parts);
+        g = 1;
+        local = count = 0;
+        if (t < end) {
+            g = tile_grain(toff, G, t);
+            local = t - toff[g];
+            count = toff[g + 1] - toff[g];
+        }
+    }
+    __device__ bool valid() const { return t < end; }
+    __device__ void next() {
+        ++t;
+        if (++local < count) return;
+        local = 0;
+        while (t < end && g < G) {  // next grain with tiles; g stays in [1, G]
+            ++g;
+            count = toff[g + 1] - toff[g];
+            if (count > 0) break;
+        }
+    }
+};
+
+// Asynchronous 4- or 8-byte global -> shared copy (cp.async): staging loops issue all
+// their copies without waiting on each load, then wait once.
+template <typename T>
+__device__ __forceinline__ void cp_async_elem(T* dst_smem, const T* src) {
+    static_assert(sizeof(T) == 4 || sizeof(T) == 8, "4- or 8-byte elements");
+    const unsigned d = (unsigned)__cvta_generic_to_shared(dst_smem);
+    asm volatile("cp.async.ca.shared.global [%0], [%1], %2;\n" ::"r"(d), "l"(src), "n"(sizeof(T)) : "memory");
+}
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;\n" ::: "memory"); }
+
 // Opt a kernel into the largest dynamic shared memory the device allows next to
 // its static shared memory.
 template <typename K>

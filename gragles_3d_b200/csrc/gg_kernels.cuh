@@ -138,7 +138,8 @@ struct RedistArgs {
     int* err;
 };
 template <typename T>
-void launch_redistance(const RedistArgs<T>& a, int grid, size_t smem_xy, size_t smem_z, cudaStream_t s);
+void launch_redistance(const RedistArgs<T>& a, int grid, int side, cudaStream_t s);
+// Shared memory of one unit (one warp) at box side nmax; must fit one CTA.
 size_t redist_smem_bytes(int nmax, bool fp64);
 
 // ---- initial distance function (gg_init.cu) ----

@@ -5,23 +5,29 @@
 // intersection except the last runs four sweeps (x forward, x backward, y forward,
 // y backward), then sweeps z forward and backward over all columns, and clamps to
 // +-delta.  Every sweep is a recurrence along one line and the lines of a sweep are
-// independent, so:
-//   kernel xy: one CTA per (grain, output z-slice); the slice sits in shared
-//              memory and each thread runs one line of a sweep;
-//   kernel z:  one CTA per (grain, output y-row); each thread runs the z
-//              recurrences of one column (x-adjacent threads read adjacent words).
-// Arithmetic is the reference's, statement by statement (no contraction), so the
-// FP64 result is bit-identical.
+// independent, so a small CTA (one thread per line: 32 or 64 threads for the usual
+// sides) owns one unit of work at a time:
+//   kernel xy: a CTA per (grain, output z-slice); the slice of the output sits in
+//              shared memory, threads run rows for the x sweeps and columns for the
+//              y sweeps;
+//   kernel z:  a CTA per (grain, output y-row); the [z][x] plane of the row sits in
+//              shared memory and threads run the z recurrences of one column each
+//              (x-adjacent threads touch adjacent words).
+// One unit's buffers are small (two n x n planes), so many CTAs share an SM.
+// The unit's input values on the in/out intersection are staged next to it with
+// coalesced loads (a recurrence that read HBM step by step would wait on every load).
+// Along a line the value that the next step updates is carried in a register, so a
+// step costs its arithmetic and shared-memory loads that do not depend on the chain.  The
+// arithmetic is the reference's, statement by statement (no contraction), and the
+// lines of a sweep run in the reference's order, so the FP64 result is bit-identical.
 #include "gg_kernels.cuh"
 
 namespace gg {
 
 namespace {
 
-constexpr int kThreadsXY = 128;
-constexpr int kThreadsZ = 128;
+constexpr int kMaxThreads = 128;  // one thread per line up to side 128, then lines loop
 
-template <typename T>
 struct Intersect {
     int xmin, xmax, ymin, ymax, zmin, zmax;
     __device__ Intersect(const Box& ib, const Box& ob) {
@@ -34,6 +40,13 @@ struct Intersect {
     }
 };
 
+// x + isgn(s) * h of the reference, without the int -> T conversion and product:
+// isgn(s) * h is exactly h, -h or +0.
+template <typename T>
+__device__ __forceinline__ T add_sgn(T x, T s, T h) {
+    return s > T(0) ? x + h : (s < T(0) ? x - h : x + T(0));
+}
+
 // The interpolation step at a sign change between a (here) and b (next), then the
 // candidate propagated to next; box.cpp:2370-2391 and the y/z twins.
 template <typename T>
@@ -43,167 +56,241 @@ __device__ __forceinline__ void step_in(T a, T b, T& out_here, T& out_next, T h)
         const T distToZero = -a / i_slope;
         if (fabs(out_here) > fabs(distToZero)) out_here = -distToZero * isgn(i_slope);
     }
-    const T candidate = out_here + (isgn(b) * h);
+    const T candidate = add_sgn(out_here, b, h);
     if (fabs(candidate) < fabs(out_next)) out_next = candidate;
 }
 template <typename T>
 __device__ __forceinline__ void step_prop(T sgn_src, T out_here, T& out_next, T h) {
-    const T candidate = out_here + (isgn(sgn_src) * h);
+    const T candidate = add_sgn(out_here, sgn_src, h);
     if (fabs(candidate) < fabs(out_next)) out_next = candidate;
 }
 
+// Forward sweep over positions p0 .. p_end - 1 of a line: o[p * so] is the output at
+// p, in[p * si] the input, valid for p in [p0, p_in_end) when `inside`.  The
+// reference's x/y/z forward loops (box.cpp:2367-2401, 2437-2472, 2501-2538) take
+// step_in while p < p_in_end - 1 (and inside), else step_prop: a prefix, so the loop
+// is split in two.
 template <typename T>
-__global__ void __launch_bounds__(kThreadsXY) redist_xy_kernel(RedistArgs<T> a) {
+__device__ __forceinline__ void sweep_forward(T* o, int so, const T* in, int si, int p0, int p_end, int p_in_end,
+                                              bool inside, T h) {
+    if (p0 >= p_end - 1) return;
+    T* op = o + p0 * so;
+    T cur = *op;
+    int p = p0;
+    const int pin = inside ? min(p_in_end - 1, p_end - 1) : p0;
+    if (p < pin) {
+        const T* ip = in + p0 * si;
+        T icur = *ip;
+        for (; p < pin; p++, op += so, ip += si) {
+            T nxt = op[so];
+            const T inx = ip[si];
+            step_in(icur, inx, cur, nxt, h);
+            *op = cur;
+            cur = nxt;
+            icur = inx;
+        }
+    }
+    for (; p < p_end - 1; p++, op += so) {
+        T nxt = op[so];
+        step_prop(nxt, cur, nxt, h);
+        *op = cur;
+        cur = nxt;
+    }
+    *op = cur;
+}
+
+// Backward propagation from p_start down to p_lo + 1 (box.cpp:2403-2435, 2474-2496):
+// step_prop with the sign of in(p - 1) while p > p_in_lo (and inside), else of the
+// output itself.  out_here is never modified.
+template <typename T>
+__device__ __forceinline__ void sweep_backward_prop(T* o, int so, const T* in, int si, int p_start, int p_lo,
+                                                    int p_in_lo, bool inside, T h) {
+    if (p_start <= p_lo) return;
+    T* op = o + p_start * so;
+    T cur = *op;
+    int p = p_start;
+    if (inside) {
+        const int plim = max(p_in_lo, p_lo);
+        const T* ip = in + (p_start - 1) * si;
+        for (; p > plim; p--, op -= so, ip -= si) {
+            T nxt = op[-so];
+            step_prop(*ip, cur, nxt, h);
+            op[-so] = nxt;
+            cur = nxt;
+        }
+    }
+    for (; p > p_lo; p--, op -= so) {
+        T nxt = op[-so];
+        step_prop(nxt, cur, nxt, h);
+        op[-so] = nxt;
+        cur = nxt;
+    }
+}
+
+// Backward sweep with interpolation (the z backward loop, box.cpp:2539-2576): step_in
+// while p > p_in_lo (and inside), else step_prop; step_in may change o(p) as well.
+template <typename T>
+__device__ __forceinline__ void sweep_backward_in(T* o, int so, const T* in, int si, int p_start, int p_lo,
+                                                  int p_in_lo, bool inside, T h) {
+    if (p_start <= p_lo) return;
+    T* op = o + p_start * so;
+    T cur = *op;
+    int p = p_start;
+    const int plim = max(p_in_lo, p_lo);
+    if (inside && p > plim) {
+        const T* ip = in + p_start * si;
+        T icur = *ip;
+        for (; p > plim; p--, op -= so, ip -= si) {
+            T nxt = op[-so];
+            const T inx = ip[-si];
+            step_in(icur, inx, cur, nxt, h);
+            *op = cur;
+            cur = nxt;
+            icur = inx;
+        }
+    }
+    for (; p > p_lo; p--, op -= so) {
+        T nxt = op[-so];
+        step_prop(nxt, cur, nxt, h);
+        *op = cur;
+        cur = nxt;
+    }
+    *op = cur;
+}
+
+template <typename T>
+__global__ void __launch_bounds__(kMaxThreads) redist_xy_kernel(RedistArgs<T> a) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
-    T* S = reinterpret_cast<T*>(smem_raw);
+    const int tid = threadIdx.x, nt = blockDim.x;
+    T* O = reinterpret_cast<T*>(smem_raw);  // out slice, [y][x] with pitch P, then in values
     const T h = (T)a.geo.h;
-    const int total = a.toff[a.G + 1];
-    for (int t = blockIdx.x; t < total; t += gridDim.x) {
-        const int g = tile_grain(a.toff, a.G, t);
+    for (TileWalk w(a.toff, a.G, blockIdx.x, gridDim.x); w.valid(); w.next()) {
+        const int g = w.g;
         const Box ob = a.out.grain_box(g);
         const Box ib = a.in.grain_box(g);
-        const int k = ob.z0 + (t - a.toff[g]);
-        const Intersect<T> I(ib, ob);
+        const int k = ob.z0 + w.local;
+        const Intersect I(ib, ob);
         const int nx = ob.nx(), ny = ob.ny();
         T* outg = a.out.grain_ptr(g) + (long long)(k - ob.z0) * nx * ny;
         if (!(k >= I.zmin && k < I.zmax - 1)) {  // no xy sweep reaches this slice
-            for (int q = threadIdx.x; q < nx * ny; q += blockDim.x) outg[q] = T(-1);
-            continue;
+            for (int q = tid; q < nx * ny; q += nt) outg[q] = T(-1);
+            continue;  // uniform across the CTA
         }
         const int P = nx | 1;
-        T* O = S;                  // out slice, [y][x] with pitch P
-        T* In = S + ny * P;        // in values on the intersection, same indexing
-        const T* ing = a.in.grain_ptr(g);
-        for (int q = threadIdx.x; q < nx * ny; q += blockDim.x) {
-            const int yy = q / nx, xx = q - yy * nx;
-            O[yy * P + xx] = T(-1);
-            const int i = ob.y0 + yy, j = ob.x0 + xx;
-            if (i >= I.ymin && i < I.ymax && j >= I.xmin && j < I.xmax) In[yy * P + xx] = ing[ib.at(i, j, k)];
+        T* In = O + ny * P;  // IN(i, j) at the same position as OUT(i, j), on the intersection
+        for (int q = tid; q < ny * P; q += nt) O[q] = T(-1);
+        {
+            // rows of the intersection, x-adjacent threads on x-adjacent words
+            const int w = I.xmax - I.xmin;
+            const T* src = a.in.grain_ptr(g) + ib.at(I.ymin, I.xmin, k);
+            T* dst = In + (I.ymin - ob.y0) * P + (I.xmin - ob.x0);
+            for (int yy = 0; yy < I.ymax - I.ymin; yy++, src += ib.nx(), dst += P)
+                for (int xx = tid; xx < w; xx += nt) cp_async_elem(dst + xx, src + xx);
         }
+        cp_async_wait_all();
         __syncthreads();
-#define OUT(i, j) O[((i) - ob.y0) * P + ((j) - ob.x0)]
-#define IN(i, j) In[((i) - ob.y0) * P + ((j) - ob.x0)]
-        // x forward, box.cpp:2367-2401
-        for (int i = I.ymin + threadIdx.x; i < ob.y1; i += blockDim.x) {
-            for (int j = I.xmin; j < ob.x1 - 1; j++) {
-                if (j < I.xmax - 1 && i < I.ymax) step_in(IN(i, j), IN(i, j + 1), OUT(i, j), OUT(i, j + 1), h);
-                else step_prop(OUT(i, j + 1), OUT(i, j), OUT(i, j + 1), h);
-            }
-        }
+        T* O0 = O - (long long)ob.y0 * P - ob.x0;  // O0[i * P + j] = OUT(i, j)
+        const T* in_k = In - (long long)ob.y0 * P - ob.x0;  // in_k[i * P + j] = IN(i, j)
+        const int inx = P;
+        for (int i = I.ymin + tid; i < ob.y1; i += nt)  // x forward, box.cpp:2367-2401
+            sweep_forward(O0 + (long long)i * P, 1, in_k + (long long)i * inx, 1, I.xmin, ob.x1, I.xmax, i < I.ymax, h);
         __syncthreads();
-        // x backward, box.cpp:2403-2435
-        for (int i = I.ymin + threadIdx.x; i < ob.y1; i += blockDim.x) {
-            for (int j = I.xmax - 1; j > ob.x0; j--) {
-                if (j > I.xmin && i < I.ymax) step_prop(IN(i, j - 1), OUT(i, j), OUT(i, j - 1), h);
-                else step_prop(OUT(i, j - 1), OUT(i, j), OUT(i, j - 1), h);
-            }
-        }
+        for (int i = I.ymin + tid; i < ob.y1; i += nt)  // x backward, box.cpp:2403-2435
+            sweep_backward_prop(O0 + (long long)i * P, 1, in_k + (long long)i * inx, 1, I.xmax - 1, ob.x0, I.xmin,
+                                i < I.ymax, h);
         __syncthreads();
-        // y forward, box.cpp:2437-2472
-        for (int j = I.xmin + threadIdx.x; j < ob.x1; j += blockDim.x) {
-            for (int i = I.ymin; i < ob.y1 - 1; i++) {
-                if (j < I.xmax && i < I.ymax - 1) step_in(IN(i, j), IN(i + 1, j), OUT(i, j), OUT(i + 1, j), h);
-                else step_prop(OUT(i + 1, j), OUT(i, j), OUT(i + 1, j), h);
-            }
-        }
+        for (int j = I.xmin + tid; j < ob.x1; j += nt)  // y forward, box.cpp:2437-2472
+            sweep_forward(O0 + j, P, in_k + j, inx, I.ymin, ob.y1, I.ymax, j < I.xmax, h);
         __syncthreads();
-        // y backward, box.cpp:2474-2496
-        for (int j = I.xmin + threadIdx.x; j < ob.x1; j += blockDim.x) {
-            for (int i = I.ymax - 1; i > ob.y0; i--) {
-                if (j < I.xmax && i > I.ymin) step_prop(IN(i - 1, j), OUT(i, j), OUT(i - 1, j), h);
-                else step_prop(OUT(i - 1, j), OUT(i, j), OUT(i - 1, j), h);
-            }
-        }
+        for (int j = I.xmin + tid; j < ob.x1; j += nt)  // y backward, box.cpp:2474-2496
+            sweep_backward_prop(O0 + j, P, in_k + j, inx, I.ymax - 1, ob.y0, I.ymin, j < I.xmax, h);
         __syncthreads();
-#undef OUT
-#undef IN
-        for (int q = threadIdx.x; q < nx * ny; q += blockDim.x) {
-            const int yy = q / nx, xx = q - yy * nx;
-            outg[q] = O[yy * P + xx];
-        }
+        for (int yy = 0; yy < ny; yy++)
+            for (int xx = tid; xx < nx; xx += nt) outg[yy * nx + xx] = O[yy * P + xx];
         __syncthreads();
     }
 }
 
 template <typename T>
-__global__ void __launch_bounds__(kThreadsZ) redist_z_kernel(RedistArgs<T> a) {
+__global__ void __launch_bounds__(kMaxThreads) redist_z_kernel(RedistArgs<T> a) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
-    T* S = reinterpret_cast<T*>(smem_raw);
+    const int tid = threadIdx.x, nt = blockDim.x;
+    T* Z = reinterpret_cast<T*>(smem_raw);  // [k][x] of this row, then the in values
     const T h = (T)a.geo.h;
     const T delta = (T)a.geo.delta;
-    const int total = a.toff[a.G + 1];
-    for (int t = blockIdx.x; t < total; t += gridDim.x) {
-        const int g = tile_grain(a.toff, a.G, t);
+    for (TileWalk w(a.toff, a.G, blockIdx.x, gridDim.x); w.valid(); w.next()) {
+        const int g = w.g;
         const Box ob = a.out.grain_box(g);
         const Box ib = a.in.grain_box(g);
-        const int i = ob.y0 + (t - a.toff[g]);
-        const Intersect<T> I(ib, ob);
+        const int i = ob.y0 + w.local;
+        const Intersect I(ib, ob);
         const int nx = ob.nx(), nz = ob.nz();
-        T* O = S;              // [k][x] of this row
-        T* In = S + nz * nx;   // in values, same indexing
-        T* outg = a.out.grain_ptr(g);
-        const T* ing = a.in.grain_ptr(g);
-        for (int q = threadIdx.x; q < nx * nz; q += blockDim.x) {
-            const int kk = q / nx, xx = q - kk * nx;
-            const int k = ob.z0 + kk, j = ob.x0 + xx;
-            O[q] = outg[ob.at(i, j, k)];
-            if (i >= I.ymin && i < I.ymax && j >= I.xmin && j < I.xmax && k >= I.zmin && k < I.zmax)
-                In[q] = ing[ib.at(i, j, k)];
+        const long long zs = (long long)nx * ob.ny();  // z stride of the output box
+        T* outr = a.out.grain_ptr(g) + (long long)(i - ob.y0) * nx;  // OUT(i, x0, z0)
+        T* Zin = Z + nx * nz;  // IN(i, j, k) at the position of OUT(i, j, k), on the intersection
+        for (int kk = 0; kk < nz; kk++)
+            for (int xx = tid; xx < nx; xx += nt) cp_async_elem(Z + kk * nx + xx, outr + kk * zs + xx);
+        if (i >= I.ymin && i < I.ymax) {
+            const int w = I.xmax - I.xmin;
+            const long long izs = (long long)ib.nx() * ib.ny();
+            const T* src = a.in.grain_ptr(g) + ib.at(i, I.xmin, I.zmin);
+            T* dst = Zin + (I.zmin - ob.z0) * nx + (I.xmin - ob.x0);
+            for (int k = I.zmin; k < I.zmax; k++, src += izs, dst += nx)
+                for (int xx = tid; xx < w; xx += nt) cp_async_elem(dst + xx, src + xx);
         }
+        cp_async_wait_all();
         __syncthreads();
-#define OUT(k, j) O[((k) - ob.z0) * nx + ((j) - ob.x0)]
-#define IN(k, j) In[((k) - ob.z0) * nx + ((j) - ob.x0)]
         if (i >= I.ymin) {
-            for (int j = I.xmin + threadIdx.x; j < ob.x1; j += blockDim.x) {
+            const int izs = nx;
+            T* Z0 = Z - (long long)ob.z0 * nx - ob.x0;  // Z0[k * nx + j] = OUT(i, j, k)
+            const T* in_i = Zin - (long long)ob.z0 * nx - ob.x0;  // in_i[k * nx + j] = IN(i, j, k)
+            for (int j = I.xmin + tid; j < ob.x1; j += nt) {
+                const bool inside = i < I.ymax && j < I.xmax;
                 // z forward, box.cpp:2501-2538
-                for (int k = I.zmin; k < ob.z1 - 1; k++) {
-                    if (k < I.zmax - 1 && i < I.ymax && j < I.xmax) step_in(IN(k, j), IN(k + 1, j), OUT(k, j), OUT(k + 1, j), h);
-                    else step_prop(OUT(k + 1, j), OUT(k, j), OUT(k + 1, j), h);
-                }
+                sweep_forward(Z0 + j, nx, in_i + j, izs, I.zmin, ob.z1, I.zmax, inside, h);
                 // z backward, box.cpp:2539-2576
-                for (int k = I.zmax - 1; k > ob.z0; k--) {
-                    if (k > I.zmin && i < I.ymax && j < I.xmax) step_in(IN(k, j), IN(k - 1, j), OUT(k, j), OUT(k - 1, j), h);
-                    else step_prop(OUT(k - 1, j), OUT(k, j), OUT(k - 1, j), h);
-                }
+                sweep_backward_in(Z0 + j, nx, in_i + j, izs, I.zmax - 1, ob.z0, I.zmin, inside, h);
             }
         }
         __syncthreads();
-#undef OUT
-#undef IN
         // clampValues(-delta, delta), dimensionalBufferReal.h:44-57
-        for (int q = threadIdx.x; q < nx * nz; q += blockDim.x) {
-            const int kk = q / nx, xx = q - kk * nx;
-            T v = O[q];
-            if (v < -delta) v = -delta;
-            else if (v > delta) v = delta;
-            outg[ob.at(i, ob.x0 + xx, ob.z0 + kk)] = v;
-        }
+        for (int kk = 0; kk < nz; kk++)
+            for (int xx = tid; xx < nx; xx += nt) {
+                T v = Z[kk * nx + xx];
+                if (v < -delta) v = -delta;
+                else if (v > delta) v = delta;
+                outr[kk * zs + xx] = v;
+            }
         __syncthreads();
     }
 }
 
 }  // namespace
 
+// Shared memory of one unit: output and input slices with odd pitch, or [z][x] planes.
 size_t redist_smem_bytes(int nmax, bool fp64) {
     const size_t e = fp64 ? 8 : 4;
-    const size_t xy = 2 * (size_t)nmax * (nmax | 1) * e;
-    const size_t z = 2 * (size_t)nmax * nmax * e;
-    return xy > z ? xy : z;
+    const size_t xy = (size_t)nmax * (nmax | 1);
+    const size_t z = (size_t)nmax * nmax;
+    return 2 * (xy > z ? xy : z) * e;
 }
 
 template <typename T>
-void launch_redistance(const RedistArgs<T>& a, int grid, size_t smem_xy, size_t smem_z, cudaStream_t s) {
+void launch_redistance(const RedistArgs<T>& a, int grid, int side, cudaStream_t s) {
     static bool configured = false;
     if (!configured) {
         allow_max_dynamic_smem(redist_xy_kernel<T>);
         allow_max_dynamic_smem(redist_z_kernel<T>);
         configured = true;
     }
-    redist_xy_kernel<T><<<grid, kThreadsXY, smem_xy, s>>>(a);
-    redist_z_kernel<T><<<grid, kThreadsZ, smem_z, s>>>(a);
+    const size_t smem = redist_smem_bytes(side, sizeof(T) == 8);
+    int threads = (side + 31) / 32 * 32;
+    threads = threads > kMaxThreads ? kMaxThreads : threads;
+    redist_xy_kernel<T><<<grid * 2, threads, smem, s>>>(a);
+    redist_z_kernel<T><<<grid * 2, threads, smem, s>>>(a);
 }
 
-template void launch_redistance<double>(const RedistArgs<double>&, int, size_t, size_t, cudaStream_t);
-template void launch_redistance<float>(const RedistArgs<float>&, int, size_t, size_t, cudaStream_t);
+template void launch_redistance<double>(const RedistArgs<double>&, int, int, cudaStream_t);
+template void launch_redistance<float>(const RedistArgs<float>&, int, int, cudaStream_t);
 
 }  // namespace gg
