@@ -454,7 +454,7 @@ int stage_level_set_t(gg_ctx* ctx) {
     a.n_nb = ctx->d_nnb;
     a.nb_cap = kNbCap;
     a.err = ctx->d_err;
-    launch_mc<T>(a, ctx->grid, ctx->stream);
+    launch_mc<T>(a, ctx->grid, ctx->side_max, ctx->stream);
     ctx->launches += 1;
     CK(cudaGetLastError());
     return GG_OK;
@@ -557,7 +557,7 @@ int supported_side(bool fp64) {
     int n = 8;
     for (;;) {
         const int m = n + 1;
-        bool ok = redist_smem_bytes(m, fp64) <= lim;
+        bool ok = redist_smem_bytes(m, fp64) <= lim && mc_slab_bytes(m) + 40 * 1024 <= lim;
         if (fp64) ok = ok && conv_f64_smem_bytes(m) <= lim;
         else ok = ok && 3 * (size_t)m * (m | 1) * 4 <= lim;
         if (!ok || m > 4096) return n;

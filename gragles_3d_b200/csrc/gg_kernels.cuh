@@ -124,7 +124,9 @@ struct MCArgs {
     int* err;
 };
 template <typename T>
-void launch_mc(const MCArgs<T>& a, int grid, cudaStream_t s);
+void launch_mc(const MCArgs<T>& a, int grid, int side, cudaStream_t s);
+// Dynamic shared memory of the marching-cubes kernel for boxes up to `side`.
+size_t mc_slab_bytes(int side);
 
 // ---- redistancing (gg_redist.cu) ----
 template <typename T>

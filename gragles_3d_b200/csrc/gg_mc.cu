@@ -8,7 +8,7 @@
 // resize of the output box to the new bounding box (dimensionalBuffer.h:120-219).
 //
 // One CTA owns one grain and walks its cubes in the reference's z, y, x order in
-// chunks of blockDim cubes.  A block scan of per-cube triangle counts gives each
+// slabs of whole cube layers.  A block scan of per-cube triangle counts gives each
 // triangle its place in the reference's emission order; the FP64 volume and area
 // terms of a chunk are then added by one thread in that order, so the sums are
 // bit-identical to the reference's sequential loop.  The distinct neighbour IDs
@@ -24,7 +24,7 @@ namespace {
 
 constexpr int kThreads = 256;
 constexpr int kHash = 1024;  // distinct neighbour IDs per grain (power of two)
-constexpr int kChunk = 2048; // cubes classified per round
+constexpr int kSlabBytes = 64 * 1024;  // shared memory for a slab's sign bytes and cube lists
 
 // cubeindex bit b <-> corner offset (dx, dy, dz), marchingCubes.cpp:376-385
 __constant__ int c_corner[8][3] = {{0, 0, 1}, {1, 0, 1}, {1, 0, 0}, {0, 0, 0},
@@ -108,7 +108,7 @@ __device__ Box resize_to_cube(Box b, int maximumLength) {
 }
 
 template <typename T>
-__global__ void __launch_bounds__(kThreads, 3) mc_kernel(MCArgs<T> a) {
+__global__ void __launch_bounds__(kThreads, 2) mc_kernel(MCArgs<T> a, int slab_bytes) {
     __shared__ double vbuf[kThreads * 5];
     __shared__ double abuf[kThreads * 5];
     __shared__ int warp_sums[33];
@@ -117,11 +117,9 @@ __global__ void __launch_bounds__(kThreads, 3) mc_kernel(MCArgs<T> a) {
     __shared__ unsigned nb_id[kHash];
     __shared__ unsigned nb_key[kHash];
     __shared__ int n_found;
-    __shared__ unsigned char cidx[kChunk];
-    __shared__ unsigned short act[kChunk];
-    const int total = a.toff[a.G + 1];
-    for (int t = blockIdx.x; t < total; t += gridDim.x) {
-        const int g = tile_grain(a.toff, a.G, t);
+    extern __shared__ __align__(16) unsigned char slab_raw[];
+    for (TileWalk w(a.toff, a.G, blockIdx.x, gridDim.x); w.valid(); w.next()) {
+        const int g = w.g;
         if (!a.exists[g]) {  // the hull vanished last step: delete, grainhdl.cpp:678-680
             if (threadIdx.x == 0) a.present[g] = 0;
             continue;
@@ -132,55 +130,105 @@ __global__ void __launch_bounds__(kThreads, 3) mc_kernel(MCArgs<T> a) {
         for (int q = threadIdx.x; q < kHash; q += blockDim.x) { hkey[q] = 0xFFFFFFFFu; hval[q] = 0xFFFFFFFFu; }
         if (threadIdx.x == 0) n_found = 0;
         const int ncx = b.nx() - 1, ncy = b.ny() - 1, ncz = b.nz() - 1;
-        const long long NC = (ncx > 0 && ncy > 0 && ncz > 0) ? (long long)ncx * ncy * ncz : 0;
+        const int ncplane = (ncx > 0 && ncy > 0 && ncz > 0) ? ncx * ncy : 0;
         double vol = 0.0, area = 0.0;
         long long ntri = 0;
-        const long long plane = (long long)b.nx() * b.ny();
+        const int nxb = b.nx(), plane = b.nx() * b.ny();
+        // Slabs of LZ cube layers: the sign bytes of their LZ + 1 voxel layers are staged
+        // with one coalesced load per voxel, then every cube is classified from shared
+        // memory; a cube-index byte and an active-list entry per cube.
+        int LZ = ncplane > 0 ? (slab_bytes - plane - 2) / (plane + 3 * ncplane) : 0;
+        if (ncplane > 0 && LZ > 65535 / ncplane) LZ = 65535 / ncplane;
+        if (LZ > ncz) LZ = ncz;
+        if (ncplane > 0 && LZ < 1) {  // a single layer does not fit the shared memory
+            if (threadIdx.x == 0) atomicOr(a.err, ERR_BOX);
+            LZ = 0;
+        }
+        unsigned char* sgn = slab_raw;
+        unsigned char* cidx = sgn + (LZ + 1) * plane;
+        // 2-byte entries at an even offset from the (16-byte aligned) buffer start
+        const int act_off = ((LZ + 1) * plane + LZ * ncplane + 1) & ~1;
+        unsigned short* act = reinterpret_cast<unsigned short*>(slab_raw + act_off);
+        // cube (lx, ly, lz) of a slab is lz * ncplane + ly * ncx + lx; a step of kThreads
+        // cubes is (sz, sy, sx) in that mixed radix, so coordinates advance without divisions
+        int sx = 0, sy = 0, sz = 0;
+        if (ncplane > 0) {
+            const int st = kThreads / ncx;
+            sx = kThreads - st * ncx;
+            sz = st / ncy;
+            sy = st - sz * ncy;
+        }
         __syncthreads();
-        for (long long round = 0; round < NC; round += kChunk) {
-          // classify kChunk cubes with coalesced loads (inside = value >= 0, marchingCubes.cpp:12-15)
-          for (int k = 0; k < kChunk; k += kThreads) {
-              const long long c = round + k + threadIdx.x;
-              int ci = 0;
-              if (c < NC) {
-                  const int x = b.x0 + (int)(c % ncx);
-                  const int y = b.y0 + (int)((c / ncx) % ncy);
-                  const int z = b.z0 + (int)(c / ((long long)ncx * ncy));
-                  const T* p = sdf + b.at(y, x, z);
+        for (int zc0 = 0; LZ > 0 && zc0 < ncz; zc0 += LZ) {
+          const int lz = min(LZ, ncz - zc0);
+          const int ncs = lz * ncplane;
+          // sign bytes of voxel layers zc0 .. zc0 + lz (inside = value >= 0, marchingCubes.cpp:12-15)
+          {
+              const T* src = sdf + (long long)zc0 * plane;
+              const int nv = (lz + 1) * plane;
+              for (int v0 = 0; v0 < nv; v0 += 8 * kThreads) {
+                  T r[8];
 #pragma unroll
-                  for (int q = 0; q < 8; q++)
-                      if (p[c_corner[q][2] * plane + c_corner[q][1] * b.nx() + c_corner[q][0]] >= 0) ci |= 1 << q;
+                  for (int u = 0; u < 8; u++) {
+                      const int v = v0 + u * kThreads + threadIdx.x;
+                      r[u] = v < nv ? src[v] : T(-1);
+                  }
+#pragma unroll
+                  for (int u = 0; u < 8; u++) {
+                      const int v = v0 + u * kThreads + threadIdx.x;
+                      if (v < nv) sgn[v] = r[u] >= T(0);
+                  }
               }
-              cidx[k + threadIdx.x] = (unsigned char)ci;
           }
           __syncthreads();
-          // active cubes of the round, in cube order
-          int nloc = 0;
+          {
+              const int q0 = threadIdx.x / ncx;
+              int cx = threadIdx.x - q0 * ncx, cz = q0 / ncy;
+              int cy = q0 - cz * ncy;
+              for (int cl = threadIdx.x; cl < ncs; cl += kThreads) {
+                  const unsigned char* p = sgn + cz * plane + cy * nxb + cx;
+                  int ci = 0;
 #pragma unroll
-          for (int q = 0; q < kChunk / kThreads; q++) nloc += gg_mc_edge_table[cidx[threadIdx.x * (kChunk / kThreads) + q]] != 0;
+                  for (int q = 0; q < 8; q++)
+                      ci |= (int)p[c_corner[q][2] * plane + c_corner[q][1] * nxb + c_corner[q][0]] << q;
+                  cidx[cl] = (unsigned char)ci;
+                  cx += sx;
+                  cy += sy;
+                  cz += sz;
+                  if (cx >= ncx) { cx -= ncx; cy++; }
+                  if (cy >= ncy) { cy -= ncy; cz++; }
+              }
+          }
+          __syncthreads();
+          // active cubes of the slab, in cube order: thread t scans cubes [t seg, (t + 1) seg)
+          const int seg = (ncs + kThreads - 1) / kThreads;
+          const int s0 = threadIdx.x * seg, s1 = min(s0 + seg, ncs);
+          int nloc = 0;
+          for (int lc = s0; lc < s1; lc++) nloc += gg_mc_edge_table[cidx[lc]] != 0;
           int n_act;
           int w = block_exclusive_scan(nloc, warp_sums, n_act);
-#pragma unroll
-          for (int q = 0; q < kChunk / kThreads; q++) {
-              const int lc = threadIdx.x * (kChunk / kThreads) + q;
+          for (int lc = s0; lc < s1; lc++)
               if (gg_mc_edge_table[cidx[lc]] != 0) act[w++] = (unsigned short)lc;
-          }
           __syncthreads();
           for (int ab = 0; ab < n_act; ab += kThreads) {
             const int ia = ab + threadIdx.x;
             int nt = 0, ci = 0;
-            int x = 0, y = 0, z = 0;
-            long long c = 0;
+            int x = 0, y = 0, z = 0, base = 0;
+            int c = 0;
             double val[8];
             if (ia < n_act) {
-                c = round + act[ia];
-                ci = cidx[act[ia]];
-                x = b.x0 + (int)(c % ncx);
-                y = b.y0 + (int)((c / ncx) % ncy);
-                z = b.z0 + (int)(c / ((long long)ncx * ncy));
+                const int cl = act[ia];
+                c = zc0 * ncplane + cl;  // cube index in the reference's z, y, x order
+                ci = cidx[cl];
+                const int lzl = cl / ncplane, rem = cl - lzl * ncplane;
+                const int ly = rem / ncx, lx = rem - ly * ncx, lzz = zc0 + lzl;
+                x = b.x0 + lx;
+                y = b.y0 + ly;
+                z = b.z0 + lzz;
+                base = lzz * plane + ly * nxb + lx;
 #pragma unroll
                 for (int k = 0; k < 8; k++)
-                    val[k] = (double)sdf[b.at(y + c_corner[k][1], x + c_corner[k][0], z + c_corner[k][2])];
+                    val[k] = (double)sdf[base + c_corner[k][2] * plane + c_corner[k][1] * nxb + c_corner[k][0]];
                 while (gg_mc_tri_table[ci][3 * nt] != -1) nt++;
             }
             int chunk_total;
@@ -219,8 +267,7 @@ __global__ void __launch_bounds__(kThreads, 3) mc_kernel(MCArgs<T> a) {
                 int cnt = 0;
 #pragma unroll
                 for (int k = 0; k < 8; k++) {
-                    const int xx = x + c_nbc[k][0], yy = y + c_nbc[k][1], zz = z + c_nbc[k][2];
-                    const long long at = b.at(yy, xx, zz);
+                    const int at = base + c_nbc[k][2] * plane + c_nbc[k][1] * nxb + c_nbc[k][0];
                     unsigned id = sdf[at] >= 0 ? (unsigned)g : idl[at];
                     bool found = false;
                     for (int q = 0; q < cnt; q++) found |= (lst[q] == id);
@@ -315,9 +362,22 @@ __global__ void count_kernel(int G, const int* present, const int* exists, const
 
 }  // namespace
 
+size_t mc_slab_bytes(int side) {
+    // at least one cube layer: two voxel layers of sign bytes, a byte and a list entry per cube
+    const size_t n = side > 1 ? side : 2;
+    const size_t one_layer = 2 * n * n + 3 * (n - 1) * (n - 1) + 2;
+    return one_layer > kSlabBytes ? one_layer : kSlabBytes;
+}
+
 template <typename T>
-void launch_mc(const MCArgs<T>& a, int grid, cudaStream_t s) {
-    mc_kernel<T><<<grid, kThreads, 0, s>>>(a);
+void launch_mc(const MCArgs<T>& a, int grid, int side, cudaStream_t s) {
+    static bool configured = false;
+    if (!configured) {
+        allow_max_dynamic_smem(mc_kernel<T>);
+        configured = true;
+    }
+    const size_t bytes = mc_slab_bytes(side);
+    mc_kernel<T><<<grid, kThreads, bytes, s>>>(a, (int)bytes);
 }
 
 void launch_count(int G, const int* present, const int* exists, const int* box, int* out3, cudaStream_t s) {
@@ -325,7 +385,7 @@ void launch_count(int G, const int* present, const int* exists, const int* box, 
     count_kernel<<<64, 256, 0, s>>>(G, present, exists, box, out3);
 }
 
-template void launch_mc<double>(const MCArgs<double>&, int, cudaStream_t);
-template void launch_mc<float>(const MCArgs<float>&, int, cudaStream_t);
+template void launch_mc<double>(const MCArgs<double>&, int, int, cudaStream_t);
+template void launch_mc<float>(const MCArgs<float>&, int, int, cudaStream_t);
 
 }  // namespace gg
