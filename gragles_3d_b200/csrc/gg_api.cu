@@ -48,6 +48,8 @@ struct gg_ctx {
     double *d_volume = nullptr, *d_surface = nullptr;
     uint32_t* d_nb = nullptr;
     uint32_t *d_cmp = nullptr, *d_son = nullptr;
+    unsigned long long* d_pt = nullptr;  // per-grain list position tables
+    int pos_cap = 0;
     int *d_ncmp = nullptr, *d_nson = nullptr;
     // pool
     void* d_arena[2] = {nullptr, nullptr};
@@ -400,6 +402,17 @@ int stage_comparison_t(gg_ctx* ctx) {
     int rc = ensure_bins(ctx);
     if (rc) return rc;
     launch_newbox_init(ctx->G, ctx->d_present, ctx->d_exists, ctx->d_box[p ^ 1], ctx->d_newbox, ctx->stream);
+    PosTableArgs pt{};
+    pt.G = ctx->G;
+    pt.toff = ctx->d_toff_one;
+    pt.cmp = ctx->d_cmp;
+    pt.n_cmp = ctx->d_ncmp;
+    pt.list_cap = ctx->list_cap;
+    pt.table = ctx->d_pt;
+    pt.pos_cap = ctx->pos_cap;
+    pt.err = ctx->d_err;
+    launch_pos_tables(pt, ctx->grid, ctx->stream);
+    ctx->launches += 1;
     launch_bin(ctx->bins, ctx->G, ctx->d_exists, ctx->d_box[p], ctx->d_err, ctx->stream);
     ctx->launches += 4;
     CK(cudaMemcpyAsync(ctx->h_maxcount, ctx->bins.max_count, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
@@ -423,6 +436,8 @@ int stage_comparison_t(gg_ctx* ctx) {
     a.cmp = ctx->d_cmp;
     a.n_cmp = ctx->d_ncmp;
     a.list_cap = ctx->list_cap;
+    a.pos_table = ctx->d_pt;
+    a.pos_cap = ctx->pos_cap;
     a.newbox = ctx->d_newbox;
     a.err = ctx->d_err;
     launch_compare<T>(a, ctx->num_sms * 4, ctx->stream);
@@ -567,7 +582,7 @@ int supported_side(bool fp64) {
 
 void free_all(gg_ctx* c) {
     void* ptrs[] = {c->d_present, c->d_exists, c->d_newbox, c->d_nnb, c->d_volume, c->d_surface, c->d_nb, c->d_cmp,
-                    c->d_son, c->d_ncmp, c->d_nson, c->d_arena[0], c->d_arena[1], c->d_box[0], c->d_box[1],
+                    c->d_son, c->d_ncmp, c->d_nson, c->d_pt, c->d_arena[0], c->d_arena[1], c->d_box[0], c->d_box[1],
                     c->d_off[0], c->d_off[1], c->d_idarena[0], c->d_idarena[1], c->d_idbox[0], c->d_idbox[1],
                     c->d_idoff[0], c->d_idoff[1], c->d_spec, c->d_spec_off, c->d_toff_n, c->d_toff_slab,
                     c->d_toff_one, c->d_toff_mc, c->d_toff_red, c->d_tw, c->d_tw_off, c->d_gtab, c->d_g_off,
@@ -632,6 +647,9 @@ int gg_create(const gg_params* params, gg_ctx** out) {
     CK(dalloc(&ctx->d_surface, G1));
     CK(dalloc(&ctx->d_nb, (size_t)kNbCap * G1));
     CK(dalloc(&ctx->d_cmp, (size_t)ctx->list_cap * G1));
+    ctx->pos_cap = 64;
+    while (ctx->pos_cap < 2 * ctx->list_cap) ctx->pos_cap <<= 1;
+    CK(dalloc(&ctx->d_pt, (size_t)ctx->pos_cap * G1));
     CK(dalloc(&ctx->d_son, (size_t)ctx->list_cap * G1));
     CK(dalloc(&ctx->d_ncmp, G1));
     CK(dalloc(&ctx->d_nson, G1));

@@ -13,9 +13,9 @@
 //   1. bin: every tile of kTX x kTY x kTZ domain voxels gets the IDs of the
 //      grains whose boxes reach it (count, scan, fill);
 //   2. compare: one CTA per tile loads every covering box's values over the tile
-//      into shared memory once and builds, by streaming each covering grain's
-//      comparison list against a small hash of the tile's grains, the position of
-//      every covering grain in every other's list.  Per voxel it keeps the kTop
+//      into shared memory once and looks up, in each covering grain's position
+//      table (built once per step from its comparison list), the position of every
+//      other covering grain in its list.  Per voxel it keeps the kTop
 //      largest values; every (grain, voxel) pair then picks the first candidate
 //      that is in that grain's list, resolving equal values by list position --
 //      falling back to a full scan of the tile's boxes whenever the kTop
@@ -43,7 +43,6 @@ constexpr int kTop = 4;                // candidates kept per voxel
 constexpr int kParts = kThreads / kTV; // threads scanning the boxes of one voxel
 constexpr unsigned kNone = 0xFFFFFFFFu;
 constexpr unsigned short kNotListed = 0xFFFF;
-constexpr int kHashT = 512;            // grain ID -> tile entry (power of two, > 2 x most entries)
 
 // One branch of the reference's boundary distance (box.cpp:1017-1082).  Returns
 // false where no branch assigns `dist`, in which case the reference keeps the value
@@ -208,13 +207,14 @@ struct TileSmem {
     int* box;           // 6 per entry
     long long* off;
     int* bbox;          // 6 per entry: new bounding box contributions
+    long long* outoff;  // per entry: offset of its output box and IDLocal box
+    long long* idoff;
+    int* tsize;         // per entry: size of its position table
     T* val;             // [entry][voxel]
     unsigned short* pos;// [entry a][entry b]: position of b in a's list, kNotListed, or kUnknown
     T* topv;            // [part][voxel][kTop], the merged list in part 0
     unsigned char* topi;
     int* ncand;         // covering entries with value > -1, per voxel
-    uint32_t* hkey;     // grain ID -> entry, open addressing
-    unsigned char* hval;
 };
 
 template <typename T>
@@ -222,16 +222,17 @@ __device__ TileSmem<T> carve(unsigned char* base, int mcap) {
     TileSmem<T> s;
     unsigned char* p = base;
     s.off = reinterpret_cast<long long*>(p); p += 8 * mcap;
+    s.outoff = reinterpret_cast<long long*>(p); p += 8 * mcap;
+    s.idoff = reinterpret_cast<long long*>(p); p += 8 * mcap;
     s.val = reinterpret_cast<T*>(p); p += sizeof(T) * (size_t)mcap * kTV;
     s.topv = reinterpret_cast<T*>(p); p += sizeof(T) * kTV * kTop * kParts;
     s.id = reinterpret_cast<uint32_t*>(p); p += 4 * mcap;
     s.box = reinterpret_cast<int*>(p); p += 24 * mcap;
     s.bbox = reinterpret_cast<int*>(p); p += 24 * mcap;
+    s.tsize = reinterpret_cast<int*>(p); p += 4 * mcap;
     s.ncand = reinterpret_cast<int*>(p); p += 4 * kTV * kParts;
-    s.hkey = reinterpret_cast<uint32_t*>(p); p += 4 * kHashT;
     s.pos = reinterpret_cast<unsigned short*>(p); p += 2 * (size_t)mcap * mcap;
-    s.topi = p; p += kTV * kTop * kParts;
-    s.hval = p;
+    s.topi = p;
     return s;
 }
 
@@ -257,15 +258,17 @@ __device__ __forceinline__ void top_insert(T (&tv)[kTop], int (&ti)[kTop], T w, 
     }
 }
 
-__device__ __forceinline__ int tile_lookup(const uint32_t* hkey, const unsigned char* hval, uint32_t id) {
-    unsigned h = (id * 2654435761u) & (kHashT - 1);
-    for (int probe = 0; probe < kHashT; probe++) {
-        const uint32_t k = hkey[h];
-        if (k == id) return hval[h];
-        if (k == kNone) return -1;
-        h = (h + 1) & (kHashT - 1);
+// Position of `id` in the list behind a position table of `size` slots, or kNotListed.
+__device__ __forceinline__ unsigned short pos_lookup(const unsigned long long* tab, int size, uint32_t id) {
+    unsigned h = (id * 2654435761u) & (unsigned)(size - 1);
+    for (int probe = 0; probe < size; probe++) {
+        const unsigned long long e = __ldg(tab + h);
+        const uint32_t k = (uint32_t)(e >> 32);
+        if (k == id) return (unsigned short)(e & 0xFFFFu);
+        if (k == kNone) return kNotListed;
+        h = (h + 1) & (unsigned)(size - 1);
     }
-    return -1;
+    return kNotListed;
 }
 
 template <typename T>
@@ -292,43 +295,36 @@ __global__ void __launch_bounds__(kThreads) compare_kernel(CompareArgs<T> a) {
 #pragma unroll
             for (int q = 0; q < 6; q++) s.box[6 * e + q] = bb[q];
             s.off[e] = a.in.off[g];
+            s.outoff[e] = a.out.off[g];
+            s.idoff[e] = a.idoff_new[g];
+            s.tsize[e] = pos_table_size(a.n_cmp[g], a.pos_cap);
             s.bbox[6 * e + 0] = INT_MAX; s.bbox[6 * e + 1] = INT_MIN;
             s.bbox[6 * e + 2] = INT_MAX; s.bbox[6 * e + 3] = INT_MIN;
             s.bbox[6 * e + 4] = INT_MAX; s.bbox[6 * e + 5] = INT_MIN;
         }
-        for (int q = threadIdx.x; q < m * m; q += blockDim.x) s.pos[q] = kNotListed;
-        for (int q = threadIdx.x; q < kHashT; q += blockDim.x) s.hkey[q] = kNone;
         __syncthreads();
-        for (int e = threadIdx.x; e < m; e += blockDim.x) {  // grain ID -> entry
-            const uint32_t id = s.id[e];
-            unsigned h = (id * 2654435761u) & (kHashT - 1);
-            while (atomicCAS(s.hkey + h, kNone, id) != kNone) h = (h + 1) & (kHashT - 1);
-            s.hval[h] = (unsigned char)e;
-        }
-        __syncthreads();
-        {  // pos[a][b] = position of b in a's list: a warp streams a's list, looks each ID up in the tile
+        {  // pos[a][b] = position of b in a's list, from a's position table
             const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nw = blockDim.x >> 5;
             for (int ea = warp; ea < m; ea += nw) {
-                const uint32_t ga = s.id[ea];
-                const uint32_t* list = a.cmp + (long long)ga * a.list_cap;
-                const int K = a.n_cmp[ga];
-                for (int i = lane; i < K; i += 32) {
-                    const int eb = tile_lookup(s.hkey, s.hval, __ldg(list + i));
-                    if (eb >= 0) s.pos[ea * m + eb] = (unsigned short)i;
-                }
+                const unsigned long long* tab = a.pos_table + (long long)s.id[ea] * a.pos_cap;
+                const int size = s.tsize[ea];
+                for (int eb = lane; eb < m; eb += 32)
+                    s.pos[ea * m + eb] = eb == ea ? kNotListed : pos_lookup(tab, size, s.id[eb]);
             }
         }
         __syncthreads();
-        // values of every covering box over the tile (-inf outside the box)
+        // values of every covering box over the tile (-inf outside the box), copied with
+        // cp.async so that no thread waits on one load before issuing the next
         for (int q = threadIdx.x; q < m * kTV; q += blockDim.x) {
             const int e = q / kTV, v = q % kTV;
             const int x = X0 + v % kTX, y = Y0 + (v / kTX) % kTY, z = Z0 + v / (kTX * kTY);
             const Box B = load_box(s.box + 6 * e);
-            T w = NEG;
             if (x >= B.x0 && x < B.x1 && y >= B.y0 && y < B.y1 && z >= B.z0 && z < B.z1)
-                w = a.in.data[s.off[e] + B.at(y, x, z)];
-            s.val[q] = w;
+                cp_async_elem(s.val + q, a.in.data + s.off[e] + B.at(y, x, z));
+            else
+                s.val[q] = NEG;
         }
+        cp_async_wait_all();
         __syncthreads();
         // per voxel: the kTop largest values > -1 (kParts threads share a voxel)
         {
@@ -440,8 +436,8 @@ __global__ void __launch_bounds__(kThreads) compare_kernel(CompareArgs<T> a) {
             T res;
             if ((double)fabs(in) < lim) res = T(0.5) * (in - cmpv);
             else res = in;
-            a.out.data[a.out.off[ga] + f] = res;
-            a.id_new[a.idoff_new[ga] + f] = idv;
+            a.out.data[s.outoff[ea] + f] = res;
+            a.id_new[s.idoff[ea] + f] = idv;
             if (res >= 0) {
                 int* bb = s.bbox + 6 * ea;
                 atomicMin(bb + 0, x); atomicMax(bb + 1, x);
@@ -476,9 +472,9 @@ __global__ void newbox_init_kernel(int G, const int* present, const int* exists,
 
 size_t compare_smem_bytes(int mcap, bool fp64) {
     const size_t e = fp64 ? 8 : 4;
-    return 8 * (size_t)mcap + e * (size_t)mcap * kTV + e * kTV * kTop * kParts + 4 * (size_t)mcap +
-           48 * (size_t)mcap + 4 * kTV * kParts + 4 * kHashT + 2 * (size_t)mcap * mcap + kTV * kTop * kParts +
-           kHashT + 64;
+    return 24 * (size_t)mcap + e * (size_t)mcap * kTV + e * kTV * kTop * kParts + 4 * (size_t)mcap +
+           48 * (size_t)mcap + 4 * (size_t)mcap + 4 * kTV * kParts + 2 * (size_t)mcap * mcap +
+           kTV * kTop * kParts + 64;
 }
 
 long long bin_capacity(int G, int side) {

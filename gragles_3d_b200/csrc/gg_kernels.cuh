@@ -79,6 +79,8 @@ struct CompareArgs {
     const uint32_t* cmp;      // comparison lists (position = list order)
     const int* n_cmp;
     int list_cap;
+    const unsigned long long* pos_table;  // per grain: neighbour ID -> list position (pos_tables)
+    int pos_cap;
     int* newbox;              // per grain min/max (pre-initialised)
     int* err;
 };
@@ -102,6 +104,26 @@ struct ListArgs {
     int* err;
 };
 void launch_update_lists(const ListArgs& a, int grid, cudaStream_t s);
+
+// Per grain an open-addressing table (ID << 32 | list position) of the comparison list,
+// pos_cap slots per grain of which pos_table_size(K) are used; built once per step
+// and probed by every comparison tile the grain's box reaches.
+struct PosTableArgs {
+    int G;
+    const int* toff;          // one tile per existing grain
+    const uint32_t* cmp;
+    const int* n_cmp;
+    int list_cap;
+    unsigned long long* table;
+    int pos_cap;              // power of two >= 2 list_cap
+    int* err;
+};
+void launch_pos_tables(const PosTableArgs& a, int grid, cudaStream_t s);
+__host__ __device__ inline int pos_table_size(int K, int cap) {
+    int n = 64;
+    while (n < 2 * K && n < cap) n <<= 1;
+    return n;
+}
 
 // ---- marching cubes + hull statistics (gg_mc.cu) ----
 template <typename T>

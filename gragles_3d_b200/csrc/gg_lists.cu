@@ -134,7 +134,36 @@ __global__ void __launch_bounds__(kThreads) update_lists_kernel(ListArgs a) {
     }
 }
 
+__global__ void __launch_bounds__(128) pos_table_kernel(PosTableArgs a) {
+    constexpr unsigned long long kFree = ~0ull;
+    for (TileWalk w(a.toff, a.G, blockIdx.x, gridDim.x); w.valid(); w.next()) {
+        const int g = w.g;
+        const int K = a.n_cmp[g];
+        const int size = pos_table_size(K, a.pos_cap);
+        unsigned long long* tab = a.table + (long long)g * a.pos_cap;
+        const uint32_t* list = a.cmp + (long long)g * a.list_cap;
+        for (int q = threadIdx.x; q < size; q += blockDim.x) tab[q] = kFree;
+        __syncthreads();
+        for (int i = threadIdx.x; i < K; i += blockDim.x) {
+            const uint32_t id = list[i];
+            const unsigned long long e = ((unsigned long long)id << 32) | (unsigned)i;
+            unsigned h = (id * 2654435761u) & (unsigned)(size - 1);
+            int probe = 0;
+            for (; probe < size; probe++) {
+                if (atomicCAS(tab + h, kFree, e) == kFree) break;
+                h = (h + 1) & (unsigned)(size - 1);
+            }
+            if (probe == size) atomicOr(a.err, ERR_HASH);
+        }
+        __syncthreads();
+    }
+}
+
 }  // namespace
+
+void launch_pos_tables(const PosTableArgs& a, int grid, cudaStream_t s) {
+    pos_table_kernel<<<grid, 128, 0, s>>>(a);
+}
 
 void launch_update_lists(const ListArgs& a, int grid, cudaStream_t s) {
     static bool configured = false;
