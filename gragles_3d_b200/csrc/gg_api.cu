@@ -648,7 +648,7 @@ int gg_create(const gg_params* params, gg_ctx** out) {
     CK(dalloc(&ctx->d_nb, (size_t)kNbCap * G1));
     CK(dalloc(&ctx->d_cmp, (size_t)ctx->list_cap * G1));
     ctx->pos_cap = 64;
-    while (ctx->pos_cap < 2 * ctx->list_cap) ctx->pos_cap <<= 1;
+    while (ctx->pos_cap < 2 * ctx->list_cap) ctx->pos_cap <<= 1;  // load factor <= 1/2 at full lists
     CK(dalloc(&ctx->d_pt, (size_t)ctx->pos_cap * G1));
     CK(dalloc(&ctx->d_son, (size_t)ctx->list_cap * G1));
     CK(dalloc(&ctx->d_ncmp, G1));

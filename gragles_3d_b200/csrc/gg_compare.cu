@@ -41,6 +41,7 @@ constexpr int kThreads = 256;
 constexpr int kTV = kTX * kTY * kTZ;   // voxels per tile (64)
 constexpr int kTop = 4;                // candidates kept per voxel
 constexpr int kParts = kThreads / kTV; // threads scanning the boxes of one voxel
+static_assert(kTV % 32 == 0 && kThreads % kTV == 0, "a warp's lanes share one tile entry per pair sweep");
 constexpr unsigned kNone = 0xFFFFFFFFu;
 constexpr unsigned short kNotListed = 0xFFFF;
 
@@ -258,21 +259,10 @@ __device__ __forceinline__ void top_insert(T (&tv)[kTop], int (&ti)[kTop], T w, 
     }
 }
 
-// Position of `id` in the list behind a position table of `size` slots, or kNotListed.
-__device__ __forceinline__ unsigned short pos_lookup(const unsigned long long* tab, int size, uint32_t id) {
-    unsigned h = (id * 2654435761u) & (unsigned)(size - 1);
-    for (int probe = 0; probe < size; probe++) {
-        const unsigned long long e = __ldg(tab + h);
-        const uint32_t k = (uint32_t)(e >> 32);
-        if (k == id) return (unsigned short)(e & 0xFFFFu);
-        if (k == kNone) return kNotListed;
-        h = (h + 1) & (unsigned)(size - 1);
-    }
-    return kNotListed;
-}
+__device__ __forceinline__ unsigned pos_home(uint32_t id, int size) { return (id * 2654435761u) & (unsigned)(size - 1); }
 
 template <typename T>
-__global__ void __launch_bounds__(kThreads) compare_kernel(CompareArgs<T> a) {
+__global__ void __launch_bounds__(kThreads, 4) compare_kernel(CompareArgs<T> a) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     TileSmem<T> s = carve<T>(smem_raw, a.mcap);
     const TileBins& tb = a.bins;
@@ -303,26 +293,73 @@ __global__ void __launch_bounds__(kThreads) compare_kernel(CompareArgs<T> a) {
             s.bbox[6 * e + 4] = INT_MAX; s.bbox[6 * e + 5] = INT_MIN;
         }
         __syncthreads();
-        {  // pos[a][b] = position of b in a's list, from a's position table
-            const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nw = blockDim.x >> 5;
-            for (int ea = warp; ea < m; ea += nw) {
-                const unsigned long long* tab = a.pos_table + (long long)s.id[ea] * a.pos_cap;
-                const int size = s.tsize[ea];
-                for (int eb = lane; eb < m; eb += 32)
-                    s.pos[ea * m + eb] = eb == ea ? kNotListed : pos_lookup(tab, size, s.id[eb]);
+        {  // pos[a][b] = position of b in a's list, from a's position table; kBatch
+           // lookups advance together, each round issuing all their next probes at once
+            constexpr int kBatch = 4;
+            const int mm = m * m;
+            for (int q0 = 0; q0 < mm; q0 += kBatch * kThreads) {
+                unsigned long long e[kBatch];
+                const unsigned long long* tab[kBatch];
+                unsigned h[kBatch], mask[kBatch];
+                uint32_t id[kBatch];
+                bool live[kBatch];
+#pragma unroll
+                for (int u = 0; u < kBatch; u++) {
+                    const int q = q0 + u * kThreads + threadIdx.x;
+                    const int ea = q / m, eb = q - ea * m;
+                    live[u] = q < mm && ea != eb;
+                    if (q < mm && ea == eb) s.pos[q] = kNotListed;
+                    tab[u] = nullptr;
+                    h[u] = mask[u] = id[u] = 0;
+                    e[u] = 0;
+                    if (live[u]) {
+                        tab[u] = a.pos_table + (long long)s.id[ea] * a.pos_cap;
+                        mask[u] = (unsigned)s.tsize[ea] - 1;
+                        id[u] = s.id[eb];
+                        h[u] = pos_home(id[u], s.tsize[ea]);
+                        e[u] = __ldg(tab[u] + h[u]);
+                    }
+                }
+                for (int round = 0; round < a.pos_cap; round++) {
+                    bool more = false;
+#pragma unroll
+                    for (int u = 0; u < kBatch; u++) {
+                        if (!live[u]) continue;
+                        const uint32_t k = (uint32_t)(e[u] >> 32);
+                        if (k == id[u] || k == kNone) {
+                            s.pos[q0 + u * kThreads + threadIdx.x] =
+                                k == id[u] ? (unsigned short)(e[u] & 0xFFFFu) : kNotListed;
+                            live[u] = false;
+                        } else {
+                            h[u] = (h[u] + 1) & mask[u];
+                            more = true;
+                        }
+                    }
+                    if (!more) break;
+#pragma unroll
+                    for (int u = 0; u < kBatch; u++)
+                        if (live[u]) e[u] = __ldg(tab[u] + h[u]);
+                }
             }
         }
         __syncthreads();
         // values of every covering box over the tile (-inf outside the box), copied with
         // cp.async so that no thread waits on one load before issuing the next
-        for (int q = threadIdx.x; q < m * kTV; q += blockDim.x) {
-            const int e = q / kTV, v = q % kTV;
-            const int x = X0 + v % kTX, y = Y0 + (v / kTX) % kTY, z = Z0 + v / (kTX * kTY);
-            const Box B = load_box(s.box + 6 * e);
-            if (x >= B.x0 && x < B.x1 && y >= B.y0 && y < B.y1 && z >= B.z0 && z < B.z1)
-                cp_async_elem(s.val + q, a.in.data + s.off[e] + B.at(y, x, z));
-            else
-                s.val[q] = NEG;
+        {
+            const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nw = blockDim.x >> 5;
+            for (int e = warp; e < m; e += nw) {
+                const Box B = load_box(s.box + 6 * e);
+                const T* src = a.in.data + s.off[e];
+#pragma unroll
+                for (int vv = 0; vv < kTV; vv += 32) {
+                    const int v = vv + lane;
+                    const int x = X0 + v % kTX, y = Y0 + (v / kTX) % kTY, z = Z0 + v / (kTX * kTY);
+                    if (x >= B.x0 && x < B.x1 && y >= B.y0 && y < B.y1 && z >= B.z0 && z < B.z1)
+                        cp_async_elem(s.val + e * kTV + v, src + B.at(y, x, z));
+                    else
+                        s.val[e * kTV + v] = NEG;
+                }
+            }
         }
         cp_async_wait_all();
         __syncthreads();
@@ -376,8 +413,9 @@ __global__ void __launch_bounds__(kThreads) compare_kernel(CompareArgs<T> a) {
         for (int q = threadIdx.x; q < m * kTV; q += blockDim.x) {
             const int ea = q / kTV, v = q % kTV;
             const T in = s.val[q];
-            if (in == NEG) continue;  // voxel outside this grain's box
             const int x = X0 + v % kTX, y = Y0 + (v / kTX) % kTY, z = Z0 + v / (kTX * kTY);
+            bool positive = false;
+            if (in != NEG) {  // else the voxel is outside this grain's box
             // the first listed neighbour among the largest values, ties to the earliest position
             int best = -1;
             unsigned short bpos = kNotListed;
@@ -438,11 +476,23 @@ __global__ void __launch_bounds__(kThreads) compare_kernel(CompareArgs<T> a) {
             else res = in;
             a.out.data[s.outoff[ea] + f] = res;
             a.id_new[s.idoff[ea] + f] = idv;
-            if (res >= 0) {
-                int* bb = s.bbox + 6 * ea;
-                atomicMin(bb + 0, x); atomicMax(bb + 1, x);
-                atomicMin(bb + 2, y); atomicMax(bb + 3, y);
-                atomicMin(bb + 4, z); atomicMax(bb + 5, z);
+            positive = res >= 0;
+            }
+            // new bounding box (executeSetComparison, box.cpp:858-877), reduced over the warp
+            // first: its 32 lanes hold the same entry (kTV and blockDim are multiples of 64)
+            if (__ballot_sync(0xffffffffu, positive)) {
+                const int x0 = __reduce_min_sync(0xffffffffu, positive ? x : INT_MAX);
+                const int x1 = __reduce_max_sync(0xffffffffu, positive ? x : INT_MIN);
+                const int y0 = __reduce_min_sync(0xffffffffu, positive ? y : INT_MAX);
+                const int y1 = __reduce_max_sync(0xffffffffu, positive ? y : INT_MIN);
+                const int z0 = __reduce_min_sync(0xffffffffu, positive ? z : INT_MAX);
+                const int z1 = __reduce_max_sync(0xffffffffu, positive ? z : INT_MIN);
+                if ((threadIdx.x & 31) == 0) {
+                    int* bb = s.bbox + 6 * ea;
+                    atomicMin(bb + 0, x0); atomicMax(bb + 1, x1);
+                    atomicMin(bb + 2, y0); atomicMax(bb + 3, y1);
+                    atomicMin(bb + 4, z0); atomicMax(bb + 5, z1);
+                }
             }
         }
         __syncthreads();

@@ -121,7 +121,7 @@ struct PosTableArgs {
 void launch_pos_tables(const PosTableArgs& a, int grid, cudaStream_t s);
 __host__ __device__ inline int pos_table_size(int K, int cap) {
     int n = 64;
-    while (n < 2 * K && n < cap) n <<= 1;
+    while (n < 4 * K && n < cap) n <<= 1;  // load factor <= 1/4 while it fits
     return n;
 }
 
