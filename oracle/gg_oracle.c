@@ -9,6 +9,7 @@
  * bit-identical to the reference compiled with the specified DFT (oracle/gg_dft.c).
  */
 #include "gg_oracle.h"
+#include "gg_oracle_gb.h"
 #include "gg_dft.h"
 #include "gg_mc_tables.h"
 
@@ -244,8 +245,44 @@ static const int EDGE[12][2] = {{0, 1}, {1, 2}, {2, 3}, {3, 0}, {4, 5}, {5, 6}, 
 /* neighbour-list corner order, marchingCubes.cpp:505-553: (x,y,z),(x+1,y,z),(x+1,y+1,z),(x,y+1,z), then z+1 */
 static const int NBC[8][3] = {{0, 0, 0}, {1, 0, 0}, {1, 1, 0}, {0, 1, 0}, {0, 0, 1}, {1, 0, 1}, {1, 1, 1}, {0, 1, 1}};
 
-int64_t ggo_mc_box(const int32_t box6[6], const double* sdf, const uint32_t* idl, uint32_t own, double h,
-                   double* volume_out, double* surface_out, uint32_t* nbrs, int* n_nbrs, int cap) {
+/* Optional outputs of the hull for the interfacial elements: the distinct neighbour
+ * lists in first-seen order (insertNeighborList, marchingCubes.cpp:605-618), and per
+ * triangle its list key and barycenter (Triangle::computeBarycenter, triangle.h:12-18). */
+typedef struct {
+    uint32_t* lists; /* 8 per list */
+    int nlists, caplists;
+    int* key;
+    double* bary;
+    int ntri, captri;
+} mc_out_t;
+
+static int mc_list_index(mc_out_t* o, const uint32_t* nl) {
+    for (int i = 0; i < o->nlists; i++)
+        if (memcmp(o->lists + 8 * i, nl, 8 * sizeof(uint32_t)) == 0) return i;
+    if (o->nlists == o->caplists) {
+        o->caplists = o->caplists ? 2 * o->caplists : 32;
+        o->lists = (uint32_t*)realloc(o->lists, sizeof(uint32_t) * 8 * o->caplists);
+    }
+    memcpy(o->lists + 8 * o->nlists, nl, 8 * sizeof(uint32_t));
+    return o->nlists++;
+}
+
+static void mc_push_tri(mc_out_t* o, int key, v3 p0, v3 p1, v3 p2) {
+    if (o->ntri == o->captri) {
+        o->captri = o->captri ? 2 * o->captri : 256;
+        o->key = (int*)realloc(o->key, sizeof(int) * o->captri);
+        o->bary = (double*)realloc(o->bary, sizeof(double) * 3 * o->captri);
+    }
+    o->key[o->ntri] = key;
+    o->bary[3 * o->ntri + 0] = (p0.x + p1.x + p2.x) / 3;
+    o->bary[3 * o->ntri + 1] = (p0.y + p1.y + p2.y) / 3;
+    o->bary[3 * o->ntri + 2] = (p0.z + p1.z + p2.z) / 3;
+    o->ntri++;
+}
+
+static int64_t mc_core(const int32_t box6[6], const double* sdf, const uint32_t* idl, uint32_t own, double h,
+                       double* volume_out, double* surface_out, uint32_t* nbrs, int* n_nbrs, int cap,
+                       mc_out_t* col) {
     box_t b = box_from(box6);
     double volume = 0.0, surface = 0.0;
     int64_t ntri = 0;
@@ -283,6 +320,12 @@ int64_t ggo_mc_box(const int32_t box6[6], const double* sdf, const uint32_t* idl
                         lst[cnt++] = id;
                     }
                 }
+                int key = -1;
+                if (col) {
+                    uint32_t nl[8];
+                    for (int q = 0; q < 8; q++) nl[q] = q < cnt ? lst[q] : 0xFFFFFFFFu;
+                    key = mc_list_index(col, nl);
+                }
                 for (int q = 0; q < cnt; q++) { /* recordNewGrains, marchingCubes.cpp:585-603 */
                     if (lst[q] == 0xFFFFFFFFu) continue;
                     int found = 0;
@@ -305,6 +348,7 @@ int64_t ggo_mc_box(const int32_t box6[6], const double* sdf, const uint32_t* idl
                     double bcx = p0.x - p2.x, bcy = p0.y - p2.y, bcz = p0.z - p2.z;
                     double cx = aby * bcz - abz * bcy, cy = abz * bcx - abx * bcz, cz = abx * bcy - aby * bcx;
                     surface += sqrt(cx * cx + (cy * cy + cz * cz)) / 2.0; /* Eigen's unrolled redux: c0 + (c1 + c2) */
+                    if (col) mc_push_tri(col, key, p0, p1, p2);
                     ntri++;
                 }
             }
@@ -312,6 +356,11 @@ int64_t ggo_mc_box(const int32_t box6[6], const double* sdf, const uint32_t* idl
     *surface_out = surface * h * h;
     *n_nbrs = nd;
     return ntri;
+}
+
+int64_t ggo_mc_box(const int32_t box6[6], const double* sdf, const uint32_t* idl, uint32_t own, double h,
+                   double* volume_out, double* surface_out, uint32_t* nbrs, int* n_nbrs, int cap) {
+    return mc_core(box6, sdf, idl, own, h, volume_out, surface_out, nbrs, n_nbrs, cap, NULL);
 }
 
 /* ------------------------------------------------------------------ */
@@ -428,6 +477,7 @@ typedef struct {
     double volume, surface;
     uint32_t* nb;
     int nnb, capnb;
+    hull_t hull;   /* interfacial elements of the last hull (m_explicitHull) */
 } grain_t;
 
 struct ggo_sim {
@@ -435,6 +485,12 @@ struct ggo_sim {
     double h, delta, dt, time_step;
     grain_t* g; /* index 0 = boundary grain (never processed) */
     int64_t last_voxels;
+    /* convolution correction (box.cpp:426-539) */
+    int correction, use_see;
+    gbphys_t ph;
+    quat_t* quats;  /* G + 1, [0] = boundary grain (0, 35 deg, 0), grainhdl.cpp:86 */
+    double* see;    /* m_StoredElasticEnergy, G + 1; the boundary grain's is pinned to 0 */
+    mc_out_t mc;    /* scratch of the hull extraction */
 };
 
 static void push(uint32_t** v, int* n, int* cap, uint32_t x) {
@@ -450,6 +506,15 @@ ggo_sim* ggo_create(int N, int border, double time_step, int n_grains) {
     s->delta = (double)border / (double)N;           /* grainhdl.cpp:1439 */
     s->h = 1 / (double)N;                            /* grainhdl.h:182 */
     s->g = (grain_t*)calloc((size_t)n_grains + 1, sizeof(grain_t));
+    s->quats = (quat_t*)calloc((size_t)n_grains + 1, sizeof(quat_t));
+    s->see = (double*)calloc((size_t)n_grains + 1, sizeof(double));
+    const double bnd[3] = {0, 35 * (3.14159265358979323846 / 180), 0};
+    for (int i = 0; i <= n_grains; i++) s->quats[i] = ggo_euler_to_quat(bnd);
+    s->ph.unique_gb = 1;
+    s->ph.mobility_model = 0;
+    s->ph.tl_drag = 0.0;
+    s->ph.ds = 1 / (double)N;
+    s->ph.quats = s->quats;
     for (int i = 0; i <= n_grains; i++) {
         s->g[i].in.esz = s->g[i].out.esz = sizeof(double);
         s->g[i].idl.esz = sizeof(uint32_t);
@@ -462,8 +527,12 @@ void ggo_destroy(ggo_sim* s) {
     for (int i = 0; i <= s->G; i++) {
         free(s->g[i].in.v); free(s->g[i].out.v); free(s->g[i].idl.v);
         free(s->g[i].cmp); free(s->g[i].son); free(s->g[i].nb);
+        ggo_hull_free(&s->g[i].hull);
     }
     free(s->g);
+    free(s->quats);
+    free(s->see);
+    free(s->mc.lists); free(s->mc.key); free(s->mc.bary);
     free(s);
 }
 
@@ -559,6 +628,63 @@ static void update_lists(ggo_sim* s, int id, uint32_t** cand, int* ncand, int* c
     }
 }
 
+/* The convolution correction of LSbox::executeConvolution (box.cpp:426-535): every
+ * voxel of the output box with |input| < delta moves by the energy x mobility of the
+ * nearest interfacial element towards its IDLocal neighbour, minus the stored-energy
+ * difference when UseStoredElasticEnergy is on.  The point is Vector3d(i, j, k), i.e.
+ * (y, x, z), while the barycenters are (x, y, z) (sic). */
+static void convolution_correction(ggo_sim* s, int id) {
+    grain_t* A = &s->g[id];
+    const box_t ob = A->out.b;
+    const double delta = s->delta;
+    const double ts = 1 / 1.21; /* TimeSlope, grainhdl.cpp:1432 */
+    for (int k = ob.z0; k < ob.z1; k++)
+        for (int i = ob.y0; i < ob.y1; i++)
+            for (int j = ob.x0; j < ob.x1; j++) {
+                const double val = D(&A->in)[at(A->in.b, i, j, k)];
+                if (!(fabs(val) < delta)) continue;
+                const double point[3] = {(double)i, (double)j, (double)k};
+                const uint32_t nb = U(&A->idl)[at(A->idl.b, i, j, k)];
+                double fe, fm;
+                ggo_hull_project(&A->hull, point, nb, &fe, &fm);
+                const size_t q = at(ob, i, j, k);
+                D(&A->out)[q] = val + (D(&A->out)[q] - val) * fe * fm * 1.0;
+                if (s->use_see) {
+                    double f = 0;
+                    const int alive = nb == 0 || (nb <= (uint32_t)s->G && s->g[nb].present);
+                    if (alive) f = (s->see[id] - s->see[nb]) * fm * s->dt / (ts * ts);
+                    D(&A->out)[q] = D(&A->out)[q] - f;
+                }
+            }
+}
+
+void ggo_set_physics(ggo_sim* s, int correction, int unique_gb_energies, int mobility_model, double triple_line_drag,
+                     int use_stored_energy) {
+    s->correction = correction;
+    s->ph.unique_gb = unique_gb_energies;
+    s->ph.mobility_model = mobility_model;
+    s->ph.tl_drag = triple_line_drag;
+    s->use_see = use_stored_energy;
+}
+
+void ggo_set_orientations(ggo_sim* s, const double* euler) {
+    for (int g = 1; g <= s->G; g++) s->quats[g] = ggo_euler_to_quat(euler + 3 * g);
+}
+
+void ggo_set_stored_energy(ggo_sim* s, const double* see) {
+    for (int g = 1; g <= s->G; g++) s->see[g] = see[g];
+}
+
+int ggo_grain_elements(const ggo_sim* s, int id, int counts[4]) {
+    if (id < 1 || id > s->G) return -1;
+    const hull_t* H = &s->g[id].hull;
+    counts[0] = H->gb.n;
+    counts[1] = H->tl.n;
+    counts[2] = H->qj.n;
+    counts[3] = H->hj.n;
+    return 0;
+}
+
 int ggo_step(ggo_sim* s) {
     const int G = s->G, M = s->M, gb = s->gb;
     const double h = s->h, delta = s->delta;
@@ -573,6 +699,7 @@ int ggo_step(ggo_sim* s) {
         ggo_convolve_box(n, s->N, s->time_step, D(&A->in), D(&A->out));
         s->last_voxels += (int64_t)n * n * n;
         buf_resize(&A->idl, A->out.b); /* resizeIDLocalToDistanceBuffer, box.cpp:426 */
+        if (s->correction && s->loop != 0) convolution_correction(s, id);
     }
     /* 3. switchDistancebuffer + updateSecondOrderNeighbors, grainhdl.cpp:852-853 */
     for (int id = 1; id <= G; id++) if (s->g[id].present) switch_in_out(&s->g[id]);
@@ -627,13 +754,19 @@ int ggo_step(ggo_sim* s) {
         for (;;) {
             if (A->capnb < cap) { A->nb = (uint32_t*)realloc(A->nb, sizeof(uint32_t) * cap); A->capnb = cap; }
             int nn = 0;
-            int64_t ntri = ggo_mc_box(ib, D(&A->in), U(&A->idl), (uint32_t)id, h, &A->volume, &A->surface,
-                                      A->nb, &nn, A->capnb);
+            s->mc.nlists = 0;
+            s->mc.ntri = 0;
+            int64_t ntri = mc_core(ib, D(&A->in), U(&A->idl), (uint32_t)id, h, &A->volume, &A->surface, A->nb,
+                                   &nn, A->capnb, s->correction ? &s->mc : NULL);
             if (nn > A->capnb) { cap = nn; continue; }
             A->nnb = nn;
             A->exists = ntri > 0;
             break;
         }
+        /* computeSurfaceElements, box.cpp:1175-1180 (only the correction reads them) */
+        if (A->exists && s->correction)
+            ggo_hull_build(&A->hull, (uint32_t)id, s->mc.nlists, s->mc.lists, s->mc.ntri, s->mc.bary, s->mc.key,
+                           &s->ph);
         if (!A->exists) continue;
         box_t nb = {A->newbox[0], A->newbox[1], A->newbox[2], A->newbox[3], A->newbox[4], A->newbox[5]};
         buf_resize(&A->out, nb);

@@ -40,6 +40,17 @@ int ggo_set_lists(ggo_sim* s, const int64_t* offsets, const uint32_t* ids);
  * R-tree search; the order of members differs). */
 int ggo_default_lists(ggo_sim* s);
 
+/* The convolution correction (box.cpp:426-535; off unless set) with its settings:
+ * UniqueGBEnergies, UseMobilityModel, TripleLineDrag, UseStoredElasticEnergy. */
+void ggo_set_physics(ggo_sim* s, int correction, int unique_gb_energies, int mobility_model,
+                     double triple_line_drag, int use_stored_energy);
+/* Bunge Euler angles (3 per grain, rows 1..G of a (G+1) x 3 array). */
+void ggo_set_orientations(ggo_sim* s, const double* euler);
+/* m_StoredElasticEnergy per grain (entries 1..G of a G+1 array). */
+void ggo_set_stored_energy(ggo_sim* s, const double* see);
+/* Interfacial elements of the grain's last hull: GB, TL, QJ, HJ counts. */
+int ggo_grain_elements(const ggo_sim* s, int id, int counts[4]);
+
 /* One loop iteration (grainhdl.cpp:837-917).  Returns currentNrGrains
  * (countGrains, grainhdl.cpp:936-943) or a negative error. */
 int ggo_step(ggo_sim* s);

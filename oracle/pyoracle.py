@@ -46,6 +46,10 @@ def lib():
         L.ggo_compare_box.argtypes = [vp, i32, vp, vp, vp, vp, vp, i32, i32, dbl]
         L.ggo_set_compare_box.argtypes = [vp, vp, vp, dbl, i32, i32, vp]
         L.ggo_resize_to_cube.argtypes = [vp, i32]
+        L.ggo_set_physics.argtypes = [vp, i32, i32, i32, dbl, i32]
+        L.ggo_set_orientations.argtypes = [vp, vp]
+        L.ggo_set_stored_energy.argtypes = [vp, vp]
+        L.ggo_grain_elements.argtypes = [vp, i32, vp]
         _lib = L
     return _lib
 
@@ -86,6 +90,30 @@ class OracleSim:
         if getattr(self, "_s", None):
             lib().ggo_destroy(self._s)
             self._s = None
+
+    def set_physics(self, correction: bool, unique_energies: bool = True, mobility_model: bool = False,
+                    triple_line_drag: float = 0.0, stored_energy: bool = False) -> None:
+        """The convolution correction and its settings (box.cpp:426-535)."""
+        lib().ggo_set_physics(self._s, int(correction), int(unique_energies), int(mobility_model),
+                              float(triple_line_drag), int(stored_energy))
+
+    def set_orientations(self, euler: np.ndarray) -> None:
+        """Bunge angles per grain, (G, 3) for IDs 1..G."""
+        e = np.zeros((self.G + 1, 3), np.float64)
+        e[1:] = euler
+        lib().ggo_set_orientations(self._s, _p(e))
+
+    def set_stored_energy(self, see: np.ndarray) -> None:
+        """m_StoredElasticEnergy per grain, (G,) for IDs 1..G."""
+        v = np.zeros(self.G + 1, np.float64)
+        v[1:] = see
+        lib().ggo_set_stored_energy(self._s, _p(v))
+
+    def elements(self, gid: int):
+        """(GB, TL, QJ, HJ) counts of the grain's last hull."""
+        c = np.zeros(4, np.int32)
+        lib().ggo_grain_elements(self._s, gid, _p(c))
+        return tuple(int(v) for v in c)
 
     def step(self) -> int:
         return int(lib().ggo_step(self._s))
