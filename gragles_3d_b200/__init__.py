@@ -31,7 +31,7 @@ EXPORTED = [
     "gg_stage_convolution", "gg_stage_update_lists", "gg_stage_comparison", "gg_stage_level_set",
     "gg_stage_redistancing", "gg_get_grain_stats", "gg_get_neighbors", "gg_get_list", "gg_get_sdf",
     "gg_get_idlocal", "gg_grain_count", "gg_loop", "gg_convolve_boxes_f64", "gg_convolve_boxes_mixed",
-    "gg_convolve_boxes_f64_noalloc",
+    "gg_convolve_boxes_f64_noalloc", "gg_set_orientations", "gg_set_stored_energy", "gg_get_elements",
 ]
 
 
@@ -46,7 +46,8 @@ class Params(C.Structure):
         ("domain_size", C.c_int32), ("border", C.c_int32), ("time_step", C.c_double),
         ("n_grains", C.c_int32), ("precision", C.c_int32), ("disable_correction", C.c_int32),
         ("list_capacity", C.c_int32), ("pool_voxels", C.c_int64), ("device", C.c_int32),
-        ("reserved", C.c_int32 * 7),
+        ("unique_gb_energies", C.c_int32), ("mobility_model", C.c_int32), ("use_stored_energy", C.c_int32),
+        ("triple_line_drag", C.c_double), ("hull_capacity", C.c_int32), ("reserved", C.c_int32 * 1),
     ]
 
 
@@ -94,6 +95,9 @@ def load_library(path: str = LIB_PATH):
     L.gg_get_idlocal.restype = i64
     L.gg_convolve_boxes_f64.argtypes = [vp, vp, vp, vp, i32, i32, C.c_double]
     L.gg_convolve_boxes_mixed.argtypes = [vp, vp, vp, vp, i32, i32, C.c_double]
+    L.gg_set_orientations.argtypes = [vp, vp]
+    L.gg_set_stored_energy.argtypes = [vp, vp]
+    L.gg_get_elements.argtypes = [vp, i32, vp]
     _lib = L
     return L
 
@@ -126,15 +130,18 @@ class GrainHandler:
 
     def __init__(self, domain_size: int, border: int, time_step: float, n_grains: int,
                  precision: int = PRECISION_FP64, list_capacity: int = 0, pool_voxels: int = 0,
-                 device: int = 0):
+                 device: int = 0, correction: bool = False, unique_energies: bool = True,
+                 mobility_model: bool = False, stored_energy: bool = False, triple_line_drag: float = 0.0,
+                 hull_capacity: int = 0):
         L = load_library()
         self.G = int(n_grains)
         self.N = int(domain_size)
         self.border = int(border)
         self.M = self.N + 2 * self.border
         self.precision = precision
-        p = Params(domain_size, border, float(time_step), n_grains, precision, 1, list_capacity, pool_voxels,
-                   device)
+        p = Params(domain_size, border, float(time_step), n_grains, precision, int(not correction), list_capacity,
+                   pool_voxels, device, int(unique_energies), int(mobility_model), int(stored_energy),
+                   float(triple_line_drag), hull_capacity)
         h = C.c_void_p()
         rc = L.gg_create(C.byref(p), C.byref(h))
         self._h = h
@@ -174,6 +181,22 @@ class GrainHandler:
 
     def default_lists(self) -> None:
         self._check(load_library().gg_default_lists(self._h))
+
+    def set_orientations(self, euler: np.ndarray) -> None:
+        """Bunge angles (G, 3) in radians for grain IDs 1..G."""
+        e = np.ascontiguousarray(euler, dtype=np.float64)
+        self._check(load_library().gg_set_orientations(self._h, _p(e)))
+
+    def set_stored_energy(self, see: np.ndarray) -> None:
+        """m_StoredElasticEnergy (G,) for grain IDs 1..G."""
+        v = np.ascontiguousarray(see, dtype=np.float64)
+        self._check(load_library().gg_set_stored_energy(self._h, _p(v)))
+
+    def elements(self, gid: int) -> tuple:
+        """(GB, TL, QJ, HJ) element counts of the grain's last hull (correction on)."""
+        c = np.zeros(4, np.int32)
+        self._check(load_library().gg_get_elements(self._h, gid, _p(c)))
+        return tuple(int(v) for v in c)
 
     # --- the loop ---------------------------------------------------------
     def step(self) -> dict:

@@ -73,6 +73,12 @@ struct gg_ctx {
     uint16_t* d_bmat = nullptr;       // the same, split FP16 hi/lo in the tensor-core operand layout
     long long* d_boff = nullptr;
     float* d_cscr = nullptr;          // mixed-path convolution scratch (out's layout)
+    // convolution correction: orientations, stored energies, hull capture, elements
+    bool correction = false;
+    double4* d_quat = nullptr;
+    double* d_see = nullptr;
+    HullCapture hull{};
+    HullElements el{};
     // scalars
     int* d_err = nullptr;
     long long* d_total_vox = nullptr;
@@ -132,12 +138,34 @@ void gaussian_table(int n, int N, double time_step, std::vector<double>& out) {
     }
 }
 
+// myQuaternion::euler2Quaternion (myQuaternion.cpp:168-191), Bunge ZXZ, host libm.
+double4 euler_to_quat(double p1, double t, double p2) {
+    const double co1 = std::cos(t / 2), s1 = std::sin(t / 2);
+    return make_double4(co1 * std::cos((p1 + p2) / 2), s1 * std::cos((p1 - p2) / 2), s1 * std::sin((p1 - p2) / 2),
+                        co1 * std::sin((p1 + p2) / 2));
+}
+
+HullPhysics physics(gg_ctx* ctx);
+
 // Twiddles of the specified DFT: (cos, sin)(2 pi j / n), angle (6.283185307179586 * j) / n.
 void twiddle_table(int n, std::vector<double2>& out) {
     for (int j = 0; j < n; j++) {
         const double a = 6.283185307179586476925286766559 * (double)j / (double)n;
         out.push_back(make_double2(std::cos(a), std::sin(a)));
     }
+}
+
+HullPhysics physics(gg_ctx* ctx) {
+    HullPhysics h{};
+    h.quat = ctx->d_quat;
+    h.see = ctx->d_see;
+    h.unique_gb = ctx->P.unique_gb_energies;
+    h.mobility_model = ctx->P.mobility_model;
+    h.use_see = ctx->P.use_stored_energy;
+    h.tl_drag = ctx->P.triple_line_drag;
+    h.ds = 1 / (double)ctx->N;                        // grainhdl.h:181-183
+    h.dt = ctx->P.time_step / double(ctx->N * ctx->N);  // grainhdl.cpp:1431
+    return h;
 }
 
 int upload_tables(gg_ctx* ctx) {
@@ -191,6 +219,10 @@ int check_err(gg_ctx* ctx, const char* where) {
     if (e & ERR_NEIGHBORS) return fail(ctx, GG_ERR_LIST_OVERFLOW, "%s: hull neighbour capacity exceeded", where);
     if (e & ERR_BOX) return fail(ctx, GG_ERR_UNSUPPORTED, "%s: a box left the grid or exceeded the supported side", where);
     if (e & ERR_TIMEOUT) return fail(ctx, GG_ERR_CUDA, "%s: a bounded tensor-core pipeline wait timed out", where);
+    if (e & ERR_BOUNDS) return fail(ctx, GG_ERR_CUDA, "%s: a kernel bounds check failed (access skipped)", where);
+    if (e & ERR_HULL)
+        return fail(ctx, GG_ERR_POOL_EXHAUSTED, "%s: hull or interfacial-element capacity exceeded (raise hull_capacity)",
+                    where);
     return GG_OK;
 }
 
@@ -291,6 +323,34 @@ int load_state_t(gg_ctx* ctx, const uint32_t* labels) {
     return check_err(ctx, "gg_load_state");
 }
 
+// The convolution correction (box.cpp:426-535) on the convolved boxes of arena p ^ 1,
+// from the input in arena p and the IDLocal of the last comparison (arena q).
+template <typename T>
+int correct_convolution(gg_ctx* ctx) {
+    if (!ctx->correction || ctx->loop == 0) return GG_OK;
+    const int p = ctx->p;
+    CorrectionArgs<T> c{};
+    c.G = ctx->G;
+    c.geo = ctx->geo;
+    c.toff = ctx->d_toff_n;
+    c.present = ctx->d_present;
+    c.box = ctx->d_box[p];
+    c.in = reinterpret_cast<const T*>(ctx->d_arena[p]);
+    c.in_off = ctx->d_off[p];
+    c.out = reinterpret_cast<T*>(ctx->d_arena[p ^ 1]);
+    c.out_off = ctx->d_off[p ^ 1];
+    c.id_old = ctx->d_idarena[ctx->q];
+    c.idbox_old = ctx->d_idbox[ctx->q];
+    c.idoff_old = ctx->d_idoff[ctx->q];
+    c.el = ctx->el;
+    c.ph = physics(ctx);
+    c.err = ctx->d_err;
+    launch_correction<T>(c, ctx->grid, ctx->stream);
+    ctx->launches += 1;
+    CK(cudaGetLastError());
+    return GG_OK;
+}
+
 template <typename T>
 int stage_convolution_t(gg_ctx* ctx) {
     ctx->p ^= 1;  // switchDistancebuffer (gridCoarsement off), grainhdl.cpp:1496
@@ -320,6 +380,7 @@ int stage_convolution_t(gg_ctx* ctx) {
         ctx->launches += 3;
     } else {
         if (umma_supported(ctx->side_max)) {
+            if (!ctx->d_cscr) return fail(ctx, GG_ERR_INVALID, "convolution scratch missing");
             UmmaConvArgs u{};
             u.G = ctx->G;
             u.toff = ctx->d_toff_slab;
@@ -335,7 +396,7 @@ int stage_convolution_t(gg_ctx* ctx) {
             launch_conv_umma(u, ctx->num_sms, ctx->side_max, ctx->stream);
             ctx->launches += 3;
             CK(cudaGetLastError());
-            return GG_OK;
+            return correct_convolution<T>(ctx);
         }
         ConvTCArgs a{};
         a.G = ctx->G;
@@ -352,7 +413,7 @@ int stage_convolution_t(gg_ctx* ctx) {
         ctx->launches += 2;
     }
     CK(cudaGetLastError());
-    return GG_OK;
+    return correct_convolution<T>(ctx);
 }
 
 int stage_update_lists_t(gg_ctx* ctx) {
@@ -469,9 +530,23 @@ int stage_level_set_t(gg_ctx* ctx) {
     a.n_nb = ctx->d_nnb;
     a.nb_cap = kNbCap;
     a.err = ctx->d_err;
+    if (ctx->correction) a.hull = ctx->hull;
     launch_mc<T>(a, ctx->grid, ctx->side_max, ctx->stream);
     ctx->launches += 1;
     CK(cudaGetLastError());
+    if (ctx->correction) {  // computeSurfaceElements, box.cpp:1175-1180
+        ElementArgs e{};
+        e.G = ctx->G;
+        e.toff = ctx->d_toff_mc;
+        e.exists = ctx->d_exists;
+        e.cap = ctx->hull;
+        e.el = ctx->el;
+        e.ph = physics(ctx);
+        e.err = ctx->d_err;
+        launch_elements(e, ctx->num_sms * 4, ctx->stream);
+        ctx->launches += 1;
+        CK(cudaGetLastError());
+    }
     return GG_OK;
 }
 
@@ -586,7 +661,9 @@ void free_all(gg_ctx* c) {
                     c->d_off[0], c->d_off[1], c->d_idarena[0], c->d_idarena[1], c->d_idbox[0], c->d_idbox[1],
                     c->d_idoff[0], c->d_idoff[1], c->d_spec, c->d_spec_off, c->d_toff_n, c->d_toff_slab,
                     c->d_toff_one, c->d_toff_mc, c->d_toff_red, c->d_tw, c->d_tw_off, c->d_gtab, c->d_g_off,
-                    c->d_circ, c->d_circ_off, c->d_bmat, c->d_boff, c->d_cscr, c->d_err, c->d_total_vox, c->d_count3, c->bins.count,
+                    c->d_circ, c->d_circ_off, c->d_bmat, c->d_boff, c->d_cscr, c->d_quat, c->d_see,
+                    c->hull.rec_list, c->hull.rec_ntri, c->hull.bary, c->hull.n_rec, c->hull.n_tri, c->el.n_elem,
+                    c->el.elem, c->el.ids, c->el.segs, c->el.ebary, c->d_err, c->d_total_vox, c->d_count3, c->bins.count,
                     c->bins.off, c->bins.cursor, c->bins.entries, c->bins.max_count};
     for (void* p : ptrs)
         if (p) cudaFree(p);
@@ -615,8 +692,7 @@ int gg_create(const gg_params* params, gg_ctx** out) {
                   P.border, P.n_grains);
     else if (P.precision != GG_PRECISION_FP64 && P.precision != GG_PRECISION_MIXED)
         rc = fail(ctx, GG_ERR_INVALID, "unknown precision mode %d", P.precision);
-    else if (!P.disable_correction)
-        rc = fail(ctx, GG_ERR_UNSUPPORTED, "the convolution correction (DisableConvolutionCorrection=0) is not on this path");
+
     if (rc) {
         *out = ctx;  // keep the message readable through gg_last_error
         return rc;
@@ -629,6 +705,7 @@ int gg_create(const gg_params* params, gg_ctx** out) {
     ctx->esz = ctx->fp64 ? 8 : 4;
     ctx->geo = Geometry{ctx->N, ctx->gb, ctx->M, 1 / (double)ctx->N, ctx->gb / double(ctx->N), P.time_step};
     ctx->list_cap = P.list_capacity > 0 ? P.list_capacity : 4096;
+    ctx->correction = !P.disable_correction;
     ctx->side_limit = supported_side(ctx->fp64);
     *out = ctx;
 #undef CK_RET
@@ -668,6 +745,15 @@ int gg_create(const gg_params* params, gg_ctx** out) {
     CK(dalloc(&ctx->d_err, 1));
     CK(dalloc(&ctx->d_total_vox, 1));
     CK(dalloc(&ctx->d_count3, 3));
+    {
+        std::vector<double4> q(G1, euler_to_quat(0, 0, 0));
+        q[0] = euler_to_quat(0, 35 * (kPi / 180), 0);  // the boundary grain, grainhdl.cpp:86
+        std::vector<double> see(G1, 0.0);
+        CK(dalloc(&ctx->d_quat, G1));
+        CK(dalloc(&ctx->d_see, G1));
+        CK(cudaMemcpy(ctx->d_quat, q.data(), sizeof(double4) * G1, cudaMemcpyHostToDevice));
+        CK(cudaMemcpy(ctx->d_see, see.data(), sizeof(double) * G1, cudaMemcpyHostToDevice));
+    }
     ctx->bins.ntx = (ctx->M + kTX - 1) / kTX;
     ctx->bins.nty = (ctx->M + kTY - 1) / kTY;
     ctx->bins.ntz = (ctx->M + kTZ - 1) / kTZ;
@@ -737,6 +823,28 @@ int gg_load_state(gg_ctx* ctx, const uint32_t* labels, const int32_t* extents, c
     }
     if (ctx->fp64) CK(dalloc(&ctx->d_spec, ctx->spec_capacity));
     else CK(dalloc(&ctx->d_cscr, ctx->pool_voxels));
+    if (ctx->correction) {
+        const long long cap = ctx->P.hull_capacity > 0 ? ctx->P.hull_capacity : 16LL * side * side + 2048;
+        const size_t G1h = (size_t)G + 1;
+        ctx->hull.cap = (int)cap;
+        CK(dalloc(&ctx->hull.rec_list, 8 * cap * G1h));
+        CK(dalloc(&ctx->hull.rec_ntri, cap * G1h));
+        CK(dalloc(&ctx->hull.bary, 3 * cap * G1h));
+        CK(dalloc(&ctx->hull.n_rec, G1h));
+        CK(dalloc(&ctx->hull.n_tri, G1h));
+        ctx->el.elem_cap = 512;
+        ctx->el.id_cap = 4096;
+        ctx->el.seg_cap = 1024;
+        ctx->el.bary_cap = (int)cap;
+        CK(dalloc(&ctx->el.n_elem, G1h));
+        CK(dalloc(&ctx->el.elem, (size_t)ctx->el.elem_cap * G1h));
+        CK(dalloc(&ctx->el.ids, (size_t)ctx->el.id_cap * G1h));
+        CK(dalloc(&ctx->el.segs, (size_t)ctx->el.seg_cap * G1h));
+        CK(dalloc(&ctx->el.ebary, 3 * cap * G1h));
+        CK(cudaMemset(ctx->el.n_elem, 0, sizeof(int) * G1h));
+        CK(cudaMemset(ctx->hull.n_rec, 0, sizeof(int) * G1h));
+        CK(cudaMemset(ctx->hull.n_tri, 0, sizeof(int) * G1h));
+    }
     const size_t G1 = (size_t)G + 1;
     CK(cudaMemcpy(ctx->d_present, present.data(), sizeof(int) * G1, cudaMemcpyHostToDevice));
     CK(cudaMemcpy(ctx->d_exists, present.data(), sizeof(int) * G1, cudaMemcpyHostToDevice));
@@ -925,6 +1033,41 @@ int64_t gg_get_idlocal(gg_ctx* ctx, int32_t id, int32_t box[6], uint32_t* out, i
 
 int gg_grain_count(gg_ctx* ctx) { return ctx ? ctx->grain_count : GG_ERR_INVALID; }
 int gg_loop(gg_ctx* ctx) { return ctx ? ctx->loop : GG_ERR_INVALID; }
+
+int gg_set_orientations(gg_ctx* ctx, const double* euler) {
+    if (!ctx || !euler) return GG_ERR_INVALID;
+    const size_t G1 = (size_t)ctx->G + 1;
+    std::vector<double4> q(G1);
+    q[0] = euler_to_quat(0, 35 * (kPi / 180), 0);
+    for (int g = 1; g <= ctx->G; g++)
+        q[g] = euler_to_quat(euler[3 * (g - 1)], euler[3 * (g - 1) + 1], euler[3 * (g - 1) + 2]);
+    CK(cudaMemcpy(ctx->d_quat, q.data(), sizeof(double4) * G1, cudaMemcpyHostToDevice));
+    return GG_OK;
+}
+
+int gg_set_stored_energy(gg_ctx* ctx, const double* see) {
+    if (!ctx || !see) return GG_ERR_INVALID;
+    std::vector<double> v((size_t)ctx->G + 1, 0.0);
+    for (int g = 1; g <= ctx->G; g++) v[g] = see[g - 1];
+    CK(cudaMemcpy(ctx->d_see, v.data(), sizeof(double) * v.size(), cudaMemcpyHostToDevice));
+    return GG_OK;
+}
+
+int gg_get_elements(gg_ctx* ctx, int32_t id, int32_t counts[4]) {
+    if (!ctx || !ctx->loaded || id < 1 || id > ctx->G || !counts) return GG_ERR_INVALID;
+    counts[0] = counts[1] = counts[2] = counts[3] = 0;
+    if (!ctx->correction) return GG_OK;
+    int ne = 0;
+    CK(cudaStreamSynchronize(ctx->stream));
+    CK(cudaMemcpy(&ne, ctx->el.n_elem + id, sizeof(int), cudaMemcpyDeviceToHost));
+    std::vector<HullElem> e(ne > 0 ? ne : 1);
+    if (ne > 0)
+        CK(cudaMemcpy(e.data(), ctx->el.elem + (size_t)id * ctx->el.elem_cap, sizeof(HullElem) * ne,
+                      cudaMemcpyDeviceToHost));
+    for (int i = 0; i < ne; i++)
+        if (e[i].type >= 1 && e[i].type <= 4) counts[e[i].type - 1]++;
+    return GG_OK;
+}
 
 int gg_convolve_boxes_f64(const double* d_in, double* d_out, const int32_t* sides, const int64_t* offs,
                           int32_t n_boxes, int32_t domain_size, double time_step) {

@@ -23,6 +23,8 @@ enum : int {
     ERR_HASH = 8,        // list-update hash table overflow
     ERR_BOX = 16,        // a box outside the grid or larger than supported
     ERR_TIMEOUT = 32,    // a bounded wait on the tensor-core pipeline gave up
+    ERR_HULL = 64,       // hull capture or interfacial-element capacity exceeded
+    ERR_BOUNDS = 128,    // an index failed a kernel's own bounds check (access skipped)
 };
 
 struct Box {

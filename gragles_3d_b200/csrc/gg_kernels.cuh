@@ -125,6 +125,83 @@ __host__ __device__ inline int pos_table_size(int K, int cap) {
     return n;
 }
 
+// ---- hull of the last level set, for the convolution correction (gg_hull.cu) ----
+// Written by the marching-cubes kernel when the correction is on: per grain, the
+// neighbour list of every active cube in cube order (8 IDs, 0xFFFFFFFF padded) with its
+// triangle count, and every triangle's barycenter in emission order.
+struct HullCapture {
+    int cap;                  // cube records and triangles per grain
+    uint32_t* rec_list;       // (G + 1) x cap x 8
+    int* rec_ntri;            // (G + 1) x cap
+    double* bary;             // (G + 1) x cap x 3
+    int* n_rec;               // G + 1
+    int* n_tri;               // G + 1
+};
+
+// One interfacial element of a grain's mesh (grainHull.cpp:187-531), in the order
+// projectPointToGrainBoundary searches them (high-order junctions, quadruple
+// junctions, triple lines, grain boundaries).
+struct HullElem {
+    int type;                 // 1 GB, 2 TL, 3 QJ, 4 HJ
+    int nids, id_off;         // neighbour IDs in the grain's ID pool
+    int seg_off, nseg;        // barycenter segments (start, count) in the grain's segment pool
+    int pad;
+    double energy, mobility;  // m_energy, m_mobility
+    double lo[3], hi[3];      // bounding box of its barycenters
+};
+
+struct HullElements {
+    int elem_cap, id_cap, seg_cap, bary_cap;
+    int* n_elem;              // G + 1
+    HullElem* elem;           // (G + 1) x elem_cap
+    uint32_t* ids;            // (G + 1) x id_cap
+    int2* segs;               // (G + 1) x seg_cap
+    double* ebary;            // (G + 1) x bary_cap x 3, barycenters grouped by neighbour list
+};
+
+struct HullPhysics {
+    const double4* quat;      // orientation of grain 0..G (0 = the boundary grain)
+    const double* see;        // m_StoredElasticEnergy of grain 0..G
+    int unique_gb;            // Settings::UniqueGBEnergies
+    int mobility_model;       // Settings::UseMobilityModel
+    int use_see;              // Settings::UseStoredElasticEnergy
+    double tl_drag;           // Settings::TripleLineDrag
+    double ds;                // 1 / realDomainSize
+    double dt;                // TimeStepSize / realDomainSize^2
+};
+
+struct ElementArgs {
+    int G;
+    const int* toff;          // one tile per present grain
+    const int* exists;
+    HullCapture cap;
+    HullElements el;
+    HullPhysics ph;
+    int* err;
+};
+void launch_elements(const ElementArgs& a, int grid, cudaStream_t s);
+
+template <typename T>
+struct CorrectionArgs {
+    int G;
+    Geometry geo;
+    const int* toff;          // n tiles per convolved grain (z-slices)
+    const int* present;
+    const int* box;           // current (cubic) boxes
+    const T* in;              // input of the convolution
+    const long long* in_off;
+    T* out;                   // convolved, corrected in place
+    const long long* out_off;
+    const uint32_t* id_old;   // IDLocal of the last comparison, flat-resized onto the box
+    const int* idbox_old;
+    const long long* idoff_old;
+    HullElements el;
+    HullPhysics ph;
+    int* err;
+};
+template <typename T>
+void launch_correction(const CorrectionArgs<T>& a, int grid, cudaStream_t s);
+
 // ---- marching cubes + hull statistics (gg_mc.cu) ----
 template <typename T>
 struct MCArgs {
@@ -143,6 +220,7 @@ struct MCArgs {
     uint32_t* nb;
     int* n_nb;
     int nb_cap;
+    HullCapture hull;         // hull.cap = 0: not captured
     int* err;
 };
 template <typename T>

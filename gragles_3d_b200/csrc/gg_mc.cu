@@ -133,6 +133,9 @@ __global__ void __launch_bounds__(kThreads, 2) mc_kernel(MCArgs<T> a, int slab_b
         const int ncplane = (ncx > 0 && ncy > 0 && ncz > 0) ? ncx * ncy : 0;
         double vol = 0.0, area = 0.0;
         long long ntri = 0;
+        int nrec = 0;  // active cubes so far (hull capture)
+        const bool capture = a.hull.cap > 0;
+        const long long hbase = (long long)g * a.hull.cap;
         const int nxb = b.nx(), plane = b.nx() * b.ny();
         // Slabs of LZ cube layers: the sign bytes of their LZ + 1 voxel layers are staged
         // with one coalesced load per voxel, then every cube is classified from shared
@@ -248,6 +251,17 @@ __global__ void __launch_bounds__(kThreads, 2) mc_kernel(MCArgs<T> a, int slab_b
                     const V3 p0 = vl[gg_mc_tri_table[ci][3 * q]];
                     const V3 p1 = vl[gg_mc_tri_table[ci][3 * q + 1]];
                     const V3 p2 = vl[gg_mc_tri_table[ci][3 * q + 2]];
+                    if (capture) {  // Triangle::computeBarycenter, triangle.h:12-18
+                        const long long ti = ntri + off + q;
+                        if (ti < a.hull.cap) {
+                            double* bb = a.hull.bary + 3 * (hbase + ti);
+                            bb[0] = (p0.x + p1.x + p2.x) / 3;
+                            bb[1] = (p0.y + p1.y + p2.y) / 3;
+                            bb[2] = (p0.z + p1.z + p2.z) / 3;
+                        } else {
+                            atomicOr(a.err, ERR_HULL);
+                        }
+                    }
                     // GrainHull::computeGrainVolume, grainHull.cpp:42-51
                     const double v321 = p2.x * p1.y * p0.z;
                     const double v231 = p1.x * p2.y * p0.z;
@@ -279,6 +293,17 @@ __global__ void __launch_bounds__(kThreads, 2) mc_kernel(MCArgs<T> a, int slab_b
                 }
                 const unsigned ck = (unsigned)c << 3;
                 for (int q = 0; q < cnt; q++) hash_insert(hkey, hval, lst[q], ck | q, a.err);
+                if (capture) {  // the cube's list, in cube order, for the interfacial elements
+                    const int ri = nrec + ia;
+                    if (ri < a.hull.cap) {
+                        uint32_t* rl = a.hull.rec_list + 8 * (hbase + ri);
+#pragma unroll
+                        for (int q = 0; q < 8; q++) rl[q] = q < cnt ? lst[q] : 0xFFFFFFFFu;
+                        a.hull.rec_ntri[hbase + ri] = nt;
+                    } else {
+                        atomicOr(a.err, ERR_HULL);
+                    }
+                }
             }
             __syncthreads();
             if (threadIdx.x == 0) {
@@ -290,6 +315,7 @@ __global__ void __launch_bounds__(kThreads, 2) mc_kernel(MCArgs<T> a, int slab_b
             ntri += chunk_total;
             __syncthreads();
           }
+          nrec += n_act;
         }
         // collect the distinct IDs and order them by first appearance
         for (int q = threadIdx.x; q < kHash; q += blockDim.x) {
@@ -311,6 +337,10 @@ __global__ void __launch_bounds__(kThreads, 2) mc_kernel(MCArgs<T> a, int slab_b
         if (threadIdx.x == 0) {
             if (nf > a.nb_cap) atomicOr(a.err, ERR_NEIGHBORS);
             a.n_nb[g] = nf;
+            if (capture) {
+                a.hull.n_rec[g] = nrec < a.hull.cap ? nrec : a.hull.cap;
+                a.hull.n_tri[g] = ntri < a.hull.cap ? (int)ntri : a.hull.cap;
+            }
             const double h = a.geo.h;
             a.volume[g] = fabs(vol) * h * h * h;
             a.surface[g] = area * h * h;

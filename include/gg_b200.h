@@ -44,11 +44,16 @@ typedef struct {
     double time_step;           /* TimeStepSize */
     int32_t n_grains;           /* NumberOfParticles */
     int32_t precision;          /* GG_PRECISION_* */
-    int32_t disable_correction; /* DisableConvolutionCorrection (must be 1 on this path) */
+    int32_t disable_correction; /* DisableConvolutionCorrection (0 = the correction, box.cpp:426-535) */
     int32_t list_capacity;      /* comparison-list capacity per grain (0 = 4096) */
     int64_t pool_voxels;        /* voxels per SDF arena (0 = 2x the initial total) */
     int32_t device;             /* CUDA device ordinal */
-    int32_t reserved[7];
+    int32_t unique_gb_energies; /* UniqueGBEnergies (correction only) */
+    int32_t mobility_model;     /* UseMobilityFactor -> Settings::UseMobilityModel (correction only) */
+    int32_t use_stored_energy;  /* UseStoredElasticEnergy (correction only) */
+    double triple_line_drag;    /* TripleLineDrag (correction only) */
+    int32_t hull_capacity;      /* triangles kept per hull for the correction (0 = 16 side^2 + 2048) */
+    int32_t reserved[1];
 } gg_params;
 
 /* Per-step report (the reference prints the same stage times, grainhdl.cpp:920-933). */
@@ -109,6 +114,20 @@ int64_t gg_get_sdf(gg_ctx* ctx, int32_t id, int32_t which, int32_t box[6], doubl
 int64_t gg_get_idlocal(gg_ctx* ctx, int32_t id, int32_t box[6], uint32_t* out, int64_t cap);
 int gg_grain_count(gg_ctx* ctx);
 int gg_loop(gg_ctx* ctx);
+
+/* Grain orientations for the convolution correction's boundary energies and
+ * mobilities: Bunge Euler angles phi1, PHI, phi2 in radians, 3 per grain for IDs
+ * 1..n_grains (the .uds columns read at grainhdl.cpp:480-504, turned into
+ * quaternions as myQuaternion::euler2Quaternion, myQuaternion.cpp:168-191).  The
+ * boundary grain 0 has (0, 35 deg, 0) (grainhdl.cpp:86).  Default: all (0, 0, 0). */
+int gg_set_orientations(gg_ctx* ctx, const double* euler);
+/* m_StoredElasticEnergy per grain for IDs 1..n_grains (box.cpp:232-233 computes it from
+ * the .uds column as DislocEnPerM * value / HAGB_Energy * Physical_Domain_Size).
+ * The boundary grain's, indeterminate in the reference, is 0. */
+int gg_set_stored_energy(gg_ctx* ctx, const double* see);
+/* Interfacial elements of the grain's last hull (computeSurfaceElements,
+ * box.cpp:1175-1180) as counts {GB, TL, QJ, HJ}; only kept with the correction on. */
+int gg_get_elements(gg_ctx* ctx, int32_t id, int32_t counts[4]);
 
 /* Single-box stage kernels on caller-owned device memory (stream 0 of the current
  * device), for testing each kernel against the oracle on arbitrary inputs.
