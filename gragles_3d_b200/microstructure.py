@@ -177,7 +177,8 @@ def write_parameters(path: str, *, n_grains: int, border: int = 10, steps: int =
                      raw_name: str = "Container.raw", uds_name: str = "Microstructure.uds",
                      breakup: int = 0, threads: int = 8, correction: bool = False,
                      unique_energies: bool = True, mobility_factor: bool = False,
-                     stored_energy: bool = False, analysis_every: int = 1000000) -> None:
+                     stored_energy: bool = False, triple_line_drag: float = 1e6,
+                     analysis_every: int = 1000000) -> None:
     """A ``parameters.xml`` for the reference (Settings.cpp:81-270) in mode 4.
 
     ``NumberOfParticles`` must already hold the grain count: the reference sizes
@@ -190,7 +191,7 @@ def write_parameters(path: str, *, n_grains: int, border: int = 10, steps: int =
         "BreakupNumber": breakup, "DiscreteSamplingRate": 25, "DomainBorderSize": border,
         "MicrostructureGenMode": 4, "ReadFromFilename": raw_name, "AdditionalFilename": uds_name,
         "HAGB_Energy": "1.", "HAGB_Mobility": "7.5e-14", "DislocEnPerM": "2.5e-10",
-        "Physical_Domain_Size": "2.52e-4", "TripleLineDrag": "1.e6",
+        "Physical_Domain_Size": "2.52e-4", "TripleLineDrag": repr(float(triple_line_drag)),
         "UseMobilityFactor": int(mobility_factor), "UseStoredElasticEnergy": int(stored_energy),
         "UseMagneticField": 0, "DisableConvolutionCorrection": int(not correction),
         "UseTexture": 0, "ExecuteInParallel": 1, "MaximumNumberOfThreads": threads,

@@ -5,6 +5,9 @@ specified DFT standing in for MKL) runs on seeded voxelised microstructures; the
 observation hooks record the initial state and, every step, each grain's
 existence, volume, surface, box, hull neighbours (first-seen order) and
 comparison list, plus single-box buffers of one grain around every stage.
+The "correction" case turns on the convolution correction (box.cpp:426-535) with
+a mix of low-angle and random orientations, the mobility model, a weak
+triple-line drag and stored elastic energies.
 
     python tests/golden/make_golden.py
 """
@@ -28,7 +31,26 @@ CASES = {
     # name: (N, grains, border, seed, steps, grain whose buffers are kept, loop of those buffers)
     "tiny": (32, 20, 5, 1032, 6, 14, 2),
     "vanish": (40, 150, 5, 1040, 40, 0, 0),
+    "correction": (32, 30, 5, 2032, 8, 0, 0),
 }
+
+# physics of the cases that run the convolution correction
+PHYSICS = {
+    "correction": dict(unique_energies=False, mobility_factor=True, stored_energy=True, triple_line_drag=20.0),
+}
+
+
+def textured(ms, seed):
+    """70 % of the grains within a few degrees of one orientation (Read-Shockley
+    energies and mobility factors well below 1), the rest random; log-normal
+    stored energies."""
+    G = ms.n_grains
+    rng = np.random.default_rng(seed)
+    low = rng.random(G) < 0.7
+    ms.euler[:] = np.where(low[:, None], np.array([0.3, 0.5, 0.2]) + rng.normal(0, 0.08, (G, 3)),
+                           np.stack([rng.uniform(0, 2 * np.pi, G), rng.uniform(0, np.pi, G),
+                                     rng.uniform(0, 2 * np.pi, G)], 1))
+    ms.stored_energy[:] = rng.lognormal(0, 0.5, G) * 1e5
 
 
 def ragged(d: dict, G: int):
@@ -43,12 +65,21 @@ def ragged(d: dict, G: int):
 
 def make(name, N, G, border, seed, steps, keep_grain, keep_loop):
     ms = msgen.voronoi(N, G, seed=seed)
+    phys = PHYSICS.get(name)
+    if phys:
+        textured(ms, seed)
     with tempfile.TemporaryDirectory() as d:
         msgen.write_mode4(ms, d)
-        msgen.write_parameters(os.path.join(d, "parameters.xml"), n_grains=G, border=border, steps=steps)
+        msgen.write_parameters(os.path.join(d, "parameters.xml"), n_grains=G, border=border, steps=steps,
+                               correction=bool(phys), **(phys or {}))
         res, _ = refdump.run_case(d, threads=4, grains=str(keep_grain) if keep_grain else None,
                                   loops=str(keep_loop) if keep_grain else None)
     out = {"N": N, "G": G, "border": border, "seed": seed, "steps": steps}
+    if phys:
+        out["euler"] = ms.euler.copy()
+        out["uds_stored_energy"] = ms.stored_energy.copy()
+        for k, v in phys.items():
+            out["phys_" + k] = v
     out["init_list_off"], out["init_list_ids"] = ragged(res["init_list"], G)
     loops = sorted(res["stats"])
     S = len(loops)

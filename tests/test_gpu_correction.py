@@ -8,6 +8,8 @@ oracle's element counts and hull neighbours exactly and its volumes to 1e-9
 (energies use CUDA's acos/log/exp/pow, a few ULP from libm); the mixed path's
 volumes stay within 1e-3.
 """
+import os
+
 import numpy as np
 import pytest
 
@@ -68,6 +70,40 @@ def test_correction_fp64_matches_oracle(gpu, oracle):
             assert gh.elements(g) == osim.elements(g), f"step {s} grain {g}: elements"
         assert worst <= 1e-9, f"step {s}: relative volume error {worst:.3g}"
         assert rep["grain_count"] == sum(osim.info(g)["present"] for g in range(1, G + 1))
+
+
+def test_correction_fp64_matches_reference_golden(gpu):
+    """The GPU against the compiled reference's own run of the correction case
+    (tests/golden/correction.npz): existence, boxes and neighbour sets exact,
+    volumes and surfaces within 1e-9 relative."""
+    d = dict(np.load(os.path.join(os.path.dirname(__file__), "golden", "correction.npz")))
+    N, G, border = int(d["N"]), int(d["G"]), int(d["border"])
+    ms = msgen.voronoi(N, G, seed=int(d["seed"]))
+    ext, counts = ms.grain_extents()
+    gh = gpu.GrainHandler(N, border, 0.2, G, precision=gpu.PRECISION_FP64, correction=True,
+                          unique_energies=bool(d["phys_unique_energies"]),
+                          mobility_model=bool(d["phys_mobility_factor"]),
+                          stored_energy=bool(d["phys_stored_energy"]),
+                          triple_line_drag=float(d["phys_triple_line_drag"]))
+    gh.load(ms.labels, ext, counts)
+    gh.set_lists(d["init_list_off"], d["init_list_ids"])
+    gh.set_orientations(d["euler"])
+    # m_StoredElasticEnergy = DislocEnPerM * storedEnergy / HAGB_Energy * Physical_Domain_Size
+    gh.set_stored_energy(2.5e-10 * d["uds_stored_energy"] / 1.0 * 2.52e-4)
+    nb_base = np.concatenate([[0], np.cumsum(d["nb_len"])])
+    for s in range(d["exists"].shape[0]):
+        gh.step()
+        st = gh.stats()
+        nb_ids = d["nb_ids"][nb_base[s]:nb_base[s + 1]]
+        for g in range(1, G + 1):
+            assert bool(st.exists[g]) == bool(d["exists"][s, g]), f"loop {s} grain {g}: exists"
+            if not st.exists[g]:
+                continue
+            assert tuple(st.boxes[g]) == tuple(d["box"][s, g]), f"loop {s} grain {g}: box"
+            assert abs(st.volume[g] - d["volume"][s, g]) <= 1e-9 * d["volume"][s, g], f"loop {s} grain {g}: volume"
+            assert abs(st.surface[g] - d["surface"][s, g]) <= 1e-9 * d["surface"][s, g], f"loop {s} grain {g}: surface"
+            want = nb_ids[d["nb_off"][s][g]:d["nb_off"][s][g + 1]]
+            assert np.array_equal(gh.neighbors(g), want), f"loop {s} grain {g}: neighbours"
 
 
 def test_correction_mixed_volume_tolerance(gpu, oracle):

@@ -71,15 +71,34 @@ def _ragged(off, ids, g):
     return ids[off[g]:off[g + 1]]
 
 
-@pytest.mark.parametrize("name", ["tiny", "vanish"])
-def test_restatement_matches_reference_golden(oracle, name):
+def golden_stored_energy(d):
+    """m_StoredElasticEnergy = DislocEnPerM * storedEnergy / HAGB_Energy *
+    Physical_Domain_Size (box.cpp:232-233) for the fixture's .uds column."""
+    return 2.5e-10 * d["uds_stored_energy"] / 1.0 * 2.52e-4
+
+
+def golden_sim(oracle, d):
     from gragles_3d_b200 import microstructure as msgen
 
-    d = _load(name)
     N, G, border, seed = int(d["N"]), int(d["G"]), int(d["border"]), int(d["seed"])
     ms = msgen.voronoi(N, G, seed=seed)
     ext, counts = ms.grain_extents()
     sim = oracle.OracleSim(N, border, 0.2, ms.labels, ext, counts, lists=(d["init_list_off"], d["init_list_ids"]))
+    if "euler" in d:
+        sim.set_physics(True, unique_energies=bool(d["phys_unique_energies"]),
+                        mobility_model=bool(d["phys_mobility_factor"]),
+                        triple_line_drag=float(d["phys_triple_line_drag"]),
+                        stored_energy=bool(d["phys_stored_energy"]))
+        sim.set_orientations(d["euler"])
+        sim.set_stored_energy(golden_stored_energy(d))
+    return sim
+
+
+@pytest.mark.parametrize("name", ["tiny", "vanish", "correction"])
+def test_restatement_matches_reference_golden(oracle, name):
+    d = _load(name)
+    G = int(d["G"])
+    sim = golden_sim(oracle, d)
     nb_base = np.concatenate([[0], np.cumsum(d["nb_len"])])
     li_base = np.concatenate([[0], np.cumsum(d["list_len"])])
     for s in range(d["exists"].shape[0]):
