@@ -663,7 +663,8 @@ void free_all(gg_ctx* c) {
                     c->d_toff_one, c->d_toff_mc, c->d_toff_red, c->d_tw, c->d_tw_off, c->d_gtab, c->d_g_off,
                     c->d_circ, c->d_circ_off, c->d_bmat, c->d_boff, c->d_cscr, c->d_quat, c->d_see,
                     c->hull.rec_list, c->hull.rec_ntri, c->hull.bary, c->hull.n_rec, c->hull.n_tri, c->el.n_elem,
-                    c->el.elem, c->el.ids, c->el.segs, c->el.ebary, c->d_err, c->d_total_vox, c->d_count3, c->bins.count,
+                    c->el.elem, c->el.ids, c->el.segs, c->el.ebary, c->el.chunks, c->el.n_idx, c->el.idx_key, c->el.idx_rng,
+                    c->el.idx_elem, c->d_err, c->d_total_vox, c->d_count3, c->bins.count,
                     c->bins.off, c->bins.cursor, c->bins.entries, c->bins.max_count};
     for (void* p : ptrs)
         if (p) cudaFree(p);
@@ -841,7 +842,16 @@ int gg_load_state(gg_ctx* ctx, const uint32_t* labels, const int32_t* extents, c
         CK(dalloc(&ctx->el.ids, (size_t)ctx->el.id_cap * G1h));
         CK(dalloc(&ctx->el.segs, (size_t)ctx->el.seg_cap * G1h));
         CK(dalloc(&ctx->el.ebary, 3 * cap * G1h));
+        ctx->el.chunk_cap = (int)(cap / kHullChunk) + ctx->el.seg_cap;
+        ctx->el.idx_cap = 256;
+        ctx->el.pair_cap = 2048;
+        CK(dalloc(&ctx->el.chunks, (size_t)ctx->el.chunk_cap * G1h));
+        CK(dalloc(&ctx->el.n_idx, G1h));
+        CK(dalloc(&ctx->el.idx_key, (size_t)ctx->el.idx_cap * G1h));
+        CK(dalloc(&ctx->el.idx_rng, (size_t)ctx->el.idx_cap * G1h));
+        CK(dalloc(&ctx->el.idx_elem, (size_t)ctx->el.pair_cap * G1h));
         CK(cudaMemset(ctx->el.n_elem, 0, sizeof(int) * G1h));
+        CK(cudaMemset(ctx->el.n_idx, 0, sizeof(int) * G1h));
         CK(cudaMemset(ctx->hull.n_rec, 0, sizeof(int) * G1h));
         CK(cudaMemset(ctx->hull.n_tri, 0, sizeof(int) * G1h));
     }

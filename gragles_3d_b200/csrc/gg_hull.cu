@@ -31,6 +31,11 @@ constexpr double kPi = 3.14159265358979323846;  // ggLS.h:25
 constexpr int kLMax = 256;    // distinct neighbour lists (= elements) per hull
 constexpr int kJIds = 48;     // IDs of one (merged) junction
 constexpr unsigned kNoId = 0xFFFFFFFFu;
+constexpr int kLHash = 2 * kLMax;  // slots of the distinct-list hash (power of two)
+constexpr unsigned kFull = 0xFFFFFFFFu;
+constexpr int kIdxMax = 256;       // distinct neighbour IDs the elements of one hull search
+constexpr int kIHash = 2 * kIdxMax;
+constexpr int kPairMax = 2048;     // (element, searched ID) pairs of one hull
 
 // ---------------------------------------------------------------------------------
 // misorientation and boundary properties
@@ -121,8 +126,52 @@ struct ElemSmem {
     double energy[kLMax], mobility[kLMax];
     Junction jn[kLMax];  // working junctions
     int qlist[kLMax], hlist[kLMax];
-    int nl, nq, nh, nj;
+    int lslot[kLHash];  // list hash: index into lists, -1 empty
+    // neighbour ID -> elements index under construction
+    unsigned ikey[kIHash];
+    short iden[kIHash];          // dense ID index of the slot
+    uint32_t dkey[kIdxMax];
+    int dcnt[kIdxMax], dlast[kIdxMax], doff[kIdxMax];
+    unsigned short pe[kPairMax]; // (element, dense ID) pairs in search order
+    unsigned short pd[kPairMax];
+    int nl, nq, nh, nj, ne, nch, nd, np;
 };
+
+// FNV-1a over the eight IDs of a cube's sorted list
+__device__ __forceinline__ unsigned list_hash(const uint32_t (&L)[8]) {
+    unsigned h = 2166136261u;
+#pragma unroll
+    for (int q = 0; q < 8; q++) h = (h ^ L[q]) * 16777619u;
+    return h ^ (h >> 15);
+}
+
+__device__ __forceinline__ bool same_list(const uint32_t* A, const uint32_t (&L)[8]) {
+    bool eq = true;
+#pragma unroll
+    for (int q = 0; q < 8; q++) eq = eq && A[q] == L[q];
+    return eq;
+}
+
+// Index of list L among the distinct lists so far, or -1.
+__device__ int find_list(const ElemSmem& S, const uint32_t (&L)[8], unsigned h) {
+    unsigned s = h & (kLHash - 1);
+    for (int probe = 0; probe < kLHash; probe++) {
+        const int k = S.lslot[s];
+        if (k < 0) return -1;
+        if (same_list(S.lists[k], L)) return k;
+        s = (s + 1) & (kLHash - 1);
+    }
+    return -1;
+}
+
+__device__ void insert_list(ElemSmem& S, unsigned h, int k, int* err) {
+    unsigned s = h & (kLHash - 1);
+    for (int probe = 0; probe < kLHash; probe++) {
+        if (atomicCAS(&S.lslot[s], -1, k) == -1) return;
+        s = (s + 1) & (kLHash - 1);
+    }
+    atomicOr(err, ERR_HULL);
+}
 
 // The junction's position: the mean of its barycenters in member order
 // (QuadrupleJunction / HighOrderJunction::computePosition, InterfacialElement.cpp:394-406)
@@ -171,66 +220,127 @@ __global__ void __launch_bounds__(32) elements_kernel(ElementArgs a) {
         int* rec_ntri = a.cap.rec_ntri + cb;
         const double* bary = a.cap.bary + 3 * cb;
         double* eb = a.el.ebary + 3 * (long long)g * a.el.bary_cap;
-        if (lane == 0) S.nl = 0;
-        __syncwarp();
         // 1. distinct lists in first-seen order (MarchingCubesAlgorithm::insertNeighborList,
-        //    marchingCubes.cpp:605-618); the key goes into the record's upper bits
-        for (int r = 0; r < nrec; r++) {
+        //    marchingCubes.cpp:605-618), 32 records at a time: lanes holding the same list
+        //    follow the lowest of them, which looks the list up among the earlier ones; new
+        //    lists take the next keys in lane order.  The key goes into the record's upper bits.
+        for (int q = lane; q < kLHash; q += 32) S.lslot[q] = -1;
+        int nl = 0;
+        __syncwarp();
+        for (int base = 0; base < nrec; base += 32) {
+            const int r = base + lane;
+            const bool valid = r < nrec;
             uint32_t mine[8];
 #pragma unroll
-            for (int q = 0; q < 8; q++) mine[q] = rec_list[8 * r + q];
-            const int nl = S.nl;
-            int found = -1;
-            for (int base = 0; base < nl && found < 0; base += 32) {
-                const int c = base + lane;
-                bool eq = c < nl;
+            for (int q = 0; q < 8; q++) mine[q] = valid ? rec_list[8 * (long long)r + q] : kNoId;
+            const unsigned h = list_hash(mine);
+            const unsigned vmask = __ballot_sync(kFull, valid);
+            const unsigned peers = __match_any_sync(kFull, h) & vmask;
+            const int leader = valid ? __ffs(peers) - 1 : lane;
+            bool same = true;
 #pragma unroll
-                for (int q = 0; q < 8; q++) eq = eq && S.lists[c < nl ? c : 0][q] == mine[q];
-                const unsigned m = __ballot_sync(0xffffffffu, eq);
-                if (m) found = base + __ffs(m) - 1;
-            }
-            if (found < 0) {
-                found = nl;
-                if (nl < kLMax) {
-                    if (lane < 8) S.lists[nl][lane] = mine[lane];
-                    if (lane == 0) S.nl = nl + 1;
-                } else if (lane == 0) {
-                    atomicOr(a.err, ERR_HULL);
+            for (int q = 0; q < 8; q++) same = same && __shfl_sync(kFull, mine[q], leader) == mine[q];
+            int found = -1;
+            if (__any_sync(kFull, valid && !same)) {
+                // two lists of this chunk share a hash: one record at a time
+                for (int src = 0; src < 32; src++) {
+                    if (!((vmask >> src) & 1)) break;
+                    uint32_t L[8];
+#pragma unroll
+                    for (int q = 0; q < 8; q++) L[q] = __shfl_sync(kFull, mine[q], src);
+                    const unsigned hs = __shfl_sync(kFull, h, src);
+                    int k = find_list(S, L, hs);
+                    if (k < 0) {
+                        k = nl < kLMax ? nl : 0;
+                        if (nl < kLMax) {
+                            if (lane < 8) S.lists[nl][lane] = L[lane];
+                            __syncwarp();
+                            if (lane == 0) insert_list(S, hs, nl, a.err);
+                        } else if (lane == 0) {
+                            atomicOr(a.err, ERR_HULL);
+                        }
+                        nl++;
+                    }
+                    if (lane == src) found = k;
+                    __syncwarp();
                 }
+            } else {
+                const bool lead = valid && leader == lane;
+                if (lead) found = find_list(S, mine, h);
+                const bool fresh = lead && found < 0;
+                const unsigned fm = __ballot_sync(kFull, fresh);
+                if (fresh) {
+                    const int k = nl + __popc(fm & ((1u << lane) - 1));
+                    if (k < kLMax) {
+#pragma unroll
+                        for (int q = 0; q < 8; q++) S.lists[k][q] = mine[q];
+                        insert_list(S, h, k, a.err);
+                        found = k;
+                    } else {
+                        atomicOr(a.err, ERR_HULL);
+                        found = 0;
+                    }
+                }
+                nl += __popc(fm);
+                found = __shfl_sync(kFull, found, leader);
             }
-            if (lane == 0) rec_ntri[r] = (rec_ntri[r] & 0xFF) | ((found < kLMax ? found : 0) << 8);
+            if (valid) rec_ntri[r] = (rec_ntri[r] & 0xFF) | ((found < kLMax && found >= 0 ? found : 0) << 8);
             __syncwarp();
         }
-        const int nl = S.nl;
+        if (nl > kLMax) nl = kLMax;
+        if (lane == 0) S.nl = nl;
         // 2. triangles per list and the grouped offsets
-        for (int k = lane; k < nl; k += 32) S.cnt[k] = 0;
+        for (int k = lane; k < nl; k += 32) {
+            S.cnt[k] = 0;
+            S.fill[k] = 0;
+            S.next_key[k] = -1;
+        }
+        __syncwarp();
+        for (int r = lane; r < nrec; r += 32) atomicAdd(&S.cnt[rec_ntri[r] >> 8], rec_ntri[r] & 0xFF);
         __syncwarp();
         if (lane == 0) {
-            for (int r = 0; r < nrec; r++) S.cnt[rec_ntri[r] >> 8] += rec_ntri[r] & 0xFF;
             int run = 0;
             for (int k = 0; k < nl; k++) {
                 S.off[k] = run;
-                S.fill[k] = 0;
-                S.next_key[k] = -1;
                 run += S.cnt[k];
             }
             if (run > a.el.bary_cap) atomicOr(a.err, ERR_HULL);
         }
         __syncwarp();
-        // 3. barycenters grouped by list, in triangle order (subDivideTrianglesToInterfacialElements)
-        if (lane == 0) {
-            int t = 0;
-            for (int r = 0; r < nrec; r++) {
-                const int k = rec_ntri[r] >> 8, nt = rec_ntri[r] & 0xFF;
-                for (int q = 0; q < nt; q++, t++) {
-                    const int pos = S.off[k] + S.fill[k]++;
-                    if (pos < a.el.bary_cap && t < ntri) {
-                        eb[3 * pos] = bary[3 * t];
-                        eb[3 * pos + 1] = bary[3 * t + 1];
-                        eb[3 * pos + 2] = bary[3 * t + 2];
-                    }
+        // 3. barycenters grouped by list, in triangle order (subDivideTrianglesToInterfacialElements):
+        //    a record's triangles go after those of the earlier records of its list
+        for (int base = 0, tbase = 0; base < nrec; base += 32) {
+            const int r = base + lane;
+            const bool valid = r < nrec;
+            const int v = valid ? rec_ntri[r] : 0;
+            const int k = valid ? (v >> 8) : -1;
+            const int nt = v & 0xFF;
+            int incl = nt;
+#pragma unroll
+            for (int o = 1; o < 32; o <<= 1) {
+                const int u = __shfl_up_sync(kFull, incl, o);
+                if (lane >= o) incl += u;
+            }
+            const int t0 = tbase + incl - nt;
+            tbase += __shfl_sync(kFull, incl, 31);
+            const unsigned peers = __match_any_sync(kFull, k);
+            int before = 0;
+            for (int src = 0; src < 32; src++) {
+                const int w = __shfl_sync(kFull, nt, src);
+                if (src < lane && ((peers >> src) & 1)) before += w;
+            }
+            const int dst = valid ? S.off[k] + S.fill[k] + before : 0;
+            __syncwarp();
+            if (valid && 31 - __clz(peers) == lane) S.fill[k] += before + nt;
+            for (int q = 0; q < nt; q++) {
+                const int pos = dst + q, t = t0 + q;
+                if (pos < a.el.bary_cap && t < ntri) {
+                    eb[3 * (long long)pos] = bary[3 * (long long)t];
+                    eb[3 * (long long)pos + 1] = bary[3 * (long long)t + 1];
+                    eb[3 * (long long)pos + 2] = bary[3 * (long long)t + 2];
                 }
             }
+            __syncwarp();
         }
         // 4. one element per list: energy and mobility (computeGrainBoundaryElements)
         for (int k = lane; k < nl; k += 32) {
@@ -344,23 +454,28 @@ __global__ void __launch_bounds__(32) elements_kernel(ElementArgs a) {
                 }
         }
         __syncwarp();
-        // 6. the element table in search order: HJ, QJ, TL, GB
+        // 6. the element table in search order: HJ, QJ, TL, GB, with its barycenter
+        //    segments cut into chunks, and the (element, searched ID) pairs
+        for (int q = lane; q < kIHash; q += 32) S.ikey[q] = kNoId;
+        __syncwarp();
         if (lane == 0) {
             HullElem* E = a.el.elem + (long long)g * a.el.elem_cap;
             uint32_t* ids = a.el.ids + (long long)g * a.el.id_cap;
             int2* segs = a.el.segs + (long long)g * a.el.seg_cap;
-            int ne = 0, ni = 0, ns = 0;
+            HullChunk* chunks = a.el.chunks + (long long)g * a.el.chunk_cap;
+            int ne = 0, ni = 0, ns = 0, nch = 0, nd = 0, np = 0;
             bool over = false;
             auto emit = [&](int type, const uint32_t* id_src, int nid, int head, bool chained, double en, double mo) {
                 if (ne >= a.el.elem_cap || ni + nid > a.el.id_cap) { over = true; return; }
-                HullElem& e = E[ne++];
+                HullElem& e = E[ne];
                 e.type = type;
                 e.id_off = ni;
                 e.nids = nid;
                 for (int q = 0; q < nid; q++) ids[ni++] = id_src[q];
                 e.seg_off = ns;
                 e.nseg = 0;
-                double lo[3] = {1e300, 1e300, 1e300}, hi[3] = {-1e300, -1e300, -1e300};
+                e.chunk_off = nch;
+                e.nchunk = 0;
                 for (int k = head; k >= 0; k = chained ? S.next_key[k] : -1) {
                     if (ns >= a.el.seg_cap) { over = true; break; }
                     if (k >= kLMax || S.off[k] < 0 || S.off[k] + S.cnt[k] > a.el.bary_cap) {
@@ -369,19 +484,46 @@ __global__ void __launch_bounds__(32) elements_kernel(ElementArgs a) {
                     }
                     segs[ns++] = make_int2(S.off[k], S.cnt[k]);
                     e.nseg++;
-                    for (int i = 0; i < S.cnt[k]; i++)
-                        for (int c = 0; c < 3; c++) {
-                            const double v = eb[3 * (long long)(S.off[k] + i) + c];
-                            lo[c] = fmin(lo[c], v);
-                            hi[c] = fmax(hi[c], v);
-                        }
+                    for (int c0 = 0; c0 < S.cnt[k]; c0 += kHullChunk) {
+                        if (nch >= a.el.chunk_cap) { over = true; break; }
+                        chunks[nch].start = S.off[k] + c0;
+                        chunks[nch].count = min(kHullChunk, S.cnt[k] - c0);
+                        nch++;
+                        e.nchunk++;
+                    }
                 }
                 e.energy = en;
                 e.mobility = mo;
-                for (int c = 0; c < 3; c++) {
-                    e.lo[c] = lo[c];
-                    e.hi[c] = hi[c];
+                // the IDs projectPointToGrainBoundary compares: all for a high-order
+                // junction, else the first 3 (QJ), 2 (TL), 1 (GB); each element once per ID
+                const int nc = type == 4 ? nid : min(nid, type);
+                for (int q = 0; q < nc; q++) {
+                    const uint32_t id = id_src[q];
+                    unsigned hs = (id * 2654435761u) & (kIHash - 1);
+                    int d = -1;
+                    for (int probe = 0; probe < kIHash; probe++) {
+                        if (S.ikey[hs] == id) { d = S.iden[hs]; break; }
+                        if (S.ikey[hs] == kNoId) {
+                            if (nd >= kIdxMax) break;
+                            S.ikey[hs] = id;
+                            S.iden[hs] = (short)nd;
+                            S.dkey[nd] = id;
+                            S.dcnt[nd] = 0;
+                            S.dlast[nd] = -1;
+                            d = nd++;
+                            break;
+                        }
+                        hs = (hs + 1) & (kIHash - 1);
+                    }
+                    if (d < 0 || np >= kPairMax) { over = true; break; }
+                    if (S.dlast[d] == ne) continue;
+                    S.dlast[d] = ne;
+                    S.dcnt[d]++;
+                    S.pe[np] = (unsigned short)ne;
+                    S.pd[np] = (unsigned short)d;
+                    np++;
                 }
+                ne++;
             };
             for (int i = 0; i < S.nh; i++) {
                 const Junction& J = S.jn[S.hlist[i]];
@@ -405,8 +547,71 @@ __global__ void __launch_bounds__(32) elements_kernel(ElementArgs a) {
                             if ((uint32_t)g != S.lists[k][q]) nb[nn++] = S.lists[k][q];
                     emit(pass, nb, nn, k, false, S.energy[k], S.mobility[k]);
                 }
+            // the index: IDs with their element ranges, elements in search order
+            int run = 0;
+            for (int d = 0; d < nd; d++) {
+                S.doff[d] = run;
+                run += S.dcnt[d];
+                S.dcnt[d] = 0;
+            }
+            if (run > a.el.pair_cap) over = true;
+            unsigned short* pairs = a.el.idx_elem + (long long)g * a.el.pair_cap;
+            for (int q = 0; q < np; q++) {
+                const int d = S.pd[q];
+                const int at = S.doff[d] + S.dcnt[d]++;
+                if (at < a.el.pair_cap) pairs[at] = S.pe[q];
+            }
             if (over) atomicOr(a.err, ERR_HULL);
             a.el.n_elem[g] = ne;
+            a.el.n_idx[g] = nd;
+            S.ne = ne;
+            S.nch = nch;
+            S.nd = nd;
+        }
+        __syncwarp();
+        {
+            const int ne = S.ne, nch = S.nch, nd = S.nd;
+            HullElem* E = a.el.elem + (long long)g * a.el.elem_cap;
+            HullChunk* chunks = a.el.chunks + (long long)g * a.el.chunk_cap;
+            uint32_t* ikey = a.el.idx_key + (long long)g * a.el.idx_cap;
+            int2* irng = a.el.idx_rng + (long long)g * a.el.idx_cap;
+            for (int d = lane; d < nd && d < a.el.idx_cap; d += 32) {
+                ikey[d] = S.dkey[d];
+                irng[d] = make_int2(S.doff[d], S.dcnt[d]);
+            }
+            // chunk bounding boxes, then element boxes from their chunks (min/max: exact in any order)
+            for (int c = lane; c < nch; c += 32) {
+                HullChunk& C = chunks[c];
+                double lo[3] = {1e300, 1e300, 1e300}, hi[3] = {-1e300, -1e300, -1e300};
+                const double* b = eb + 3 * (long long)C.start;
+                for (int i = 0; i < C.count; i++)
+#pragma unroll
+                    for (int q = 0; q < 3; q++) {
+                        lo[q] = fmin(lo[q], b[3 * i + q]);
+                        hi[q] = fmax(hi[q], b[3 * i + q]);
+                    }
+#pragma unroll
+                for (int q = 0; q < 3; q++) {
+                    C.lo[q] = lo[q];
+                    C.hi[q] = hi[q];
+                }
+            }
+            __syncwarp();
+            for (int e = lane; e < ne; e += 32) {
+                HullElem& el = E[e];
+                double lo[3] = {1e300, 1e300, 1e300}, hi[3] = {-1e300, -1e300, -1e300};
+                for (int c = el.chunk_off; c < el.chunk_off + el.nchunk; c++)
+#pragma unroll
+                    for (int q = 0; q < 3; q++) {
+                        lo[q] = fmin(lo[q], chunks[c].lo[q]);
+                        hi[q] = fmax(hi[q], chunks[c].hi[q]);
+                    }
+#pragma unroll
+                for (int q = 0; q < 3; q++) {
+                    el.lo[q] = lo[q];
+                    el.hi[q] = hi[q];
+                }
+            }
         }
         __syncwarp();
     }
@@ -416,62 +621,143 @@ __global__ void __launch_bounds__(32) elements_kernel(ElementArgs a) {
 // the correction
 // ---------------------------------------------------------------------------------
 
-// projectPointToGrainBoundary: the nearest barycenter among the elements holding id;
-// returns (m_energy, m_mobility) of its element, (1, 1) when none holds id.
-__device__ void project(const HullElements& el, int g, const double* p, uint32_t id, double& E, double& M,
-                        int* err) {
-    int ne = el.n_elem[g];
-    if (ne < 0 || ne > el.elem_cap) {
-        atomicOr(err, ERR_BOUNDS);
-        ne = 0;
-    }
-    const HullElem* elem = el.elem + (long long)g * el.elem_cap;
-    const uint32_t* ids = el.ids + (long long)g * el.id_cap;
-    const int2* segs = el.segs + (long long)g * el.seg_cap;
-    const double* eb = el.ebary + 3 * (long long)g * el.bary_cap;
-    double best = 10000000.0;
-    E = 1.;
-    M = 1.;
-    for (int i = 0; i < ne; i++) {
-        const HullElem& e = elem[i];
-        // the IDs the reference compares: all for a high-order junction, else 3, 2, 1
-        const int nc = e.type == 4 ? e.nids : min(e.nids, e.type);
-        if (e.id_off < 0 || nc < 0 || e.id_off + nc > el.id_cap || e.seg_off < 0 || e.nseg < 0 ||
-            e.seg_off + e.nseg > el.seg_cap) {
-            atomicOr(err, ERR_BOUNDS);
+constexpr int kCHash = 512;  // slots of a CTA's ID -> elements hash (>= 2 kIdxMax)
+
+// Squared distance of (x, y, z) to b, summed as Vector3d::squaredNorm (c0 + (c1 + c2)).
+__device__ __forceinline__ double sqdist3(double x, double y, double z, const double* b) {
+    const double d0 = x - b[0], d1 = y - b[1], d2 = z - b[2];
+    return d0 * d0 + (d1 * d1 + d2 * d2);
+}
+
+// Can a barycenter inside [lo, hi], in element e, beat the best (distance, element)
+// so far?  The distance to the clamped point is computed like the barycenter
+// distances, and rounding is monotone, so no barycenter in the box has a computed
+// distance below it.
+__device__ __forceinline__ bool may_beat(double x, double y, double z, const double* lo, const double* hi,
+                                         double best, int e, int win) {
+    const double c[3] = {x < lo[0] ? lo[0] : (x > hi[0] ? hi[0] : x), y < lo[1] ? lo[1] : (y > hi[1] ? hi[1] : y),
+                         z < lo[2] ? lo[2] : (z > hi[2] ? hi[2] : z)};
+    const double lb = sqdist3(x, y, z, c);
+    return lb < best || (lb == best && e < win);
+}
+
+constexpr int kCThreads = 256;
+constexpr int kCVox = 4096;           // voxels of one pass over a slice (whole rows)
+constexpr unsigned short kNoD = 0xFFFF;
+
+// projectPointToGrainBoundary (grainHull.cpp:570-660) searches the elements holding id
+// in order and keeps a barycenter only when strictly nearer than every earlier one: the
+// winner is the least (distance, element index) over all candidates, whatever order
+// they are visited in.  A warp searches for 32 voxels with the same IDLocal neighbour
+// at once (a packet): the candidate elements and chunks are the same for all, a box is
+// skipped when no lane's voxel can beat its best through it, and every barycenter load
+// is a broadcast.  (best, win, wb) comes in as any candidate already known, or (1e7,
+// -1, -1), and leaves as the winner and its barycenter.
+__device__ __forceinline__ void project_packet(const HullElem* __restrict__ elem,
+                                               const HullChunk* __restrict__ chunks, const double* __restrict__ eb,
+                                               const unsigned short* __restrict__ pairs, int2 rng, bool active,
+                                               double x, double y, double z, const HullElements& el, int ne,
+                                               double& best, int& win, int& wb, int* err) {
+    for (int c = 0; c < rng.y; c++) {
+        const int e = pairs[rng.x + c];
+        if (e >= ne) {
+            if ((threadIdx.x & 31) == 0) atomicOr(err, ERR_BOUNDS);
             continue;
         }
-        bool found = false;
-        for (int q = 0; q < nc; q++) found |= ids[e.id_off + q] == id;
-        if (!found) continue;
-        // lower bound of every barycenter's distance: none can beat best if it is >= best
-        double lo[3];
-        for (int c = 0; c < 3; c++) lo[c] = p[c] < e.lo[c] ? e.lo[c] : (p[c] > e.hi[c] ? e.hi[c] : p[c]);
-        if (sqdist(p, lo) >= best) continue;
-        for (int sgi = 0; sgi < e.nseg; sgi++) {
-            const int2 sg = segs[e.seg_off + sgi];
-            if (sg.x < 0 || sg.y < 0 || sg.x + sg.y > el.bary_cap) {
-                atomicOr(err, ERR_BOUNDS);
+        const HullElem& E = elem[e];
+        if (!__any_sync(kFull, active && may_beat(x, y, z, E.lo, E.hi, best, e, win))) continue;
+        const int c0 = E.chunk_off, c1 = E.chunk_off + E.nchunk;
+        if (c0 < 0 || c1 > el.chunk_cap) {
+            if ((threadIdx.x & 31) == 0) atomicOr(err, ERR_BOUNDS);
+            continue;
+        }
+        for (int ch = c0; ch < c1; ch++) {
+            const HullChunk& C = chunks[ch];
+            if (!__any_sync(kFull, active && may_beat(x, y, z, C.lo, C.hi, best, e, win))) continue;
+            if (C.start < 0 || C.count < 0 || C.start + C.count > el.bary_cap) {
+                if ((threadIdx.x & 31) == 0) atomicOr(err, ERR_BOUNDS);
                 continue;
             }
-            for (int b = 0; b < sg.y; b++) {
-                const double d = sqdist(p, eb + 3 * (long long)(sg.x + b));
-                if (d < best) {
+            const double* b = eb + 3 * (long long)C.start;
+            for (int i = 0; i < C.count; i++) {
+                const double d = sqdist3(x, y, z, b + 3 * i);
+                if (d < best || (d == best && e < win)) {
                     best = d;
-                    E = e.energy;
-                    M = e.mobility;
+                    win = e;
+                    wb = C.start + i;
                 }
             }
         }
     }
 }
 
+// The update of one band voxel, box.cpp:476-533, given the element that won (-1: none).
 template <typename T>
-__global__ void __launch_bounds__(128) correction_kernel(CorrectionArgs<T> a) {
-    const double delta = a.geo.delta;
+__device__ __forceinline__ void correct_voxel(const CorrectionArgs<T>& a, const HullElem* elem, int g, int win,
+                                              uint32_t id, double val, T* outp) {
     const double ts = 1 / 1.21;  // TimeSlope, grainhdl.cpp:1432
+    const double E = win >= 0 ? elem[win].energy : 1.0, M = win >= 0 ? elem[win].mobility : 1.0;
+    // GBInfo(m_energy, m_mobility) fills (mobility, energy): field energy = M, field mobility = E
+    const double fe = M, fm = E;
+    double o = val + ((double)*outp - val) * fe * fm * 1.0;
+    if (a.ph.use_see) {
+        const bool alive = id == 0 || (id <= (uint32_t)a.G && a.present[id]);
+        const double fs = alive ? (a.ph.see[g] - a.ph.see[id]) * fm * a.ph.dt / (ts * ts) : 0.0;
+        o = o - fs;
+    }
+    *outp = (T)o;
+}
+
+// A CTA per (grain, z-slice): the band voxels of a pass (whole rows, <= kCVox voxels)
+// are grouped by IDLocal neighbour (counting sort in shared memory), then the warps take
+// packets of 32 voxels of one neighbour.
+template <typename T>
+__global__ void __launch_bounds__(kCThreads, 2) correction_kernel(CorrectionArgs<T> a) {
+    __shared__ uint32_t hkey[kCHash];
+    __shared__ unsigned short hden[kCHash];
+    __shared__ int2 drng[kIdxMax];
+    __shared__ int dcnt[kIdxMax], doff[kIdxMax], dcur[kIdxMax], dpk[kIdxMax + 1];
+    __shared__ unsigned short vd[kCVox];     // dense neighbour index of the pass's voxels, kNoD: no search
+    __shared__ unsigned short vlist[kCVox];  // pass voxels grouped by neighbour
+    const double delta = a.geo.delta;
+    const HullElements& el = a.el;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
+    int staged = -1;  // grain whose index is in shared memory (the same in every thread)
+    int nd = 0;
     for (TileWalk w(a.toff, a.G, blockIdx.x, gridDim.x); w.valid(); w.next()) {
         const int g = w.g;
+        const int ne = min(max(el.n_elem[g], 0), el.elem_cap);
+        // the winner of this lane's last packet, a first bound for the next one of the
+        // same neighbour (packets of a neighbour follow its voxels in row order)
+        if (staged != g) {  // the grain's neighbour -> elements index in shared memory
+            __syncthreads();
+            for (int q = threadIdx.x; q < kCHash; q += blockDim.x) hkey[q] = kNoId;
+            nd = el.n_idx[g];
+            if (nd < 0 || nd > el.idx_cap || nd > kIdxMax) {
+                if (threadIdx.x == 0) atomicOr(a.err, ERR_BOUNDS);
+                nd = 0;
+            }
+            __syncthreads();
+            for (int d = threadIdx.x; d < nd; d += blockDim.x) {
+                const uint32_t id = el.idx_key[(long long)g * el.idx_cap + d];
+                int2 r = el.idx_rng[(long long)g * el.idx_cap + d];
+                if (r.x < 0 || r.y < 0 || r.x + r.y > el.pair_cap) {
+                    atomicOr(a.err, ERR_BOUNDS);
+                    r = make_int2(0, 0);
+                }
+                drng[d] = r;
+                unsigned hs = (id * 2654435761u) & (kCHash - 1);
+                for (int probe = 0; probe < kCHash; probe++) {
+                    if (atomicCAS(&hkey[hs], kNoId, id) == kNoId) {
+                        hden[hs] = (unsigned short)d;
+                        break;
+                    }
+                    hs = (hs + 1) & (kCHash - 1);
+                }
+            }
+            __syncthreads();
+            staged = g;
+        }
         const Box b = load_box(a.box + 6 * g);
         const int k = b.z0 + w.local;
         const Box bo = load_box(a.idbox_old + 6 * g);
@@ -479,26 +765,106 @@ __global__ void __launch_bounds__(128) correction_kernel(CorrectionArgs<T> a) {
         const T* in = a.in + a.in_off[g];
         T* out = a.out + a.out_off[g];
         const uint32_t* idl = a.id_old + a.idoff_old[g];
+        const HullElem* elem = el.elem + (long long)g * el.elem_cap;
+        const HullChunk* chunks = el.chunks + (long long)g * el.chunk_cap;
+        const double* eb = el.ebary + 3 * (long long)g * el.bary_cap;
+        const unsigned short* pairs = el.idx_elem + (long long)g * el.pair_cap;
         const int nx = b.nx(), ny = b.ny();
-        for (int q = threadIdx.x; q < nx * ny; q += blockDim.x) {
-            const int i = b.y0 + q / nx, j = b.x0 + q % nx;
-            const long long f = b.at(i, j, k);
-            const double val = (double)in[f];
-            if (!(fabs(val) < delta)) continue;
-            // IDLocal flat-resized onto the box (dimensionalBuffer.h:120-131)
-            const uint32_t id = f < old_count ? idl[f] : 0u;
-            const double p[3] = {(double)i, (double)j, (double)k};  // Vector3d(i, j, k), box.cpp:481
-            double E, M;
-            project(a.el, g, p, id, E, M, a.err);
-            // GBInfo(m_energy, m_mobility) fills (mobility, energy): field energy = M, field mobility = E
-            const double fe = M, fm = E;
-            double o = val + ((double)out[f] - val) * fe * fm * 1.0;
-            if (a.ph.use_see) {
-                const bool alive = id == 0 || (id <= (uint32_t)a.G && a.present[id]);
-                const double fs = alive ? (a.ph.see[g] - a.ph.see[id]) * fm * a.ph.dt / (ts * ts) : 0.0;
-                o = o - fs;
+        if (nx > kCVox) {
+            if (threadIdx.x == 0) atomicOr(a.err, ERR_BOX);
+            continue;
+        }
+        const int R = kCVox / nx;
+        int prev_d = -1, prev_e = -1, prev_b = -1;
+        for (int yp = 0; yp < ny; yp += R) {
+            const int nv = min(R, ny - yp) * nx;
+            for (int d = threadIdx.x; d < nd; d += blockDim.x) dcnt[d] = 0;
+            __syncthreads();
+            // band voxels: their neighbour; voxels whose neighbour no element holds get (1, 1) now
+            for (int q = threadIdx.x; q < nv; q += blockDim.x) {
+                const int i = b.y0 + yp + q / nx, j = b.x0 + q % nx;
+                const long long f = b.at(i, j, k);
+                const double val = (double)in[f];
+                unsigned short dd = kNoD;
+                if (fabs(val) < delta) {
+                    // IDLocal flat-resized onto the box (dimensionalBuffer.h:120-131)
+                    const uint32_t id = f < old_count ? idl[f] : 0u;
+                    unsigned hs = (id * 2654435761u) & (kCHash - 1);
+                    for (int probe = 0; probe < kCHash; probe++) {
+                        const uint32_t key = hkey[hs];
+                        if (key == id) { dd = hden[hs]; break; }
+                        if (key == kNoId) break;
+                        hs = (hs + 1) & (kCHash - 1);
+                    }
+                    if (dd != kNoD) atomicAdd(&dcnt[dd], 1);
+                    else correct_voxel(a, elem, g, -1, id, val, out + f);
+                }
+                vd[q] = dd;
             }
-            out[f] = (T)o;
+            __syncthreads();
+            if (warp == 0) {  // bucket offsets and packet counts: warp scans over the neighbours
+                int run = 0, prun = 0;
+                for (int d0 = 0; d0 < nd; d0 += 32) {
+                    const int d = d0 + lane;
+                    const int c = d < nd ? dcnt[d] : 0, pk = (c + 31) >> 5;
+                    int ic = c, ip = pk;
+#pragma unroll
+                    for (int o = 1; o < 32; o <<= 1) {
+                        const int u = __shfl_up_sync(kFull, ic, o), v = __shfl_up_sync(kFull, ip, o);
+                        if (lane >= o) { ic += u; ip += v; }
+                    }
+                    if (d < nd) {
+                        doff[d] = dcur[d] = run + ic - c;
+                        dpk[d] = prun + ip - pk;
+                    }
+                    run += __shfl_sync(kFull, ic, 31);
+                    prun += __shfl_sync(kFull, ip, 31);
+                }
+                if (lane == 0) dpk[nd] = prun;
+            }
+            __syncthreads();
+            for (int q = threadIdx.x; q < nv; q += blockDim.x) {
+                const unsigned short dd = vd[q];
+                if (dd != kNoD) vlist[atomicAdd(&dcur[dd], 1)] = (unsigned short)q;
+            }
+            __syncthreads();
+            const int P = dpk[nd];
+            for (int pk = warp; pk < P; pk += nwarps) {
+                int lo = 0, hi = nd - 1;  // the neighbour whose packets hold pk
+                while (lo < hi) {
+                    const int mid = (lo + hi + 1) >> 1;
+                    if (dpk[mid] <= pk) lo = mid;
+                    else hi = mid - 1;
+                }
+                const int d = lo;
+                const int start = doff[d] + ((pk - dpk[d]) << 5);
+                const int cnt = min(32, doff[d] + dcnt[d] - start);
+                const bool active = lane < cnt;
+                const int q = vlist[start + (active ? lane : 0)];
+                const int i = b.y0 + yp + q / nx, j = b.x0 + q % nx;
+                const long long f = b.at(i, j, k);
+                double best = 10000000.0;
+                int win = -1, wb = -1;
+                if (d == prev_d && prev_e >= 0 && prev_b >= 0) {
+                    const double s = sqdist3((double)i, (double)j, (double)k, eb + 3 * (long long)prev_b);
+                    if (s < best) {  // the reference keeps only distances below its 1e7 start
+                        best = s;
+                        win = prev_e;
+                        wb = prev_b;
+                    }
+                }
+                // the point is Vector3d(i, j, k), box.cpp:481
+                project_packet(elem, chunks, eb, pairs, drng[d], active, (double)i, (double)j, (double)k, el, ne,
+                               best, win, wb, a.err);
+                if (active) {
+                    prev_d = d;
+                    prev_e = win;
+                    prev_b = wb;
+                    const uint32_t id = f < old_count ? idl[f] : 0u;
+                    correct_voxel(a, elem, g, win, id, (double)in[f], out + f);
+                }
+            }
+            __syncthreads();
         }
     }
 }

@@ -145,18 +145,33 @@ struct HullElem {
     int type;                 // 1 GB, 2 TL, 3 QJ, 4 HJ
     int nids, id_off;         // neighbour IDs in the grain's ID pool
     int seg_off, nseg;        // barycenter segments (start, count) in the grain's segment pool
+    int chunk_off, nchunk;    // barycenter chunks (each inside one segment) in the chunk pool
     int pad;
     double energy, mobility;  // m_energy, m_mobility
     double lo[3], hi[3];      // bounding box of its barycenters
 };
 
+// At most kHullChunk consecutive barycenters of one segment with their bounding box:
+// the correction skips a chunk whose box is no nearer than the best barycenter so far.
+constexpr int kHullChunk = 16;
+struct HullChunk {
+    double lo[3], hi[3];
+    int start, count;         // barycenters [start, start + count) of the grouped array
+};
+
 struct HullElements {
-    int elem_cap, id_cap, seg_cap, bary_cap;
+    int elem_cap, id_cap, seg_cap, bary_cap, chunk_cap, idx_cap, pair_cap;
     int* n_elem;              // G + 1
     HullElem* elem;           // (G + 1) x elem_cap
     uint32_t* ids;            // (G + 1) x id_cap
     int2* segs;               // (G + 1) x seg_cap
     double* ebary;            // (G + 1) x bary_cap x 3, barycenters grouped by neighbour list
+    HullChunk* chunks;        // (G + 1) x chunk_cap
+    // neighbour ID -> the elements whose searched IDs hold it, in search order
+    int* n_idx;               // G + 1: distinct IDs
+    uint32_t* idx_key;        // (G + 1) x idx_cap
+    int2* idx_rng;            // (G + 1) x idx_cap: (first, count) in idx_elem
+    unsigned short* idx_elem; // (G + 1) x pair_cap
 };
 
 struct HullPhysics {
