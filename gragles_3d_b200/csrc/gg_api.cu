@@ -73,6 +73,8 @@ struct gg_ctx {
     uint16_t* d_bmat = nullptr;       // the same, split FP16 hi/lo in the tensor-core operand layout
     long long* d_boff = nullptr;
     float* d_cscr = nullptr;          // mixed-path convolution scratch (out's layout)
+    unsigned char* d_elscr = nullptr; // element build: per-CTA junction and pair scratch
+    int elscr_ctas = 0;
     // convolution correction: orientations, stored energies, hull capture, elements
     bool correction = false;
     double4* d_quat = nullptr;
@@ -95,7 +97,7 @@ struct gg_ctx {
     int grain_count = 0, live = 0;
     int side_max = 0;      // largest box side of the current layout
     int side_limit = 0;    // largest side the shared-memory kernels accept
-    int list_cap = 4096, slab = 8, hash_cap = 8192;
+    int list_cap = 4096, slab = 8;
     long long launches = 0;  // kernels launched by this context
     cudaEvent_t ev[7] = {};
 };
@@ -428,7 +430,6 @@ int stage_update_lists_t(gg_ctx* ctx) {
     a.cmp = ctx->d_cmp;
     a.n_cmp = ctx->d_ncmp;
     a.list_cap = ctx->list_cap;
-    a.hash_cap = ctx->hash_cap;
     a.err = ctx->d_err;
     launch_update_lists(a, ctx->grid, ctx->stream);
     // m_secondOrderNeighbours = m_comparisonList (box.cpp:895), once every list is rebuilt
@@ -542,8 +543,10 @@ int stage_level_set_t(gg_ctx* ctx) {
         e.cap = ctx->hull;
         e.el = ctx->el;
         e.ph = physics(ctx);
+        e.scratch = ctx->d_elscr;
+        e.scratch_ctas = ctx->elscr_ctas;
         e.err = ctx->d_err;
-        launch_elements(e, ctx->num_sms * 4, ctx->stream);
+        launch_elements(e, ctx->elscr_ctas, ctx->stream);
         ctx->launches += 1;
         CK(cudaGetLastError());
     }
@@ -661,7 +664,7 @@ void free_all(gg_ctx* c) {
                     c->d_off[0], c->d_off[1], c->d_idarena[0], c->d_idarena[1], c->d_idbox[0], c->d_idbox[1],
                     c->d_idoff[0], c->d_idoff[1], c->d_spec, c->d_spec_off, c->d_toff_n, c->d_toff_slab,
                     c->d_toff_one, c->d_toff_mc, c->d_toff_red, c->d_tw, c->d_tw_off, c->d_gtab, c->d_g_off,
-                    c->d_circ, c->d_circ_off, c->d_bmat, c->d_boff, c->d_cscr, c->d_quat, c->d_see,
+                    c->d_circ, c->d_circ_off, c->d_bmat, c->d_boff, c->d_cscr, c->d_elscr, c->d_quat, c->d_see,
                     c->hull.rec_list, c->hull.rec_ntri, c->hull.bary, c->hull.n_rec, c->hull.n_tri, c->el.n_elem,
                     c->el.elem, c->el.ids, c->el.segs, c->el.ebary, c->el.chunks, c->el.n_idx, c->el.idx_key, c->el.idx_rng,
                     c->el.idx_elem, c->d_err, c->d_total_vox, c->d_count3, c->bins.count,
@@ -693,6 +696,9 @@ int gg_create(const gg_params* params, gg_ctx** out) {
                   P.border, P.n_grains);
     else if (P.precision != GG_PRECISION_FP64 && P.precision != GG_PRECISION_MIXED)
         rc = fail(ctx, GG_ERR_INVALID, "unknown precision mode %d", P.precision);
+    else if (list_smem_bytes(P.n_grains) > 227 * 1024)
+        rc = fail(ctx, GG_ERR_UNSUPPORTED, "%d grains: the list update's ID bitmaps exceed shared memory",
+                  P.n_grains);
 
     if (rc) {
         *out = ctx;  // keep the message readable through gg_last_error
@@ -850,6 +856,8 @@ int gg_load_state(gg_ctx* ctx, const uint32_t* labels, const int32_t* extents, c
         CK(dalloc(&ctx->el.idx_key, (size_t)ctx->el.idx_cap * G1h));
         CK(dalloc(&ctx->el.idx_rng, (size_t)ctx->el.idx_cap * G1h));
         CK(dalloc(&ctx->el.idx_elem, (size_t)ctx->el.pair_cap * G1h));
+        ctx->elscr_ctas = ctx->num_sms * 8;
+        CK(dalloc(&ctx->d_elscr, elements_scratch_per_cta() * ctx->elscr_ctas));
         CK(cudaMemset(ctx->el.n_elem, 0, sizeof(int) * G1h));
         CK(cudaMemset(ctx->el.n_idx, 0, sizeof(int) * G1h));
         CK(cudaMemset(ctx->hull.n_rec, 0, sizeof(int) * G1h));

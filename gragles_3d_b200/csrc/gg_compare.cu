@@ -216,6 +216,9 @@ struct TileSmem {
     T* topv;            // [part][voxel][kTop], the merged list in part 0
     unsigned char* topi;
     int* ncand;         // covering entries with value > -1, per voxel
+    unsigned* umask;    // 8 words: entries among some voxel's kTop candidates
+    unsigned char* ulist;  // those entries, ascending
+    int* nu;            // their count
 };
 
 template <typename T>
@@ -232,7 +235,10 @@ __device__ TileSmem<T> carve(unsigned char* base, int mcap) {
     s.bbox = reinterpret_cast<int*>(p); p += 24 * mcap;
     s.tsize = reinterpret_cast<int*>(p); p += 4 * mcap;
     s.ncand = reinterpret_cast<int*>(p); p += 4 * kTV * kParts;
+    s.umask = reinterpret_cast<unsigned*>(p); p += 4 * 8;
+    s.nu = reinterpret_cast<int*>(p); p += 16;
     s.pos = reinterpret_cast<unsigned short*>(p); p += 2 * (size_t)mcap * mcap;
+    s.ulist = p; p += 256;
     s.topi = p;
     return s;
 }
@@ -260,6 +266,22 @@ __device__ __forceinline__ void top_insert(T (&tv)[kTop], int (&ti)[kTop], T w, 
 }
 
 __device__ __forceinline__ unsigned pos_home(uint32_t id, int size) { return (id * 2654435761u) & (unsigned)(size - 1); }
+
+// Position of grain b in grain a's comparison list (a's position table of tsize slots),
+// or kNotListed.
+template <typename T>
+__device__ unsigned short list_position(const CompareArgs<T>& a, uint32_t ga, int tsize, uint32_t gb) {
+    const unsigned long long* tab = a.pos_table + (long long)ga * a.pos_cap;
+    unsigned h = pos_home(gb, tsize);
+    for (int probe = 0; probe < tsize; probe++) {
+        const unsigned long long e = __ldg(tab + h);
+        const uint32_t k = (uint32_t)(e >> 32);
+        if (k == gb) return (unsigned short)(e & 0xFFFFu);
+        if (k == kNone) return kNotListed;
+        h = (h + 1) & (unsigned)(tsize - 1);
+    }
+    return kNotListed;
+}
 
 template <typename T>
 __global__ void __launch_bounds__(kThreads, 4) compare_kernel(CompareArgs<T> a) {
@@ -292,56 +314,7 @@ __global__ void __launch_bounds__(kThreads, 4) compare_kernel(CompareArgs<T> a) 
             s.bbox[6 * e + 2] = INT_MAX; s.bbox[6 * e + 3] = INT_MIN;
             s.bbox[6 * e + 4] = INT_MAX; s.bbox[6 * e + 5] = INT_MIN;
         }
-        __syncthreads();
-        {  // pos[a][b] = position of b in a's list, from a's position table; kBatch
-           // lookups advance together, each round issuing all their next probes at once
-            constexpr int kBatch = 4;
-            const int mm = m * m;
-            for (int q0 = 0; q0 < mm; q0 += kBatch * kThreads) {
-                unsigned long long e[kBatch];
-                const unsigned long long* tab[kBatch];
-                unsigned h[kBatch], mask[kBatch];
-                uint32_t id[kBatch];
-                bool live[kBatch];
-#pragma unroll
-                for (int u = 0; u < kBatch; u++) {
-                    const int q = q0 + u * kThreads + threadIdx.x;
-                    const int ea = q / m, eb = q - ea * m;
-                    live[u] = q < mm && ea != eb;
-                    if (q < mm && ea == eb) s.pos[q] = kNotListed;
-                    tab[u] = nullptr;
-                    h[u] = mask[u] = id[u] = 0;
-                    e[u] = 0;
-                    if (live[u]) {
-                        tab[u] = a.pos_table + (long long)s.id[ea] * a.pos_cap;
-                        mask[u] = (unsigned)s.tsize[ea] - 1;
-                        id[u] = s.id[eb];
-                        h[u] = pos_home(id[u], s.tsize[ea]);
-                        e[u] = __ldg(tab[u] + h[u]);
-                    }
-                }
-                for (int round = 0; round < a.pos_cap; round++) {
-                    bool more = false;
-#pragma unroll
-                    for (int u = 0; u < kBatch; u++) {
-                        if (!live[u]) continue;
-                        const uint32_t k = (uint32_t)(e[u] >> 32);
-                        if (k == id[u] || k == kNone) {
-                            s.pos[q0 + u * kThreads + threadIdx.x] =
-                                k == id[u] ? (unsigned short)(e[u] & 0xFFFFu) : kNotListed;
-                            live[u] = false;
-                        } else {
-                            h[u] = (h[u] + 1) & mask[u];
-                            more = true;
-                        }
-                    }
-                    if (!more) break;
-#pragma unroll
-                    for (int u = 0; u < kBatch; u++)
-                        if (live[u]) e[u] = __ldg(tab[u] + h[u]);
-                }
-            }
-        }
+        if (threadIdx.x < 8) s.umask[threadIdx.x] = 0u;
         __syncthreads();
         // values of every covering box over the tile (-inf outside the box), copied with
         // cp.async so that no thread waits on one load before issuing the next
@@ -404,8 +377,74 @@ __global__ void __launch_bounds__(kThreads, 4) compare_kernel(CompareArgs<T> a) 
             for (int k = 0; k < kTop; k++) {
                 s.topv[v * kTop + k] = tv[k];
                 s.topi[v * kTop + k] = (unsigned char)ti[k];
+                if (ti[k] != 0xFF) atomicOr(s.umask + (ti[k] >> 5), 1u << (ti[k] & 31));
             }
             s.ncand[v] = nc;
+        }
+        __syncthreads();
+        // the columns of pos the pair loop reads: every entry that is among some voxel's
+        // kTop candidates.  pos[a][b] = position of b in a's list, from a's position
+        // table; kBatch lookups advance together, each round issuing all their next probes
+        if (threadIdx.x < 32) {
+            int nu = 0;
+            for (int b0 = 0; b0 < m; b0 += 32) {
+                const int b = b0 + threadIdx.x;
+                const bool in_u = b < m && ((s.umask[b >> 5] >> (b & 31)) & 1u);
+                const unsigned bal = __ballot_sync(0xffffffffu, in_u);
+                if (in_u) s.ulist[nu + __popc(bal & ((1u << threadIdx.x) - 1))] = (unsigned char)b;
+                nu += __popc(bal);
+            }
+            if (threadIdx.x == 0) s.nu[0] = nu;
+        }
+        __syncthreads();
+        {
+            constexpr int kBatch = 4;
+            const int nu = s.nu[0];
+            const int mm = m * nu;
+            for (int q0 = 0; q0 < mm; q0 += kBatch * kThreads) {
+                unsigned long long e[kBatch];
+                const unsigned long long* tab[kBatch];
+                unsigned h[kBatch], mask[kBatch];
+                uint32_t id[kBatch];
+                bool live[kBatch];
+                int dst[kBatch];
+#pragma unroll
+                for (int u = 0; u < kBatch; u++) {
+                    const int q = q0 + u * kThreads + threadIdx.x;
+                    const int ea = q / nu, eb = q < mm ? s.ulist[q - ea * nu] : 0;
+                    live[u] = q < mm && ea != eb;
+                    dst[u] = ea * m + eb;
+                    tab[u] = nullptr;
+                    h[u] = mask[u] = id[u] = 0;
+                    e[u] = 0;
+                    if (live[u]) {
+                        tab[u] = a.pos_table + (long long)s.id[ea] * a.pos_cap;
+                        mask[u] = (unsigned)s.tsize[ea] - 1;
+                        id[u] = s.id[eb];
+                        h[u] = pos_home(id[u], s.tsize[ea]);
+                        e[u] = __ldg(tab[u] + h[u]);
+                    }
+                }
+                for (int round = 0; round < a.pos_cap; round++) {
+                    bool more = false;
+#pragma unroll
+                    for (int u = 0; u < kBatch; u++) {
+                        if (!live[u]) continue;
+                        const uint32_t k = (uint32_t)(e[u] >> 32);
+                        if (k == id[u] || k == kNone) {
+                            s.pos[dst[u]] = k == id[u] ? (unsigned short)(e[u] & 0xFFFFu) : kNotListed;
+                            live[u] = false;
+                        } else {
+                            h[u] = (h[u] + 1) & mask[u];
+                            more = true;
+                        }
+                    }
+                    if (!more) break;
+#pragma unroll
+                    for (int u = 0; u < kBatch; u++)
+                        if (live[u]) e[u] = __ldg(tab[u] + h[u]);
+                }
+            }
         }
         __syncthreads();
         // every (grain, voxel) pair of the tile
@@ -443,7 +482,9 @@ __global__ void __launch_bounds__(kThreads, 4) compare_kernel(CompareArgs<T> a) 
                     const T w = s.val[eb * kTV + v];
                     if (!(w > T(-1))) continue;
                     if (best >= 0 && w < level) continue;
-                    const unsigned short p = s.pos[ea * m + eb];
+                    const unsigned short p = ((s.umask[eb >> 5] >> (eb & 31)) & 1u)
+                                                 ? s.pos[ea * m + eb]
+                                                 : list_position(a, s.id[ea], s.tsize[ea], s.id[eb]);
                     if (p == kNotListed) continue;
                     if (best < 0 || w > level || (w == level && p < bpos)) { best = eb; bpos = p; level = w; }
                 }
@@ -523,7 +564,7 @@ __global__ void newbox_init_kernel(int G, const int* present, const int* exists,
 size_t compare_smem_bytes(int mcap, bool fp64) {
     const size_t e = fp64 ? 8 : 4;
     return 24 * (size_t)mcap + e * (size_t)mcap * kTV + e * kTV * kTop * kParts + 4 * (size_t)mcap +
-           48 * (size_t)mcap + 4 * (size_t)mcap + 4 * kTV * kParts + 2 * (size_t)mcap * mcap +
+           48 * (size_t)mcap + 4 * (size_t)mcap + 4 * kTV * kParts + 48 + 2 * (size_t)mcap * mcap + 256 +
            kTV * kTop * kParts + 64;
 }
 

@@ -15,12 +15,13 @@
 //     as the reference does (including its ID-list quirks), and writes the elements in
 //     search order with their barycenter segments, bounding boxes and an ID -> elements
 //     index.
-//   correction_kernel: a CTA per (grain, z-slice); every voxel with |input| < delta
-//     looks its IDLocal neighbour up in the index and scans only the elements that hold
-//     it, in search order, skipping an element when the distance to its bounding box is
-//     already >= the best distance (an exact bound: no barycenter inside can win under
-//     the strict <).  The energies use CUDA's acos/log/exp/pow: within a few ULP of the
-//     reference's libm, not bit-identical.
+//   correction_kernel: a CTA per (grain, z-slice); the voxels with |input| < delta are
+//     grouped by IDLocal neighbour, and a warp takes 32 voxels of one neighbour at a
+//     time.  It scans only the elements whose searched IDs hold that neighbour (from the
+//     index), skipping an element or a chunk of 16 barycenters when the distance to its
+//     bounding box cannot beat any lane's best (an exact bound: no barycenter inside can
+//     win under the strict <).  The energies use CUDA's acos/log/exp/pow: within a few
+//     ULP of the reference's libm, not bit-identical.
 #include "gg_kernels.cuh"
 
 namespace gg {
@@ -117,6 +118,9 @@ struct Junction {
     uint32_t ids[kJIds];
 };
 
+// bytes of one CTA's global scratch: the junctions and the (element, ID) pairs
+constexpr size_t kElemScratch = ((sizeof(Junction) * kLMax + 4 * kPairMax) + 255) & ~(size_t)255;
+
 struct ElemSmem {
     uint32_t lists[kLMax][8];
     int cnt[kLMax];     // triangles per list
@@ -124,7 +128,7 @@ struct ElemSmem {
     int fill[kLMax];
     int next_key[kLMax];
     double energy[kLMax], mobility[kLMax];
-    Junction jn[kLMax];  // working junctions
+    Junction* jn;        // kLMax working junctions (this CTA's global scratch, cached in L1)
     int qlist[kLMax], hlist[kLMax];
     int lslot[kLHash];  // list hash: index into lists, -1 empty
     // neighbour ID -> elements index under construction
@@ -132,8 +136,8 @@ struct ElemSmem {
     short iden[kIHash];          // dense ID index of the slot
     uint32_t dkey[kIdxMax];
     int dcnt[kIdxMax], dlast[kIdxMax], doff[kIdxMax];
-    unsigned short pe[kPairMax]; // (element, dense ID) pairs in search order
-    unsigned short pd[kPairMax];
+    unsigned short* pe;          // kPairMax (element, dense ID) pairs in search order (global scratch)
+    unsigned short* pd;
     int nl, nq, nh, nj, ne, nch, nd, np;
 };
 
@@ -211,6 +215,13 @@ __global__ void __launch_bounds__(32) elements_kernel(ElementArgs a) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     ElemSmem& S = *reinterpret_cast<ElemSmem*>(smem_raw);
     const int lane = threadIdx.x;
+    if (lane == 0) {  // the large, rarely touched arrays live in this CTA's slice of global scratch
+        unsigned char* scr = a.scratch + (long long)blockIdx.x * kElemScratch;
+        S.jn = reinterpret_cast<Junction*>(scr);
+        S.pe = reinterpret_cast<unsigned short*>(scr + sizeof(Junction) * kLMax);
+        S.pd = S.pe + kPairMax;
+    }
+    __syncwarp();
     for (TileWalk w(a.toff, a.G, blockIdx.x, gridDim.x); w.valid(); w.next()) {
         const int g = w.g;
         if (!a.exists[g]) continue;
@@ -871,12 +882,15 @@ __global__ void __launch_bounds__(kCThreads, 2) correction_kernel(CorrectionArgs
 
 }  // namespace
 
+size_t elements_scratch_per_cta() { return kElemScratch; }
+
 void launch_elements(const ElementArgs& a, int grid, cudaStream_t s) {
     static bool configured = false;
     if (!configured) {
         allow_max_dynamic_smem(elements_kernel);
         configured = true;
     }
+    if (grid > a.scratch_ctas) grid = a.scratch_ctas;
     elements_kernel<<<grid, 32, sizeof(ElemSmem), s>>>(a);
 }
 

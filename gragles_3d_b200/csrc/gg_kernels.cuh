@@ -100,9 +100,12 @@ struct ListArgs {
     uint32_t* cmp;
     int* n_cmp;
     int list_cap;
-    int hash_cap;             // power of two
     int* err;
 };
+// Shared memory of the list update: two bitmaps over the IDs 0..G, a 4096-slot hash
+// of new IDs with their first positions, and 2048 selected (position, ID) pairs.
+__host__ __device__ inline int list_bitmap_words(int G) { return (G + 32) >> 5; }
+inline size_t list_smem_bytes(int G) { return (size_t)list_bitmap_words(G) * 8 + 4096 * 8 + 2048 * 8; }
 void launch_update_lists(const ListArgs& a, int grid, cudaStream_t s);
 
 // Per grain an open-addressing table (ID << 32 | list position) of the comparison list,
@@ -192,8 +195,11 @@ struct ElementArgs {
     HullCapture cap;
     HullElements el;
     HullPhysics ph;
+    unsigned char* scratch;   // scratch_ctas x elements_scratch_per_cta() bytes
+    int scratch_ctas;         // the launch uses at most this many CTAs
     int* err;
 };
+size_t elements_scratch_per_cta();
 void launch_elements(const ElementArgs& a, int grid, cudaStream_t s);
 
 template <typename T>

@@ -8,11 +8,14 @@
 // box.cpp:880-889), in order of first appearance.
 //
 // The reference scans member lists pairwise with linear de-duplication.  Here one
-// CTA per grain hashes every (member i, entry j) of the neighbours' lists into
-// shared memory keeping the smallest enumeration position i * cap + j per ID.
-// Whether an ID qualifies depends on the ID alone, so its first position overall
-// is its first qualifying position; the qualifying new IDs are then ranked by
-// that position, which reproduces the reference's order exactly.
+// CTA per grain walks every (member i, entry j) of the neighbours' lists against two
+// bitmaps over all grain IDs in shared memory: the previous list's existing members
+// (plus the grain itself and the boundary grain), which most entries are, and the IDs
+// already found not to qualify.  Whether an ID qualifies depends on the ID alone, so
+// each distinct ID is checked about once, and only the qualifying new IDs go into a
+// small hash keeping their smallest enumeration position i * cap + j.  Their first
+// position overall is their first qualifying position; ranked by it, they come in
+// the reference's order exactly.
 #include "gg_kernels.cuh"
 
 namespace gg {
@@ -20,7 +23,8 @@ namespace gg {
 namespace {
 
 constexpr int kThreads = 512;
-constexpr int kSel = 2048;
+constexpr int kSel = 2048;          // new IDs of one grain per step
+constexpr int kNewHash = 2 * kSel;  // slots of the new-ID hash (power of two)
 constexpr unsigned kEmpty = 0xFFFFFFFFu;
 
 __device__ __forceinline__ int hash_slot(unsigned* hkey, unsigned id, int cap, int* err) {
@@ -40,30 +44,37 @@ __device__ __forceinline__ bool touch(const Box& a, const Box& b) {  // LSbox::c
 
 __global__ void __launch_bounds__(kThreads) update_lists_kernel(ListArgs a) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
-    const int HC = a.hash_cap;
-    unsigned* hkey = reinterpret_cast<unsigned*>(smem_raw);
-    unsigned* hval = hkey + HC;
-    unsigned* hflag = hval + HC;
-    unsigned* sel_pos = hflag + HC;
-    unsigned* sel_id = sel_pos + kSel;
+    const int W = list_bitmap_words(a.G);
+    unsigned* member = reinterpret_cast<unsigned*>(smem_raw);  // W words
+    unsigned* rejected = member + W;                          // W words
+    unsigned* nkey = rejected + W;                            // kNewHash
+    unsigned* npos = nkey + kNewHash;                         // kNewHash
+    unsigned* sel_pos = npos + kNewHash;                      // kSel
+    unsigned* sel_id = sel_pos + kSel;                        // kSel
     __shared__ int warp_sums[33];
     __shared__ int n_sel;
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
     const int total = a.toff[a.G + 1];
+    const unsigned G = (unsigned)a.G;
     for (int t = blockIdx.x; t < total; t += gridDim.x) {
         const int g = tile_grain(a.toff, a.G, t);
         const int K = a.n_son[g];
         const uint32_t* son = a.son + (long long)g * a.list_cap;
         uint32_t* cmp = a.cmp + (long long)g * a.list_cap;
-        for (int q = threadIdx.x; q < HC; q += blockDim.x) { hkey[q] = kEmpty; hval[q] = kEmpty; hflag[q] = 0; }
+        for (int q = threadIdx.x; q < 2 * W; q += blockDim.x) member[q] = 0u;
+        for (int q = threadIdx.x; q < kNewHash; q += blockDim.x) { nkey[q] = kEmpty; npos[q] = kEmpty; }
         if (threadIdx.x == 0) n_sel = 0;
         __syncthreads();
+        if (threadIdx.x == 0) {  // never candidates: the grain itself and the boundary grain
+            atomicOr(member + (g >> 5), 1u << (g & 31));
+            atomicOr(member, 1u);
+        }
         // 1. existing members of the previous list, in order (block compaction)
         int prefix = 0;
         for (int base = 0; base < K; base += blockDim.x) {
             const int i = base + threadIdx.x;
             const unsigned id = i < K ? son[i] : 0u;
-            const int f = (i < K && a.exists[id]) ? 1 : 0;
+            const int f = (i < K && id <= G && a.exists[id]) ? 1 : 0;
             int incl = f;
 #pragma unroll
             for (int o = 1; o < 32; o <<= 1) {
@@ -87,33 +98,39 @@ __global__ void __launch_bounds__(kThreads) update_lists_kernel(ListArgs a) {
             if (f) {
                 const int pos = prefix + warp_sums[warp] + incl - f;
                 if (pos < a.list_cap) cmp[pos] = id;
-                const int slot = hash_slot(hkey, id, HC, a.err);
-                if (slot >= 0) hflag[slot] = 1;
+                atomicOr(member + (id >> 5), 1u << (id & 31));
             }
             prefix += warp_sums[32];
             __syncthreads();
         }
-        // 2. hash every entry of every member's list with its first position
+        // 2. every entry of every member's list: skip members and known rejects, check
+        //    the rest (exists, box touches), keep the first position of each new ID
+        const Box self = load_box(a.box + 6 * g);
         for (int i = warp; i < K; i += nw) {
             const unsigned c = son[i];
-            const int Kc = a.n_son[c];
+            if (c > G) continue;
+            const int Kc = min(a.n_son[c], a.list_cap);
             const uint32_t* sc = a.son + (long long)c * a.list_cap;
             for (int j = lane; j < Kc; j += 32) {
                 const unsigned id = sc[j];
-                const int slot = hash_slot(hkey, id, HC, a.err);
-                if (slot >= 0) atomicMin(hval + slot, (unsigned)i * (unsigned)a.list_cap + (unsigned)j);
+                if (id > G) continue;
+                const unsigned bit = 1u << (id & 31);
+                if ((member[id >> 5] | rejected[id >> 5]) & bit) continue;
+                if (!a.exists[id] || !touch(self, load_box(a.box + 6 * id))) {
+                    atomicOr(rejected + (id >> 5), bit);
+                    continue;
+                }
+                const int slot = hash_slot(nkey, id, kNewHash, a.err);
+                if (slot >= 0) atomicMin(npos + slot, (unsigned)i * (unsigned)a.list_cap + (unsigned)j);
             }
         }
         __syncthreads();
-        // 3. keep the qualifying new IDs
-        const Box self = load_box(a.box + 6 * g);
-        for (int q = threadIdx.x; q < HC; q += blockDim.x) {
-            const unsigned id = hkey[q];
-            if (id == kEmpty || hflag[q] || hval[q] == kEmpty) continue;
-            if (id == (unsigned)g || id == 0u || id > (unsigned)a.G || !a.exists[id]) continue;
-            if (!touch(self, load_box(a.box + 6 * id))) continue;
+        // 3. collect the new IDs
+        for (int q = threadIdx.x; q < kNewHash; q += blockDim.x) {
+            const unsigned id = nkey[q];
+            if (id == kEmpty) continue;
             const int s = atomicAdd(&n_sel, 1);
-            if (s < kSel) { sel_pos[s] = hval[q]; sel_id[s] = id; }
+            if (s < kSel) { sel_pos[s] = npos[q]; sel_id[s] = id; }
         }
         __syncthreads();
         // 4. append them by first position
@@ -171,7 +188,7 @@ void launch_update_lists(const ListArgs& a, int grid, cudaStream_t s) {
         allow_max_dynamic_smem(update_lists_kernel);
         configured = true;
     }
-    const size_t smem = (size_t)a.hash_cap * 12 + (size_t)kSel * 8;
+    const size_t smem = list_smem_bytes(a.G);
     update_lists_kernel<<<grid, kThreads, smem, s>>>(a);
 }
 
