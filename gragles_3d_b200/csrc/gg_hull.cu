@@ -36,7 +36,8 @@ constexpr int kLHash = 2 * kLMax;  // slots of the distinct-list hash (power of 
 constexpr unsigned kFull = 0xFFFFFFFFu;
 constexpr int kIdxMax = 256;       // distinct neighbour IDs the elements of one hull search
 constexpr int kIHash = 2 * kIdxMax;
-constexpr int kPairMax = 2048;     // (element, searched ID) pairs of one hull
+constexpr int kPairMax = 1024;     // (element, searched ID) pairs of one hull
+constexpr int kJobMax = 9 * kLMax; // misorientations of one hull's elements (9 per QJ list)
 
 // ---------------------------------------------------------------------------------
 // misorientation and boundary properties
@@ -82,23 +83,6 @@ __device__ double energy_of(const HullPhysics& ph, double misori) {
     return 1.0 * (misori / theta_ref) * (1.0 - log(misori / theta_ref));
 }
 
-// TripleLine of (me, n0, n1): energy and mobility (InterfacialElement.cpp:119-170)
-__device__ void triple_line(const HullPhysics& ph, uint32_t me, uint32_t n0, uint32_t n1, double& energy,
-                            double& mobility) {
-    const double t0 = misorientation(ph, me, n0), t1 = misorientation(ph, n0, n1), t2 = misorientation(ph, me, n1);
-    double avg = 0;
-    avg += mobility_of(ph, t0);
-    avg += mobility_of(ph, t1);
-    avg += mobility_of(ph, t2);
-    avg /= 3;
-    const double ds = 3 * sqrt(3 * ph.ds * ph.ds);
-    mobility = 1. / ((1. / (ds * ph.tl_drag)) + 1. / avg);
-    double sigma = energy_of(ph, t0) - energy_of(ph, t1) + energy_of(ph, t2);
-    if (sigma < 0.01) sigma = 0.01;
-    if (sigma > 1.0) sigma = 1.0;
-    energy = sigma;
-}
-
 // Vector3d (a - b).squaredNorm(): Eigen's unrolled sum c0 + (c1 + c2)
 __device__ __forceinline__ double sqdist(const double* a, const double* b) {
     const double d0 = a[0] - b[0], d1 = a[1] - b[1], d2 = a[2] - b[2];
@@ -109,26 +93,28 @@ __device__ __forceinline__ double sqdist(const double* a, const double* b) {
 // element construction
 // ---------------------------------------------------------------------------------
 
-// A junction being merged: its member lists (keys) chained through next_key, its IDs.
-struct Junction {
+// A junction being merged: its member lists (keys) chained through next_key; its IDs
+// (at most kJIds) are in the CTA's global scratch.
+struct JHead {
     int head, tail;   // member keys
     int nids;
     int type;         // 3 QJ, 4 HJ
     double pos[3];
-    uint32_t ids[kJIds];
 };
 
-// bytes of one CTA's global scratch: the junctions and the (element, ID) pairs
-constexpr size_t kElemScratch = ((sizeof(Junction) * kLMax + 4 * kPairMax) + 255) & ~(size_t)255;
+// One CTA's global scratch: the junction IDs and the (mobility, energy) of every
+// misorientation job.  Neither is on a latency-critical path.
+constexpr size_t kJIdBytes = (size_t)kLMax * kJIds * 4;
+constexpr size_t kElemScratch = ((kJIdBytes + sizeof(double2) * kJobMax) + 255) & ~(size_t)255;
 
 struct ElemSmem {
     uint32_t lists[kLMax][8];
     int cnt[kLMax];     // triangles per list
     int off[kLMax];     // first barycenter of the list in the grouped array
-    int fill[kLMax];
+    int fill[kLMax];    // barycenters placed so far; then the list's first misorientation job
     int next_key[kLMax];
     double energy[kLMax], mobility[kLMax];
-    Junction* jn;        // kLMax working junctions (this CTA's global scratch, cached in L1)
+    JHead jh[kLMax];    // working junctions
     int qlist[kLMax], hlist[kLMax];
     int lslot[kLHash];  // list hash: index into lists, -1 empty
     // neighbour ID -> elements index under construction
@@ -136,8 +122,10 @@ struct ElemSmem {
     short iden[kIHash];          // dense ID index of the slot
     uint32_t dkey[kIdxMax];
     int dcnt[kIdxMax], dlast[kIdxMax], doff[kIdxMax];
-    unsigned short* pe;          // kPairMax (element, dense ID) pairs in search order (global scratch)
-    unsigned short* pd;
+    unsigned short pe[kPairMax]; // (element, dense ID) pairs in search order
+    unsigned short pd[kPairMax];
+    uint32_t* jids;              // kLMax x kJIds junction IDs (global scratch)
+    double2* jres;               // kJobMax (mobility, energy) (global scratch)
     int nl, nq, nh, nj, ne, nch, nd, np;
 };
 
@@ -177,9 +165,31 @@ __device__ void insert_list(ElemSmem& S, unsigned h, int k, int* err) {
     atomicOr(err, ERR_HULL);
 }
 
+// The mean of n barycenters of the grouped array from b on, summed in order (the
+// loads run ahead of the sequential sums).
+__device__ __forceinline__ void bary_sum(const double* b, int n, double& p0, double& p1, double& p2) {
+    int i = 0;
+    for (; i + 4 <= n; i += 4) {
+        double v[12];
+#pragma unroll
+        for (int u = 0; u < 12; u++) v[u] = b[3 * i + u];
+#pragma unroll
+        for (int u = 0; u < 4; u++) {
+            p0 += v[3 * u];
+            p1 += v[3 * u + 1];
+            p2 += v[3 * u + 2];
+        }
+    }
+    for (; i < n; i++) {
+        p0 += b[3 * i];
+        p1 += b[3 * i + 1];
+        p2 += b[3 * i + 2];
+    }
+}
+
 // The junction's position: the mean of its barycenters in member order
 // (QuadrupleJunction / HighOrderJunction::computePosition, InterfacialElement.cpp:394-406)
-__device__ void junction_position(Junction& J, const ElemSmem& S, const double* eb, int bary_cap, int* err) {
+__device__ void junction_position(JHead& J, const ElemSmem& S, const double* eb, int bary_cap, int* err) {
     double p0 = 0, p1 = 0, p2 = 0;
     int n = 0;
     for (int k = J.head; k >= 0; k = S.next_key[k]) {
@@ -187,12 +197,7 @@ __device__ void junction_position(Junction& J, const ElemSmem& S, const double* 
             atomicOr(err, ERR_BOUNDS);
             break;
         }
-        const double* b = eb + 3 * (long long)S.off[k];
-        for (int i = 0; i < S.cnt[k]; i++) {
-            p0 += b[3 * i];
-            p1 += b[3 * i + 1];
-            p2 += b[3 * i + 2];
-        }
+        bary_sum(eb + 3 * (long long)S.off[k], S.cnt[k], p0, p1, p2);
         n += S.cnt[k];
     }
     const double d = (double)n;
@@ -201,25 +206,105 @@ __device__ void junction_position(Junction& J, const ElemSmem& S, const double* 
     J.pos[2] = p2 / d;
 }
 
-__device__ __forceinline__ void push_id(Junction& J, uint32_t id, int* err) {
-    if (J.nids < kJIds) J.ids[J.nids++] = id;
+__device__ __forceinline__ void push_id(JHead& J, uint32_t* ids, uint32_t id, int* err) {
+    if (J.nids < kJIds) ids[J.nids++] = id;
     else atomicOr(err, ERR_HULL);
 }
 
-__device__ __forceinline__ void chain(ElemSmem& S, Junction& A, const Junction& B) {
+__device__ __forceinline__ void chain(ElemSmem& S, JHead& A, const JHead& B) {
     S.next_key[A.tail] = B.head;
     A.tail = B.tail;
+}
+
+// Warp-wide exclusive scan of v[0, n) in place (n <= kLMax); returns the total.
+__device__ int warp_scan_excl(int* v, int n) {
+    const int lane = threadIdx.x & 31;
+    int run = 0;
+    for (int b = 0; b < n; b += 32) {
+        const int i = b + lane;
+        const int x = i < n ? v[i] : 0;
+        int incl = x;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const int u = __shfl_up_sync(kFull, incl, o);
+            if (lane >= o) incl += u;
+        }
+        if (i < n) v[i] = run + incl - x;
+        run += __shfl_sync(kFull, incl, 31);
+    }
+    __syncwarp();
+    return run;
+}
+
+__device__ __forceinline__ int id_count(const uint32_t* L) {
+    int count = 0;
+#pragma unroll
+    for (int j = 0; j < 8; j++) count += L[j] == kNoId ? 0 : 1;
+    return count;
+}
+
+// The neighbours computeGrainBoundaryElements takes from a list of `count` IDs:
+// the other ID of a GB list, else the IDs other than g among the first min(count, 4).
+__device__ __forceinline__ int list_neighbours(const uint32_t* L, int count, uint32_t g, uint32_t (&nb)[4]) {
+    if (count == 2) {
+        nb[0] = g != L[0] ? L[0] : L[1];
+        return 1;
+    }
+    const int lim = count < 4 ? count : 4;
+    int nn = 0;
+    for (int i = 0; i < lim; i++)
+        if (g != L[i]) nb[nn++] = L[i];
+    return nn;
+}
+
+// Misorientation jobs of a list: 1 for a GB (2 IDs), 3 for a TL (3 IDs, one triple
+// line), 9 for a QJ list (4 IDs, three triple lines); none otherwise (E = M = 1).
+__device__ __forceinline__ int list_jobs(int count) { return count == 2 ? 1 : (count == 3 ? 3 : (count == 4 ? 9 : 0)); }
+
+// The ordered grain pair of job jj of a list: TripleLine(me, n0, n1) computes
+// (me, n0), (n0, n1), (me, n1) (InterfacialElement.cpp:119-170); a QJ list's three
+// triple lines are (nb0, nb1), (nb1, nb2), (nb0, nb2) (InterfacialElement.cpp:436-456).
+__device__ __forceinline__ void job_pair(int count, int jj, uint32_t g, const uint32_t (&nb)[4], uint32_t& x,
+                                         uint32_t& y) {
+    if (count == 2) {
+        x = g;
+        y = nb[0];
+        return;
+    }
+    uint32_t u = nb[0], v = nb[1];
+    const int tl = jj / 3, r = jj % 3;
+    if (tl == 1) { u = nb[1]; v = nb[2]; }
+    if (tl == 2) { u = nb[0]; v = nb[2]; }
+    if (r == 0) { x = g; y = u; }
+    else if (r == 1) { x = u; y = v; }
+    else { x = g; y = v; }
+}
+
+// TripleLine's energy and mobility (InterfacialElement.cpp:117-160) from its three
+// jobs' (mobility, energy).
+__device__ __forceinline__ void triple_line_of(const HullPhysics& ph, const double2* r, double& energy,
+                                               double& mobility) {
+    double avg = 0;
+    avg += r[0].x;
+    avg += r[1].x;
+    avg += r[2].x;
+    avg /= 3;
+    const double ds = 3 * sqrt(3 * ph.ds * ph.ds);
+    mobility = 1. / ((1. / (ds * ph.tl_drag)) + 1. / avg);
+    double sigma = r[0].y - r[1].y + r[2].y;
+    if (sigma < 0.01) sigma = 0.01;
+    if (sigma > 1.0) sigma = 1.0;
+    energy = sigma;
 }
 
 __global__ void __launch_bounds__(32) elements_kernel(ElementArgs a) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     ElemSmem& S = *reinterpret_cast<ElemSmem*>(smem_raw);
     const int lane = threadIdx.x;
-    if (lane == 0) {  // the large, rarely touched arrays live in this CTA's slice of global scratch
+    if (lane == 0) {  // the bulky, rarely touched arrays live in this CTA's slice of global scratch
         unsigned char* scr = a.scratch + (long long)blockIdx.x * kElemScratch;
-        S.jn = reinterpret_cast<Junction*>(scr);
-        S.pe = reinterpret_cast<unsigned short*>(scr + sizeof(Junction) * kLMax);
-        S.pd = S.pe + kPairMax;
+        S.jids = reinterpret_cast<uint32_t*>(scr);
+        S.jres = reinterpret_cast<double2*>(scr + kJIdBytes);
     }
     __syncwarp();
     for (TileWalk w(a.toff, a.G, blockIdx.x, gridDim.x); w.valid(); w.next()) {
@@ -309,17 +394,12 @@ __global__ void __launch_bounds__(32) elements_kernel(ElementArgs a) {
         __syncwarp();
         for (int r = lane; r < nrec; r += 32) atomicAdd(&S.cnt[rec_ntri[r] >> 8], rec_ntri[r] & 0xFF);
         __syncwarp();
-        if (lane == 0) {
-            int run = 0;
-            for (int k = 0; k < nl; k++) {
-                S.off[k] = run;
-                run += S.cnt[k];
-            }
-            if (run > a.el.bary_cap) atomicOr(a.err, ERR_HULL);
-        }
+        for (int k = lane; k < nl; k += 32) S.off[k] = S.cnt[k];
         __syncwarp();
+        if (warp_scan_excl(S.off, nl) > a.el.bary_cap && lane == 0) atomicOr(a.err, ERR_HULL);
         // 3. barycenters grouped by list, in triangle order (subDivideTrianglesToInterfacialElements):
-        //    a record's triangles go after those of the earlier records of its list
+        //    a record's triangles go after those of the earlier records of its list.  The
+        //    warp first places its 32 records, then copies their triangles together.
         for (int base = 0, tbase = 0; base < nrec; base += 32) {
             const int r = base + lane;
             const bool valid = r < nrec;
@@ -332,8 +412,8 @@ __global__ void __launch_bounds__(32) elements_kernel(ElementArgs a) {
                 const int u = __shfl_up_sync(kFull, incl, o);
                 if (lane >= o) incl += u;
             }
-            const int t0 = tbase + incl - nt;
-            tbase += __shfl_sync(kFull, incl, 31);
+            const int excl = incl - nt;
+            const int total = __shfl_sync(kFull, incl, 31);
             const unsigned peers = __match_any_sync(kFull, k);
             int before = 0;
             for (int src = 0; src < 32; src++) {
@@ -343,84 +423,141 @@ __global__ void __launch_bounds__(32) elements_kernel(ElementArgs a) {
             const int dst = valid ? S.off[k] + S.fill[k] + before : 0;
             __syncwarp();
             if (valid && 31 - __clz(peers) == lane) S.fill[k] += before + nt;
-            for (int q = 0; q < nt; q++) {
-                const int pos = dst + q, t = t0 + q;
-                if (pos < a.el.bary_cap && t < ntri) {
-                    eb[3 * (long long)pos] = bary[3 * (long long)t];
-                    eb[3 * (long long)pos + 1] = bary[3 * (long long)t + 1];
-                    eb[3 * (long long)pos + 2] = bary[3 * (long long)t + 2];
+            // triangle tbase + q belongs to the last record whose first triangle is <= it
+            // (the loop is warp-uniform: every lane takes part in the shuffles)
+            for (int q0 = 0; q0 < total; q0 += 32) {
+                const int q = q0 + lane;
+                int rr = 0;
+#pragma unroll
+                for (int st = 16; st > 0; st >>= 1) {
+                    const int cand = rr + st;
+                    const int ex = __shfl_sync(kFull, excl, cand & 31);
+                    if (cand < 32 && ex <= q) rr = cand;
+                }
+                const int pos = __shfl_sync(kFull, dst, rr) + q - __shfl_sync(kFull, excl, rr);
+                const int t = tbase + q;
+                if (q < total && pos >= 0 && pos < a.el.bary_cap && t < ntri) {
+                    const double b0 = bary[3 * (long long)t], b1 = bary[3 * (long long)t + 1],
+                                 b2 = bary[3 * (long long)t + 2];
+                    eb[3 * (long long)pos] = b0;
+                    eb[3 * (long long)pos + 1] = b1;
+                    eb[3 * (long long)pos + 2] = b2;
                 }
             }
+            tbase += total;
             __syncwarp();
         }
-        // 4. one element per list: energy and mobility (computeGrainBoundaryElements)
-        for (int k = lane; k < nl; k += 32) {
-            const uint32_t* L = S.lists[k];
-            int count = 0;
-            for (int j = 0; j < 8; j++) count += L[j] == kNoId ? 0 : 1;
-            double E = 1.0, M = 1.0;
-            uint32_t nb[8];
-            int nn = 0;
-            if (count == 2) {
-                nb[nn++] = (uint32_t)g != L[0] ? L[0] : L[1];
-            } else {
-                const int lim = count == 3 ? 3 : (count == 4 ? 4 : count);
-                for (int i = 0; i < lim; i++)
-                    if ((uint32_t)g != L[i]) nb[nn++] = L[i];
+        // 4. one element per list: energy and mobility (computeGrainBoundaryElements).
+        //    Every misorientation a list needs is a job; the warp runs the jobs of all
+        //    lists side by side, then each list combines its own in the reference's order.
+        for (int k = lane; k < nl; k += 32) S.fill[k] = list_jobs(id_count(S.lists[k]));
+        __syncwarp();
+        int njobs = warp_scan_excl(S.fill, nl);
+        if (njobs > kJobMax) {
+            if (lane == 0) atomicOr(a.err, ERR_HULL);
+            njobs = kJobMax;
+        }
+        for (int j = lane; j < njobs; j += 32) {
+            int lo = 0, hi = nl - 1;  // the last list whose first job is <= j
+            while (lo < hi) {
+                const int mid = (lo + hi + 1) >> 1;
+                if (S.fill[mid] <= j) lo = mid;
+                else hi = mid - 1;
             }
-            if (count == 2) {
-                const double t = misorientation(a.ph, g, nb[0]);
-                M = mobility_of(a.ph, t);
-                E = energy_of(a.ph, t);
-            } else if (count == 3) {
-                triple_line(a.ph, g, nb[0], nb[1], E, M);
-            } else if (count == 4) {
-                double E1, M1, E2, M2, E3, M3;
-                triple_line(a.ph, g, nb[0], nb[1], E1, M1);
-                triple_line(a.ph, g, nb[1], nb[2], E2, M2);
-                triple_line(a.ph, g, nb[0], nb[2], E3, M3);
-                M = (M1 + M2 + M3) / 3.0;
-                E = (E1 + E2 + E3) / 3.0;
+            const uint32_t* L = S.lists[lo];
+            const int count = id_count(L);
+            uint32_t nb[4] = {0, 0, 0, 0};
+            list_neighbours(L, count, (uint32_t)g, nb);
+            uint32_t x, y;
+            job_pair(count, j - S.fill[lo], (uint32_t)g, nb, x, y);
+            const double t = misorientation(a.ph, x, y);
+            S.jres[j] = make_double2(mobility_of(a.ph, t), energy_of(a.ph, t));
+        }
+        __syncwarp();
+        for (int k = lane; k < nl; k += 32) {
+            const int count = id_count(S.lists[k]);
+            const int j0 = S.fill[k];
+            double E = 1.0, M = 1.0;
+            if (j0 + list_jobs(count) <= njobs) {
+                const double2* r = S.jres + j0;
+                if (count == 2) {
+                    M = r[0].x;
+                    E = r[0].y;
+                } else if (count == 3) {
+                    triple_line_of(a.ph, r, E, M);
+                } else if (count == 4) {
+                    double E1, M1, E2, M2, E3, M3;
+                    triple_line_of(a.ph, r, E1, M1);
+                    triple_line_of(a.ph, r + 3, E2, M2);
+                    triple_line_of(a.ph, r + 6, E3, M3);
+                    M = (M1 + M2 + M3) / 3.0;
+                    E = (E1 + E2 + E3) / 3.0;
+                }
             }
             S.energy[k] = E;
             S.mobility[k] = M;
         }
         __syncwarp();
         // 5. junctions and their merging (computeJunctionPosition + mergeJunction,
-        //    grainHull.cpp:267-275, 483-531); sequential, as the reference
-        if (lane == 0) {
-            S.nq = S.nh = S.nj = 0;
-            for (int k = 0; k < nl; k++) {
-                int count = 0;
-                for (int j = 0; j < 8; j++) count += S.lists[k][j] == kNoId ? 0 : 1;
-                if (count < 4 && count > 1) continue;  // 2 GB, 3 TL; everything else is a junction
-                Junction& J = S.jn[S.nj];
-                J.head = J.tail = k;
-                J.nids = 0;
-                J.type = count == 4 ? 3 : 4;
-                for (int i = 0; i < count; i++)
-                    if ((uint32_t)g != S.lists[k][i]) push_id(J, S.lists[k][i], a.err);
-                junction_position(J, S, eb, a.el.bary_cap, a.err);
-                if (J.type == 3) S.qlist[S.nq++] = S.nj;
-                else S.hlist[S.nh++] = S.nj;
-                S.nj++;
+        //    grainHull.cpp:267-275, 483-531).  Every list with 4 IDs (QJ) or with 5 or more,
+        //    or fewer than 2 (HJ), starts a junction, in list order; the lanes build them
+        //    side by side.  The merges are sequential, as the reference's.
+        {
+            int nj = 0, nq = 0, nh = 0;
+            for (int b = 0; b < nl; b += 32) {
+                const int k = b + lane;
+                const int count = k < nl ? id_count(S.lists[k]) : 2;
+                const bool isj = k < nl && !(count < 4 && count > 1);
+                const bool isq = isj && count == 4;
+                const unsigned bj = __ballot_sync(kFull, isj), bq = __ballot_sync(kFull, isq),
+                               bh = __ballot_sync(kFull, isj && !isq);
+                const unsigned lt = (1u << lane) - 1;
+                if (isj) {
+                    const int j = nj + __popc(bj & lt);
+                    JHead& J = S.jh[j];
+                    J.head = J.tail = k;
+                    J.type = isq ? 3 : 4;
+                    J.nids = 0;
+                    uint32_t* ids = S.jids + (long long)j * kJIds;
+                    for (int i = 0; i < count; i++)
+                        if ((uint32_t)g != S.lists[k][i]) push_id(J, ids, S.lists[k][i], a.err);
+                    junction_position(J, S, eb, a.el.bary_cap, a.err);
+                    if (isq) S.qlist[nq + __popc(bq & lt)] = j;
+                    else S.hlist[nh + __popc(bh & lt)] = j;
+                }
+                nj += __popc(bj);
+                nq += __popc(bq);
+                nh += __popc(bh);
             }
+            __syncwarp();
+            if (lane == 0) {
+                S.nj = nj;
+                S.nq = nq;
+                S.nh = nh;
+            }
+            __syncwarp();
+        }
+        if (lane == 0) {
             // quadruple points closer than 2: a new high-order junction from the pair
             for (int i = 0; i < S.nq; i++) {
                 for (int j = i + 1; j < S.nq; j++) {
-                    Junction& A = S.jn[S.qlist[i]];
-                    Junction& B = S.jn[S.qlist[j]];
+                    JHead& A = S.jh[S.qlist[i]];
+                    JHead& B = S.jh[S.qlist[j]];
                     if (sqrt(sqdist(A.pos, B.pos)) < 2) {
                         if (S.nj >= kLMax) { atomicOr(a.err, ERR_HULL); break; }
-                        Junction& H = S.jn[S.nj];
+                        const uint32_t* aid = S.jids + (long long)S.qlist[i] * kJIds;
+                        const uint32_t* bid = S.jids + (long long)S.qlist[j] * kJIds;
+                        const uint32_t a0 = aid[0], a1 = aid[1], a2 = aid[2], b0 = bid[0], b1 = bid[1], b2 = bid[2];
+                        JHead& H = S.jh[S.nj];
+                        uint32_t* hid = S.jids + (long long)S.nj * kJIds;
                         H.type = 4;
                         H.nids = 0;
-                        for (int q = 0; q < 3; q++) push_id(H, A.ids[q], a.err);
-                        for (int q = 0; q < 3; q++) {  // B's IDs that A already has (sic)
-                            bool dup = false;
-                            for (int u = 0; u < 3; u++) dup |= H.ids[u] == B.ids[q];
-                            if (dup) push_id(H, B.ids[q], a.err);
-                        }
+                        push_id(H, hid, a0, a.err);
+                        push_id(H, hid, a1, a.err);
+                        push_id(H, hid, a2, a.err);
+                        const uint32_t bq[3] = {b0, b1, b2};
+                        for (int q = 0; q < 3; q++)  // B's IDs that A already has (sic)
+                            if (bq[q] == a0 || bq[q] == a1 || bq[q] == a2) push_id(H, hid, bq[q], a.err);
                         H.head = A.head;
                         H.tail = A.tail;
                         chain(S, H, B);
@@ -438,11 +575,13 @@ __global__ void __launch_bounds__(32) elements_kernel(ElementArgs a) {
             // quadruple points closer than 2 to a high-order junction join it
             for (int k = 0; k < S.nh; k++)
                 for (int i = 0; i < S.nq; i++) {
-                    Junction& H = S.jn[S.hlist[k]];
-                    Junction& Q = S.jn[S.qlist[i]];
+                    JHead& H = S.jh[S.hlist[k]];
+                    JHead& Q = S.jh[S.qlist[i]];
                     if (sqrt(sqdist(Q.pos, H.pos)) < 2) {
                         chain(S, H, Q);
-                        for (int q = 0; q < Q.nids; q++) push_id(H, Q.ids[q], a.err);
+                        uint32_t* hid = S.jids + (long long)S.hlist[k] * kJIds;
+                        const uint32_t* qid = S.jids + (long long)S.qlist[i] * kJIds;
+                        for (int q = 0; q < Q.nids; q++) push_id(H, hid, qid[q], a.err);
                         junction_position(H, S, eb, a.el.bary_cap, a.err);
                         for (int u = i; u < S.nq - 1; u++) S.qlist[u] = S.qlist[u + 1];
                         S.nq--;
@@ -452,11 +591,13 @@ __global__ void __launch_bounds__(32) elements_kernel(ElementArgs a) {
             // high-order junctions closer than 2 merge
             for (int i = 0; i < S.nh; i++)
                 for (int k = i + 1; k < S.nh; k++) {
-                    Junction& A = S.jn[S.hlist[i]];
-                    Junction& B = S.jn[S.hlist[k]];
+                    JHead& A = S.jh[S.hlist[i]];
+                    JHead& B = S.jh[S.hlist[k]];
                     if (sqrt(sqdist(A.pos, B.pos)) < 2) {
                         chain(S, A, B);
-                        for (int q = 0; q < B.nids; q++) push_id(A, B.ids[q], a.err);
+                        uint32_t* aid = S.jids + (long long)S.hlist[i] * kJIds;
+                        const uint32_t* bid = S.jids + (long long)S.hlist[k] * kJIds;
+                        for (int q = 0; q < B.nids; q++) push_id(A, aid, bid[q], a.err);
                         junction_position(A, S, eb, a.el.bary_cap, a.err);
                         for (int u = k; u < S.nh - 1; u++) S.hlist[u] = S.hlist[u + 1];
                         S.nh--;
@@ -478,38 +619,43 @@ __global__ void __launch_bounds__(32) elements_kernel(ElementArgs a) {
             bool over = false;
             auto emit = [&](int type, const uint32_t* id_src, int nid, int head, bool chained, double en, double mo) {
                 if (ne >= a.el.elem_cap || ni + nid > a.el.id_cap) { over = true; return; }
-                HullElem& e = E[ne];
-                e.type = type;
-                e.id_off = ni;
-                e.nids = nid;
-                for (int q = 0; q < nid; q++) ids[ni++] = id_src[q];
-                e.seg_off = ns;
-                e.nseg = 0;
-                e.chunk_off = nch;
-                e.nchunk = 0;
+                uint32_t idv[kJIds];
+                for (int q = 0; q < nid && q < kJIds; q++) idv[q] = id_src[q];
+                const int id_off = ni, seg_off = ns, chunk_off = nch;
+                for (int q = 0; q < nid; q++) ids[ni++] = idv[q];
+                int nseg = 0, nchunk = 0;
                 for (int k = head; k >= 0; k = chained ? S.next_key[k] : -1) {
                     if (ns >= a.el.seg_cap) { over = true; break; }
                     if (k >= kLMax || S.off[k] < 0 || S.off[k] + S.cnt[k] > a.el.bary_cap) {
                         atomicOr(a.err, ERR_BOUNDS);
                         break;
                     }
-                    segs[ns++] = make_int2(S.off[k], S.cnt[k]);
-                    e.nseg++;
-                    for (int c0 = 0; c0 < S.cnt[k]; c0 += kHullChunk) {
+                    const int off = S.off[k], cnt = S.cnt[k];
+                    segs[ns++] = make_int2(off, cnt);
+                    nseg++;
+                    for (int c0 = 0; c0 < cnt; c0 += kHullChunk) {
                         if (nch >= a.el.chunk_cap) { over = true; break; }
-                        chunks[nch].start = S.off[k] + c0;
-                        chunks[nch].count = min(kHullChunk, S.cnt[k] - c0);
+                        chunks[nch].start = off + c0;
+                        chunks[nch].count = min(kHullChunk, cnt - c0);
                         nch++;
-                        e.nchunk++;
+                        nchunk++;
                     }
                 }
+                HullElem& e = E[ne];
+                e.type = type;
+                e.id_off = id_off;
+                e.nids = nid;
+                e.seg_off = seg_off;
+                e.nseg = nseg;
+                e.chunk_off = chunk_off;
+                e.nchunk = nchunk;
                 e.energy = en;
                 e.mobility = mo;
                 // the IDs projectPointToGrainBoundary compares: all for a high-order
                 // junction, else the first 3 (QJ), 2 (TL), 1 (GB); each element once per ID
                 const int nc = type == 4 ? nid : min(nid, type);
                 for (int q = 0; q < nc; q++) {
-                    const uint32_t id = id_src[q];
+                    const uint32_t id = idv[q];
                     unsigned hs = (id * 2654435761u) & (kIHash - 1);
                     int d = -1;
                     for (int probe = 0; probe < kIHash; probe++) {
@@ -537,18 +683,18 @@ __global__ void __launch_bounds__(32) elements_kernel(ElementArgs a) {
                 ne++;
             };
             for (int i = 0; i < S.nh; i++) {
-                const Junction& J = S.jn[S.hlist[i]];
+                const JHead& J = S.jh[S.hlist[i]];
                 // a junction made from one list keeps that list's energy (1 for HJ)
-                emit(4, J.ids, J.nids, J.head, true, 1.0, 1.0);
+                emit(4, S.jids + (long long)S.hlist[i] * kJIds, min(J.nids, kJIds), J.head, true, 1.0, 1.0);
             }
             for (int i = 0; i < S.nq; i++) {
-                const Junction& J = S.jn[S.qlist[i]];
-                emit(3, J.ids, J.nids, J.head, true, S.energy[J.head], S.mobility[J.head]);
+                const JHead& J = S.jh[S.qlist[i]];
+                emit(3, S.jids + (long long)S.qlist[i] * kJIds, min(J.nids, kJIds), J.head, true, S.energy[J.head],
+                     S.mobility[J.head]);
             }
             for (int pass = 2; pass >= 1; pass--)  // TL, then GB, each in key order
                 for (int k = 0; k < nl; k++) {
-                    int count = 0;
-                    for (int j = 0; j < 8; j++) count += S.lists[k][j] == kNoId ? 0 : 1;
+                    const int count = id_count(S.lists[k]);
                     if ((pass == 2 && count != 3) || (pass == 1 && count != 2)) continue;
                     uint32_t nb[3];
                     int nn = 0;
@@ -890,6 +1036,15 @@ void launch_elements(const ElementArgs& a, int grid, cudaStream_t s) {
         allow_max_dynamic_smem(elements_kernel);
         configured = true;
     }
+    static int resident = 0;  // CTAs that fit on the device at once
+    if (resident == 0) {
+        int dev = 0, sms = 0, per_sm = 0;
+        cudaGetDevice(&dev);
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, elements_kernel, 32, sizeof(ElemSmem));
+        resident = sms * (per_sm > 0 ? per_sm : 1);
+    }
+    if (grid > resident) grid = resident;
     if (grid > a.scratch_ctas) grid = a.scratch_ctas;
     elements_kernel<<<grid, 32, sizeof(ElemSmem), s>>>(a);
 }
