@@ -504,7 +504,11 @@ __global__ void __launch_bounds__(kThreads, 4) compare_kernel(CompareArgs<T> a) 
             }
             const bool boundary = !(A.x0 > a.geo.gb && A.x1 < a.geo.M - a.geo.gb && A.y0 > a.geo.gb &&
                                     A.y1 < a.geo.M - a.geo.gb && A.z0 > a.geo.gb && A.z1 < a.geo.M - a.geo.gb);
-            if (boundary) {
+            // A voxel at least gb from every face of the boundary grain's zone gets an
+            // all-negative distance <= -gb from bc_assign, which changes nothing: skip it.
+            const int lo_in = 2 * a.geo.gb - 1, hi_in = a.geo.M - 1 - 2 * a.geo.gb;
+            const bool deep = x >= lo_in && x <= hi_in && y >= lo_in && y <= hi_in && z >= lo_in && z <= hi_in;
+            if (boundary && !deep) {
                 const double d = bc_dist(A, y, x, z, a.geo.M, a.geo.gb);
                 if (d > -a.geo.gb)
                     if (d * a.geo.h > (double)cmpv) {

@@ -24,7 +24,7 @@ namespace {
 
 constexpr int kThreads = 256;
 constexpr int kHash = 1024;  // distinct neighbour IDs per grain (power of two)
-constexpr int kSlabBytes = 64 * 1024;  // shared memory for a slab's sign bytes and cube lists
+constexpr int kSlabBytes = 36 * 1024;  // shared memory for a slab's sign bytes and cube lists
 
 // cubeindex bit b <-> corner offset (dx, dy, dz), marchingCubes.cpp:376-385
 __constant__ int c_corner[8][3] = {{0, 0, 1}, {1, 0, 1}, {1, 0, 0}, {0, 0, 0},
@@ -108,7 +108,7 @@ __device__ Box resize_to_cube(Box b, int maximumLength) {
 }
 
 template <typename T>
-__global__ void __launch_bounds__(kThreads, 2) mc_kernel(MCArgs<T> a, int slab_bytes) {
+__global__ void __launch_bounds__(kThreads, 3) mc_kernel(MCArgs<T> a, int slab_bytes) {
     __shared__ double vbuf[kThreads * 5];
     __shared__ double abuf[kThreads * 5];
     __shared__ int warp_sums[33];
