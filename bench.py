@@ -39,6 +39,13 @@ METRIC = "voxel-updates/s per timestep, mixed vs FP64 path on 1 B200, at vol err
 UNIT = "voxel-updates/s"
 WORKLOAD = dict(workload="voronoi-128^3-2000-grains-isotropic", domain=128, grains=2000, border=10,
                 time_step=0.2, seed=1002)
+# --workload anisotropic-256: 256^3, 20,000 Voronoi grains with uniform random orientations,
+# Read-Shockley energies (15 degree cutoff), the misorientation mobility model and the
+# convolution correction on; the configuration the mixed-over-FP64 target is quoted on
+ANISOTROPIC = dict(workload="voronoi-256^3-20000-grains-read-shockley-mobility-correction", domain=256,
+                   grains=20000, border=10, time_step=0.2, seed=1003)
+PHYSICS = {}  # GrainHandler physics keywords of the workload (isotropic: none)
+HULL_CAPACITY = 12000  # triangles per hull for the correction's element build
 
 
 # ----------------------------------------------------------------------------------
@@ -120,8 +127,18 @@ STAGE_BYTES = {
     "mixed": {"ms_convolution": 8, "ms_comparison": 12, "ms_levelset": 4, "ms_redistancing": 8},
     "fp64": {"ms_convolution": 16, "ms_comparison": 20, "ms_levelset": 8, "ms_redistancing": 16},
 }
-STAGE_KERNEL = {"ms_convolution": "convolution", "ms_comparison": "compare_kernel", "ms_levelset": "mc_kernel",
-                "ms_redistancing": "redist_xy/z", "ms_lists": "update_lists_kernel"}
+
+
+def measured_traffic(kernel: str, voxels: float):
+    """DRAM bytes (read + write) of one launch of `kernel` over `voxels` box voxels,
+    scaled from the ncu capture summarised in profiles/dram_traffic.json (bytes per
+    voxel-update of the captured launch); None when no capture is recorded."""
+    path = os.path.join(ROOT, "profiles", "dram_traffic.json")
+    if not os.path.exists(path):
+        return None
+    with open(path) as f:
+        rec = json.load(f).get(kernel)
+    return None if rec is None else rec["bytes_per_voxel_update"] * voxels
 
 
 def run_device(gg, precision, ms, ext, counts, steps, warmup, device, dist):
@@ -129,9 +146,11 @@ def run_device(gg, precision, ms, ext, counts, steps, warmup, device, dist):
     import torch
 
     gh = gg.GrainHandler(WORKLOAD["domain"], WORKLOAD["border"], WORKLOAD["time_step"], WORKLOAD["grains"],
-                         precision=precision, device=device)
+                         precision=precision, device=device, **PHYSICS)
     gh.load(ms.labels, ext, counts)
     gh.default_lists()
+    if PHYSICS:
+        gh.set_orientations(ms.euler)
     for _ in range(warmup):
         gh.step()
     reps = []
@@ -160,13 +179,15 @@ def run_e2e(gg, precision, ms, ext, counts, steps, device):
     import torch
 
     gh = gg.GrainHandler(WORKLOAD["domain"], WORKLOAD["border"], WORKLOAD["time_step"], WORKLOAD["grains"],
-                         precision=precision, device=device)
+                         precision=precision, device=device, **PHYSICS)
     labels = np.ascontiguousarray(ms.labels)
     torch.cuda.synchronize()
     ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     ev0.record()
     gh.load(labels, ext, counts)
     gh.default_lists()
+    if PHYSICS:
+        gh.set_orientations(ms.euler)
     vox = 0
     for _ in range(steps):
         vox += gh.step()["voxel_updates"]
@@ -176,6 +197,8 @@ def run_e2e(gg, precision, ms, ext, counts, steps, device):
     ms_elapsed = ev0.elapsed_time(ev1)
     G1 = WORKLOAD["grains"] + 1
     h2d = labels.nbytes + ext.astype(np.int32).nbytes + counts.astype(np.int64).nbytes
+    if PHYSICS:
+        h2d += ms.euler.astype(np.float64).nbytes
     d2h = G1 * (1 + 8 + 8 + 24 + 4)
     gh.close()
     return {"value": vox / (ms_elapsed / 1e3), "unit": UNIT, "h2d_bytes_per_step": int(h2d // steps),
@@ -228,6 +251,10 @@ def reference_arm(args):
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return
+    if PHYSICS:
+        print(json.dumps({"impl": "reference", "unavailable": "the host reference is timed on the default "
+                          "workload only; one anisotropic 256^3 step takes it many minutes"}))
+        return
     ms, _, _ = microstructure()
     threads = os.cpu_count() or 1
     value, sample, cores, kind = run_reference_cpu(ms, args.steps, args.warmup, threads)
@@ -267,8 +294,15 @@ def main():
                     help="profiling aid: run only one precision path")
     ap.add_argument("--domain", type=int, default=None, help="profiling aid: smaller domain of the same kind")
     ap.add_argument("--grains", type=int, default=None, help="profiling aid: grain count for --domain")
+    ap.add_argument("--workload", default="voronoi-128", choices=["voronoi-128", "anisotropic-256"],
+                    help="anisotropic-256: the 256^3 / 20,000-grain anisotropic workload with the correction")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
+    if args.workload == "anisotropic-256":
+        WORKLOAD.clear()
+        WORKLOAD.update(ANISOTROPIC)
+        PHYSICS.update(correction=True, unique_energies=False, mobility_model=True, hull_capacity=HULL_CAPACITY)
+        args.no_cpu_baseline = True  # the host reference needs many minutes per step here
     if args.domain:
         WORKLOAD.update(workload=f"voronoi-{args.domain}^3-{args.grains}-grains-isotropic", domain=args.domain,
                         grains=args.grains)
@@ -328,11 +362,14 @@ def main():
         return {k: float(np.mean([r[k] for r in reps])) for k in keys}
 
     st_m, st_d = stage_means(reps_m), stage_means(reps_d)
-    dom = max((k for k in st_m if k not in ("ms_total",)), key=lambda k: st_m[k])
     peak, peak_kind = read_peaks()
-    vox_per_step = np.mean([r["voxel_updates"] for r in reps_m])
-    bytes_per = STAGE_BYTES["mixed"].get(dom)
-    achieved = (bytes_per * vox_per_step / (st_m[dom] / 1e3) / 1e9) if bytes_per else None
+    # the dominant kernel (the largest share of the launch list): the comparison,
+    # timed alone by the library's events on its stream
+    ms_k = float(np.mean([r["ms_compare_kernel"] for r in reps_m]))
+    vox_k = float(np.mean([r["compare_voxels"] for r in reps_m]))
+    bytes_per = STAGE_BYTES["mixed"]["ms_comparison"]
+    achieved = bytes_per * vox_k / (ms_k / 1e3) / 1e9
+    traffic = measured_traffic("compare_kernel", vox_k)
 
     e2e = None
     out = None
@@ -354,9 +391,10 @@ def main():
             "mixed_over_fp64": value / value_fp64,
             "max_rel_volume_err_mixed_vs_fp64": max_rel,
             "stage_ms": st_m,
-            "roofline": {"bound": "hbm", "kernel": STAGE_KERNEL[dom], "achieved": achieved, "peak": peak,
-                         "unit": "GB/s", "frac": (achieved / peak) if achieved else None, "traffic": None,
-                         "peak_source": peak_kind, "bytes_per_voxel_update": bytes_per},
+            "roofline": {"bound": "hbm", "kernel": "compare_kernel", "achieved": achieved, "peak": peak,
+                         "unit": "GB/s", "frac": achieved / peak, "traffic": traffic,
+                         "peak_source": peak_kind, "bytes_per_voxel_update": bytes_per,
+                         "ms_per_launch": ms_k, "voxels_per_launch": vox_k},
             "cpu_baseline": cpu,
             "e2e": {k: e2e[k] for k in ("value", "unit", "h2d_bytes_per_step", "d2h_bytes_per_step")},
             "gpu_launches": int(sum(r["kernel_launches"] for r in reps_m)),

@@ -56,7 +56,7 @@ class StepStats(C.Structure):
         ("loop", C.c_int32), ("grain_count", C.c_int32), ("live_grains", C.c_int32), ("kernel_launches", C.c_int32),
         ("voxel_updates", C.c_int64), ("ms_convolution", C.c_float), ("ms_lists", C.c_float),
         ("ms_comparison", C.c_float), ("ms_levelset", C.c_float), ("ms_redistancing", C.c_float),
-        ("ms_total", C.c_float),
+        ("ms_total", C.c_float), ("ms_compare_kernel", C.c_float), ("compare_voxels", C.c_int64),
     ]
 
     def as_dict(self) -> dict:

@@ -99,7 +99,7 @@ struct gg_ctx {
     int side_limit = 0;    // largest side the shared-memory kernels accept
     int list_cap = 4096, slab = 8;
     long long launches = 0;  // kernels launched by this context
-    cudaEvent_t ev[7] = {};
+    cudaEvent_t ev[8] = {};  // stage boundaries (0-5), the comparison kernel (6, 7)
 };
 
 namespace {
@@ -502,7 +502,9 @@ int stage_comparison_t(gg_ctx* ctx) {
     a.pos_cap = ctx->pos_cap;
     a.newbox = ctx->d_newbox;
     a.err = ctx->d_err;
+    cudaEventRecord(ctx->ev[6], ctx->stream);
     launch_compare<T>(a, ctx->num_sms * 4, ctx->stream);
+    cudaEventRecord(ctx->ev[7], ctx->stream);
     ctx->launches += 1;
     CK(cudaGetLastError());
     ctx->q ^= 1;
@@ -602,6 +604,8 @@ int step_t(gg_ctx* ctx, gg_step_stats* st) {
         float* f[5] = {&st->ms_convolution, &st->ms_lists, &st->ms_comparison, &st->ms_levelset, &st->ms_redistancing};
         for (int i = 0; i < 5; i++) cudaEventElapsedTime(f[i], ctx->ev[i], ctx->ev[i + 1]);
         cudaEventElapsedTime(&st->ms_total, ctx->ev[0], ctx->ev[5]);
+        cudaEventElapsedTime(&st->ms_compare_kernel, ctx->ev[6], ctx->ev[7]);
+        st->compare_voxels = *ctx->h_total_vox;
     }
     ctx->loop++;
     return GG_OK;

@@ -64,6 +64,8 @@ typedef struct {
     int32_t kernel_launches;    /* kernels this library launched for the step */
     int64_t voxel_updates;      /* sum of n^3 over the boxes convolved this step */
     float ms_convolution, ms_lists, ms_comparison, ms_levelset, ms_redistancing, ms_total;
+    float ms_compare_kernel;    /* the comparison kernel alone (device time) */
+    int64_t compare_voxels;     /* box voxels that kernel compared */
 } gg_step_stats;
 
 /* grainhdl::grainhdl + initializeSimulation (grainhdl.cpp:50-128): allocate the
