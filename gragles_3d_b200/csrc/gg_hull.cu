@@ -937,26 +937,46 @@ __global__ void __launch_bounds__(kCThreads, 2) correction_kernel(CorrectionArgs
             const int nv = min(R, ny - yp) * nx;
             for (int d = threadIdx.x; d < nd; d += blockDim.x) dcnt[d] = 0;
             __syncthreads();
-            // band voxels: their neighbour; voxels whose neighbour no element holds get (1, 1) now
-            for (int q = threadIdx.x; q < nv; q += blockDim.x) {
-                const int i = b.y0 + yp + q / nx, j = b.x0 + q % nx;
-                const long long f = b.at(i, j, k);
-                const double val = (double)in[f];
-                unsigned short dd = kNoD;
-                if (fabs(val) < delta) {
-                    // IDLocal flat-resized onto the box (dimensionalBuffer.h:120-131)
-                    const uint32_t id = f < old_count ? idl[f] : 0u;
-                    unsigned hs = (id * 2654435761u) & (kCHash - 1);
-                    for (int probe = 0; probe < kCHash; probe++) {
-                        const uint32_t key = hkey[hs];
-                        if (key == id) { dd = hden[hs]; break; }
-                        if (key == kNoId) break;
-                        hs = (hs + 1) & (kCHash - 1);
+            // band voxels: their neighbour; voxels whose neighbour no element holds get (1, 1)
+            // now.  Four voxels per thread at a time: their loads are in flight together.
+            constexpr int kBatch = 4;
+            for (int q0 = threadIdx.x; q0 < nv; q0 += kBatch * blockDim.x) {
+                double vals[kBatch];
+                uint32_t ids[kBatch];
+                long long fs[kBatch];
+#pragma unroll
+                for (int u = 0; u < kBatch; u++) {
+                    const int q = q0 + u * blockDim.x;
+                    fs[u] = 0;
+                    vals[u] = delta;  // outside the band
+                    ids[u] = 0u;
+                    if (q < nv) {
+                        const int i = b.y0 + yp + q / nx, j = b.x0 + q % nx;
+                        fs[u] = b.at(i, j, k);
+                        vals[u] = (double)in[fs[u]];
+                        // IDLocal flat-resized onto the box (dimensionalBuffer.h:120-131)
+                        ids[u] = fs[u] < old_count ? idl[fs[u]] : 0u;
                     }
-                    if (dd != kNoD) atomicAdd(&dcnt[dd], 1);
-                    else correct_voxel(a, elem, g, -1, id, val, out + f);
                 }
-                vd[q] = dd;
+#pragma unroll
+                for (int u = 0; u < kBatch; u++) {
+                    const int q = q0 + u * blockDim.x;
+                    if (q >= nv) continue;
+                    unsigned short dd = kNoD;
+                    if (fabs(vals[u]) < delta) {
+                        const uint32_t id = ids[u];
+                        unsigned hs = (id * 2654435761u) & (kCHash - 1);
+                        for (int probe = 0; probe < kCHash; probe++) {
+                            const uint32_t key = hkey[hs];
+                            if (key == id) { dd = hden[hs]; break; }
+                            if (key == kNoId) break;
+                            hs = (hs + 1) & (kCHash - 1);
+                        }
+                        if (dd != kNoD) atomicAdd(&dcnt[dd], 1);
+                        else correct_voxel(a, elem, g, -1, id, vals[u], out + fs[u]);
+                    }
+                    vd[q] = dd;
+                }
             }
             __syncthreads();
             if (warp == 0) {  // bucket offsets and packet counts: warp scans over the neighbours
