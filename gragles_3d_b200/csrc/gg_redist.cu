@@ -44,7 +44,7 @@ struct Intersect {
 // isgn(s) * h is exactly h, -h or +0.
 template <typename T>
 __device__ __forceinline__ T add_sgn(T x, T s, T h) {
-    return s > T(0) ? x + h : (s < T(0) ? x - h : x + T(0));
+    return x + (s > T(0) ? h : (s < T(0) ? -h : T(0)));  // x - h is x + (-h) in IEEE arithmetic
 }
 
 // The interpolation step at a sign change between a (here) and b (next), then the
@@ -81,6 +81,7 @@ __device__ __forceinline__ void sweep_forward(T* o, int so, const T* in, int si,
     if (p < pin) {
         const T* ip = in + p0 * si;
         T icur = *ip;
+#pragma unroll 4
         for (; p < pin; p++, op += so, ip += si) {
             T nxt = op[so];
             const T inx = ip[si];
@@ -90,6 +91,7 @@ __device__ __forceinline__ void sweep_forward(T* o, int so, const T* in, int si,
             icur = inx;
         }
     }
+#pragma unroll 4
     for (; p < p_end - 1; p++, op += so) {
         T nxt = op[so];
         step_prop(nxt, cur, nxt, h);
@@ -112,6 +114,7 @@ __device__ __forceinline__ void sweep_backward_prop(T* o, int so, const T* in, i
     if (inside) {
         const int plim = max(p_in_lo, p_lo);
         const T* ip = in + (p_start - 1) * si;
+#pragma unroll 4
         for (; p > plim; p--, op -= so, ip -= si) {
             T nxt = op[-so];
             step_prop(*ip, cur, nxt, h);
@@ -119,6 +122,7 @@ __device__ __forceinline__ void sweep_backward_prop(T* o, int so, const T* in, i
             cur = nxt;
         }
     }
+#pragma unroll 4
     for (; p > p_lo; p--, op -= so) {
         T nxt = op[-so];
         step_prop(nxt, cur, nxt, h);
@@ -140,6 +144,7 @@ __device__ __forceinline__ void sweep_backward_in(T* o, int so, const T* in, int
     if (inside && p > plim) {
         const T* ip = in + p_start * si;
         T icur = *ip;
+#pragma unroll 4
         for (; p > plim; p--, op -= so, ip -= si) {
             T nxt = op[-so];
             const T inx = ip[-si];
@@ -149,6 +154,7 @@ __device__ __forceinline__ void sweep_backward_in(T* o, int so, const T* in, int
             icur = inx;
         }
     }
+#pragma unroll 4
     for (; p > p_lo; p--, op -= so) {
         T nxt = op[-so];
         step_prop(nxt, cur, nxt, h);
