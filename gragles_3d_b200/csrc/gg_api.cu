@@ -883,68 +883,47 @@ int gg_load_state(gg_ctx* ctx, const uint32_t* labels, const int32_t* extents, c
 int gg_set_lists(gg_ctx* ctx, const int64_t* offsets, const uint32_t* ids) {
     if (!ctx || !offsets || (!ids && offsets[ctx->G + 1] > 0)) return GG_ERR_INVALID;
     const int G = ctx->G, cap = ctx->list_cap;
-    std::vector<uint32_t> rows((size_t)cap * (G + 1), 0);
-    std::vector<int> n(G + 1, 0);
     for (int g = 1; g <= G; g++) {
         const int64_t len = offsets[g + 1] - offsets[g];
         if (len < 0 || len > cap) return fail(ctx, GG_ERR_LIST_OVERFLOW, "list of grain %d has %lld entries", g, (long long)len);
         for (int64_t k = 0; k < len; k++) {
             const uint32_t v = ids[offsets[g] + k];
             if (v < 1 || v > (uint32_t)G) return fail(ctx, GG_ERR_INVALID, "list of grain %d names grain %u", g, v);
-            rows[(size_t)g * cap + k] = v;
         }
-        n[g] = (int)len;
     }
-    CK(cudaMemcpy(ctx->d_son, rows.data(), rows.size() * sizeof(uint32_t), cudaMemcpyHostToDevice));
-    CK(cudaMemcpy(ctx->d_nson, n.data(), n.size() * sizeof(int), cudaMemcpyHostToDevice));
-    CK(cudaMemcpy(ctx->d_cmp, rows.data(), rows.size() * sizeof(uint32_t), cudaMemcpyHostToDevice));
-    CK(cudaMemcpy(ctx->d_ncmp, n.data(), n.size() * sizeof(int), cudaMemcpyHostToDevice));
+    // the packed lists cross once; a kernel spreads them over the fixed-capacity rows
+    const int64_t total = offsets[G + 1];
+    int64_t* d_off = nullptr;
+    uint32_t* d_ids = nullptr;
+    CK(dalloc(&d_off, (size_t)G + 2));
+    CK(dalloc(&d_ids, (size_t)(total > 0 ? total : 1)));
+    CK(cudaMemcpyAsync(d_off, offsets, sizeof(int64_t) * (G + 2), cudaMemcpyHostToDevice, ctx->stream));
+    if (total > 0) CK(cudaMemcpyAsync(d_ids, ids, sizeof(uint32_t) * total, cudaMemcpyHostToDevice, ctx->stream));
+    launch_scatter_lists(G, d_off, d_ids, ctx->d_cmp, ctx->d_ncmp, ctx->d_son, ctx->d_nson, cap, ctx->stream);
+    ctx->launches += 1;
+    CK(cudaGetLastError());
+    CK(cudaStreamSynchronize(ctx->stream));
+    CK(cudaFree(d_off));
+    CK(cudaFree(d_ids));
     return GG_OK;
 }
 
 int gg_default_lists(gg_ctx* ctx) {
     if (!ctx || !ctx->loaded) return GG_ERR_INVALID;
-    const int G = ctx->G;
-    std::vector<int> box(6 * (G + 1)), present(G + 1);
-    CK(cudaMemcpy(box.data(), ctx->d_box[ctx->p ^ 1], sizeof(int) * box.size(), cudaMemcpyDeviceToHost));
-    CK(cudaMemcpy(present.data(), ctx->d_present, sizeof(int) * present.size(), cudaMemcpyDeviceToHost));
-    // uniform grid of cells no smaller than the largest box: each box meets at most 8 cells
-    const int cell = std::max(1, ctx->side_max + 1);
-    const int nc = ctx->M / cell + 2;
-    std::vector<std::vector<int>> cells((size_t)nc * nc * nc);
-    auto cid = [&](int x, int y, int z) { return ((size_t)z * nc + y) * nc + x; };
-    for (int g = 1; g <= G; g++) {
-        if (!present[g]) continue;
-        const int* b = &box[6 * g];
-        for (int z = b[4] / cell; z <= b[5] / cell; z++)
-            for (int y = b[2] / cell; y <= b[3] / cell; y++)
-                for (int x = b[0] / cell; x <= b[1] / cell; x++) cells[cid(x, y, z)].push_back(g);
-    }
-    std::vector<int64_t> off(G + 2, 0);
-    std::vector<uint32_t> ids;
-    std::vector<int> seen(G + 1, 0);
-    for (int g = 1; g <= G; g++) {
-        off[g] = (int64_t)ids.size();
-        if (!present[g]) continue;
-        const int* a = &box[6 * g];
-        std::vector<uint32_t> mine;
-        for (int z = a[4] / cell; z <= a[5] / cell; z++)
-            for (int y = a[2] / cell; y <= a[3] / cell; y++)
-                for (int x = a[0] / cell; x <= a[1] / cell; x++)
-                    for (int o : cells[cid(x, y, z)]) {
-                        if (o == g || seen[o] == g) continue;
-                        const int* b = &box[6 * o];
-                        // inclusive overlap, as the reference's R-tree search (RTree.h Overlap)
-                        if (a[0] > b[1] || a[1] < b[0] || a[2] > b[3] || a[3] < b[2] || a[4] > b[5] || a[5] < b[4])
-                            continue;
-                        seen[o] = g;
-                        mine.push_back((uint32_t)o);
-                    }
-        std::sort(mine.begin(), mine.end());
-        ids.insert(ids.end(), mine.begin(), mine.end());
-    }
-    off[G + 1] = (int64_t)ids.size();
-    return gg_set_lists(ctx, off.data(), ids.data());
+    DefaultListArgs a{};
+    a.G = ctx->G;
+    a.present = ctx->d_present;
+    a.box = ctx->d_box[ctx->p ^ 1];
+    a.cmp = ctx->d_cmp;
+    a.n_cmp = ctx->d_ncmp;
+    a.son = ctx->d_son;
+    a.n_son = ctx->d_nson;
+    a.list_cap = ctx->list_cap;
+    a.err = ctx->d_err;
+    launch_default_lists(a, ctx->stream);
+    ctx->launches += 1;
+    CK(cudaGetLastError());
+    return check_err(ctx, "gg_default_lists");
 }
 
 int gg_stage_convolution(gg_ctx* ctx) {

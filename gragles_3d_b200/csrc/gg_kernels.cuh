@@ -64,6 +64,26 @@ struct ListCopyArgs {
 };
 void launch_copy_lists(const ListCopyArgs& a, int grid, cudaStream_t s);
 
+// Initial comparison lists (the reference's R-tree search, grainhdl.cpp:1029-1054):
+// every present grain whose box touches the grain's box (inclusive), in ascending ID
+// order, written to both list rows.
+struct DefaultListArgs {
+    int G;
+    const int* present;
+    const int* box;
+    uint32_t* cmp;
+    int* n_cmp;
+    uint32_t* son;
+    int* n_son;
+    int list_cap;
+    int* err;
+};
+void launch_default_lists(const DefaultListArgs& a, cudaStream_t s);
+
+// Caller-given lists: packed IDs with per-grain offsets scattered into both list rows.
+void launch_scatter_lists(int G, const int64_t* offsets, const uint32_t* ids, uint32_t* cmp, int* n_cmp,
+                          uint32_t* son, int* n_son, int list_cap, cudaStream_t s);
+
 template <typename T>
 struct CompareArgs {
     Geometry geo;

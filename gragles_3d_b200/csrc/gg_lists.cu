@@ -176,7 +176,61 @@ __global__ void __launch_bounds__(128) pos_table_kernel(PosTableArgs a) {
     }
 }
 
+// One warp per grain: the lanes test 32 candidate IDs at a time in ascending order and
+// append the touching ones by ballot, so the row comes out sorted.
+__global__ void __launch_bounds__(256) default_lists_kernel(DefaultListArgs a) {
+    const int lane = threadIdx.x & 31;
+    const int warps = (gridDim.x * blockDim.x) >> 5;
+    for (int g = 1 + ((blockIdx.x * blockDim.x + threadIdx.x) >> 5); g <= a.G; g += warps) {
+        uint32_t* cmp = a.cmp + (long long)g * a.list_cap;
+        uint32_t* son = a.son + (long long)g * a.list_cap;
+        int n = 0;
+        if (a.present[g]) {
+            const Box self = load_box(a.box + 6 * g);
+            for (int o0 = 1; o0 <= a.G; o0 += 32) {
+                const int o = o0 + lane;
+                bool hit = false;
+                if (o <= a.G && o != g && a.present[o]) hit = touch(self, load_box(a.box + 6 * o));
+                const unsigned m = __ballot_sync(0xffffffffu, hit);
+                const int at = n + __popc(m & ((1u << lane) - 1));
+                if (hit && at < a.list_cap) {
+                    cmp[at] = (uint32_t)o;
+                    son[at] = (uint32_t)o;
+                }
+                n += __popc(m);
+            }
+        }
+        if (lane == 0) {
+            if (n > a.list_cap) atomicOr(a.err, ERR_LIST);
+            a.n_cmp[g] = a.n_son[g] = min(n, a.list_cap);
+        }
+    }
+}
+
+__global__ void scatter_lists_kernel(int G, const int64_t* offsets, const uint32_t* ids, uint32_t* cmp, int* n_cmp,
+                                     uint32_t* son, int* n_son, int list_cap) {
+    for (int g = blockIdx.x; g <= G; g += gridDim.x) {
+        const long long o = g >= 1 ? offsets[g] : 0, len = g >= 1 ? offsets[g + 1] - o : 0;
+        for (int k = threadIdx.x; k < len; k += blockDim.x) {
+            cmp[(long long)g * list_cap + k] = ids[o + k];
+            son[(long long)g * list_cap + k] = ids[o + k];
+        }
+        if (threadIdx.x == 0) n_cmp[g] = n_son[g] = (int)len;
+    }
+}
+
 }  // namespace
+
+void launch_default_lists(const DefaultListArgs& a, cudaStream_t s) {
+    const int warps = a.G + 1;
+    default_lists_kernel<<<(warps + 7) / 8, 256, 0, s>>>(a);
+}
+
+void launch_scatter_lists(int G, const int64_t* offsets, const uint32_t* ids, uint32_t* cmp, int* n_cmp,
+                          uint32_t* son, int* n_son, int list_cap, cudaStream_t s) {
+    scatter_lists_kernel<<<G + 1 < 4096 ? G + 1 : 4096, 128, 0, s>>>(G, offsets, ids, cmp, n_cmp, son, n_son,
+                                                                   list_cap);
+}
 
 void launch_pos_tables(const PosTableArgs& a, int grid, cudaStream_t s) {
     pos_table_kernel<<<grid, 128, 0, s>>>(a);
