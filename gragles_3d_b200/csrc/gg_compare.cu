@@ -213,7 +213,7 @@ struct TileSmem {
     int* tsize;         // per entry: size of its position table
     T* val;             // [entry][voxel]
     unsigned short* pos;// [entry a][entry b]: position of b in a's list, kNotListed, or kUnknown
-    T* topv;            // [part][voxel][kTop], the merged list in part 0
+    T* topv;            // [part][kTop][voxel], the merged list in part 0
     unsigned char* topi;
     int* ncand;         // covering entries with value > -1, per voxel
     unsigned* umask;    // 8 words: entries among some voxel's kTop candidates
@@ -352,8 +352,8 @@ __global__ void __launch_bounds__(kThreads, 4) compare_kernel(CompareArgs<T> a) 
             }
 #pragma unroll
             for (int k = 0; k < kTop; k++) {
-                s.topv[(part * kTV + v) * kTop + k] = tv[k];
-                s.topi[(part * kTV + v) * kTop + k] = (unsigned char)ti[k];
+                s.topv[(part * kTop + k) * kTV + v] = tv[k];
+                s.topi[(part * kTop + k) * kTV + v] = (unsigned char)ti[k];
             }
             s.ncand[part * kTV + v] = nc;
         }
@@ -369,14 +369,14 @@ __global__ void __launch_bounds__(kThreads, 4) compare_kernel(CompareArgs<T> a) 
                 nc += s.ncand[part * kTV + v];
 #pragma unroll
                 for (int k = 0; k < kTop; k++) {
-                    const int e = s.topi[(part * kTV + v) * kTop + k];
-                    if (e != 0xFF) top_insert(tv, ti, s.topv[(part * kTV + v) * kTop + k], e);
+                    const int e = s.topi[(part * kTop + k) * kTV + v];
+                    if (e != 0xFF) top_insert(tv, ti, s.topv[(part * kTop + k) * kTV + v], e);
                 }
             }
 #pragma unroll
             for (int k = 0; k < kTop; k++) {
-                s.topv[v * kTop + k] = tv[k];
-                s.topi[v * kTop + k] = (unsigned char)ti[k];
+                s.topv[k * kTV + v] = tv[k];
+                s.topi[k * kTV + v] = (unsigned char)ti[k];
                 if (ti[k] != 0xFF) atomicOr(s.umask + (ti[k] >> 5), 1u << (ti[k] & 31));
             }
             s.ncand[v] = nc;
@@ -462,9 +462,9 @@ __global__ void __launch_bounds__(kThreads, 4) compare_kernel(CompareArgs<T> a) 
             bool decided = false;
             int k = 0;
             for (; k < kTop; k++) {
-                const int eb = s.topi[v * kTop + k];
+                const int eb = s.topi[k * kTV + v];
                 if (eb == 0xFF) break;
-                const T w = s.topv[v * kTop + k];
+                const T w = s.topv[k * kTV + v];
                 if (best >= 0 && !(w == level)) { decided = true; break; }
                 if (eb == ea) continue;
                 const unsigned short p = s.pos[ea * m + eb];
