@@ -41,7 +41,11 @@ constexpr int kThreads = 256;
 constexpr int kTV = kTX * kTY * kTZ;   // voxels per tile (64)
 constexpr int kTop = 4;                // candidates kept per voxel
 constexpr int kParts = kThreads / kTV; // threads scanning the boxes of one voxel
+// row stride of the staged values: the kParts lanes of a voxel read kVS apart, which
+// puts the 32 lanes of a warp on 32 different banks
+constexpr int kVS = kTV + 8;
 static_assert(kTV % 32 == 0 && kThreads % kTV == 0, "a warp's lanes share one tile entry per pair sweep");
+static_assert(kThreads == kTV * kParts && kTop == 4 && (kParts & (kParts - 1)) == 0, "top-4 merge layout");
 constexpr unsigned kNone = 0xFFFFFFFFu;
 constexpr unsigned short kNotListed = 0xFFFF;
 
@@ -213,7 +217,7 @@ struct TileSmem {
     int* tsize;         // per entry: size of its position table
     T* val;             // [entry][voxel]
     unsigned short* pos;// [entry a][entry b]: position of b in a's list, kNotListed, or kUnknown
-    T* topv;            // [part][kTop][voxel], the merged list in part 0
+    T* topv;            // [kTop][voxel]
     unsigned char* topi;
     int* ncand;         // covering entries with value > -1, per voxel
     unsigned* umask;    // 8 words: entries among some voxel's kTop candidates
@@ -228,13 +232,13 @@ __device__ TileSmem<T> carve(unsigned char* base, int mcap) {
     s.off = reinterpret_cast<long long*>(p); p += 8 * mcap;
     s.outoff = reinterpret_cast<long long*>(p); p += 8 * mcap;
     s.idoff = reinterpret_cast<long long*>(p); p += 8 * mcap;
-    s.val = reinterpret_cast<T*>(p); p += sizeof(T) * (size_t)mcap * kTV;
-    s.topv = reinterpret_cast<T*>(p); p += sizeof(T) * kTV * kTop * kParts;
+    s.val = reinterpret_cast<T*>(p); p += sizeof(T) * (size_t)mcap * kVS;
+    s.topv = reinterpret_cast<T*>(p); p += sizeof(T) * kTV * kTop;
     s.id = reinterpret_cast<uint32_t*>(p); p += 4 * mcap;
     s.box = reinterpret_cast<int*>(p); p += 24 * mcap;
     s.bbox = reinterpret_cast<int*>(p); p += 24 * mcap;
     s.tsize = reinterpret_cast<int*>(p); p += 4 * mcap;
-    s.ncand = reinterpret_cast<int*>(p); p += 4 * kTV * kParts;
+    s.ncand = reinterpret_cast<int*>(p); p += 4 * kTV;
     s.umask = reinterpret_cast<unsigned*>(p); p += 4 * 8;
     s.nu = reinterpret_cast<int*>(p); p += 16;
     s.pos = reinterpret_cast<unsigned short*>(p); p += 2 * (size_t)mcap * mcap;
@@ -328,58 +332,78 @@ __global__ void __launch_bounds__(kThreads, 4) compare_kernel(CompareArgs<T> a) 
                     const int v = vv + lane;
                     const int x = X0 + v % kTX, y = Y0 + (v / kTX) % kTY, z = Z0 + v / (kTX * kTY);
                     if (x >= B.x0 && x < B.x1 && y >= B.y0 && y < B.y1 && z >= B.z0 && z < B.z1)
-                        cp_async_elem(s.val + e * kTV + v, src + B.at(y, x, z));
+                        cp_async_elem(s.val + e * kVS + v, src + B.at(y, x, z));
                     else
-                        s.val[e * kTV + v] = NEG;
+                        s.val[e * kVS + v] = NEG;
                 }
             }
         }
         cp_async_wait_all();
         __syncthreads();
-        // per voxel: the kTop largest values > -1 (kParts threads share a voxel)
+        // per voxel: the kTop largest values > -1.  The kParts lanes of a voxel are
+        // neighbours in one warp; each keeps the top of every kParts-th box, then two
+        // shuffle rounds merge their lists (a bitonic merge of two sorted lists of kTop).
         {
-            const int v = threadIdx.x % kTV, part = threadIdx.x / kTV;
+            const int lane = threadIdx.x & 31;
+            const int part = lane & (kParts - 1), v = (threadIdx.x >> 5) * (32 / kParts) + (lane / kParts);
             T tv[kTop];
             int ti[kTop];
 #pragma unroll
             for (int k = 0; k < kTop; k++) { tv[k] = NEG; ti[k] = 0xFF; }
             int nc = 0;
             for (int e = part; e < m; e += kParts) {
-                const T w = s.val[e * kTV + v];
+                const T w = s.val[e * kVS + v];
                 if (!(w > T(-1))) continue;
                 nc++;
                 top_insert(tv, ti, w, e);
             }
 #pragma unroll
-            for (int k = 0; k < kTop; k++) {
-                s.topv[(part * kTop + k) * kTV + v] = tv[k];
-                s.topi[(part * kTop + k) * kTV + v] = (unsigned char)ti[k];
-            }
-            s.ncand[part * kTV + v] = nc;
-        }
-        __syncthreads();
-        if (threadIdx.x < kTV) {  // merge the kParts partial lists
-            const int v = threadIdx.x;
-            T tv[kTop];
-            int ti[kTop];
-#pragma unroll
-            for (int k = 0; k < kTop; k++) { tv[k] = NEG; ti[k] = 0xFF; }
-            int nc = 0;
-            for (int part = 0; part < kParts; part++) {
-                nc += s.ncand[part * kTV + v];
+            for (int o = 1; o < kParts; o <<= 1) {
+                T pv[kTop];
+                int pi[kTop];
 #pragma unroll
                 for (int k = 0; k < kTop; k++) {
-                    const int e = s.topi[(part * kTop + k) * kTV + v];
-                    if (e != 0xFF) top_insert(tv, ti, s.topv[(part * kTop + k) * kTV + v], e);
+                    pv[k] = __shfl_xor_sync(0xffffffffu, tv[k], o);
+                    pi[k] = __shfl_xor_sync(0xffffffffu, ti[k], o);
                 }
-            }
+                nc += __shfl_xor_sync(0xffffffffu, nc, o);
+                // both lanes merge (lower part's list, higher part's list) alike
+                const bool low = (lane & o) == 0;
+                T av[kTop], bv[kTop];
+                int ai[kTop], bi[kTop];
 #pragma unroll
-            for (int k = 0; k < kTop; k++) {
-                s.topv[k * kTV + v] = tv[k];
-                s.topi[k * kTV + v] = (unsigned char)ti[k];
-                if (ti[k] != 0xFF) atomicOr(s.umask + (ti[k] >> 5), 1u << (ti[k] & 31));
+                for (int k = 0; k < kTop; k++) {
+                    av[k] = low ? tv[k] : pv[k];
+                    ai[k] = low ? ti[k] : pi[k];
+                    bv[k] = low ? pv[k] : tv[k];
+                    bi[k] = low ? pi[k] : ti[k];
+                }
+                // the kTop largest of both: max(a[k], b[kTop-1-k]), a bitonic sequence
+#pragma unroll
+                for (int k = 0; k < kTop; k++) {
+                    const bool ta = !(bv[kTop - 1 - k] > av[k]);
+                    tv[k] = ta ? av[k] : bv[kTop - 1 - k];
+                    ti[k] = ta ? ai[k] : bi[kTop - 1 - k];
+                }
+                // sorted descending by a bitonic half-cleaner cascade
+#pragma unroll
+                for (int j = kTop / 2; j > 0; j >>= 1)
+#pragma unroll
+                    for (int k = 0; k < kTop; k++)
+                        if ((k & j) == 0 && tv[k + j] > tv[k]) {
+                            const T t = tv[k]; tv[k] = tv[k + j]; tv[k + j] = t;
+                            const int u = ti[k]; ti[k] = ti[k + j]; ti[k + j] = u;
+                        }
             }
-            s.ncand[v] = nc;
+            if (part == 0) {
+#pragma unroll
+                for (int k = 0; k < kTop; k++) {
+                    s.topv[k * kTV + v] = tv[k];
+                    s.topi[k * kTV + v] = (unsigned char)ti[k];
+                    if (ti[k] != 0xFF) atomicOr(s.umask + (ti[k] >> 5), 1u << (ti[k] & 31));
+                }
+                s.ncand[v] = nc;
+            }
         }
         __syncthreads();
         // the columns of pos the pair loop reads: every entry that is among some voxel's
@@ -451,7 +475,7 @@ __global__ void __launch_bounds__(kThreads, 4) compare_kernel(CompareArgs<T> a) 
         const double lim = 0.7 * a.geo.delta;
         for (int q = threadIdx.x; q < m * kTV; q += blockDim.x) {
             const int ea = q / kTV, v = q % kTV;
-            const T in = s.val[q];
+            const T in = s.val[ea * kVS + v];
             const int x = X0 + v % kTX, y = Y0 + (v / kTX) % kTY, z = Z0 + v / (kTX * kTY);
             bool positive = false;
             if (in != NEG) {  // else the voxel is outside this grain's box
@@ -479,7 +503,7 @@ __global__ void __launch_bounds__(kThreads, 4) compare_kernel(CompareArgs<T> a) 
                 level = NEG;
                 for (int eb = 0; eb < m; eb++) {
                     if (eb == ea) continue;
-                    const T w = s.val[eb * kTV + v];
+                    const T w = s.val[eb * kVS + v];
                     if (!(w > T(-1))) continue;
                     if (best >= 0 && w < level) continue;
                     const unsigned short p = ((s.umask[eb >> 5] >> (eb & 31)) & 1u)
@@ -495,7 +519,7 @@ __global__ void __launch_bounds__(kThreads, 4) compare_kernel(CompareArgs<T> a) 
             T cmpv;
             uint32_t idv;
             if (best >= 0) {
-                cmpv = s.val[best * kTV + v];
+                cmpv = s.val[best * kVS + v];
                 idv = s.id[best];
             } else {  // no listed neighbour covers the voxel: value -1, IDLocal kept
                 cmpv = T(-1);
@@ -567,9 +591,9 @@ __global__ void newbox_init_kernel(int G, const int* present, const int* exists,
 
 size_t compare_smem_bytes(int mcap, bool fp64) {
     const size_t e = fp64 ? 8 : 4;
-    return 24 * (size_t)mcap + e * (size_t)mcap * kTV + e * kTV * kTop * kParts + 4 * (size_t)mcap +
-           48 * (size_t)mcap + 4 * (size_t)mcap + 4 * kTV * kParts + 48 + 2 * (size_t)mcap * mcap + 256 +
-           kTV * kTop * kParts + 64;
+    return 24 * (size_t)mcap + e * (size_t)mcap * kVS + e * kTV * kTop + 4 * (size_t)mcap +
+           48 * (size_t)mcap + 4 * (size_t)mcap + 4 * kTV + 48 + 2 * (size_t)mcap * mcap + 256 +
+           kTV * kTop + 64;
 }
 
 long long bin_capacity(int G, int side) {
