@@ -282,7 +282,9 @@ __global__ void __launch_bounds__(kThreads, 3) mc_kernel(MCArgs<T> a, int slab_b
 #pragma unroll
                 for (int k = 0; k < 8; k++) {
                     const int at = base + c_nbc[k][2] * plane + c_nbc[k][1] * nxb + c_nbc[k][0];
-                    unsigned id = sdf[at] >= 0 ? (unsigned)g : idl[at];
+                    // inside = value >= 0: the staged sign byte of the corner (slab-relative)
+                    const int sat = at - zc0 * plane;
+                    unsigned id = sgn[sat] ? (unsigned)g : idl[at];
                     bool found = false;
                     for (int q = 0; q < cnt; q++) found |= (lst[q] == id);
                     if (!found) {
@@ -306,8 +308,22 @@ __global__ void __launch_bounds__(kThreads, 3) mc_kernel(MCArgs<T> a, int slab_b
                 }
             }
             __syncthreads();
-            if (threadIdx.x == 0) {
-                for (int q = 0; q < chunk_total; q++) {
+            if (threadIdx.x == 0) {  // in triangle order; eight terms' loads in flight at a time
+                int q = 0;
+                for (; q + 8 <= chunk_total; q += 8) {
+                    double tv[8], ta[8];
+#pragma unroll
+                    for (int u = 0; u < 8; u++) {
+                        tv[u] = vbuf[q + u];
+                        ta[u] = abuf[q + u];
+                    }
+#pragma unroll
+                    for (int u = 0; u < 8; u++) {
+                        vol += tv[u];
+                        area += ta[u];
+                    }
+                }
+                for (; q < chunk_total; q++) {
                     vol += vbuf[q];
                     area += abuf[q];
                 }
