@@ -86,7 +86,7 @@ int gg_load_state(gg_ctx* ctx, const uint32_t* labels, const int32_t* extents, c
  * lists as CSR (offsets[n_grains + 2], row = grain ID).  The reference fills them
  * from an R-tree search; the order of each row sets the comparison tie-break. */
 int gg_set_lists(gg_ctx* ctx, const int64_t* offsets, const uint32_t* ids);
-/* The same membership (inclusive box overlap) in grain-ID order. */
+/* The same membership (inclusive box overlap) in grain-ID order, built on the device. */
 int gg_default_lists(gg_ctx* ctx);
 
 /* One loop iteration of grainhdl::run_sim (grainhdl.cpp:837-917). */
@@ -138,8 +138,9 @@ int gg_convolve_boxes_f64(const double* d_in, double* d_out, const int32_t* side
                           int32_t n_boxes, int32_t domain_size, double time_step);
 
 /* The mixed-precision convolution of GG_PRECISION_MIXED on FP32 boxes: three per-axis
- * contractions with the circulant C_n on the tcgen05 tensor cores (3xTF32, FP32
- * accumulation) when every side is <= 64, on the FP32 SIMT kernels otherwise.  Same packing
+ * contractions with the circulant C_n on the tcgen05 tensor cores (operands split into
+ * FP16 hi + lo, three MMAs per K-step, FP32 accumulation in TMEM) when every side is
+ * within the tensor-core kernel's limit, on the FP32 SIMT kernels otherwise.  Same packing
  * and stream as gg_convolve_boxes_f64, except that the offsets must be multiples of 4
  * elements and the buffers must extend to a multiple of 4 elements past the last box
  * (boxes are read as 16-byte aligned spans); allocates its scratch.  Replaces the same
