@@ -48,6 +48,7 @@ static_assert(kTV % 32 == 0 && kThreads % kTV == 0, "a warp's lanes share one ti
 static_assert(kThreads == kTV * kParts && kTop == 4 && (kParts & (kParts - 1)) == 0, "top-4 merge layout");
 constexpr unsigned kNone = 0xFFFFFFFFu;
 constexpr unsigned short kNotListed = 0xFFFF;
+constexpr int kUCap = 32;              // candidate columns of the position matrix
 
 // One branch of the reference's boundary distance (box.cpp:1017-1082).  Returns
 // false where no branch assigns `dist`, in which case the reference keeps the value
@@ -222,6 +223,7 @@ struct TileSmem {
     int* ncand;         // covering entries with value > -1, per voxel
     unsigned* umask;    // 8 words: entries among some voxel's kTop candidates
     unsigned char* ulist;  // those entries, ascending
+    unsigned char* ucol;   // per entry: its column of pos (the first kUCap of ulist), 0xFF: none
     int* nu;            // their count
 };
 
@@ -241,8 +243,9 @@ __device__ TileSmem<T> carve(unsigned char* base, int mcap) {
     s.ncand = reinterpret_cast<int*>(p); p += 4 * kTV;
     s.umask = reinterpret_cast<unsigned*>(p); p += 4 * 8;
     s.nu = reinterpret_cast<int*>(p); p += 16;
-    s.pos = reinterpret_cast<unsigned short*>(p); p += 2 * (size_t)mcap * mcap;
+    s.pos = reinterpret_cast<unsigned short*>(p); p += 2 * (size_t)mcap * kUCap;
     s.ulist = p; p += 256;
+    s.ucol = p; p += 256;
     s.topi = p;
     return s;
 }
@@ -415,7 +418,9 @@ __global__ void __launch_bounds__(kThreads, 4) compare_kernel(CompareArgs<T> a) 
                 const int b = b0 + threadIdx.x;
                 const bool in_u = b < m && ((s.umask[b >> 5] >> (b & 31)) & 1u);
                 const unsigned bal = __ballot_sync(0xffffffffu, in_u);
-                if (in_u) s.ulist[nu + __popc(bal & ((1u << threadIdx.x) - 1))] = (unsigned char)b;
+                const int r = nu + __popc(bal & ((1u << threadIdx.x) - 1));
+                if (in_u) s.ulist[r] = (unsigned char)b;
+                if (b < m) s.ucol[b] = (in_u && r < kUCap) ? (unsigned char)r : (unsigned char)0xFF;
                 nu += __popc(bal);
             }
             if (threadIdx.x == 0) s.nu[0] = nu;
@@ -423,7 +428,7 @@ __global__ void __launch_bounds__(kThreads, 4) compare_kernel(CompareArgs<T> a) 
         __syncthreads();
         {
             constexpr int kBatch = 4;
-            const int nu = s.nu[0];
+            const int nu = min(s.nu[0], kUCap);  // columns beyond kUCap are looked up when needed
             const int mm = m * nu;
             for (int q0 = 0; q0 < mm; q0 += kBatch * kThreads) {
                 unsigned long long e[kBatch];
@@ -435,9 +440,9 @@ __global__ void __launch_bounds__(kThreads, 4) compare_kernel(CompareArgs<T> a) 
 #pragma unroll
                 for (int u = 0; u < kBatch; u++) {
                     const int q = q0 + u * kThreads + threadIdx.x;
-                    const int ea = q / nu, eb = q < mm ? s.ulist[q - ea * nu] : 0;
+                    const int ea = q / nu, col = q - ea * nu, eb = q < mm ? s.ulist[col] : 0;
                     live[u] = q < mm && ea != eb;
-                    dst[u] = ea * m + eb;
+                    dst[u] = ea * kUCap + col;
                     tab[u] = nullptr;
                     h[u] = mask[u] = id[u] = 0;
                     e[u] = 0;
@@ -491,7 +496,9 @@ __global__ void __launch_bounds__(kThreads, 4) compare_kernel(CompareArgs<T> a) 
                 const T w = s.topv[k * kTV + v];
                 if (best >= 0 && !(w == level)) { decided = true; break; }
                 if (eb == ea) continue;
-                const unsigned short p = s.pos[ea * m + eb];
+                const int col = s.ucol[eb];
+                const unsigned short p = col != 0xFF ? s.pos[ea * kUCap + col]
+                                                     : list_position(a, s.id[ea], s.tsize[ea], s.id[eb]);
                 if (p == kNotListed) continue;
                 if (best < 0 || p < bpos) { best = eb; bpos = p; level = w; }
             }
@@ -506,9 +513,9 @@ __global__ void __launch_bounds__(kThreads, 4) compare_kernel(CompareArgs<T> a) 
                     const T w = s.val[eb * kVS + v];
                     if (!(w > T(-1))) continue;
                     if (best >= 0 && w < level) continue;
-                    const unsigned short p = ((s.umask[eb >> 5] >> (eb & 31)) & 1u)
-                                                 ? s.pos[ea * m + eb]
-                                                 : list_position(a, s.id[ea], s.tsize[ea], s.id[eb]);
+                    const int col = s.ucol[eb];
+                    const unsigned short p = col != 0xFF ? s.pos[ea * kUCap + col]
+                                                         : list_position(a, s.id[ea], s.tsize[ea], s.id[eb]);
                     if (p == kNotListed) continue;
                     if (best < 0 || w > level || (w == level && p < bpos)) { best = eb; bpos = p; level = w; }
                 }
@@ -592,7 +599,7 @@ __global__ void newbox_init_kernel(int G, const int* present, const int* exists,
 size_t compare_smem_bytes(int mcap, bool fp64) {
     const size_t e = fp64 ? 8 : 4;
     return 24 * (size_t)mcap + e * (size_t)mcap * kVS + e * kTV * kTop + 4 * (size_t)mcap +
-           48 * (size_t)mcap + 4 * (size_t)mcap + 4 * kTV + 48 + 2 * (size_t)mcap * mcap + 256 +
+           48 * (size_t)mcap + 4 * (size_t)mcap + 4 * kTV + 48 + 2 * (size_t)mcap * kUCap + 512 +
            kTV * kTop + 64;
 }
 
