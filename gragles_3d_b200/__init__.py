@@ -32,6 +32,7 @@ EXPORTED = [
     "gg_stage_redistancing", "gg_get_grain_stats", "gg_get_neighbors", "gg_get_list", "gg_get_sdf",
     "gg_get_idlocal", "gg_grain_count", "gg_loop", "gg_convolve_boxes_f64", "gg_convolve_boxes_mixed",
     "gg_convolve_boxes_f64_noalloc", "gg_set_orientations", "gg_set_stored_energy", "gg_get_elements",
+    "gg_voxel_container",
 ]
 
 
@@ -98,6 +99,7 @@ def load_library(path: str = LIB_PATH):
     L.gg_set_orientations.argtypes = [vp, vp]
     L.gg_set_stored_energy.argtypes = [vp, vp]
     L.gg_get_elements.argtypes = [vp, i32, vp]
+    L.gg_voxel_container.argtypes = [vp, vp]
     _lib = L
     return L
 
@@ -239,6 +241,13 @@ class GrainHandler:
         out = np.zeros(n, np.float64)
         load_library().gg_get_sdf(self._h, gid, which, _p(box), _p(out), n)
         return tuple(int(v) for v in box), out.reshape(box_shape(box))
+
+    def voxel_container(self) -> np.ndarray:
+        """The network as an (N, N, N) [z][y][x] array of grain IDs (the reference's
+        Container_size_N_t_loop.raw)."""
+        out = np.zeros((self.N, self.N, self.N), np.uint32)
+        self._check(load_library().gg_voxel_container(self._h, _p(out)))
+        return out
 
     def idlocal(self, gid: int):
         box = np.zeros(6, np.int32)

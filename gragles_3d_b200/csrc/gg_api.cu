@@ -611,6 +611,22 @@ int step_t(gg_ctx* ctx, gg_step_stats* st) {
     return GG_OK;
 }
 
+template <typename T>
+int voxel_container_t(gg_ctx* ctx, uint32_t* d_labels) {
+    const int a = ctx->p ^ 1;  // m_outputDistance
+    // n tiles per existing grain of the current layout
+    plan(ctx, ctx->d_box[a], 1, nullptr, nullptr, ctx->d_toff_n, nullptr, nullptr);
+    ContainerArgs<T> c{};
+    c.G = ctx->G;
+    c.geo = ctx->geo;
+    c.toff = ctx->d_toff_n;
+    c.src = Arena<const T>{reinterpret_cast<const T*>(ctx->d_arena[a]), ctx->d_box[a], ctx->d_off[a]};
+    c.labels = d_labels;
+    launch_container<T>(c, ctx->grid, ctx->stream);
+    ctx->launches += 1;
+    CK(cudaGetLastError());
+    return GG_OK;
+}
 }  // namespace
 
 // ===================================================================================
@@ -1034,6 +1050,21 @@ int64_t gg_get_idlocal(gg_ctx* ctx, int32_t id, int32_t box[6], uint32_t* out, i
 
 int gg_grain_count(gg_ctx* ctx) { return ctx ? ctx->grain_count : GG_ERR_INVALID; }
 int gg_loop(gg_ctx* ctx) { return ctx ? ctx->loop : GG_ERR_INVALID; }
+
+int gg_voxel_container(gg_ctx* ctx, uint32_t* labels) {
+    if (!ctx || !labels || !ctx->loaded) return GG_ERR_INVALID;
+    const size_t n = (size_t)ctx->N * ctx->N * ctx->N;
+    uint32_t* d = nullptr;
+    CK(dalloc(&d, n));
+    CK(cudaMemsetAsync(d, 0, sizeof(uint32_t) * n, ctx->stream));
+    int rc = ctx->fp64 ? voxel_container_t<double>(ctx, d) : voxel_container_t<float>(ctx, d);
+    if (rc == GG_OK) {
+        CK(cudaMemcpyAsync(labels, d, sizeof(uint32_t) * n, cudaMemcpyDeviceToHost, ctx->stream));
+        CK(cudaStreamSynchronize(ctx->stream));
+    }
+    CK(cudaFree(d));
+    return rc == GG_OK ? check_err(ctx, "gg_voxel_container") : rc;
+}
 
 int gg_set_orientations(gg_ctx* ctx, const double* euler) {
     if (!ctx || !euler) return GG_ERR_INVALID;

@@ -298,6 +298,18 @@ struct InitArgs {
 template <typename T>
 void launch_init_sdf(const InitArgs<T>& a, int grid, cudaStream_t s);
 
+// Voxel container of the network: N^3 grain IDs [z][y][x], 0 where no grain's SDF is >= 0.
+template <typename T>
+struct ContainerArgs {
+    int G;
+    Geometry geo;
+    const int* toff;          // n tiles per existing grain of `src`
+    Arena<const T> src;       // m_outputDistance of every grain
+    uint32_t* labels;         // zeroed by the caller
+};
+template <typename T>
+void launch_container(const ContainerArgs<T>& a, int grid, cudaStream_t s);
+
 // out3 = {present grains, present and existing grains, largest side of `box` among the latter}
 void launch_count(int G, const int* present, const int* exists, const int* box, int* out3, cudaStream_t s);
 

@@ -202,3 +202,13 @@ def write_parameters(path: str, *, n_grains: int, border: int = 10, steps: int =
     body = "\n".join(f"   <{k}>{v}</{k}>" for k, v in p.items())
     with open(path, "w") as f:
         f.write('<?xml version="1.0" encoding="utf-8"?>\n<Parameters>\n' + body + "\n</Parameters>\n")
+
+
+def write_container(directory: str, labels: np.ndarray, loop: int) -> str:
+    """The voxel container of a network (GrainHandler.voxel_container) as the reference's
+    saveNetworkAsVoxelContainer names and writes it (grainhdl.cpp:1116-1123): raw uint32
+    grain IDs, x fastest, in Container_size_<N>_t_<loop>.raw."""
+    lab = np.ascontiguousarray(labels, dtype=np.uint32)
+    path = os.path.join(directory, f"Container_size_{lab.shape[0]}_t_{int(loop)}.raw")
+    lab.tofile(path)
+    return path

@@ -117,6 +117,14 @@ int64_t gg_get_idlocal(gg_ctx* ctx, int32_t id, int32_t box[6], uint32_t* out, i
 int gg_grain_count(gg_ctx* ctx);
 int gg_loop(gg_ctx* ctx);
 
+/* The voxel container of the current network (grainhdl::saveNetworkAsVoxelContainer with
+ * LSbox::copyDataToContainer, grainhdl.cpp:1074-1095, box.cpp:3008-3032): labels =
+ * N^3 grain IDs [z][y][x] (host memory), the largest ID of the grains whose current SDF
+ * (m_outputDistance) is >= 0 at the voxel -- the reference's last writer in ascending
+ * ID order -- and 0 where there is none.  Grains whose hull vanished in the last step
+ * are left out (their buffer is not kept; in the reference it holds no voxel >= 0 then). */
+int gg_voxel_container(gg_ctx* ctx, uint32_t* labels);
+
 /* Grain orientations for the convolution correction's boundary energies and
  * mobilities: Bunge Euler angles phi1, PHI, phi2 in radians, 3 per grain for IDs
  * 1..n_grains (the .uds columns read at grainhdl.cpp:480-504, turned into

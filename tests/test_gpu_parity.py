@@ -180,3 +180,46 @@ def test_loop_mixed_volume_tolerance(gpu, oracle):
             if inf["exists"] and st.exists[g]:
                 worst = max(worst, abs(st.volume[g] - inf["volume"]) / inf["volume"])
     assert worst <= 1e-3, f"max relative volume error {worst}"
+
+
+def _container_from_oracle(osim, N, border, G):
+    """LSbox::copyDataToContainer (box.cpp:3008-3032) over the oracle's grains in
+    ascending ID order: a voxel takes the ID of the last grain whose output SDF is >= 0
+    there.  Grains whose hull vanished must hold no such voxel (the GPU leaves them out)."""
+    want = np.zeros((N, N, N), np.uint32)
+    for g in range(1, G + 1):
+        inf = osim.info(g)
+        if not inf["present"]:
+            continue
+        (x0, x1, y0, y1, z0, z1), sdf = osim.sdf(g)
+        if sdf.size == 0:
+            continue
+        inside = sdf >= 0
+        if not inf["exists"]:
+            assert not inside.any(), f"grain {g}: vanished hull with voxels >= 0"
+            continue
+        zs, ys, xs = np.nonzero(inside)
+        zs, ys, xs = zs + z0 - border, ys + y0 - border, xs + x0 - border
+        ok = (zs >= 0) & (ys >= 0) & (xs >= 0) & (zs < N) & (ys < N) & (xs < N)
+        want[zs[ok], ys[ok], xs[ok]] = g
+    return want
+
+
+@pytest.mark.parametrize("precision", [0, 1])
+def test_voxel_container_matches_oracle(gpu, oracle, precision):
+    """saveNetworkAsVoxelContainer's label volume: exact on the FP64 path at every
+    checked step, including steps where grains vanish; the mixed path's differs only
+    where an SDF sits within its rounding of 0."""
+    c, gh, osim = _pair(gpu, oracle, "vanish", precision=precision)
+    N, G = c["N"], c["G"]
+    for s in range(30):
+        osim.step()
+        gh.step()
+        if s % 6 != 5:
+            continue
+        got = gh.voxel_container()
+        want = _container_from_oracle(osim, N, c["border"], G)
+        if precision == 0:
+            assert np.array_equal(got, want), f"step {s}: {(got != want).sum()} voxels differ"
+        else:
+            assert (got != want).mean() < 1e-3, f"step {s}: {(got != want).sum()} voxels differ"

@@ -126,3 +126,14 @@ def test_replica_aggregation_two_ranks_gloo():
     for r in (0, 1):
         elapsed, vox = res[r]
         assert elapsed == 14.0 and vox == 2200.0
+
+
+def test_container_file_layout(tmp_path):
+    """write_container writes the reference's raw uint32 layout (x fastest) under its name."""
+    from gragles_3d_b200 import microstructure as msgen
+
+    lab = np.arange(4 * 4 * 4, dtype=np.uint32).reshape(4, 4, 4)
+    path = msgen.write_container(str(tmp_path), lab, 7)
+    assert os.path.basename(path) == "Container_size_4_t_7.raw"
+    back = np.fromfile(path, np.uint32)
+    assert np.array_equal(back, lab.ravel())
