@@ -8,6 +8,7 @@ loading fails loudly when the extension is missing.
 from __future__ import annotations
 
 import ctypes as C
+import math
 import dataclasses
 import os
 from typing import Optional
@@ -32,7 +33,7 @@ EXPORTED = [
     "gg_stage_redistancing", "gg_get_grain_stats", "gg_get_neighbors", "gg_get_list", "gg_get_sdf",
     "gg_get_idlocal", "gg_grain_count", "gg_loop", "gg_convolve_boxes_f64", "gg_convolve_boxes_mixed",
     "gg_convolve_boxes_f64_noalloc", "gg_set_orientations", "gg_set_stored_energy", "gg_get_elements",
-    "gg_voxel_container",
+    "gg_voxel_container", "gg_get_faces",
 ]
 
 
@@ -48,7 +49,7 @@ class Params(C.Structure):
         ("n_grains", C.c_int32), ("precision", C.c_int32), ("disable_correction", C.c_int32),
         ("list_capacity", C.c_int32), ("pool_voxels", C.c_int64), ("device", C.c_int32),
         ("unique_gb_energies", C.c_int32), ("mobility_model", C.c_int32), ("use_stored_energy", C.c_int32),
-        ("triple_line_drag", C.c_double), ("hull_capacity", C.c_int32), ("reserved", C.c_int32 * 1),
+        ("triple_line_drag", C.c_double), ("hull_capacity", C.c_int32), ("keep_elements", C.c_int32),
     ]
 
 
@@ -100,8 +101,51 @@ def load_library(path: str = LIB_PATH):
     L.gg_set_stored_energy.argtypes = [vp, vp]
     L.gg_get_elements.argtypes = [vp, i32, vp]
     L.gg_voxel_container.argtypes = [vp, vp]
+    L.gg_get_faces.argtypes = [vp, vp, vp, vp, i64]
+    L.gg_get_faces.restype = i64
     _lib = L
     return L
+
+
+# the reference's analysis records (Structs.h: TextureData, Face), 8-byte aligned
+TEXTURE_DTYPE = np.dtype([("volume", "<f8"), ("surfaceArea", "<f8"), ("GBEnergy", "<f8"), ("BulkEnergy", "<f8"),
+                          ("phi1", "<f8"), ("PHI", "<f8"), ("phi2", "<f8"), ("x", "<f8"), ("y", "<f8"),
+                          ("z", "<f8"), ("id", "<u4"), ("NeighbourCount", "<u4"),
+                          ("intersectsBoundaryGrain", "<u4"), ("pad", "<u4")])
+FACE_DTYPE = np.dtype([("area", "<f8"), ("grainA", "<u4"), ("grainB", "<u4")])
+
+
+def euler_to_quaternion(e) -> tuple:
+    """myQuaternion::euler2Quaternion (myQuaternion.cpp:168-191), Bunge ZXZ."""
+    p1, t, p2 = float(e[0]), float(e[1]), float(e[2])
+    co1, s1 = math.cos(t / 2), math.sin(t / 2)
+    return (co1 * math.cos((p1 + p2) / 2), s1 * math.cos((p1 - p2) / 2), s1 * math.sin((p1 - p2) / 2),
+            co1 * math.sin((p1 + p2) / 2))
+
+
+def quaternion_to_euler(q) -> tuple:
+    """myQuaternion::Quaternion2Euler (myQuaternion.cpp:193-240): (phi1, PHI, phi2)."""
+    q0, q1, q2, q3 = q
+    cos_phi = q3 * q3 - q2 * q2 - q1 * q1 + q0 * q0
+    y0 = 2 * q1 * q3 - 2 * q0 * q2
+    x0 = 2 * q2 * q3 + 2 * q0 * q1
+    y1 = 2 * q1 * q3 + 2 * q0 * q2
+    x1 = -2 * q2 * q3 + 2 * q0 * q1
+    if cos_phi > 1.0:
+        cos_phi = 1.0
+    PHI = 0.0 if (1.0 - cos_phi) * (1.0 - cos_phi) <= 1e-20 else math.acos(cos_phi)  # QUAT2EUL_ETA
+    sP = math.sin(PHI)
+    if sP != 0:
+        phi2 = math.atan2(y0 / sP, x0 / sP)
+        phi1 = math.atan2(y1 / sP, x1 / sP)
+    else:
+        phi1 = math.atan2(2 * q1 * q2 + 2 * q0 * q3, q0 * q0 + q1 * q1 - q2 * q2 - q3 * q3)
+        phi2 = 0.0
+    if phi1 < 0.0:
+        phi1 += 2 * math.pi
+    if phi2 < 0.0:
+        phi2 += 2 * math.pi
+    return phi1, PHI, phi2
 
 
 def _p(a: np.ndarray):
@@ -134,7 +178,7 @@ class GrainHandler:
                  precision: int = PRECISION_FP64, list_capacity: int = 0, pool_voxels: int = 0,
                  device: int = 0, correction: bool = False, unique_energies: bool = True,
                  mobility_model: bool = False, stored_energy: bool = False, triple_line_drag: float = 0.0,
-                 hull_capacity: int = 0):
+                 hull_capacity: int = 0, keep_elements: bool = False):
         L = load_library()
         self.G = int(n_grains)
         self.N = int(domain_size)
@@ -143,7 +187,10 @@ class GrainHandler:
         self.precision = precision
         p = Params(domain_size, border, float(time_step), n_grains, precision, int(not correction), list_capacity,
                    pool_voxels, device, int(unique_energies), int(mobility_model), int(stored_energy),
-                   float(triple_line_drag), hull_capacity)
+                   float(triple_line_drag), hull_capacity, int(keep_elements))
+        self._euler = np.zeros((self.G, 3))
+        self._see = np.zeros(self.G)
+        self._h_grid = 1.0 / self.N
         h = C.c_void_p()
         rc = L.gg_create(C.byref(p), C.byref(h))
         self._h = h
@@ -188,11 +235,13 @@ class GrainHandler:
         """Bunge angles (G, 3) in radians for grain IDs 1..G."""
         e = np.ascontiguousarray(euler, dtype=np.float64)
         self._check(load_library().gg_set_orientations(self._h, _p(e)))
+        self._euler = e.reshape(self.G, 3).copy()
 
     def set_stored_energy(self, see: np.ndarray) -> None:
         """m_StoredElasticEnergy (G,) for grain IDs 1..G."""
         v = np.ascontiguousarray(see, dtype=np.float64)
         self._check(load_library().gg_set_stored_energy(self._h, _p(v)))
+        self._see = v.reshape(self.G).copy()
 
     def elements(self, gid: int) -> tuple:
         """(GB, TL, QJ, HJ) element counts of the grain's last hull (correction on)."""
@@ -241,6 +290,33 @@ class GrainHandler:
         out = np.zeros(n, np.float64)
         load_library().gg_get_sdf(self._h, gid, which, _p(box), _p(out), n)
         return tuple(int(v) for v in box), out.reshape(box_shape(box))
+
+    def faces(self) -> np.ndarray:
+        """Faces_<loop>.bin's records (grainhdl.cpp:753-775): FACE_DTYPE, every existing
+        grain's boundaries toward lower IDs (needs correction or keep_elements)."""
+        L = load_library()
+        n = self._check(L.gg_get_faces(self._h, None, None, None, 0))
+        area = np.zeros(n); ga = np.zeros(n, np.uint32); gb = np.zeros(n, np.uint32)
+        self._check(L.gg_get_faces(self._h, _p(area), _p(ga), _p(gb), n))
+        out = np.zeros(n, FACE_DTYPE)
+        out["area"], out["grainA"], out["grainB"] = area, ga, gb
+        return out
+
+    def texture(self) -> np.ndarray:
+        """Texture_<loop>.bin's records (LSbox::collectTextureData, box.cpp:3034-3045):
+        TEXTURE_DTYPE, one per existing grain in ascending ID order.  GBEnergy is the
+        reference's m_energy, which no code path of it assigns (0)."""
+        st = self.stats()
+        ids = [g for g in range(1, self.G + 1) if st.exists[g]]
+        out = np.zeros(len(ids), TEXTURE_DTYPE)
+        for r, g in enumerate(ids):
+            x0, x1, y0, y1, z0, z1 = (int(v) for v in st.boxes[g])
+            phi1, PHI, phi2 = quaternion_to_euler(euler_to_quaternion(self._euler[g - 1]))
+            out[r] = (st.volume[g], st.surface[g], 0.0, self._see[g - 1], phi1, PHI, phi2,
+                      ((x1 - x0) // 2 + x0) * self._h_grid, ((y1 - y0) // 2 + y0) * self._h_grid,
+                      ((z1 - z0) // 2 + z0) * self._h_grid, g, st.n_neighbors[g],
+                      int(0 in set(self.neighbors(g).tolist())), 0)
+        return out
 
     def voxel_container(self) -> np.ndarray:
         """The network as an (N, N, N) [z][y][x] array of grain IDs (the reference's

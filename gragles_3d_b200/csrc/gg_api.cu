@@ -74,6 +74,7 @@ struct gg_ctx {
     long long* d_boff = nullptr;
     float* d_cscr = nullptr;          // mixed-path convolution scratch (out's layout)
     unsigned char* d_elscr = nullptr; // element build: per-CTA junction and pair scratch
+    bool elements = false;            // interfacial elements built every step (correction or keep_elements)
     int elscr_ctas = 0;
     // convolution correction: orientations, stored energies, hull capture, elements
     bool correction = false;
@@ -533,11 +534,11 @@ int stage_level_set_t(gg_ctx* ctx) {
     a.n_nb = ctx->d_nnb;
     a.nb_cap = kNbCap;
     a.err = ctx->d_err;
-    if (ctx->correction) a.hull = ctx->hull;
+    if (ctx->elements) a.hull = ctx->hull;
     launch_mc<T>(a, ctx->grid, ctx->side_max, ctx->stream);
     ctx->launches += 1;
     CK(cudaGetLastError());
-    if (ctx->correction) {  // computeSurfaceElements, box.cpp:1175-1180
+    if (ctx->elements) {  // computeSurfaceElements, box.cpp:1175-1180
         ElementArgs e{};
         e.G = ctx->G;
         e.toff = ctx->d_toff_mc;
@@ -685,7 +686,7 @@ void free_all(gg_ctx* c) {
                     c->d_idoff[0], c->d_idoff[1], c->d_spec, c->d_spec_off, c->d_toff_n, c->d_toff_slab,
                     c->d_toff_one, c->d_toff_mc, c->d_toff_red, c->d_tw, c->d_tw_off, c->d_gtab, c->d_g_off,
                     c->d_circ, c->d_circ_off, c->d_bmat, c->d_boff, c->d_cscr, c->d_elscr, c->d_quat, c->d_see,
-                    c->hull.rec_list, c->hull.rec_ntri, c->hull.bary, c->hull.n_rec, c->hull.n_tri, c->el.n_elem,
+                    c->hull.rec_list, c->hull.rec_ntri, c->hull.bary, c->hull.tarea, c->el.earea, c->hull.n_rec, c->hull.n_tri, c->el.n_elem,
                     c->el.elem, c->el.ids, c->el.segs, c->el.ebary, c->el.chunks, c->el.n_idx, c->el.idx_key, c->el.idx_rng,
                     c->el.idx_elem, c->d_err, c->d_total_vox, c->d_count3, c->bins.count,
                     c->bins.off, c->bins.cursor, c->bins.entries, c->bins.max_count};
@@ -733,6 +734,7 @@ int gg_create(const gg_params* params, gg_ctx** out) {
     ctx->geo = Geometry{ctx->N, ctx->gb, ctx->M, 1 / (double)ctx->N, ctx->gb / double(ctx->N), P.time_step};
     ctx->list_cap = P.list_capacity > 0 ? P.list_capacity : 4096;
     ctx->correction = !P.disable_correction;
+    ctx->elements = ctx->correction || P.keep_elements;
     ctx->side_limit = supported_side(ctx->fp64);
     *out = ctx;
 #undef CK_RET
@@ -850,13 +852,14 @@ int gg_load_state(gg_ctx* ctx, const uint32_t* labels, const int32_t* extents, c
     }
     if (ctx->fp64) CK(dalloc(&ctx->d_spec, ctx->spec_capacity));
     else CK(dalloc(&ctx->d_cscr, ctx->pool_voxels));
-    if (ctx->correction) {
+    if (ctx->elements) {
         const long long cap = ctx->P.hull_capacity > 0 ? ctx->P.hull_capacity : 16LL * side * side + 2048;
         const size_t G1h = (size_t)G + 1;
         ctx->hull.cap = (int)cap;
         CK(dalloc(&ctx->hull.rec_list, 8 * cap * G1h));
         CK(dalloc(&ctx->hull.rec_ntri, cap * G1h));
         CK(dalloc(&ctx->hull.bary, 3 * cap * G1h));
+        CK(dalloc(&ctx->hull.tarea, cap * G1h));
         CK(dalloc(&ctx->hull.n_rec, G1h));
         CK(dalloc(&ctx->hull.n_tri, G1h));
         ctx->el.elem_cap = 512;
@@ -868,6 +871,7 @@ int gg_load_state(gg_ctx* ctx, const uint32_t* labels, const int32_t* extents, c
         CK(dalloc(&ctx->el.ids, (size_t)ctx->el.id_cap * G1h));
         CK(dalloc(&ctx->el.segs, (size_t)ctx->el.seg_cap * G1h));
         CK(dalloc(&ctx->el.ebary, 3 * cap * G1h));
+        CK(dalloc(&ctx->el.earea, cap * G1h));
         ctx->el.chunk_cap = (int)(cap / kHullChunk) + ctx->el.seg_cap;
         ctx->el.idx_cap = 256;
         ctx->el.pair_cap = 2048;
@@ -1066,6 +1070,46 @@ int gg_voxel_container(gg_ctx* ctx, uint32_t* labels) {
     return rc == GG_OK ? check_err(ctx, "gg_voxel_container") : rc;
 }
 
+int64_t gg_get_faces(gg_ctx* ctx, double* area, uint32_t* grain_a, uint32_t* grain_b, int64_t cap) {
+    if (!ctx || !ctx->loaded || cap < 0 || (cap > 0 && (!area || !grain_a || !grain_b))) return GG_ERR_INVALID;
+    if (!ctx->elements)
+        return fail(ctx, GG_ERR_UNSUPPORTED, "gg_get_faces needs the interfacial elements (correction or keep_elements)");
+    const int G = ctx->G;
+    int* d_count = nullptr;
+    long long* d_off = nullptr;
+    CK(dalloc(&d_count, (size_t)G + 1));
+    CK(dalloc(&d_off, (size_t)G + 1));
+    CK(cudaMemsetAsync(d_count, 0, sizeof(int) * (G + 1), ctx->stream));
+    launch_faces(G, ctx->d_exists, ctx->el, ctx->geo.h, nullptr, d_count, nullptr, nullptr, nullptr, ctx->stream);
+    std::vector<int> count(G + 1);
+    std::vector<long long> off(G + 1, 0);
+    CK(cudaMemcpyAsync(count.data(), d_count, sizeof(int) * (G + 1), cudaMemcpyDeviceToHost, ctx->stream));
+    CK(cudaStreamSynchronize(ctx->stream));
+    long long total = 0;
+    for (int g = 1; g <= G; g++) {
+        off[g] = total;
+        total += count[g];
+    }
+    double* d_area = nullptr;
+    uint32_t *d_a = nullptr, *d_b = nullptr;
+    CK(dalloc(&d_area, (size_t)(total > 0 ? total : 1)));
+    CK(dalloc(&d_a, (size_t)(total > 0 ? total : 1)));
+    CK(dalloc(&d_b, (size_t)(total > 0 ? total : 1)));
+    CK(cudaMemcpyAsync(d_off, off.data(), sizeof(long long) * (G + 1), cudaMemcpyHostToDevice, ctx->stream));
+    launch_faces(G, ctx->d_exists, ctx->el, ctx->geo.h, d_off, d_count, d_area, d_a, d_b, ctx->stream);
+    ctx->launches += 2;
+    CK(cudaGetLastError());
+    const long long n = std::min<long long>(total, cap);
+    if (n > 0) {
+        CK(cudaMemcpyAsync(area, d_area, sizeof(double) * n, cudaMemcpyDeviceToHost, ctx->stream));
+        CK(cudaMemcpyAsync(grain_a, d_a, sizeof(uint32_t) * n, cudaMemcpyDeviceToHost, ctx->stream));
+        CK(cudaMemcpyAsync(grain_b, d_b, sizeof(uint32_t) * n, cudaMemcpyDeviceToHost, ctx->stream));
+    }
+    CK(cudaStreamSynchronize(ctx->stream));
+    for (void* p : {(void*)d_count, (void*)d_off, (void*)d_area, (void*)d_a, (void*)d_b}) CK(cudaFree(p));
+    return total;
+}
+
 int gg_set_orientations(gg_ctx* ctx, const double* euler) {
     if (!ctx || !euler) return GG_ERR_INVALID;
     const size_t G1 = (size_t)ctx->G + 1;
@@ -1088,7 +1132,7 @@ int gg_set_stored_energy(gg_ctx* ctx, const double* see) {
 int gg_get_elements(gg_ctx* ctx, int32_t id, int32_t counts[4]) {
     if (!ctx || !ctx->loaded || id < 1 || id > ctx->G || !counts) return GG_ERR_INVALID;
     counts[0] = counts[1] = counts[2] = counts[3] = 0;
-    if (!ctx->correction) return GG_OK;
+    if (!ctx->elements) return GG_OK;
     int ne = 0;
     CK(cudaStreamSynchronize(ctx->stream));
     CK(cudaMemcpy(&ne, ctx->el.n_elem + id, sizeof(int), cudaMemcpyDeviceToHost));

@@ -315,7 +315,9 @@ __global__ void __launch_bounds__(32) elements_kernel(ElementArgs a) {
         uint32_t* rec_list = a.cap.rec_list + 8 * cb;
         int* rec_ntri = a.cap.rec_ntri + cb;
         const double* bary = a.cap.bary + 3 * cb;
+        const double* tarea = a.cap.tarea + cb;
         double* eb = a.el.ebary + 3 * (long long)g * a.el.bary_cap;
+        double* ea = a.el.earea + (long long)g * a.el.bary_cap;
         // 1. distinct lists in first-seen order (MarchingCubesAlgorithm::insertNeighborList,
         //    marchingCubes.cpp:605-618), 32 records at a time: lanes holding the same list
         //    follow the lowest of them, which looks the list up among the earlier ones; new
@@ -438,10 +440,11 @@ __global__ void __launch_bounds__(32) elements_kernel(ElementArgs a) {
                 const int t = tbase + q;
                 if (q < total && pos >= 0 && pos < a.el.bary_cap && t < ntri) {
                     const double b0 = bary[3 * (long long)t], b1 = bary[3 * (long long)t + 1],
-                                 b2 = bary[3 * (long long)t + 2];
+                                 b2 = bary[3 * (long long)t + 2], ta = tarea[t];
                     eb[3 * (long long)pos] = b0;
                     eb[3 * (long long)pos + 1] = b1;
                     eb[3 * (long long)pos + 2] = b2;
+                    ea[pos] = ta;
                 }
             }
             tbase += total;
@@ -651,6 +654,7 @@ __global__ void __launch_bounds__(32) elements_kernel(ElementArgs a) {
                 e.nchunk = nchunk;
                 e.energy = en;
                 e.mobility = mo;
+                e.area = 0.0;
                 // the IDs projectPointToGrainBoundary compares: all for a high-order
                 // junction, else the first 3 (QJ), 2 (TL), 1 (GB); each element once per ID
                 const int nc = type == 4 ? nid : min(nid, type);
@@ -754,6 +758,17 @@ __global__ void __launch_bounds__(32) elements_kernel(ElementArgs a) {
                 }
             }
             __syncwarp();
+            // GrainBoundary::computeArea (InterfacialElement.cpp:81-91): its triangles'
+            // terms summed in triangle order, times h^2
+            for (int e = lane; e < ne; e += 32) {
+                HullElem& el = E[e];
+                if (el.type != 1 || el.nseg != 1) continue;
+                const int2 sg = a.el.segs[(long long)g * a.el.seg_cap + el.seg_off];
+                if (sg.x < 0 || sg.y < 0 || sg.x + sg.y > a.el.bary_cap) continue;
+                double surface = 0;
+                for (int i = 0; i < sg.y; i++) surface += ea[sg.x + i];
+                el.area = surface * a.ph.ds * a.ph.ds;  // ds = h = 1 / realDomainSize
+            }
             for (int e = lane; e < ne; e += 32) {
                 HullElem& el = E[e];
                 double lo[3] = {1e300, 1e300, 1e300}, hi[3] = {-1e300, -1e300, -1e300};
@@ -1049,6 +1064,37 @@ __global__ void __launch_bounds__(kCThreads, 2) correction_kernel(CorrectionArgs
 }  // namespace
 
 size_t elements_scratch_per_cta() { return kElemScratch; }
+
+namespace {
+__global__ void faces_kernel(int G, const int* exists, HullElements el, const long long* off, int* count,
+                             double* area, uint32_t* grain_a, uint32_t* grain_b) {
+    for (int g = 1 + blockIdx.x * blockDim.x + threadIdx.x; g <= G; g += gridDim.x * blockDim.x) {
+        int n = 0;
+        if (exists[g]) {
+            const int ne = min(max(el.n_elem[g], 0), el.elem_cap);
+            const HullElem* E = el.elem + (long long)g * el.elem_cap;
+            const uint32_t* ids = el.ids + (long long)g * el.id_cap;
+            for (int e = 0; e < ne; e++) {
+                if (E[e].type != 1 || E[e].nids < 1) continue;
+                const uint32_t nb = ids[E[e].id_off];
+                if ((uint32_t)g <= nb) continue;  // each face once, from its higher ID
+                if (area) {
+                    area[off[g] + n] = E[e].area;
+                    grain_a[off[g] + n] = (uint32_t)g;
+                    grain_b[off[g] + n] = nb;
+                }
+                n++;
+            }
+        }
+        if (!area) count[g] = n;
+    }
+}
+}  // namespace
+
+void launch_faces(int G, const int* exists, HullElements el, double /*h*/, const long long* off, int* count,
+                  double* area, uint32_t* grain_a, uint32_t* grain_b, cudaStream_t s) {
+    faces_kernel<<<(G + 256) / 256, 256, 0, s>>>(G, exists, el, off, count, area, grain_a, grain_b);
+}
 
 void launch_elements(const ElementArgs& a, int grid, cudaStream_t s) {
     static bool configured = false;

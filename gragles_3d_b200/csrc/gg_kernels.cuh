@@ -157,6 +157,7 @@ struct HullCapture {
     uint32_t* rec_list;       // (G + 1) x cap x 8
     int* rec_ntri;            // (G + 1) x cap
     double* bary;             // (G + 1) x cap x 3
+    double* tarea;            // (G + 1) x cap: |AB x BC| / 2 of each triangle (computeSurfaceArea's term)
     int* n_rec;               // G + 1
     int* n_tri;               // G + 1
 };
@@ -171,6 +172,7 @@ struct HullElem {
     int chunk_off, nchunk;    // barycenter chunks (each inside one segment) in the chunk pool
     int pad;
     double energy, mobility;  // m_energy, m_mobility
+    double area;              // GrainBoundary::computeArea (InterfacialElement.cpp:81-91); 0 for junctions
     double lo[3], hi[3];      // bounding box of its barycenters
 };
 
@@ -189,6 +191,7 @@ struct HullElements {
     uint32_t* ids;            // (G + 1) x id_cap
     int2* segs;               // (G + 1) x seg_cap
     double* ebary;            // (G + 1) x bary_cap x 3, barycenters grouped by neighbour list
+    double* earea;            // (G + 1) x bary_cap, their triangles' area terms in the same order
     HullChunk* chunks;        // (G + 1) x chunk_cap
     // neighbour ID -> the elements whose searched IDs hold it, in search order
     int* n_idx;               // G + 1: distinct IDs
@@ -221,6 +224,12 @@ struct ElementArgs {
 };
 size_t elements_scratch_per_cta();
 void launch_elements(const ElementArgs& a, int grid, cudaStream_t s);
+
+// GrainHull::get_Faces (grainHull.cpp:1330-1339) of every existing grain: its grain
+// boundary elements toward lower IDs.  Counting pass (out == nullptr: count[g] = faces of
+// g), then writing pass at the exclusive offsets off[g].
+void launch_faces(int G, const int* exists, HullElements el, double h, const long long* off, int* count,
+                  double* area, uint32_t* grain_a, uint32_t* grain_b, cudaStream_t s);
 
 template <typename T>
 struct CorrectionArgs {

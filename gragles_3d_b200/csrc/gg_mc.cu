@@ -275,6 +275,7 @@ __global__ void __launch_bounds__(kThreads, 3) mc_kernel(MCArgs<T> a, int slab_b
                     const double bcx = p0.x - p2.x, bcy = p0.y - p2.y, bcz = p0.z - p2.z;
                     const double cx = aby * bcz - abz * bcy, cy = abz * bcx - abx * bcz, cz = abx * bcy - aby * bcx;
                     abuf[off + q] = sqrt(cx * cx + (cy * cy + cz * cz)) / 2.0;
+                    if (capture && ntri + off + q < a.hull.cap) a.hull.tarea[hbase + ntri + off + q] = abuf[off + q];
                 }
                 // generateAdditionalInformation: sorted distinct corner IDs, marchingCubes.cpp:501-583
                 unsigned lst[8];

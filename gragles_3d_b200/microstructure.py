@@ -178,7 +178,8 @@ def write_parameters(path: str, *, n_grains: int, border: int = 10, steps: int =
                      breakup: int = 0, threads: int = 8, correction: bool = False,
                      unique_energies: bool = True, mobility_factor: bool = False,
                      stored_energy: bool = False, triple_line_drag: float = 1e6,
-                     analysis_every: int = 1000000) -> None:
+                     analysis_every: int = 1000000, neighbor_tracking: bool = False,
+                     plot_interval: int = 1000000) -> None:
     """A ``parameters.xml`` for the reference (Settings.cpp:81-270) in mode 4.
 
     ``NumberOfParticles`` must already hold the grain count: the reference sizes
@@ -187,7 +188,7 @@ def write_parameters(path: str, *, n_grains: int, border: int = 10, steps: int =
     p = {
         "StartTime": 0, "NumberOfParticles": n_grains, "NumberOfPointsPerGrain": 10,
         "AnalysisTimestep": analysis_every, "NumberOfTimesteps": steps,
-        "PlotInterval": 1000000, "TimeStepSize": repr(float(time_step)),
+        "PlotInterval": plot_interval, "TimeStepSize": repr(float(time_step)),
         "BreakupNumber": breakup, "DiscreteSamplingRate": 25, "DomainBorderSize": border,
         "MicrostructureGenMode": 4, "ReadFromFilename": raw_name, "AdditionalFilename": uds_name,
         "HAGB_Energy": "1.", "HAGB_Mobility": "7.5e-14", "DislocEnPerM": "2.5e-10",
@@ -197,7 +198,7 @@ def write_parameters(path: str, *, n_grains: int, border: int = 10, steps: int =
         "UseTexture": 0, "ExecuteInParallel": 1, "MaximumNumberOfThreads": threads,
         "GridCoarsement": 0, "GridCoarsementGradient": 0.95, "ConvolutionMode": 2,
         "UniqueGBEnergies": int(unique_energies), "GrainScheduler": 0, "DecoupleGrains": 0,
-        "NeighborTracking": 0, "StoreTaskDistribution": 0,
+        "NeighborTracking": int(neighbor_tracking), "StoreTaskDistribution": 0,
     }
     body = "\n".join(f"   <{k}>{v}</{k}>" for k, v in p.items())
     with open(path, "w") as f:
@@ -211,4 +212,19 @@ def write_container(directory: str, labels: np.ndarray, loop: int) -> str:
     lab = np.ascontiguousarray(labels, dtype=np.uint32)
     path = os.path.join(directory, f"Container_size_{lab.shape[0]}_t_{int(loop)}.raw")
     lab.tofile(path)
+    return path
+
+
+def write_texture(directory: str, records: np.ndarray, loop: int) -> str:
+    """Texture_<loop>.bin as save_Texture writes it with NeighborTracking on
+    (grainhdl.cpp:753-771): the records of GrainHandler.texture(), back to back."""
+    path = os.path.join(directory, f"Texture_{int(loop)}.bin")
+    np.ascontiguousarray(records).tofile(path)
+    return path
+
+
+def write_faces(directory: str, records: np.ndarray, loop: int) -> str:
+    """Faces_<loop>.bin (grainhdl.cpp:758-775): the records of GrainHandler.faces()."""
+    path = os.path.join(directory, f"Faces_{int(loop)}.bin")
+    np.ascontiguousarray(records).tofile(path)
     return path

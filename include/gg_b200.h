@@ -53,7 +53,8 @@ typedef struct {
     int32_t use_stored_energy;  /* UseStoredElasticEnergy (correction only) */
     double triple_line_drag;    /* TripleLineDrag (correction only) */
     int32_t hull_capacity;      /* triangles kept per hull for the correction (0 = 16 side^2 + 2048) */
-    int32_t reserved[1];
+    int32_t keep_elements;      /* build the interfacial elements every step even without the
+                                   correction (computeSurfaceElements, box.cpp:1175-1180), for gg_get_faces */
 } gg_params;
 
 /* Per-step report (the reference prints the same stage times, grainhdl.cpp:920-933). */
@@ -124,6 +125,13 @@ int gg_loop(gg_ctx* ctx);
  * ID order -- and 0 where there is none.  Grains whose hull vanished in the last step
  * are left out (their buffer is not kept; in the reference it holds no voxel >= 0 then). */
 int gg_voxel_container(gg_ctx* ctx, uint32_t* labels);
+
+/* GrainHull::get_Faces of every existing grain (grainHull.cpp:1330-1339), as save_Texture
+ * writes them to Faces_<loop>.bin (grainhdl.cpp:753-775): per grain in ascending ID order,
+ * its grain-boundary elements toward lower IDs in element order, each with its area
+ * (GrainBoundary::computeArea, InterfacialElement.cpp:81-91).  Fills at most cap faces and
+ * returns the total; needs the elements (the correction on, or keep_elements). */
+int64_t gg_get_faces(gg_ctx* ctx, double* area, uint32_t* grain_a, uint32_t* grain_b, int64_t cap);
 
 /* Grain orientations for the convolution correction's boundary energies and
  * mobilities: Bunge Euler angles phi1, PHI, phi2 in radians, 3 per grain for IDs

@@ -9,7 +9,10 @@ The "correction" case turns on the convolution correction (box.cpp:426-535) with
 a mix of low-angle and random orientations, the mobility model, a weak
 triple-line drag and stored elastic energies.
 
-    python tests/golden/make_golden.py
+The "analysis" case reruns the correction case on one thread with the reference's
+analysis outputs on: Texture and Faces records every loop and the voxel container.
+
+    python tests/golden/make_golden.py [case ...]
 """
 from __future__ import annotations
 
@@ -110,6 +113,50 @@ def make(name, N, G, border, seed, steps, keep_grain, keep_loop):
     print(name, "ok", {k: v.shape for k, v in out.items() if hasattr(v, "shape")})
 
 
+# the reference's analysis output records (Structs.h: Face, TextureData)
+TEXTURE_DTYPE = np.dtype([("volume", "<f8"), ("surfaceArea", "<f8"), ("GBEnergy", "<f8"), ("BulkEnergy", "<f8"),
+                          ("phi1", "<f8"), ("PHI", "<f8"), ("phi2", "<f8"), ("x", "<f8"), ("y", "<f8"),
+                          ("z", "<f8"), ("id", "<u4"), ("NeighbourCount", "<u4"),
+                          ("intersectsBoundaryGrain", "<u4"), ("pad", "<u4")])
+FACE_DTYPE = np.dtype([("area", "<f8"), ("grainA", "<u4"), ("grainB", "<u4")])
+
+
+def make_analysis(N=32, G=30, border=5, seed=2032, steps=8, plot_every=2):
+    """The correction case again, one thread (the voxel container's writer order), with
+    NeighborTracking on (Texture_<loop>.bin, Faces_<loop>.bin every loop, grainhdl.cpp:
+    750-790) and the voxel container every plot_every loops (grainhdl.cpp:1074-1123)."""
+    ms = msgen.voronoi(N, G, seed=seed)
+    textured(ms, seed)
+    phys = PHYSICS["correction"]
+    with tempfile.TemporaryDirectory() as d:
+        msgen.write_mode4(ms, d)
+        msgen.write_parameters(os.path.join(d, "parameters.xml"), n_grains=G, border=border, steps=steps,
+                               correction=True, analysis_every=1, neighbor_tracking=True,
+                               plot_interval=plot_every, **phys)
+        res, _ = refdump.run_case(d, threads=1)
+        out = {"N": N, "G": G, "border": border, "seed": seed, "steps": steps, "plot_every": plot_every,
+               "euler": ms.euler.copy(), "uds_stored_energy": ms.stored_energy.copy()}
+        for k, v in phys.items():
+            out["phys_" + k] = v
+        out["init_list_off"], out["init_list_ids"] = ragged(res["init_list"], G)
+        tex, tex_len, faces, face_len, cont, cont_loops = [], [], [], [], [], []
+        for loop in range(1, steps + 1):
+            t = np.fromfile(os.path.join(d, f"Texture_{loop}.bin"), TEXTURE_DTYPE)
+            f = np.fromfile(os.path.join(d, f"Faces_{loop}.bin"), FACE_DTYPE)
+            tex.append(t); tex_len.append(len(t)); faces.append(f); face_len.append(len(f))
+            path = os.path.join(d, f"Container_size_{N}_t_{loop}.raw")
+            if os.path.exists(path):
+                cont.append(np.fromfile(path, np.uint32).reshape(N, N, N)); cont_loops.append(loop)
+    out.update(texture=np.concatenate(tex), texture_len=np.array(tex_len), faces=np.concatenate(faces),
+               faces_len=np.array(face_len), container=np.stack(cont), container_loops=np.array(cont_loops))
+    np.savez_compressed(os.path.join(HERE, "analysis.npz"), **out)
+    print("analysis ok", {k: v.shape for k, v in out.items() if hasattr(v, "shape")})
+
+
 if __name__ == "__main__":
+    only = sys.argv[1:]
     for name, args in CASES.items():
-        make(name, *args)
+        if not only or name in only:
+            make(name, *args)
+    if not only or "analysis" in only:
+        make_analysis()

@@ -137,3 +137,15 @@ def test_container_file_layout(tmp_path):
     assert os.path.basename(path) == "Container_size_4_t_7.raw"
     back = np.fromfile(path, np.uint32)
     assert np.array_equal(back, lab.ravel())
+
+
+def test_texture_euler_angles_follow_the_reference():
+    """The Texture records' angles: Quaternion2Euler(euler2Quaternion(.uds angles)) as the
+    reference computes them, checked against its own Texture_1.bin (tests/golden/analysis.npz)."""
+    import gragles_3d_b200 as gg
+
+    d = dict(np.load(os.path.join(os.path.dirname(__file__), "golden", "analysis.npz")))
+    t = d["texture"][:int(d["texture_len"][0])]
+    for rec in t:
+        e = gg.quaternion_to_euler(gg.euler_to_quaternion(d["euler"][rec["id"] - 1]))
+        assert np.allclose(e, (rec["phi1"], rec["PHI"], rec["phi2"]), rtol=0, atol=1e-12)
