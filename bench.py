@@ -180,7 +180,9 @@ def run_e2e(gg, precision, ms, ext, counts, steps, device):
 
     gh = gg.GrainHandler(WORKLOAD["domain"], WORKLOAD["border"], WORKLOAD["time_step"], WORKLOAD["grains"],
                          precision=precision, device=device, **PHYSICS)
-    labels = np.ascontiguousarray(ms.labels)
+    # the step inputs sit in pinned host memory (the tensor keeps it alive; numpy views it)
+    pinned = torch.from_numpy(np.ascontiguousarray(ms.labels)).pin_memory()
+    labels = pinned.numpy()
     torch.cuda.synchronize()
     ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     ev0.record()
