@@ -192,6 +192,7 @@ class GrainHandler:
         self._see = np.zeros(self.G)
         self._h_grid = 1.0 / self.N
         h = C.c_void_p()
+        self._lib = L  # held for close() at interpreter exit, when module globals are gone
         rc = L.gg_create(C.byref(p), C.byref(h))
         self._h = h
         self._check(rc)
@@ -204,7 +205,7 @@ class GrainHandler:
 
     def close(self):
         if getattr(self, "_h", None):
-            load_library().gg_destroy(self._h)
+            self._lib.gg_destroy(self._h)
             self._h = None
 
     def __del__(self):

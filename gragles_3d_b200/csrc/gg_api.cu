@@ -223,9 +223,19 @@ int check_err(gg_ctx* ctx, const char* where) {
     if (e & ERR_BOX) return fail(ctx, GG_ERR_UNSUPPORTED, "%s: a box left the grid or exceeded the supported side", where);
     if (e & ERR_TIMEOUT) return fail(ctx, GG_ERR_CUDA, "%s: a bounded tensor-core pipeline wait timed out", where);
     if (e & ERR_BOUNDS) return fail(ctx, GG_ERR_CUDA, "%s: a kernel bounds check failed (access skipped)", where);
-    if (e & ERR_HULL)
-        return fail(ctx, GG_ERR_POOL_EXHAUSTED, "%s: hull or interfacial-element capacity exceeded (raise hull_capacity)",
-                    where);
+    if (e & ERR_HULL) {
+        int d = 0;
+        if (ctx->hull.diag) CK(cudaMemcpy(&d, ctx->hull.diag, sizeof(int), cudaMemcpyDeviceToHost));
+        const char* what = (d & (HULL_TRIANGLES | HULL_RECORDS)) ? "triangles or active cubes of a hull beyond hull_capacity"
+                           : (d & HULL_LISTS)        ? "more than 256 distinct neighbour lists on one hull"
+                           : (d & HULL_JUNCTION_IDS) ? "a merged junction with more IDs than the element build holds"
+                           : (d & HULL_JUNCTIONS)    ? "more than 256 junctions on one hull"
+                           : (d & HULL_JOBS)         ? "more misorientations on one hull than the element build holds"
+                           : (d & HULL_INDEX)        ? "a hull's neighbour -> elements index beyond its capacity"
+                           : (d & HULL_TABLE)        ? "a hull's element, ID, segment or chunk table beyond its capacity"
+                                                     : "hull or interfacial-element capacity exceeded";
+        return fail(ctx, GG_ERR_POOL_EXHAUSTED, "%s: %s (diag %d)", where, what, d);
+    }
     return GG_OK;
 }
 
@@ -686,7 +696,7 @@ void free_all(gg_ctx* c) {
                     c->d_idoff[0], c->d_idoff[1], c->d_spec, c->d_spec_off, c->d_toff_n, c->d_toff_slab,
                     c->d_toff_one, c->d_toff_mc, c->d_toff_red, c->d_tw, c->d_tw_off, c->d_gtab, c->d_g_off,
                     c->d_circ, c->d_circ_off, c->d_bmat, c->d_boff, c->d_cscr, c->d_elscr, c->d_quat, c->d_see,
-                    c->hull.rec_list, c->hull.rec_ntri, c->hull.bary, c->hull.tarea, c->el.earea, c->hull.n_rec, c->hull.n_tri, c->el.n_elem,
+                    c->hull.rec_list, c->hull.rec_ntri, c->hull.bary, c->hull.tarea, c->hull.diag, c->el.earea, c->hull.n_rec, c->hull.n_tri, c->el.n_elem,
                     c->el.elem, c->el.ids, c->el.segs, c->el.ebary, c->el.chunks, c->el.n_idx, c->el.idx_key, c->el.idx_rng,
                     c->el.idx_elem, c->d_err, c->d_total_vox, c->d_count3, c->bins.count,
                     c->bins.off, c->bins.cursor, c->bins.entries, c->bins.max_count};
@@ -860,6 +870,8 @@ int gg_load_state(gg_ctx* ctx, const uint32_t* labels, const int32_t* extents, c
         CK(dalloc(&ctx->hull.rec_ntri, cap * G1h));
         CK(dalloc(&ctx->hull.bary, 3 * cap * G1h));
         CK(dalloc(&ctx->hull.tarea, cap * G1h));
+        CK(dalloc(&ctx->hull.diag, 1));
+        CK(cudaMemset(ctx->hull.diag, 0, sizeof(int)));
         CK(dalloc(&ctx->hull.n_rec, G1h));
         CK(dalloc(&ctx->hull.n_tri, G1h));
         ctx->el.elem_cap = 512;

@@ -30,7 +30,7 @@ namespace {
 
 constexpr double kPi = 3.14159265358979323846;  // ggLS.h:25
 constexpr int kLMax = 256;    // distinct neighbour lists (= elements) per hull
-constexpr int kJIds = 48;     // IDs of one (merged) junction
+constexpr int kJIds = 8;      // IDs a junction brings itself (a list's IDs other than the grain's)
 constexpr unsigned kNoId = 0xFFFFFFFFu;
 constexpr int kLHash = 2 * kLMax;  // slots of the distinct-list hash (power of two)
 constexpr unsigned kFull = 0xFFFFFFFFu;
@@ -93,11 +93,15 @@ __device__ __forceinline__ double sqdist(const double* a, const double* b) {
 // element construction
 // ---------------------------------------------------------------------------------
 
-// A junction being merged: its member lists (keys) chained through next_key; its IDs
-// (at most kJIds) are in the CTA's global scratch.
+// A junction being merged: its member lists (keys) chained through next_key.  Its IDs
+// are a chain of per-junction segments: its own (at most kJIds, in the CTA's global
+// scratch) followed by those of the junctions merged into it, linked through id_next.
+// A merge appends the whole chain, duplicates included, as the reference's does.
 struct JHead {
     int head, tail;   // member keys
-    int nids;
+    int own;          // IDs in this junction's own segment
+    int nids;         // IDs along the whole chain
+    int id_next, id_tail;  // junction whose segment follows (-1: none); last junction of the chain
     int type;         // 3 QJ, 4 HJ
     double pos[3];
 };
@@ -206,14 +210,30 @@ __device__ void junction_position(JHead& J, const ElemSmem& S, const double* eb,
     J.pos[2] = p2 / d;
 }
 
-__device__ __forceinline__ void push_id(JHead& J, uint32_t* ids, uint32_t id, int* err) {
-    if (J.nids < kJIds) ids[J.nids++] = id;
-    else atomicOr(err, ERR_HULL);
+// Starts junction j's own ID segment (j is its own chain).
+__device__ __forceinline__ void start_ids(JHead& J, int j) {
+    J.own = J.nids = 0;
+    J.id_next = -1;
+    J.id_tail = j;
 }
 
-__device__ __forceinline__ void chain(ElemSmem& S, JHead& A, const JHead& B) {
+__device__ __forceinline__ void push_id(JHead& J, uint32_t* ids, uint32_t id, int* err, int* diag) {
+    if (J.own < kJIds) {
+        ids[J.own++] = id;
+        J.nids++;
+    } else {
+        atomicOr(err, ERR_HULL);
+        atomicOr(diag, HULL_JUNCTION_IDS);
+    }
+}
+
+// A takes B's member lists and then B's IDs (junction b's chain) after its own.
+__device__ __forceinline__ void chain(ElemSmem& S, JHead& A, const JHead& B, int b) {
     S.next_key[A.tail] = B.head;
     A.tail = B.tail;
+    S.jh[A.id_tail].id_next = b;
+    A.id_tail = B.id_tail;
+    A.nids += B.nids;
 }
 
 // Warp-wide exclusive scan of v[0, n) in place (n <= kLMax); returns the total.
@@ -355,7 +375,7 @@ __global__ void __launch_bounds__(32) elements_kernel(ElementArgs a) {
                             __syncwarp();
                             if (lane == 0) insert_list(S, hs, nl, a.err);
                         } else if (lane == 0) {
-                            atomicOr(a.err, ERR_HULL);
+                            { atomicOr(a.err, ERR_HULL); atomicOr(a.cap.diag, HULL_LISTS); }
                         }
                         nl++;
                     }
@@ -375,7 +395,7 @@ __global__ void __launch_bounds__(32) elements_kernel(ElementArgs a) {
                         insert_list(S, h, k, a.err);
                         found = k;
                     } else {
-                        atomicOr(a.err, ERR_HULL);
+                        { atomicOr(a.err, ERR_HULL); atomicOr(a.cap.diag, HULL_LISTS); }
                         found = 0;
                     }
                 }
@@ -398,7 +418,7 @@ __global__ void __launch_bounds__(32) elements_kernel(ElementArgs a) {
         __syncwarp();
         for (int k = lane; k < nl; k += 32) S.off[k] = S.cnt[k];
         __syncwarp();
-        if (warp_scan_excl(S.off, nl) > a.el.bary_cap && lane == 0) atomicOr(a.err, ERR_HULL);
+        if (warp_scan_excl(S.off, nl) > a.el.bary_cap && lane == 0) { atomicOr(a.err, ERR_HULL); atomicOr(a.cap.diag, HULL_TRIANGLES); }
         // 3. barycenters grouped by list, in triangle order (subDivideTrianglesToInterfacialElements):
         //    a record's triangles go after those of the earlier records of its list.  The
         //    warp first places its 32 records, then copies their triangles together.
@@ -457,7 +477,7 @@ __global__ void __launch_bounds__(32) elements_kernel(ElementArgs a) {
         __syncwarp();
         int njobs = warp_scan_excl(S.fill, nl);
         if (njobs > kJobMax) {
-            if (lane == 0) atomicOr(a.err, ERR_HULL);
+            if (lane == 0) { atomicOr(a.err, ERR_HULL); atomicOr(a.cap.diag, HULL_JOBS); }
             njobs = kJobMax;
         }
         for (int j = lane; j < njobs; j += 32) {
@@ -520,10 +540,10 @@ __global__ void __launch_bounds__(32) elements_kernel(ElementArgs a) {
                     JHead& J = S.jh[j];
                     J.head = J.tail = k;
                     J.type = isq ? 3 : 4;
-                    J.nids = 0;
+                    start_ids(J, j);
                     uint32_t* ids = S.jids + (long long)j * kJIds;
                     for (int i = 0; i < count; i++)
-                        if ((uint32_t)g != S.lists[k][i]) push_id(J, ids, S.lists[k][i], a.err);
+                        if ((uint32_t)g != S.lists[k][i]) push_id(J, ids, S.lists[k][i], a.err, a.cap.diag);
                     junction_position(J, S, eb, a.el.bary_cap, a.err);
                     if (isq) S.qlist[nq + __popc(bq & lt)] = j;
                     else S.hlist[nh + __popc(bh & lt)] = j;
@@ -547,23 +567,24 @@ __global__ void __launch_bounds__(32) elements_kernel(ElementArgs a) {
                     JHead& A = S.jh[S.qlist[i]];
                     JHead& B = S.jh[S.qlist[j]];
                     if (sqrt(sqdist(A.pos, B.pos)) < 2) {
-                        if (S.nj >= kLMax) { atomicOr(a.err, ERR_HULL); break; }
+                        if (S.nj >= kLMax) { atomicOr(a.err, ERR_HULL); atomicOr(a.cap.diag, HULL_JUNCTIONS); break; }
                         const uint32_t* aid = S.jids + (long long)S.qlist[i] * kJIds;
                         const uint32_t* bid = S.jids + (long long)S.qlist[j] * kJIds;
                         const uint32_t a0 = aid[0], a1 = aid[1], a2 = aid[2], b0 = bid[0], b1 = bid[1], b2 = bid[2];
                         JHead& H = S.jh[S.nj];
                         uint32_t* hid = S.jids + (long long)S.nj * kJIds;
                         H.type = 4;
-                        H.nids = 0;
-                        push_id(H, hid, a0, a.err);
-                        push_id(H, hid, a1, a.err);
-                        push_id(H, hid, a2, a.err);
+                        start_ids(H, S.nj);
+                        push_id(H, hid, a0, a.err, a.cap.diag);
+                        push_id(H, hid, a1, a.err, a.cap.diag);
+                        push_id(H, hid, a2, a.err, a.cap.diag);
                         const uint32_t bq[3] = {b0, b1, b2};
                         for (int q = 0; q < 3; q++)  // B's IDs that A already has (sic)
-                            if (bq[q] == a0 || bq[q] == a1 || bq[q] == a2) push_id(H, hid, bq[q], a.err);
+                            if (bq[q] == a0 || bq[q] == a1 || bq[q] == a2) push_id(H, hid, bq[q], a.err, a.cap.diag);
                         H.head = A.head;
                         H.tail = A.tail;
-                        chain(S, H, B);
+                        S.next_key[H.tail] = B.head;  // the lists of A, then of B; IDs as above
+                        H.tail = B.tail;
                         junction_position(H, S, eb, a.el.bary_cap, a.err);
                         // erase i and j (j - 1 after the first erase), then append H
                         for (int u = j; u < S.nq - 1; u++) S.qlist[u] = S.qlist[u + 1];
@@ -581,10 +602,7 @@ __global__ void __launch_bounds__(32) elements_kernel(ElementArgs a) {
                     JHead& H = S.jh[S.hlist[k]];
                     JHead& Q = S.jh[S.qlist[i]];
                     if (sqrt(sqdist(Q.pos, H.pos)) < 2) {
-                        chain(S, H, Q);
-                        uint32_t* hid = S.jids + (long long)S.hlist[k] * kJIds;
-                        const uint32_t* qid = S.jids + (long long)S.qlist[i] * kJIds;
-                        for (int q = 0; q < Q.nids; q++) push_id(H, hid, qid[q], a.err);
+                        chain(S, H, Q, S.qlist[i]);
                         junction_position(H, S, eb, a.el.bary_cap, a.err);
                         for (int u = i; u < S.nq - 1; u++) S.qlist[u] = S.qlist[u + 1];
                         S.nq--;
@@ -597,10 +615,7 @@ __global__ void __launch_bounds__(32) elements_kernel(ElementArgs a) {
                     JHead& A = S.jh[S.hlist[i]];
                     JHead& B = S.jh[S.hlist[k]];
                     if (sqrt(sqdist(A.pos, B.pos)) < 2) {
-                        chain(S, A, B);
-                        uint32_t* aid = S.jids + (long long)S.hlist[i] * kJIds;
-                        const uint32_t* bid = S.jids + (long long)S.hlist[k] * kJIds;
-                        for (int q = 0; q < B.nids; q++) push_id(A, aid, bid[q], a.err);
+                        chain(S, A, B, S.hlist[k]);
                         junction_position(A, S, eb, a.el.bary_cap, a.err);
                         for (int u = k; u < S.nh - 1; u++) S.hlist[u] = S.hlist[u + 1];
                         S.nh--;
@@ -619,13 +634,22 @@ __global__ void __launch_bounds__(32) elements_kernel(ElementArgs a) {
             int2* segs = a.el.segs + (long long)g * a.el.seg_cap;
             HullChunk* chunks = a.el.chunks + (long long)g * a.el.chunk_cap;
             int ne = 0, ni = 0, ns = 0, nch = 0, nd = 0, np = 0;
-            bool over = false;
-            auto emit = [&](int type, const uint32_t* id_src, int nid, int head, bool chained, double en, double mo) {
+            bool over = false, over_index = false;
+            // IDs from junction j's segment chain (j >= 0), else the nid IDs of id_src
+            auto emit = [&](int type, const uint32_t* id_src, int j, int nid, int head, bool chained, double en,
+                            double mo) {
                 if (ne >= a.el.elem_cap || ni + nid > a.el.id_cap) { over = true; return; }
-                uint32_t idv[kJIds];
-                for (int q = 0; q < nid && q < kJIds; q++) idv[q] = id_src[q];
                 const int id_off = ni, seg_off = ns, chunk_off = nch;
-                for (int q = 0; q < nid; q++) ids[ni++] = idv[q];
+                if (j < 0) {
+                    for (int q = 0; q < nid; q++) ids[ni++] = id_src[q];
+                } else {
+                    for (int walk = 0; j >= 0 && walk < kLMax; walk++, j = S.jh[j].id_next) {
+                        const uint32_t* seg = S.jids + (long long)j * kJIds;
+                        for (int q = 0; q < S.jh[j].own && ni < id_off + nid; q++) ids[ni++] = seg[q];
+                    }
+                    if (ni != id_off + nid) atomicOr(a.err, ERR_BOUNDS);
+                    nid = ni - id_off;
+                }
                 int nseg = 0, nchunk = 0;
                 for (int k = head; k >= 0; k = chained ? S.next_key[k] : -1) {
                     if (ns >= a.el.seg_cap) { over = true; break; }
@@ -659,7 +683,7 @@ __global__ void __launch_bounds__(32) elements_kernel(ElementArgs a) {
                 // junction, else the first 3 (QJ), 2 (TL), 1 (GB); each element once per ID
                 const int nc = type == 4 ? nid : min(nid, type);
                 for (int q = 0; q < nc; q++) {
-                    const uint32_t id = idv[q];
+                    const uint32_t id = ids[id_off + q];
                     unsigned hs = (id * 2654435761u) & (kIHash - 1);
                     int d = -1;
                     for (int probe = 0; probe < kIHash; probe++) {
@@ -676,7 +700,7 @@ __global__ void __launch_bounds__(32) elements_kernel(ElementArgs a) {
                         }
                         hs = (hs + 1) & (kIHash - 1);
                     }
-                    if (d < 0 || np >= kPairMax) { over = true; break; }
+                    if (d < 0 || np >= kPairMax) { over = over_index = true; break; }
                     if (S.dlast[d] == ne) continue;
                     S.dlast[d] = ne;
                     S.dcnt[d]++;
@@ -689,12 +713,11 @@ __global__ void __launch_bounds__(32) elements_kernel(ElementArgs a) {
             for (int i = 0; i < S.nh; i++) {
                 const JHead& J = S.jh[S.hlist[i]];
                 // a junction made from one list keeps that list's energy (1 for HJ)
-                emit(4, S.jids + (long long)S.hlist[i] * kJIds, min(J.nids, kJIds), J.head, true, 1.0, 1.0);
+                emit(4, nullptr, S.hlist[i], J.nids, J.head, true, 1.0, 1.0);
             }
             for (int i = 0; i < S.nq; i++) {
                 const JHead& J = S.jh[S.qlist[i]];
-                emit(3, S.jids + (long long)S.qlist[i] * kJIds, min(J.nids, kJIds), J.head, true, S.energy[J.head],
-                     S.mobility[J.head]);
+                emit(3, nullptr, S.qlist[i], J.nids, J.head, true, S.energy[J.head], S.mobility[J.head]);
             }
             for (int pass = 2; pass >= 1; pass--)  // TL, then GB, each in key order
                 for (int k = 0; k < nl; k++) {
@@ -706,7 +729,7 @@ __global__ void __launch_bounds__(32) elements_kernel(ElementArgs a) {
                     else
                         for (int q = 0; q < 3; q++)
                             if ((uint32_t)g != S.lists[k][q]) nb[nn++] = S.lists[k][q];
-                    emit(pass, nb, nn, k, false, S.energy[k], S.mobility[k]);
+                    emit(pass, nb, -1, nn, k, false, S.energy[k], S.mobility[k]);
                 }
             // the index: IDs with their element ranges, elements in search order
             int run = 0;
@@ -715,14 +738,14 @@ __global__ void __launch_bounds__(32) elements_kernel(ElementArgs a) {
                 run += S.dcnt[d];
                 S.dcnt[d] = 0;
             }
-            if (run > a.el.pair_cap) over = true;
+            if (run > a.el.pair_cap) over = over_index = true;
             unsigned short* pairs = a.el.idx_elem + (long long)g * a.el.pair_cap;
             for (int q = 0; q < np; q++) {
                 const int d = S.pd[q];
                 const int at = S.doff[d] + S.dcnt[d]++;
                 if (at < a.el.pair_cap) pairs[at] = S.pe[q];
             }
-            if (over) atomicOr(a.err, ERR_HULL);
+            if (over) { atomicOr(a.err, ERR_HULL); atomicOr(a.cap.diag, over_index ? HULL_INDEX : HULL_TABLE); }
             a.el.n_elem[g] = ne;
             a.el.n_idx[g] = nd;
             S.ne = ne;

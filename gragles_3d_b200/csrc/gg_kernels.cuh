@@ -160,6 +160,19 @@ struct HullCapture {
     double* tarea;            // (G + 1) x cap: |AB x BC| / 2 of each triangle (computeSurfaceArea's term)
     int* n_rec;               // G + 1
     int* n_tri;               // G + 1
+    int* diag;                // which hull capacity overflowed (HULL_* bits)
+};
+
+// The capacity behind an ERR_HULL, for the error message.
+enum HullDiag : int {
+    HULL_TRIANGLES = 1,   // triangles of one hull beyond hull_capacity
+    HULL_RECORDS = 2,     // active cubes of one hull beyond hull_capacity
+    HULL_LISTS = 4,       // distinct neighbour lists of one hull (256)
+    HULL_JUNCTION_IDS = 8,// IDs of one merged junction
+    HULL_JUNCTIONS = 16,  // junctions of one hull (256)
+    HULL_JOBS = 32,       // misorientations of one hull's elements
+    HULL_TABLE = 64,      // element, ID, segment or chunk table of one hull
+    HULL_INDEX = 128,     // neighbour -> elements index of one hull
 };
 
 // One interfacial element of a grain's mesh (grainHull.cpp:187-531), in the order

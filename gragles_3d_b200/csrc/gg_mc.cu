@@ -259,7 +259,7 @@ __global__ void __launch_bounds__(kThreads, 3) mc_kernel(MCArgs<T> a, int slab_b
                             bb[1] = (p0.y + p1.y + p2.y) / 3;
                             bb[2] = (p0.z + p1.z + p2.z) / 3;
                         } else {
-                            atomicOr(a.err, ERR_HULL);
+                            { atomicOr(a.err, ERR_HULL); atomicOr(a.hull.diag, HULL_TRIANGLES); }
                         }
                     }
                     // GrainHull::computeGrainVolume, grainHull.cpp:42-51
@@ -304,7 +304,7 @@ __global__ void __launch_bounds__(kThreads, 3) mc_kernel(MCArgs<T> a, int slab_b
                         for (int q = 0; q < 8; q++) rl[q] = q < cnt ? lst[q] : 0xFFFFFFFFu;
                         a.hull.rec_ntri[hbase + ri] = nt;
                     } else {
-                        atomicOr(a.err, ERR_HULL);
+                        { atomicOr(a.err, ERR_HULL); atomicOr(a.hull.diag, HULL_RECORDS); }
                     }
                 }
             }
