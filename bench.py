@@ -141,7 +141,7 @@ def measured_traffic(kernel: str, voxels: float):
     return None if rec is None else rec["bytes_per_voxel_update"] * voxels
 
 
-def run_device(gg, precision, ms, ext, counts, steps, warmup, device, dist):
+def run_device(gg, precision, ms, ext, counts, steps, warmup, device, dist, keep=False):
     """Device-resident run: state loaded before the timed region."""
     import torch
 
@@ -170,8 +170,27 @@ def run_device(gg, precision, ms, ext, counts, steps, warmup, device, dist):
     st = gh.stats()
     vol = st.volume.copy()
     ex = st.exists.copy()
+    if keep:
+        return reps, ms_elapsed, clk.summary(), vol, ex, gh
     gh.close()
     return reps, ms_elapsed, clk.summary(), vol, ex
+
+
+def max_sdf_difference(gh_a, gh_b, exists):
+    """max |SDF_a - SDF_b| over the current SDF of every grain both runs hold in the same
+    box, and how many existing grains hold different boxes."""
+    worst, differ = 0.0, 0
+    for g in np.nonzero(exists)[0]:
+        if g == 0:
+            continue
+        box_a, a = gh_a.sdf(int(g), 1)
+        box_b, b = gh_b.sdf(int(g), 1)
+        if box_a != box_b:
+            differ += 1
+            continue
+        if a.size:
+            worst = max(worst, float(np.abs(a - b).max()))
+    return worst, differ
 
 
 def run_e2e(gg, precision, ms, ext, counts, steps, warmup, device):
@@ -351,10 +370,18 @@ def main():
             dist.destroy_process_group()
         return
 
-    reps_m, ms_m, clk_m, vol_m, ex_m = run_device(gg, gg.PRECISION_MIXED, ms, ext, counts, args.steps, args.warmup,
-                                                  local, dist)
-    reps_d, ms_d, clk_d, vol_d, ex_d = run_device(gg, gg.PRECISION_FP64, ms, ext, counts, args.steps, args.warmup,
-                                                  local, dist)
+    reps_m, ms_m, clk_m, vol_m, ex_m, gh_m = run_device(gg, gg.PRECISION_MIXED, ms, ext, counts, args.steps,
+                                                        args.warmup, local, dist, keep=True)
+    reps_d, ms_d, clk_d, vol_d, ex_d, gh_d = run_device(gg, gg.PRECISION_FP64, ms, ext, counts, args.steps,
+                                                        args.warmup, local, dist, keep=True)
+    # the SDF error of the mixed path against FP64 after the same loops (host-side, untimed)
+    try:
+        sdf_err, boxes_differ = max_sdf_difference(gh_m, gh_d, ex_m & ex_d)
+    except Exception as exc:  # a report field only: never lose the timed line over it
+        print(f"SDF comparison skipped: {exc}", file=sys.stderr)
+        sdf_err, boxes_differ = None, None
+    gh_m.close()
+    gh_d.close()
     vox_m = sum(r["voxel_updates"] for r in reps_m)
     vox_d = sum(r["voxel_updates"] for r in reps_d)
     elapsed_m, vox_m = aggregate_replicas(ms_m, vox_m, dist)
@@ -405,6 +432,8 @@ def main():
             "mixed_over_fp64": value / value_fp64,
             "max_rel_volume_err_mixed_vs_fp64": max_rel,
             "rel_volume_err_spread": rel_spread,
+            "max_abs_sdf_err_mixed_vs_fp64": sdf_err,
+            "grains_with_different_boxes": boxes_differ,
             "stage_ms": st_m,
             "roofline": {"bound": "hbm", "kernel": "compare_kernel", "achieved": achieved, "peak": peak,
                          "unit": "GB/s", "frac": achieved / peak, "traffic": traffic,
