@@ -12,6 +12,10 @@ triple-line drag and stored elastic energies.
 The "analysis" case reruns the correction case on one thread with the reference's
 analysis outputs on: Texture and Faces records every loop and the voxel container.
 
+The "wall" case keeps one grain's field where it meets the domain wall (from the
+oracle restatement): the evidence that the reference's hull volume jumps when one
+voxel within 1e-8 of zero changes sign.
+
     python tests/golden/make_golden.py [case ...]
 """
 from __future__ import annotations
@@ -153,6 +157,38 @@ def make_analysis(N=32, G=30, border=5, seed=2032, steps=8, plot_every=2):
     print("analysis ok", {k: v.shape for k, v in out.items() if hasattr(v, "shape")})
 
 
+def make_wall(N=64, G=600, border=10, seed=2064, loops=19, gid=159):
+    """One grain's field where it meets the domain wall, from the oracle restatement (bit-
+    exact with the reference on the device path's parity cases): Voronoi 64^3 / 600 grains,
+    random orientations, Read-Shockley energies, the mobility model and the correction,
+    after `loops` loops.  Its wall plane holds voxels with |phi| < 1e-6; the fixture keeps
+    the one whose sign change moves the reference's hull volume the most."""
+    import pyoracle
+
+    ms = msgen.voronoi(N, G, seed=seed)
+    ext, cnt = ms.grain_extents()
+    sim = pyoracle.OracleSim(N, border, 0.2, ms.labels, ext, cnt)
+    sim.set_physics(True, unique_energies=False, mobility_model=True)
+    sim.set_orientations(ms.euler)
+    for _ in range(loops):
+        sim.step()
+    box, sdf = sim.sdf(gid)
+    ibox, idl = sim.idlocal(gid)
+    assert ibox == box
+    h = 1.0 / N
+    base = pyoracle.mc_box(box, sdf, idl, gid, h)[1]
+    best, at = 0.0, None
+    for z, y, x in np.argwhere(np.abs(sdf) < 1e-6):
+        f = sdf.copy()
+        f[z, y, x] = -f[z, y, x]
+        d = abs(pyoracle.mc_box(box, f, idl, gid, h)[1] - base)
+        if d > best:
+            best, at = d, (int(z), int(y), int(x))
+    np.savez_compressed(os.path.join(HERE, "wall.npz"), N=N, gid=gid, loops=loops, box=np.array(box, np.int32),
+                        sdf=sdf, idlocal=idl, flip=np.array(at, np.int32))
+    print("wall ok", box, at, best * N ** 3)
+
+
 if __name__ == "__main__":
     only = sys.argv[1:]
     for name, args in CASES.items():
@@ -160,3 +196,5 @@ if __name__ == "__main__":
             make(name, *args)
     if not only or "analysis" in only:
         make_analysis()
+    if not only or "wall" in only:
+        make_wall()
