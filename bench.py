@@ -195,7 +195,7 @@ def max_sdf_difference(gh_a, gh_b, exists):
 
 def run_e2e(gg, precision, ms, ext, counts, steps, warmup, device):
     """Through the public API with host buffers: upload, steps, per-step read-back.
-    One untimed pass of `warmup` steps first, then the timed pass of `steps`."""
+    One untimed pass of `warmup` steps first, then three timed passes of `steps`."""
     import torch
 
     # the step inputs sit in pinned host memory (the tensor keeps it alive; numpy views it)
@@ -224,7 +224,10 @@ def run_e2e(gg, precision, ms, ext, counts, steps, warmup, device):
         return vox, ev0.elapsed_time(ev1), t_setup * 1e3
 
     one_pass(max(warmup, 1), False)
-    vox, ms_elapsed, ms_setup = one_pass(steps, True)
+    # three timed passes, the median reported: a pass's set-up includes the device
+    # allocations of gg_load_state, whose time varies with the driver's memory state
+    passes = sorted((one_pass(steps, True) for _ in range(3)), key=lambda r: r[1])
+    vox, ms_elapsed, ms_setup = passes[1]
     G1 = WORKLOAD["grains"] + 1
     h2d = labels.nbytes + ext.astype(np.int32).nbytes + counts.astype(np.int64).nbytes
     if PHYSICS:
