@@ -149,3 +149,34 @@ def test_texture_euler_angles_follow_the_reference():
     for rec in t:
         e = gg.quaternion_to_euler(gg.euler_to_quaternion(d["euler"][rec["id"] - 1]))
         assert np.allclose(e, (rec["phi1"], rec["PHI"], rec["phi2"]), rtol=0, atol=1e-12)
+
+
+def test_ctypes_structs_match_the_c_header(tmp_path):
+    """The Python mirrors of gg_params and gg_step_stats have the C layout: size and
+    every field's offset, from a program gcc compiles against include/gg_b200.h."""
+    import ctypes as C
+    import shutil
+    import subprocess
+
+    if not shutil.which("gcc"):
+        pytest.skip("gcc missing")
+    from gragles_3d_b200 import Params, StepStats
+
+    lines = ['#include <stdio.h>', '#include <stddef.h>', '#include "gg_b200.h"', "int main(void) {"]
+    for cname, py in (("gg_params", Params), ("gg_step_stats", StepStats)):
+        lines.append(f'printf("{cname} size %zu\\n", sizeof({cname}));')
+        for field, _ in py._fields_:
+            lines.append(f'printf("{cname} {field} %zu\\n", offsetof({cname}, {field}));')
+    lines.append("return 0; }")
+    src = tmp_path / "layout.c"
+    src.write_text("\n".join(lines))
+    exe = tmp_path / "layout"
+    subprocess.run(["gcc", "-I", os.path.join(ROOT, "include"), str(src), "-o", str(exe)], check=True)
+    got = {}
+    for row in subprocess.run([str(exe)], check=True, capture_output=True, text=True).stdout.splitlines():
+        cname, field, value = row.split()
+        got[(cname, field)] = int(value)
+    for cname, py in (("gg_params", Params), ("gg_step_stats", StepStats)):
+        assert got[(cname, "size")] == C.sizeof(py), cname
+        for field, _ in py._fields_:
+            assert got[(cname, field)] == getattr(py, field).offset, (cname, field)
