@@ -1163,7 +1163,11 @@ int gg_convolve_boxes_f64(const double* d_in, double* d_out, const int32_t* side
     if (!d_in || !d_out || !sides || !offs || n_boxes < 1 || domain_size < 1) return GG_ERR_INVALID;
     int nmax = 0;
     for (int b = 0; b < n_boxes; b++) nmax = std::max(nmax, (int)sides[b]);
-    if (nmax < 1 || conv_f64_smem_bytes(nmax) > 227 * 1024) return GG_ERR_UNSUPPORTED;
+    int dev = 0, sms = 0, optin = 0;
+    CK(cudaGetDevice(&dev));
+    CK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+    CK(cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev));
+    if (nmax < 1 || conv_f64_smem_bytes(nmax) > (size_t)optin) return GG_ERR_UNSUPPORTED;
     std::vector<double2> tw;
     std::vector<long long> tw_off(nmax + 2, 0), g_off(nmax + 2, 0);
     std::vector<double> gt;
@@ -1222,9 +1226,7 @@ int gg_convolve_boxes_f64(const double* d_in, double* d_out, const int32_t* side
     a.tw_off = d_tw_off;
     a.gtab = d_gt;
     a.g_off = d_g_off;
-    int sms = 148;
-    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, 0);
-    launch_conv_f64(a, sms * 8, conv_f64_smem_bytes(nmax), 0);
+    launch_conv_f64(a, (sms > 0 ? sms : 148) * 8, conv_f64_smem_bytes(nmax), 0);
     CK(cudaGetLastError());
     CK(cudaDeviceSynchronize());
     void* ptrs[] = {d_tw, d_gt, d_tw_off, d_g_off, d_spec, d_box, d_off, d_spec_off, d_toff};

@@ -11,6 +11,7 @@
 #pragma once
 
 #include <cstdint>
+#include <mutex>
 #include <cuda_runtime.h>
 
 namespace gg {
@@ -146,6 +147,30 @@ inline cudaError_t allow_max_dynamic_smem(K* kernel) {
     if (e != cudaSuccess) return e;
     return cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, optin - (int)fa.sharedSizeBytes);
 }
+
+// Runs a set-up action once per CUDA device, on the device current at the call.
+// Kernel attributes such as the dynamic shared-memory opt-in belong to the
+// device (context) they were set on, so a process that drives a second device
+// must set them there again.  Calls from several host threads are serialised.
+class PerDevice {
+  public:
+    template <typename F>
+    void once(F&& f) {
+        int dev = 0;
+        if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) {
+            f();
+            return;
+        }
+        std::lock_guard<std::mutex> lock(mu_);
+        if ((done_ >> dev) & 1ull) return;
+        f();
+        done_ |= 1ull << dev;
+    }
+
+  private:
+    std::mutex mu_;
+    unsigned long long done_ = 0;
+};
 
 __device__ __forceinline__ int isgn(double v) { return (0.0 < v) - (v < 0.0); }  // utilities.h:27-30
 __device__ __forceinline__ int isgn(float v) { return (0.0f < v) - (v < 0.0f); }

@@ -624,11 +624,10 @@ void launch_bin(const TileBins& tb, int G, const int* exists, const int* box, in
 
 template <typename T>
 void launch_compare(const CompareArgs<T>& a, int grid, cudaStream_t s) {
-    static bool configured = false;
-    if (!configured) {
+    static PerDevice configured;
+    configured.once([] {
         allow_max_dynamic_smem(compare_kernel<T>);
-        configured = true;
-    }
+    });
     compare_kernel<T><<<grid, kThreads, compare_smem_bytes(a.mcap, sizeof(T) == 8), s>>>(a);
 }
 

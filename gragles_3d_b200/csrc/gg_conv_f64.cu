@@ -278,13 +278,12 @@ int conv_f64_max_side(size_t smem_limit) {
 }
 
 void launch_conv_f64(const ConvArgs& a, int grid, size_t smem, cudaStream_t s) {
-    static bool configured = false;
-    if (!configured) {
+    static PerDevice configured;
+    configured.once([] {
         allow_max_dynamic_smem(conv_pass_a);
         allow_max_dynamic_smem(conv_pass_b);
         allow_max_dynamic_smem(conv_pass_c);
-        configured = true;
-    }
+    });
     conv_pass_a<<<grid, 256, smem, s>>>(a);
     conv_pass_b<<<grid, 256, smem, s>>>(a);
     conv_pass_c<<<grid, 256, smem, s>>>(a);

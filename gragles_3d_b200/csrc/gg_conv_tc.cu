@@ -152,12 +152,11 @@ __global__ void __launch_bounds__(kThreads) conv_z_kernel(ConvTCArgs a) {
 }  // namespace
 
 void launch_conv_tc(const ConvTCArgs& a, int num_sms, int side_max, cudaStream_t s) {
-    static bool configured = false;
-    if (!configured) {
+    static PerDevice configured;
+    configured.once([] {
         allow_max_dynamic_smem(conv_xy_kernel);
         allow_max_dynamic_smem(conv_z_kernel);
-        configured = true;
-    }
+    });
     const int n = side_max;
     const size_t smem = 3 * (size_t)n * (n | 1) * sizeof(float);
     const int grid = num_sms * 8;

@@ -21,7 +21,11 @@
 //   epilogue (8 warps, two tiles at a time): tcgen05.ld of one tile row per thread, column c' stored to
 //     U[c'][row]; lanes hold consecutive rows, so each store writes 128 contiguous bytes.
 // Every wait is bounded: a timeout flags ERR_TIMEOUT and raises a CTA abort flag that
-// ends the other roles' waits too; TMEM is freed on every exit path.
+// ends the other roles' waits too.  Before the CTA exits, on every path, the TMA thread
+// waits (bounded, whatever the abort flag says) for the last bulk copy it issued into
+// each shared-memory buffer, and the MMA thread commits and waits for its last MMAs,
+// so that no asynchronous write to this CTA's shared memory or TMEM is still in flight
+// when TMEM is freed and the CTA's shared memory is released.
 #include <cstring>
 #include <cuda_fp16.h>
 
@@ -38,7 +42,7 @@ constexpr int kEpiWarps = 8;                         // two groups of four (one 
 constexpr int kAcc = 4;                              // TMEM accumulators
 constexpr int kThreadsU = (kSplitWarps + kEpiWarps + 2) * 32;  // split, epilogue, MMA, TMA warps
 constexpr int kMaxR = 4, kMaxS = 4;                  // staged tiles, operand stages
-constexpr int kBars = 2 * kMaxR + 2 * kMaxS + 2 * kAcc + 2 + 2;
+constexpr int kBars = 2 * kMaxR + 2 * kMaxS + 2 * kAcc + 2 + 2 + 1;
 constexpr uint32_t kAccCols = 64;   // one accumulator: N <= round16(kUmmaMaxSide) columns
 constexpr uint32_t kTmemCols = kAcc * kAccCols;
 constexpr long long kWaitCycles = 1LL << 31;  // ~1 s at the B200 clock
@@ -189,6 +193,18 @@ __device__ __forceinline__ bool wait_bar(uint32_t bar, uint32_t parity, volatile
     return false;
 }
 
+// Bounded wait at exit for asynchronous work this thread issued (a bulk copy's
+// complete_tx, or a tcgen05.commit): it ignores the abort flag, since the point is to
+// let that work land before the CTA's shared memory and TMEM are released.
+__device__ __forceinline__ void drain_bar(uint32_t bar, uint32_t parity, int* err) {
+    const long long t0 = clock64();
+    for (int it = 0; it < (1 << 24); it++) {
+        if (mbar_try_wait(bar, parity)) return;
+        if (clock64() - t0 > kWaitCycles) break;
+    }
+    atomicOr(err, ERR_TIMEOUT);
+}
+
 // Re-layout one staged tile (rows x n floats, row-major) into the MMA's K-major
 // core-matrix layout, split into FP16 hi and lo.  Core matrix q = mg KC + kc holds
 // rows 8 mg .. 8 mg + 7, columns 8 kc .. 8 kc + 7 as 8 rows of 16 B at byte 128 q;
@@ -241,7 +257,7 @@ __global__ void __launch_bounds__(kThreadsU, 1)
     const int b_halves = 2 * np_max * kp_max;
     auto bar = [&](int i) { return smem_u32(&bars[i]); };
     constexpr int RFULL = 0, REMPTY = kMaxR, FULL = 2 * kMaxR, EMPTY = FULL + kMaxS, TFULL = EMPTY + kMaxS,
-                  TEMPTY = TFULL + kAcc, BFULL = TEMPTY + kAcc, BFREE = BFULL + 2;
+                  TEMPTY = TFULL + kAcc, BFULL = TEMPTY + kAcc, BFREE = BFULL + 2, DRAIN = BFREE + 2;
 
     const int total = a.toff[a.G + 1];
     const int t_begin = (int)((long long)total * blockIdx.x / gridDim.x);
@@ -267,6 +283,7 @@ __global__ void __launch_bounds__(kThreadsU, 1)
             mbar_init(bar(BFULL + b), 1);
             mbar_init(bar(BFREE + b), 1);
         }
+        mbar_init(bar(DRAIN), 1);
         abort_flag = 0;
     }
     // a side beyond the launch's shared-memory sizing would overrun the buffers
@@ -343,6 +360,7 @@ __global__ void __launch_bounds__(kThreadsU, 1)
         Cursor c;
         c.init(&a, t_begin);
         int cur_n = -1, nsw = 0, kb = 0;
+        bool issued = false;
         for (int i = 0; i < count; i++, c.advance()) {
             const int s = i % S, b = i % kAcc;
             if (!wait_bar(bar(FULL + s), (i / S) & 1, ab, a.err)) break;
@@ -369,14 +387,20 @@ __global__ void __launch_bounds__(kThreadsU, 1)
                 mma_f16(d, smem_desc(a_hi + o, sbo), smem_desc(b_lo + o, sbo), idesc, 1);
                 mma_f16(d, smem_desc(a_hi + o, sbo), smem_desc(b_hi + o, sbo), idesc, 1);
             }
+            issued = true;
             mma_commit(bar(EMPTY + s));
             mma_commit(bar(TFULL + b));
+        }
+        if (issued) {  // every MMA issued above has completed before TMEM is freed
+            mma_commit(bar(DRAIN));
+            drain_bar(bar(DRAIN), 0, a.err);
         }
     } else if (warp == kSplitWarps + kEpiWarps + 1 && lane == 0) {
         // ---------------- TMA loads ----------------
         Cursor c;
         c.init(&a, t_begin);
         int cur_n = -1, nsw = 0;
+        int last_tile[kMaxR] = {-1, -1, -1, -1}, last_b[2] = {-1, -1};  // last copy into each buffer
         for (int i = 0; i < count; i++, c.advance()) {
             const int r = i % R;
             if (i >= R && !wait_bar(bar(REMPTY + r), (i / R - 1) & 1, ab, a.err)) break;
@@ -386,6 +410,7 @@ __global__ void __launch_bounds__(kThreadsU, 1)
                 const uint32_t bytes = 2u * round_n(c.n) * round_k(c.n) * 2u;
                 mbar_expect_tx(bar(BFULL + kb), bytes);
                 bulk_load(smem_u32(b_base + kb * b_halves), a.bmat + a.boff[c.n], bytes, bar(BFULL + kb));
+                last_b[kb] = nsw;
                 cur_n = c.n;
                 nsw++;
             }
@@ -394,7 +419,13 @@ __global__ void __launch_bounds__(kThreadsU, 1)
             mbar_expect_tx(bar(RFULL + r), bytes);
             bulk_load(smem_u32(raw_base + r * tile_floats), a.src + a.src_off[c.g] + (long long)c.r0() * c.n, bytes,
                       bar(RFULL + r));
+            last_tile[r] = i;
         }
+        // the copies land before the CTA exits, also when a role gave up early
+        for (int r = 0; r < R && r < kMaxR; r++)
+            if (last_tile[r] >= 0) drain_bar(bar(RFULL + r), (last_tile[r] / R) & 1, a.err);
+        for (int kb = 0; kb < 2; kb++)
+            if (last_b[kb] >= 0) drain_bar(bar(BFULL + kb), (last_b[kb] >> 1) & 1, a.err);
     }
     tc_fence_before();
     __syncthreads();
@@ -461,11 +492,10 @@ void umma_tables(int N, double time_step, int nmax, std::vector<uint16_t>& bmat,
 }
 
 void launch_conv_umma(const UmmaConvArgs& c, int num_sms, int side_max, cudaStream_t s) {
-    static bool configured = false;
-    if (!configured) {
+    static PerDevice configured;
+    configured.once([] {
         allow_max_dynamic_smem(conv_umma_kernel);
-        configured = true;
-    }
+    });
     const UmmaShape sh = umma_shape(side_max);
     UmmaPassArgs p{};
     p.G = c.G;

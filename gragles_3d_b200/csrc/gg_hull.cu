@@ -1120,15 +1120,16 @@ void launch_faces(int G, const int* exists, HullElements el, double /*h*/, const
 }
 
 void launch_elements(const ElementArgs& a, int grid, cudaStream_t s) {
-    static bool configured = false;
-    if (!configured) {
+    static PerDevice configured;
+    configured.once([] {
         allow_max_dynamic_smem(elements_kernel);
-        configured = true;
-    }
-    static int resident = 0;  // CTAs that fit on the device at once
+    });
+    static int resident_on[64] = {};  // CTAs that fit on each device at once
+    int dev = 0;
+    cudaGetDevice(&dev);
+    int& resident = resident_on[dev >= 0 && dev < 64 ? dev : 0];
     if (resident == 0) {
-        int dev = 0, sms = 0, per_sm = 0;
-        cudaGetDevice(&dev);
+        int sms = 0, per_sm = 0;
         cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
         cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, elements_kernel, 32, sizeof(ElemSmem));
         resident = sms * (per_sm > 0 ? per_sm : 1);

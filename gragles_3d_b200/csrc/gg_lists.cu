@@ -237,11 +237,10 @@ void launch_pos_tables(const PosTableArgs& a, int grid, cudaStream_t s) {
 }
 
 void launch_update_lists(const ListArgs& a, int grid, cudaStream_t s) {
-    static bool configured = false;
-    if (!configured) {
+    static PerDevice configured;
+    configured.once([] {
         allow_max_dynamic_smem(update_lists_kernel);
-        configured = true;
-    }
+    });
     const size_t smem = list_smem_bytes(a.G);
     update_lists_kernel<<<grid, kThreads, smem, s>>>(a);
 }

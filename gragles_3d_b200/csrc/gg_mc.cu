@@ -418,11 +418,10 @@ size_t mc_slab_bytes(int side) {
 
 template <typename T>
 void launch_mc(const MCArgs<T>& a, int grid, int side, cudaStream_t s) {
-    static bool configured = false;
-    if (!configured) {
+    static PerDevice configured;
+    configured.once([] {
         allow_max_dynamic_smem(mc_kernel<T>);
-        configured = true;
-    }
+    });
     const size_t bytes = mc_slab_bytes(side);
     mc_kernel<T><<<grid, kThreads, bytes, s>>>(a, (int)bytes);
 }

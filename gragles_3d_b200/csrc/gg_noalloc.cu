@@ -1,26 +1,29 @@
 // gg_noalloc.cu -- FP64 box convolution that allocates no device memory.
 //
 // gg_convolve_boxes_f64 allocates its half-spectrum scratch and its tables with
-// cudaMalloc on every call.  Some callers cannot do that: a host program that hands
-// all device memory to its own pool when it starts, or a time-stepping loop in which
-// a cudaMalloc/cudaFree (which synchronise the device) would stall work queued on
-// other streams.  gg_convolve_boxes_f64_noalloc computes exactly the same result with
-// every buffer it needs -- the half-spectrum scratch, the DFT twiddles, the Gaussian
-// table and the per-box metadata -- in file-scope __device__ arrays of fixed size
-// (32 MiB of scratch plus under 2 MiB of tables, held by every GPU that loads the
-// library until the process exits).  The caller still owns and passes the input and
-// output boxes.
+// cudaMalloc on every call.  Some callers cannot allocate device memory: a host
+// program that hands all of the GPU's memory to its own pool allocator when it starts
+// (so a cudaMalloc from a library would fail or take memory the pool counts on), or
+// one that forbids allocation after start-up so that its memory footprint stays
+// fixed.  gg_convolve_boxes_f64_noalloc computes exactly the same result with every
+// buffer it needs -- the half-spectrum scratch, the DFT twiddles, the Gaussian table
+// and the per-box metadata -- in file-scope __device__ arrays of fixed size (32 MiB of
+// scratch plus under 2 MiB of tables, held by every GPU that loads the library until
+// the process exits).  The caller still owns and passes the input and output boxes.
 //
 // Limits: at most kMaxBoxes boxes per call, sides up to kMaxSide, and
 // sum over boxes of n*n*(n/2+1) <= kScratchComplex; larger requests are refused with
 // GG_ERR_UNSUPPORTED before anything runs.  The first call on each device looks up
-// the arrays' device addresses (cudaGetSymbolAddress) and uploads the twiddles, so
-// that first call should come before any stream capture.  All calls share the
-// arrays and the last call's contents stay in them; every buffer is fully rewritten
-// before it is read, and each call synchronises the device before it returns, so
-// consecutive calls from one host thread are safe.  Calls that overlap on the GPU
-// (several host threads, or several processes driving the same device through one
-// context) race on the shared arrays.
+// the arrays' device addresses (cudaGetSymbolAddress) and uploads the twiddles.
+//
+// The call is synchronous: it copies the per-box metadata with cudaMemcpy from static
+// host staging, launches on the legacy default stream and ends with
+// cudaDeviceSynchronize, so it waits for all work on the device.  Because every call
+// uses the same device arrays, calls from the threads of one process are serialised
+// by a mutex held from the metadata upload until the device has finished; the arrays
+// keep the last call's contents, and every buffer a call reads is rewritten by that
+// call first.  (Other processes have their own contexts and so their own copies of
+// the arrays.)
 #include <cmath>
 #include <cstdint>
 #include <mutex>
@@ -196,6 +199,9 @@ extern "C" int gg_convolve_boxes_f64_noalloc(const double* d_in, double* d_out, 
     a.tw_off = d.tw_off;
     a.gtab = d.gauss;
     a.g_off = d.g_off;
+    // an error left over from earlier, unrelated work is not this launch's: clear it
+    // first (a sticky error has already failed the copies above)
+    (void)cudaGetLastError();
     gg::launch_conv_f64(a, (sms > 0 ? sms : 148) * 8, smem, 0);
     if (cudaGetLastError() != cudaSuccess) return GG_ERR_CUDA;
     if (cudaDeviceSynchronize() != cudaSuccess) return GG_ERR_CUDA;

@@ -283,12 +283,11 @@ size_t redist_smem_bytes(int nmax, bool fp64) {
 
 template <typename T>
 void launch_redistance(const RedistArgs<T>& a, int grid, int side, cudaStream_t s) {
-    static bool configured = false;
-    if (!configured) {
+    static PerDevice configured;
+    configured.once([] {
         allow_max_dynamic_smem(redist_xy_kernel<T>);
         allow_max_dynamic_smem(redist_z_kernel<T>);
-        configured = true;
-    }
+    });
     const size_t smem = redist_smem_bytes(side, sizeof(T) == 8);
     int threads = (side + 31) / 32 * 32;
     threads = threads > kMaxThreads ? kMaxThreads : threads;

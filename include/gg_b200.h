@@ -167,12 +167,13 @@ int gg_convolve_boxes_mixed(const float* d_in, float* d_out, const int32_t* side
 /* The same FP64 convolution, bit for bit, without allocating any device memory.
  * No counterpart in the reference: it exists for callers that cannot call
  * cudaMalloc -- programs that give all device memory to their own pool at start-up,
- * or loops where an allocation's device-wide synchronisation would stall other work.
- * Its scratch (32 MiB half-spectrum) and tables live in fixed device arrays that every
- * GPU loading the library holds until exit.  Limits: n_boxes <= 256, sides <= 96,
- * sum of n*n*(n/2+1) <= 2^21; beyond them it returns GG_ERR_UNSUPPORTED.  The first
- * call on a device sets up the arrays (make it before any stream capture); calls share
- * the arrays, so calls that overlap on the GPU race.  Synchronous, like the above. */
+ * or that keep their device footprint fixed after start-up.  Its scratch (32 MiB
+ * half-spectrum) and tables live in fixed device arrays that every GPU loading the
+ * library holds until exit.  Limits: n_boxes <= 256, sides <= 96, sum of
+ * n*n*(n/2+1) <= 2^21; beyond them it returns GG_ERR_UNSUPPORTED.  The first call on a
+ * device looks up the arrays and uploads the twiddles.  Synchronous: it ends with
+ * cudaDeviceSynchronize, so it waits for all work on the device.  Calls from one
+ * process share the arrays and are therefore serialised by a lock, one at a time. */
 int gg_convolve_boxes_f64_noalloc(const double* d_in, double* d_out, const int32_t* sides, const int64_t* offs,
                                   int32_t n_boxes, int32_t domain_size, double time_step);
 

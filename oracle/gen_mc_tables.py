@@ -12,7 +12,8 @@ and by the triangle table, and writes them as C headers:
     oracle/gg_mc_tables.h                    (oracle restatement)
     gragles_3d_b200/csrc/gg_mc_tables.inc    (CUDA path)
 
-Run:  python oracle/gen_mc_tables.py [/root/reference/src/marchingCubes.cpp]
+Run:  python oracle/gen_mc_tables.py [path/to/reference/src/marchingCubes.cpp]
+(default: the reference beside this repository, or $GG_REFERENCE_SRC/marchingCubes.cpp)
 """
 from __future__ import annotations
 
@@ -73,7 +74,9 @@ def emit(edge, tri, qualifier: str) -> str:
 
 
 def main():
-    path = sys.argv[1] if len(sys.argv) > 1 else "/root/reference/src/marchingCubes.cpp"
+    here = os.path.dirname(os.path.abspath(__file__))
+    src = os.environ.get("GG_REFERENCE_SRC", os.path.join(here, "..", "..", "reference", "src"))
+    path = sys.argv[1] if len(sys.argv) > 1 else os.path.join(src, "marchingCubes.cpp")
     edge, tri = parse(path)
     check(edge, tri)
     with open(os.path.join(HERE, "gg_mc_tables.h"), "w") as f:

@@ -60,8 +60,8 @@ def test_convolution_kernel_bitexact(gpu, oracle):
 
 
 def test_mixed_convolution_kernel_accuracy(gpu, oracle):
-    """The mixed path's convolution (tcgen05 3xTF32 when all sides are <= 64, FP32 SIMT
-    otherwise) against the FP64 specified DFT: FP32-level error, far below plain TF32's
+    """The mixed path's convolution (tcgen05 with operands split into FP16 hi + lo, three MMAs per
+    K-step, when all sides are <= 64; FP32 SIMT otherwise) against the FP64 specified DFT: FP32-level error, far below plain TF32's
     ~5e-4.  Side sets with repeated and alternating sides exercise the kernel's switch
     between its two C_n buffers."""
     rng = np.random.default_rng(8)

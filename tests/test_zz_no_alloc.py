@@ -1,9 +1,8 @@
 """The allocation-free FP64 box convolution (gg_convolve_boxes_f64_noalloc).
 
 It serves callers of this library that cannot call cudaMalloc -- a program that
-gives all device memory to its own pool at start-up, or a loop that must not stall
-on an allocation's device-wide synchronisation -- by keeping its scratch in fixed
-device arrays.  Its output must be bit-identical to gg_convolve_boxes_f64 (the
+gives all device memory to its own pool at start-up, or one whose device footprint
+must stay fixed after start-up -- by keeping its scratch in fixed device arrays.  Its output must be bit-identical to gg_convolve_boxes_f64 (the
 FP64 path's tolerance is exactness), call after call, although every call reuses
 and leaves behind the same scratch.  This file is collected last on purpose.
 """
@@ -52,6 +51,22 @@ def test_noalloc_convolution_matches_the_allocating_one_twice(gpu):
         boxes = [rng.uniform(-0.1, 0.1, (n, n, n)) for n in sides]
         want = _run(lib, "gg_convolve_boxes_f64", boxes, N, ts)
         got = _run(lib, "gg_convolve_boxes_f64_noalloc", boxes, N, ts)
+        for w, g in zip(want, got):
+            assert np.array_equal(w, g), f"side {w.shape[0]}: max diff {np.abs(w - g).max()}"
+
+
+def test_noalloc_convolution_at_its_limits(gpu):
+    """The largest side the arrays take (96) and a call that fills the 2^21-complex
+    scratch to 99%, each compared bit for bit with the allocating entry point."""
+    lib = gpu.load_library()
+    rng = np.random.default_rng(12)
+    near_full = [96, 96, 96, 96, 64, 48, 40, 36, 32]
+    used = sum(n * n * (n // 2 + 1) for n in near_full)
+    assert 0.98 * (1 << 21) < used <= (1 << 21)
+    for sides in ([96], near_full):
+        boxes = [rng.uniform(-0.05, 0.05, (n, n, n)) for n in sides]
+        want = _run(lib, "gg_convolve_boxes_f64", boxes, 256, 0.2)
+        got = _run(lib, "gg_convolve_boxes_f64_noalloc", boxes, 256, 0.2)
         for w, g in zip(want, got):
             assert np.array_equal(w, g), f"side {w.shape[0]}: max diff {np.abs(w - g).max()}"
 
