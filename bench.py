@@ -1,13 +1,16 @@
 #!/usr/bin/env python
 """Throughput of the GraGLeS_3D level-set timestep on B200.
 
-Workload: a 128^3 voxel domain, 2,000 grains from a Voronoi tessellation of
-seeded uniform-random points, isotropic grain-boundary energy and mobility,
-10-voxel box border, TimeStepSize 0.2 (the reference's non-periodic domain with
-the boundary grain).  A *step* is one full timestep of the loop (convolution,
-list update, comparison, marching cubes, redistancing, box bookkeeping) over
-every live grain box.  The unit of work is a voxel-update: one box voxel carried
-through one timestep (the sum of n^3 over the boxes the step convolves).
+Workload (default): a 256^3 voxel domain, 20,000 grains from a Voronoi tessellation of
+seeded uniform-random points with uniformly random orientations, Read-Shockley
+grain-boundary energies (15 degree cutoff), the misorientation mobility model and the
+convolution correction on, 10-voxel box border, TimeStepSize 0.2 (the reference's
+non-periodic domain with the boundary grain).  ``--workload voronoi-128`` runs the
+isotropic 128^3 / 2,000-grain workload instead.  A *step* is one full timestep of the
+loop (convolution with its correction, list update, comparison, marching cubes, element
+mesh, redistancing, box bookkeeping) over every live grain box.  The unit of work is a
+voxel-update: one box voxel carried through one timestep (the sum of n^3 over the boxes
+the step convolves).
 
 Headline: the mixed path (FP32 storage, per-axis circulant convolution, FP64
 volume tallies).  The FP64 path (bit-exact with the reference) runs beside it
@@ -37,15 +40,18 @@ sys.path.insert(0, ROOT)
 
 METRIC = "voxel-updates/s per timestep, mixed vs FP64 path on 1 B200, at vol err ≤1e-3"
 UNIT = "voxel-updates/s"
-WORKLOAD = dict(workload="voronoi-128^3-2000-grains-isotropic", domain=128, grains=2000, border=10,
-                time_step=0.2, seed=1002)
-# --workload anisotropic-256: 256^3, 20,000 Voronoi grains with uniform random orientations,
-# Read-Shockley energies (15 degree cutoff), the misorientation mobility model and the
-# convolution correction on; the configuration the mixed-over-FP64 target is quoted on
-ANISOTROPIC = dict(workload="voronoi-256^3-20000-grains-read-shockley-mobility-correction", domain=256,
-                   grains=20000, border=10, time_step=0.2, seed=1003)
-PHYSICS = {}  # GrainHandler physics keywords of the workload (isotropic: none)
 HULL_CAPACITY = 12000  # triangles per hull for the correction's element build
+WORKLOADS = {
+    # the configuration the mixed-over-FP64 target is quoted on
+    "anisotropic-256": (dict(workload="voronoi-256^3-20000-grains-read-shockley-mobility-correction", domain=256,
+                             grains=20000, border=10, time_step=0.2, seed=1003),
+                        dict(correction=True, unique_energies=False, mobility_model=True,
+                             hull_capacity=HULL_CAPACITY)),
+    "voronoi-128": (dict(workload="voronoi-128^3-2000-grains-isotropic", domain=128, grains=2000, border=10,
+                         time_step=0.2, seed=1002), {}),
+}
+WORKLOAD = dict(WORKLOADS["anisotropic-256"][0])
+PHYSICS = dict(WORKLOADS["anisotropic-256"][1])  # GrainHandler physics keywords of the workload
 
 
 # ----------------------------------------------------------------------------------
@@ -129,16 +135,30 @@ STAGE_BYTES = {
 }
 
 
+def source_digest(path: str) -> str:
+    import hashlib
+
+    with open(path, "rb") as f:
+        return hashlib.sha256(f.read()).hexdigest()[:16]
+
+
 def measured_traffic(kernel: str, voxels: float):
     """DRAM bytes (read + write) of one launch of `kernel` over `voxels` box voxels,
     scaled from the ncu capture summarised in profiles/dram_traffic.json (bytes per
-    voxel-update of the captured launch); None when no capture is recorded."""
+    voxel-update of the captured launch).  Returns (bytes or None, note): None when no
+    capture is recorded, or when the kernel's source has changed since the capture (the
+    record keeps a digest of the source it was made from)."""
     path = os.path.join(ROOT, "profiles", "dram_traffic.json")
     if not os.path.exists(path):
-        return None
+        return None, "no capture recorded"
     with open(path) as f:
         rec = json.load(f).get(kernel)
-    return None if rec is None else rec["bytes_per_voxel_update"] * voxels
+    if rec is None:
+        return None, "no capture recorded"
+    src = os.path.join(ROOT, "gragles_3d_b200", "csrc", rec.get("source", ""))
+    if not os.path.isfile(src) or source_digest(src) != rec.get("source_sha256"):
+        return None, "stale: the kernel source changed after the capture"
+    return rec["bytes_per_voxel_update"] * voxels, rec.get("workload", "")
 
 
 def run_device(gg, precision, ms, ext, counts, steps, warmup, device, dist, keep=False):
@@ -174,6 +194,32 @@ def run_device(gg, precision, ms, ext, counts, steps, warmup, device, dist, keep
         return reps, ms_elapsed, clk.summary(), vol, ex, gh
     gh.close()
     return reps, ms_elapsed, clk.summary(), vol, ex
+
+
+def bench_config(world: int) -> dict:
+    """The workload keys both arms report (identical for the GPU and the reference arm)."""
+    return dict(WORKLOAD, parallelism=f"replicas{world}",
+                l2="inputs larger than L2 (box pool >= 0.3 GB per arena)")
+
+
+def over_bound_causes(rel, ids, vol_ref, boxes):
+    """The grains above 1e-3 relative volume difference, by the cause each falls under:
+    a box that reaches a domain-wall plane (where the boundary grain's value is exactly
+    0), else a grain of under 50 voxels, else other."""
+    N, gb = WORKLOAD["domain"], WORKLOAD["border"]
+    lo, hi = gb - 1, N + gb - 1
+    out = {"wall": 0, "under_50_voxels": 0, "other": 0}
+    for r, g in zip(rel, ids):
+        if r <= 1e-3:
+            continue
+        b = boxes[g]
+        if any(b[2 * a] <= lo or b[2 * a + 1] > hi for a in range(3)):
+            out["wall"] += 1
+        elif vol_ref[g] * N ** 3 < 50:
+            out["under_50_voxels"] += 1
+        else:
+            out["other"] += 1
+    return out
 
 
 def max_sdf_difference(gh_a, gh_b, exists):
@@ -242,7 +288,9 @@ def run_e2e(gg, precision, ms, ext, counts, steps, warmup, device):
 # ----------------------------------------------------------------------------------
 def run_reference_cpu(ms, steps: int, warmup: int, threads: int):
     """Time `steps` loop iterations after `warmup` of the compiled reference on the
-    host cores.  Returns (voxel-updates/s, sample description, cores, kind)."""
+    host cores, on the full workload (loops warmup .. warmup + steps - 1; loop 0 is the
+    one without the convolution correction).  Returns (voxel-updates/s, sample
+    description, cores, kind)."""
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     import refdump
     from gragles_3d_b200 import microstructure as msgen
@@ -252,19 +300,23 @@ def run_reference_cpu(ms, steps: int, warmup: int, threads: int):
             msgen.write_mode4(ms, d)
             msgen.write_parameters(os.path.join(d, "parameters.xml"), n_grains=ms.n_grains,
                                    border=WORKLOAD["border"], steps=warmup + steps, threads=threads,
-                                   time_step=WORKLOAD["time_step"])
-            res, _ = refdump.run_case(d, threads=threads, timeout=3600)
+                                   time_step=WORKLOAD["time_step"], correction=bool(PHYSICS.get("correction")),
+                                   unique_energies=PHYSICS.get("unique_energies", True),
+                                   mobility_factor=bool(PHYSICS.get("mobility_model")))
+            # the initial boxes' SDF records are needed only when loop 0 is timed
+            res, _ = refdump.run_case(d, threads=threads, timeout=3600, init=warmup == 0)
         lt = res["loop_time"]
         # voxels convolved in loop t: boxes of the grains alive entering loop t
         vox = {}
-        init = sum(int(np.prod([r.box[1] - r.box[0]] * 3)) for r in res["init_sdf"].values())
-        vox[0] = init
+        if res["init_sdf"]:
+            vox[0] = sum(int(np.prod([r.box[1] - r.box[0]] * 3)) for r in res["init_sdf"].values())
         for loop, st in res["stats"].items():
             vox[loop + 1] = sum((b[1] - b[0]) ** 3 for (d_, b) in st.values() if d_[0] == 1.0)
         t = lt[warmup + steps] - lt[warmup]
         v = sum(vox[l] for l in range(warmup, warmup + steps))
-        sample = (f"reference solver (g++ -O2, OpenMP, shim DFT) on the full workload: loops {warmup}.."
-                  f"{warmup + steps - 1} of {warmup + steps + 1}, {v} voxel-updates in {t:.2f} s")
+        sample = (f"reference solver (g++ -O2, OpenMP, shim DFT) on the full {WORKLOAD['workload']} workload: "
+                  f"loops {warmup}..{warmup + steps - 1} of {warmup + steps + 1} timed, {v} voxel-updates "
+                  f"in {t:.2f} s")
         return v / t, sample, threads, "reference"
     # the C restatement (single thread) on a smaller slice of the loop
     import pyoracle
@@ -279,21 +331,22 @@ def run_reference_cpu(ms, steps: int, warmup: int, threads: int):
     return v / t, f"oracle restatement, 1 thread, 1 timestep of the full workload ({v} voxel-updates)", 1, "port"
 
 
+REF_LOOPS = 2  # loops the host reference times per run (each takes it tens of seconds on 256^3)
+
+
 def reference_arm(args):
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return
-    if PHYSICS:
-        print(json.dumps({"impl": "reference", "unavailable": "the host reference is timed on the default "
-                          "workload only; one anisotropic 256^3 step takes it many minutes"}))
-        return
     ms, _, _ = microstructure()
     threads = os.cpu_count() or 1
-    value, sample, cores, kind = run_reference_cpu(ms, args.steps, args.warmup, threads)
+    # a bounded sample: loop 0 (no correction) runs untimed, then at most REF_LOOPS loops
+    # of the requested steps are timed, so that the run ends within a few minutes
+    value, sample, cores, kind = run_reference_cpu(ms, min(args.steps, REF_LOOPS), 1, threads)
     print(json.dumps({
         "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
         "steps": args.steps, "warmup": args.warmup, "higher_is_better": True, "scaling": "weak",
-        "vs_baseline": None, "dtype": "f64", "data": "synthetic", "config": dict(WORKLOAD),
+        "vs_baseline": None, "dtype": "f64", "data": "synthetic", "config": bench_config(args.gpus),
         "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores, "kind": kind, "sample": sample},
         "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }))
@@ -326,17 +379,17 @@ def main():
                     help="profiling aid: run only one precision path")
     ap.add_argument("--domain", type=int, default=None, help="profiling aid: smaller domain of the same kind")
     ap.add_argument("--grains", type=int, default=None, help="profiling aid: grain count for --domain")
-    ap.add_argument("--workload", default="voronoi-128", choices=["voronoi-128", "anisotropic-256"],
-                    help="anisotropic-256: the 256^3 / 20,000-grain anisotropic workload with the correction")
+    ap.add_argument("--workload", default="anisotropic-256", choices=sorted(WORKLOADS),
+                    help="anisotropic-256 (default): the 256^3 / 20,000-grain anisotropic workload with the "
+                         "correction; voronoi-128: the isotropic 128^3 / 2,000-grain workload")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
-    if args.workload == "anisotropic-256":
-        WORKLOAD.clear()
-        WORKLOAD.update(ANISOTROPIC)
-        PHYSICS.update(correction=True, unique_energies=False, mobility_model=True, hull_capacity=HULL_CAPACITY)
-        args.no_cpu_baseline = True  # the host reference needs many minutes per step here
+    WORKLOAD.clear()
+    WORKLOAD.update(WORKLOADS[args.workload][0])
+    PHYSICS.clear()
+    PHYSICS.update(WORKLOADS[args.workload][1])
     if args.domain:
-        WORKLOAD.update(workload=f"voronoi-{args.domain}^3-{args.grains}-grains-isotropic", domain=args.domain,
+        WORKLOAD.update(workload=f"{args.workload}-at-{args.domain}^3-{args.grains}-grains", domain=args.domain,
                         grains=args.grains)
     if args.impl == "reference":
         return reference_arm(args)
@@ -383,6 +436,7 @@ def main():
     except Exception as exc:  # a report field only: never lose the timed line over it
         print(f"SDF comparison skipped: {exc}", file=sys.stderr)
         sdf_err, boxes_differ = None, None
+    boxes_d = gh_d.stats().boxes
     gh_m.close()
     gh_d.close()
     vox_m = sum(r["voxel_updates"] for r in reps_m)
@@ -399,7 +453,9 @@ def main():
     # the reference's hull volume jumps when a voxel within ~1e-7 of zero changes sign
     # (its vertex snapping leaves the triangulation open there), so the spread matters too
     rel_spread = ({"median": float(np.median(rel)), "p99": float(np.quantile(rel, 0.99)),
-                   "grains_over_1e-3": int((rel > 1e-3).sum()), "grains": int(rel.size)} if rel.size else None)
+                   "grains_over_1e-3": int((rel > 1e-3).sum()), "grains": int(rel.size),
+                   "over_by_cause": over_bound_causes(rel, np.nonzero(both)[0], vol_d, boxes_d)}
+                  if rel.size else None)
 
     def stage_means(reps):
         keys = ["ms_convolution", "ms_lists", "ms_comparison", "ms_levelset", "ms_redistancing", "ms_total"]
@@ -413,7 +469,7 @@ def main():
     vox_k = float(np.mean([r["compare_voxels"] for r in reps_m]))
     bytes_per = STAGE_BYTES["mixed"]["ms_comparison"]
     achieved = bytes_per * vox_k / (ms_k / 1e3) / 1e9
-    traffic = measured_traffic("compare_kernel", vox_k)
+    traffic, traffic_note = measured_traffic("compare_kernel", vox_k)
 
     e2e = None
     out = None
@@ -428,8 +484,7 @@ def main():
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": elapsed_m / args.steps, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-            "config": dict(WORKLOAD, path="mixed", parallelism=f"replicas{world}",
-                           l2="inputs larger than L2 (box pool >= 0.3 GB per arena)"),
+            "config": bench_config(world), "path": "mixed",
             "fp64": {"value": value_fp64, "ms_per_step": elapsed_d / args.steps, "dtype": "f64",
                      "stage_ms": st_d, "clocks": clk_d},
             "mixed_over_fp64": value / value_fp64,
@@ -440,7 +495,8 @@ def main():
             "stage_ms": st_m,
             "roofline": {"bound": "hbm", "kernel": "compare_kernel", "achieved": achieved, "peak": peak,
                          "unit": "GB/s", "frac": achieved / peak, "traffic": traffic,
-                         "peak_source": peak_kind, "bytes_per_voxel_update": bytes_per,
+                         "peak_source": peak_kind, "traffic_source": traffic_note,
+                         "bytes_per_voxel_update": bytes_per,
                          "ms_per_launch": ms_k, "voxels_per_launch": vox_k},
             "cpu_baseline": cpu,
             "e2e": {k: e2e.get(k) for k in ("value", "unit", "h2d_bytes_per_step", "d2h_bytes_per_step", "ms",

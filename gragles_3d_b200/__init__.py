@@ -33,7 +33,7 @@ EXPORTED = [
     "gg_stage_redistancing", "gg_get_grain_stats", "gg_get_neighbors", "gg_get_list", "gg_get_sdf",
     "gg_get_idlocal", "gg_grain_count", "gg_loop", "gg_convolve_boxes_f64", "gg_convolve_boxes_mixed",
     "gg_convolve_boxes_f64_noalloc", "gg_set_orientations", "gg_set_stored_energy", "gg_get_elements",
-    "gg_voxel_container", "gg_get_faces",
+    "gg_voxel_container", "gg_get_faces", "gg_domain_size",
 ]
 
 
@@ -50,6 +50,7 @@ class Params(C.Structure):
         ("list_capacity", C.c_int32), ("pool_voxels", C.c_int64), ("device", C.c_int32),
         ("unique_gb_energies", C.c_int32), ("mobility_model", C.c_int32), ("use_stored_energy", C.c_int32),
         ("triple_line_drag", C.c_double), ("hull_capacity", C.c_int32), ("keep_elements", C.c_int32),
+        ("grid_coarsening", C.c_int32), ("points_per_grain", C.c_int32), ("coarsening_gradient", C.c_double),
     ]
 
 
@@ -86,7 +87,7 @@ def load_library(path: str = LIB_PATH):
     L.gg_default_lists.argtypes = [vp]
     L.gg_step.argtypes = [vp, C.POINTER(StepStats)]
     for s in ("gg_stage_convolution", "gg_stage_update_lists", "gg_stage_comparison", "gg_stage_level_set",
-              "gg_stage_redistancing", "gg_grain_count", "gg_loop"):
+              "gg_stage_redistancing", "gg_grain_count", "gg_loop", "gg_domain_size"):
         getattr(L, s).argtypes = [vp]
     L.gg_get_grain_stats.argtypes = [vp, vp, vp, vp, vp, vp]
     L.gg_get_neighbors.argtypes = [vp, i32, vp, i32]
@@ -178,7 +179,8 @@ class GrainHandler:
                  precision: int = PRECISION_FP64, list_capacity: int = 0, pool_voxels: int = 0,
                  device: int = 0, correction: bool = False, unique_energies: bool = True,
                  mobility_model: bool = False, stored_energy: bool = False, triple_line_drag: float = 0.0,
-                 hull_capacity: int = 0, keep_elements: bool = False):
+                 hull_capacity: int = 0, keep_elements: bool = False, grid_coarsening: bool = False,
+                 points_per_grain: int = 0, coarsening_gradient: float = 0.0):
         L = load_library()
         self.G = int(n_grains)
         self.N = int(domain_size)
@@ -187,10 +189,10 @@ class GrainHandler:
         self.precision = precision
         p = Params(domain_size, border, float(time_step), n_grains, precision, int(not correction), list_capacity,
                    pool_voxels, device, int(unique_energies), int(mobility_model), int(stored_energy),
-                   float(triple_line_drag), hull_capacity, int(keep_elements))
+                   float(triple_line_drag), hull_capacity, int(keep_elements), int(grid_coarsening),
+                   int(points_per_grain), float(coarsening_gradient))
         self._euler = np.zeros((self.G, 3))
         self._see = np.zeros(self.G)
-        self._h_grid = 1.0 / self.N
         h = C.c_void_p()
         self._lib = L  # held for close() at interpreter exit, when module globals are gone
         rc = L.gg_create(C.byref(p), C.byref(h))
@@ -267,6 +269,11 @@ class GrainHandler:
     def loop(self) -> int:
         return self._check(load_library().gg_loop(self._h))
 
+    @property
+    def domain_size(self) -> int:
+        """The current grid size N (grainhdl::realDomainSize; shrinks with grid coarsening)."""
+        return self._check(load_library().gg_domain_size(self._h))
+
     # --- read-back ---------------------------------------------------------
     def stats(self) -> GrainStats:
         G1 = self.G + 1
@@ -308,21 +315,23 @@ class GrainHandler:
         TEXTURE_DTYPE, one per existing grain in ascending ID order.  GBEnergy is the
         reference's m_energy, which no code path of it assigns (0)."""
         st = self.stats()
+        h_grid = 1.0 / self.domain_size
         ids = [g for g in range(1, self.G + 1) if st.exists[g]]
         out = np.zeros(len(ids), TEXTURE_DTYPE)
         for r, g in enumerate(ids):
             x0, x1, y0, y1, z0, z1 = (int(v) for v in st.boxes[g])
             phi1, PHI, phi2 = quaternion_to_euler(euler_to_quaternion(self._euler[g - 1]))
             out[r] = (st.volume[g], st.surface[g], 0.0, self._see[g - 1], phi1, PHI, phi2,
-                      ((x1 - x0) // 2 + x0) * self._h_grid, ((y1 - y0) // 2 + y0) * self._h_grid,
-                      ((z1 - z0) // 2 + z0) * self._h_grid, g, st.n_neighbors[g],
+                      ((x1 - x0) // 2 + x0) * h_grid, ((y1 - y0) // 2 + y0) * h_grid,
+                      ((z1 - z0) // 2 + z0) * h_grid, g, st.n_neighbors[g],
                       int(0 in set(self.neighbors(g).tolist())), 0)
         return out
 
     def voxel_container(self) -> np.ndarray:
         """The network as an (N, N, N) [z][y][x] array of grain IDs (the reference's
         Container_size_N_t_loop.raw)."""
-        out = np.zeros((self.N, self.N, self.N), np.uint32)
+        n = self.domain_size
+        out = np.zeros((n, n, n), np.uint32)
         self._check(load_library().gg_voxel_container(self._h, _p(out)))
         return out
 

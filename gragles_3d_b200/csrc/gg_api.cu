@@ -100,6 +100,12 @@ struct gg_ctx {
     int side_limit = 0;    // largest side the shared-memory kernels accept
     int list_cap = 4096, slab = 8;
     long long launches = 0;  // kernels launched by this context
+    // grid coarsening (grainhdl::gridCoarsement): ngrains at the last coarsening, and
+    // NumberOfPointsPerGrain
+    int coarse_ref = 0, points_per_grain = 0;
+    // element counts of the N-dependent tables' device buffers (reused when they fit)
+    size_t tw_cap = 0, gt_cap = 0, circ_cap = 0, bmat_cap = 0;
+    size_t tw_off_cap = 0, g_off_cap = 0, c_off_cap = 0, boff_cap = 0;
     cudaEvent_t ev[8] = {};  // stage boundaries (0-5), the comparison kernel (6, 7)
 };
 
@@ -171,6 +177,22 @@ HullPhysics physics(gg_ctx* ctx) {
     return h;
 }
 
+// Copies a host table into a device buffer, reallocating it only when it has grown.
+template <typename X>
+int put_table(gg_ctx* ctx, X** d, size_t* cap, const std::vector<X>& h) {
+    if (h.size() > *cap || !*d) {
+        if (*d) CK(cudaFree(*d));
+        *d = nullptr;
+        CK(dalloc(d, h.size()));
+        *cap = h.size() ? h.size() : 1;
+    }
+    if (!h.empty()) CK(cudaMemcpy(*d, h.data(), sizeof(X) * h.size(), cudaMemcpyHostToDevice));
+    return GG_OK;
+}
+
+// The tables of the current grid (N, M): DFT twiddles and the Gaussian multiplier per side,
+// and on the mixed path the circulant matrices.  Run at set-up and after a grid coarsening
+// (the Gaussian's dt N^2 is computed from the new N, grainhdl.cpp:1419-1442).
 int upload_tables(gg_ctx* ctx) {
     const int M = ctx->M;
     std::vector<double2> tw;
@@ -183,14 +205,11 @@ int upload_tables(gg_ctx* ctx) {
         g_off[n] = (long long)gt.size();
         gaussian_table(n, ctx->N, ctx->P.time_step, gt);
     }
-    CK(dalloc(&ctx->d_tw, tw.size()));
-    CK(dalloc(&ctx->d_tw_off, tw_off.size()));
-    CK(dalloc(&ctx->d_gtab, gt.size()));
-    CK(dalloc(&ctx->d_g_off, g_off.size()));
-    CK(cudaMemcpy(ctx->d_tw, tw.data(), tw.size() * sizeof(double2), cudaMemcpyHostToDevice));
-    CK(cudaMemcpy(ctx->d_tw_off, tw_off.data(), tw_off.size() * sizeof(long long), cudaMemcpyHostToDevice));
-    CK(cudaMemcpy(ctx->d_gtab, gt.data(), gt.size() * sizeof(double), cudaMemcpyHostToDevice));
-    CK(cudaMemcpy(ctx->d_g_off, g_off.data(), g_off.size() * sizeof(long long), cudaMemcpyHostToDevice));
+    int rc = put_table(ctx, &ctx->d_tw, &ctx->tw_cap, tw);
+    if (!rc) rc = put_table(ctx, &ctx->d_tw_off, &ctx->tw_off_cap, tw_off);
+    if (!rc) rc = put_table(ctx, &ctx->d_gtab, &ctx->gt_cap, gt);
+    if (!rc) rc = put_table(ctx, &ctx->d_g_off, &ctx->g_off_cap, g_off);
+    if (rc) return rc;
     if (!ctx->fp64) {
         std::vector<float> circ;
         std::vector<long long> c_off(M + 2, 0);
@@ -198,17 +217,14 @@ int upload_tables(gg_ctx* ctx) {
             c_off[n] = (long long)circ.size();
             circulant_matrix(n, ctx->N, ctx->P.time_step, circ);
         }
-        CK(dalloc(&ctx->d_circ, circ.size()));
-        CK(dalloc(&ctx->d_circ_off, c_off.size()));
-        CK(cudaMemcpy(ctx->d_circ, circ.data(), circ.size() * sizeof(float), cudaMemcpyHostToDevice));
-        CK(cudaMemcpy(ctx->d_circ_off, c_off.data(), c_off.size() * sizeof(long long), cudaMemcpyHostToDevice));
+        rc = put_table(ctx, &ctx->d_circ, &ctx->circ_cap, circ);
+        if (!rc) rc = put_table(ctx, &ctx->d_circ_off, &ctx->c_off_cap, c_off);
         std::vector<uint16_t> bmat;
         std::vector<long long> boff;
         umma_tables(ctx->N, ctx->P.time_step, std::min(M, kUmmaMaxSide), bmat, boff);
-        CK(dalloc(&ctx->d_bmat, bmat.size()));
-        CK(dalloc(&ctx->d_boff, boff.size()));
-        CK(cudaMemcpy(ctx->d_bmat, bmat.data(), bmat.size() * sizeof(uint16_t), cudaMemcpyHostToDevice));
-        CK(cudaMemcpy(ctx->d_boff, boff.data(), boff.size() * sizeof(long long), cudaMemcpyHostToDevice));
+        if (!rc) rc = put_table(ctx, &ctx->d_bmat, &ctx->bmat_cap, bmat);
+        if (!rc) rc = put_table(ctx, &ctx->d_boff, &ctx->boff_cap, boff);
+        if (rc) return rc;
     }
     return GG_OK;
 }
@@ -221,8 +237,7 @@ int check_err(gg_ctx* ctx, const char* where) {
     if (e & (ERR_LIST | ERR_HASH)) return fail(ctx, GG_ERR_LIST_OVERFLOW, "%s: comparison list capacity exceeded", where);
     if (e & ERR_NEIGHBORS) return fail(ctx, GG_ERR_LIST_OVERFLOW, "%s: hull neighbour capacity exceeded", where);
     if (e & ERR_BOX) return fail(ctx, GG_ERR_UNSUPPORTED, "%s: a box left the grid or exceeded the supported side", where);
-    if (e & ERR_TIMEOUT) return fail(ctx, GG_ERR_CUDA, "%s: a bounded tensor-core pipeline wait timed out", where);
-    if (e & ERR_BOUNDS) return fail(ctx, GG_ERR_CUDA, "%s: a kernel bounds check failed (access skipped)", where);
+    // a capacity overflow comes before the bounds checks it may trip further down the step
     if (e & ERR_HULL) {
         int d = 0;
         if (ctx->hull.diag) CK(cudaMemcpy(&d, ctx->hull.diag, sizeof(int), cudaMemcpyDeviceToHost));
@@ -236,6 +251,8 @@ int check_err(gg_ctx* ctx, const char* where) {
                                                      : "hull or interfacial-element capacity exceeded";
         return fail(ctx, GG_ERR_POOL_EXHAUSTED, "%s: %s (diag %d)", where, what, d);
     }
+    if (e & ERR_TIMEOUT) return fail(ctx, GG_ERR_CUDA, "%s: a bounded tensor-core pipeline wait timed out", where);
+    if (e & ERR_BOUNDS) return fail(ctx, GG_ERR_CUDA, "%s: a kernel bounds check failed (access skipped)", where);
     return GG_OK;
 }
 
@@ -345,7 +362,7 @@ int correct_convolution(gg_ctx* ctx) {
     CorrectionArgs<T> c{};
     c.G = ctx->G;
     c.geo = ctx->geo;
-    c.toff = ctx->d_toff_n;
+    c.toff = ctx->d_toff_one;
     c.present = ctx->d_present;
     c.box = ctx->d_box[p];
     c.in = reinterpret_cast<const T*>(ctx->d_arena[p]);
@@ -365,8 +382,17 @@ int correct_convolution(gg_ctx* ctx) {
 }
 
 template <typename T>
+int coarsen_t(gg_ctx* ctx, int new_size);
+int coarsening_size(const gg_ctx* ctx);
+
+template <typename T>
 int stage_convolution_t(gg_ctx* ctx) {
-    ctx->p ^= 1;  // switchDistancebuffer (gridCoarsement off), grainhdl.cpp:1496
+    // gridCoarsement (grainhdl.cpp:1446-1498): re-grid, or switchDistancebuffer (:1496)
+    if (const int new_size = coarsening_size(ctx)) {
+        const int rc = coarsen_t<T>(ctx, new_size);
+        if (rc) return rc;
+    }
+    ctx->p ^= 1;
     const int p = ctx->p;
     plan(ctx, ctx->d_box[p], 1, nullptr, sizeof(T) == 8 ? ctx->d_spec_off : nullptr, ctx->d_toff_n,
          ctx->d_toff_slab, ctx->d_toff_one, ctx->d_total_vox);
@@ -469,12 +495,18 @@ int ensure_bins(gg_ctx* ctx) {
     return GG_OK;
 }
 
+// executeComparison (+ executeSetComparison when set_comparison) of every grain: the
+// neighbours' fields in arena `in_a`, the result into arena `out_a`, IDLocal from arena
+// q into q ^ 1.  After a grid coarsening (set_comparison 0) every present grain's field
+// takes part as a neighbour: comparison lists may still name a grain whose hull vanished
+// in the last step, and the reference has re-gridded it too.
 template <typename T>
-int stage_comparison_t(gg_ctx* ctx) {
-    const int p = ctx->p, q = ctx->q;
+int compare_t(gg_ctx* ctx, int in_a, int out_a, int set_comparison) {
+    const int q = ctx->q;
     int rc = ensure_bins(ctx);
     if (rc) return rc;
-    launch_newbox_init(ctx->G, ctx->d_present, ctx->d_exists, ctx->d_box[p ^ 1], ctx->d_newbox, ctx->stream);
+    if (set_comparison)
+        launch_newbox_init(ctx->G, ctx->d_present, ctx->d_exists, ctx->d_box[out_a], ctx->d_newbox, ctx->stream);
     PosTableArgs pt{};
     pt.G = ctx->G;
     pt.toff = ctx->d_toff_one;
@@ -486,7 +518,8 @@ int stage_comparison_t(gg_ctx* ctx) {
     pt.err = ctx->d_err;
     launch_pos_tables(pt, ctx->grid, ctx->stream);
     ctx->launches += 1;
-    launch_bin(ctx->bins, ctx->G, ctx->d_exists, ctx->d_box[p], ctx->d_err, ctx->stream);
+    launch_bin(ctx->bins, ctx->G, set_comparison ? ctx->d_exists : ctx->d_present, ctx->d_box[in_a], ctx->d_err,
+               ctx->stream);
     ctx->launches += 4;
     CK(cudaMemcpyAsync(ctx->h_maxcount, ctx->bins.max_count, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
     CK(cudaStreamSynchronize(ctx->stream));
@@ -499,8 +532,8 @@ int stage_comparison_t(gg_ctx* ctx) {
     a.geo = ctx->geo;
     a.bins = ctx->bins;
     a.mcap = mcap;
-    a.in = arena<T>(ctx, p);
-    a.out = arena<T>(ctx, p ^ 1);
+    a.in = arena<T>(ctx, in_a);
+    a.out = arena<T>(ctx, out_a);
     a.id_old = ctx->d_idarena[q];
     a.idbox_old = ctx->d_idbox[q];
     a.idoff_old = ctx->d_idoff[q];
@@ -513,19 +546,30 @@ int stage_comparison_t(gg_ctx* ctx) {
     a.pos_cap = ctx->pos_cap;
     a.newbox = ctx->d_newbox;
     a.err = ctx->d_err;
-    cudaEventRecord(ctx->ev[6], ctx->stream);
+    a.set_comparison = set_comparison;
+    a.exists = ctx->d_exists;
+    if (set_comparison) cudaEventRecord(ctx->ev[6], ctx->stream);
     launch_compare<T>(a, ctx->num_sms * 4, ctx->stream);
-    cudaEventRecord(ctx->ev[7], ctx->stream);
+    if (set_comparison) cudaEventRecord(ctx->ev[7], ctx->stream);
     ctx->launches += 1;
     CK(cudaGetLastError());
     ctx->q ^= 1;
-    ctx->p ^= 1;  // switchDistancebuffer, grainhdl.cpp:865
     return GG_OK;
 }
 
 template <typename T>
-int stage_level_set_t(gg_ctx* ctx) {
-    const int p = ctx->p;
+int stage_comparison_t(gg_ctx* ctx) {
+    const int rc = compare_t<T>(ctx, ctx->p, ctx->p ^ 1, 1);
+    if (rc) return rc;
+    ctx->p ^= 1;  // switchDistancebuffer, grainhdl.cpp:865
+    return GG_OK;
+}
+
+// extractContour of every present grain on the field in arena p (the new box of the
+// grains that exist goes to arena p ^ 1), then computeSurfaceElements.  regrid: the
+// extractContour that follows a grid coarsening (see MCArgs).
+template <typename T>
+int level_set_t(gg_ctx* ctx, int p, int regrid) {
     plan(ctx, ctx->d_box[p], 0, nullptr, nullptr, nullptr, nullptr, ctx->d_toff_mc);
     MCArgs<T> a{};
     a.G = ctx->G;
@@ -544,6 +588,7 @@ int stage_level_set_t(gg_ctx* ctx) {
     a.n_nb = ctx->d_nnb;
     a.nb_cap = kNbCap;
     a.err = ctx->d_err;
+    a.regrid = regrid;
     if (ctx->elements) a.hull = ctx->hull;
     launch_mc<T>(a, ctx->grid, ctx->side_max, ctx->stream);
     ctx->launches += 1;
@@ -564,6 +609,96 @@ int stage_level_set_t(gg_ctx* ctx) {
         CK(cudaGetLastError());
     }
     return GG_OK;
+}
+
+template <typename T>
+int stage_level_set_t(gg_ctx* ctx) {
+    return level_set_t<T>(ctx, ctx->p, 0);
+}
+
+// grainhdl::gridCoarsement (grainhdl.cpp:1446-1498) when it re-grids: the geometry and
+// time variables of the new size (updateGridAndTimeVariables, grainhdl.cpp:1419-1443) and
+// their tables, LSbox::resizeGrid of every present grain (box.cpp:2595-2694), then
+// recalculateIDLocal (box.cpp:2697-2700) and extractContour of every present grain.
+// The last redistancing's result (arena p ^ 1, the reference's m_outputDistance) is
+// re-sampled into arena p, which the convolution then reads without the usual
+// switchDistancebuffer: p is left pointing at the other arena so that the convolution
+// stage's switch lands on the re-sampled field.
+template <typename T>
+int coarsen_t(gg_ctx* ctx, int new_size) {
+    const int src = ctx->p ^ 1, dst = ctx->p;
+    const double h_old = ctx->geo.h;
+    ctx->N = new_size;
+    ctx->M = ctx->N + 2 * ctx->gb;
+    ctx->geo = Geometry{ctx->N, ctx->gb, ctx->M, 1 / (double)ctx->N, ctx->gb / double(ctx->N), ctx->P.time_step};
+    int rc = upload_tables(ctx);
+    if (rc) return rc;
+    ctx->bins.ntx = (ctx->M + kTX - 1) / kTX;  // fewer tiles than the arrays hold
+    ctx->bins.nty = (ctx->M + kTY - 1) / kTY;
+    ctx->bins.ntz = (ctx->M + kTZ - 1) / kTZ;
+    RegridBoxArgs rb{};
+    rb.G = ctx->G;
+    rb.present = ctx->d_present;
+    rb.old_box = ctx->d_box[src];
+    rb.scaled = ctx->d_newbox;
+    rb.new_box = ctx->d_box[dst];
+    rb.ratio = h_old / ctx->geo.h;  // h / hn of resizeGrid
+    rb.gb = ctx->gb;
+    rb.M_new = ctx->M;
+    rb.err = ctx->d_err;
+    launch_regrid_boxes(rb, ctx->stream);
+    ctx->launches += 1;
+    plan(ctx, ctx->d_box[dst], 0, ctx->d_off[dst], nullptr, ctx->d_toff_n, nullptr, nullptr);
+    rc = check_err(ctx, "grid coarsening");
+    if (rc) return rc;
+    ResampleArgs<T> rs{};
+    rs.G = ctx->G;
+    rs.toff = ctx->d_toff_n;
+    rs.src = Arena<const T>{reinterpret_cast<const T*>(ctx->d_arena[src]), ctx->d_box[src], ctx->d_off[src]};
+    rs.dst = arena<T>(ctx, dst);
+    rs.ratio_inv = ctx->geo.h / h_old;  // hn / h
+    rs.gb = ctx->gb;
+    rs.delta_new = ctx->geo.delta;
+    launch_resample<T>(rs, ctx->grid, ctx->stream);
+    ctx->launches += 1;
+    CK(cudaGetLastError());
+    // m_outputDistance->resize(the input's box); IDLocal follows it (resizeIDLocalToDistanceBuffer)
+    launch_copy_layout(ctx->G, ctx->d_present, ctx->d_box[dst], ctx->d_off[dst], ctx->d_box[src], ctx->d_off[src],
+                       ctx->stream);
+    launch_copy_layout(ctx->G, ctx->d_present, ctx->d_box[dst], ctx->d_off[dst], ctx->d_idbox[ctx->q ^ 1],
+                       ctx->d_idoff[ctx->q ^ 1], ctx->stream);
+    IdResizeArgs ir{};
+    ir.G = ctx->G;
+    ir.present = ctx->d_present;
+    ir.exists = ctx->d_exists;
+    ir.id_old = ctx->d_idarena[ctx->q];
+    ir.idbox_old = ctx->d_idbox[ctx->q];
+    ir.idoff_old = ctx->d_idoff[ctx->q];
+    ir.id_new = ctx->d_idarena[ctx->q ^ 1];
+    ir.idbox_new = ctx->d_idbox[ctx->q ^ 1];
+    ir.idoff_new = ctx->d_idoff[ctx->q ^ 1];
+    launch_id_resize(ir, ctx->grid, ctx->stream);
+    ctx->launches += 3;
+    CK(cudaGetLastError());
+    ctx->coarse_ref = ctx->grain_count;  // ngrains = currentNrGrains
+    rc = compare_t<T>(ctx, dst, src, 0);
+    if (rc) return rc;
+    rc = level_set_t<T>(ctx, dst, 1);
+    if (rc) return rc;
+    ctx->p = src;
+    return check_err(ctx, "grid coarsening");
+}
+
+// The size gridCoarsement would re-grid to now, or 0 when it keeps the grid
+// (grainhdl.cpp:1447-1451).
+int coarsening_size(const gg_ctx* ctx) {
+    if (!ctx->P.grid_coarsening || ctx->loop == 0) return 0;
+    const int cur = ctx->grain_count;  // currentNrGrains: countGrains of the last loop
+    const int new_size = (int)(std::pow((double)cur, 1 / 3.0) * std::pow(kPi * 4 / 3, 1. / 3) / 2 *
+                               ctx->points_per_grain);
+    const double gradient = ctx->P.coarsening_gradient > 0 ? ctx->P.coarsening_gradient : 0.95;
+    if ((double)cur / (double)ctx->coarse_ref < gradient && new_size < ctx->N) return new_size;
+    return 0;
 }
 
 template <typename T>
@@ -657,23 +792,8 @@ Box initial_box(const int32_t* e, int gb, int M) {
     if (ymin < 0) ymin = 0;
     if (xmin < 0) xmin = 0;
     if (zmin < 0) zmin = 0;
-    Box b{xmin, xmax, ymin, ymax, zmin, zmax};
     // DimensionalBuffer::resizeToCube, dimensionalBuffer.h:139-219
-    const int grid_size = M - 1;
-    const unsigned height = b.y1 - b.y0, width = b.x1 - b.x0, depth = b.z1 - b.z0;
-    if (width == height && width == depth) return b;
-    int ref = width > height ? (int)width : (int)height;
-    if (ref < (int)depth) ref = (int)depth;
-    if (ref > (int)width) { const int d = ref - (int)width; b.x0 -= d / 2; b.x1 += d / 2 + d % 2; }
-    if (ref > (int)height) { const int d = ref - (int)height; b.y0 -= d / 2; b.y1 += d / 2 + d % 2; }
-    if (ref > (int)depth) { const int d = ref - (int)depth; b.z0 -= d / 2; b.z1 += d / 2 + d % 2; }
-    if (b.x0 < 0) { const int d = -b.x0; b.x1 += d; b.x0 += d; }
-    else if (b.x1 > grid_size) { const int d = grid_size - b.x1; b.x1 += d; b.x0 += d; }
-    if (b.y0 < 0) { const int d = -b.y0; b.y1 += d; b.y0 += d; }
-    else if (b.y1 > grid_size) { const int d = grid_size - b.y1; b.y1 += d; b.y0 += d; }
-    if (b.z0 < 0) { const int d = -b.z0; b.z1 += d; b.z0 += d; }
-    else if (b.z1 > grid_size) { const int d = grid_size - b.z1; b.z1 += d; b.z0 += d; }
-    return b;
+    return resize_to_cube(Box{xmin, xmax, ymin, ymax, zmin, zmax}, M);
 }
 
 int supported_side(bool fp64) {
@@ -696,7 +816,7 @@ void free_all(gg_ctx* c) {
                     c->d_idoff[0], c->d_idoff[1], c->d_spec, c->d_spec_off, c->d_toff_n, c->d_toff_slab,
                     c->d_toff_one, c->d_toff_mc, c->d_toff_red, c->d_tw, c->d_tw_off, c->d_gtab, c->d_g_off,
                     c->d_circ, c->d_circ_off, c->d_bmat, c->d_boff, c->d_cscr, c->d_elscr, c->d_quat, c->d_see,
-                    c->hull.rec_list, c->hull.rec_ntri, c->hull.bary, c->hull.tarea, c->hull.diag, c->el.earea, c->hull.n_rec, c->hull.n_tri, c->el.n_elem,
+                    c->hull.rec_list, c->hull.rec_ntri, c->hull.bary, c->hull.tarea, c->hull.diag, c->el.earea, c->el.ebf, c->el.eidx, c->el.n_flat, c->el.eorg, c->hull.n_rec, c->hull.n_tri, c->el.n_elem,
                     c->el.elem, c->el.ids, c->el.segs, c->el.ebary, c->el.chunks, c->el.n_idx, c->el.idx_key, c->el.idx_rng,
                     c->el.idx_elem, c->d_err, c->d_total_vox, c->d_count3, c->bins.count,
                     c->bins.off, c->bins.cursor, c->bins.entries, c->bins.max_count};
@@ -746,6 +866,10 @@ int gg_create(const gg_params* params, gg_ctx** out) {
     ctx->correction = !P.disable_correction;
     ctx->elements = ctx->correction || P.keep_elements;
     ctx->side_limit = supported_side(ctx->fp64);
+    // NumberOfPointsPerGrain as the mode-4 reader sets it (grainhdl.cpp:221); ngrains
+    ctx->points_per_grain = P.points_per_grain > 0 ? P.points_per_grain
+                                                   : (int)(ctx->N / std::pow(ctx->G, 1 / 3.0) + 0.5);
+    ctx->coarse_ref = ctx->G;
     *out = ctx;
 #undef CK_RET
     cudaError_t e = cudaSetDevice(P.device);
@@ -884,6 +1008,12 @@ int gg_load_state(gg_ctx* ctx, const uint32_t* labels, const int32_t* extents, c
         CK(dalloc(&ctx->el.segs, (size_t)ctx->el.seg_cap * G1h));
         CK(dalloc(&ctx->el.ebary, 3 * cap * G1h));
         CK(dalloc(&ctx->el.earea, cap * G1h));
+        CK(dalloc(&ctx->el.ebf, cap * G1h));
+        CK(dalloc(&ctx->el.eidx, cap * G1h));
+        CK(dalloc(&ctx->el.n_flat, G1h));
+        CK(cudaMemset(ctx->el.n_flat, 0, sizeof(int) * G1h));
+        CK(dalloc(&ctx->el.eorg, G1h));
+        CK(cudaMemset(ctx->el.eorg, 0, sizeof(float4) * G1h));
         ctx->el.chunk_cap = (int)(cap / kHullChunk) + ctx->el.seg_cap;
         ctx->el.idx_cap = 256;
         ctx->el.pair_cap = 2048;
@@ -1065,6 +1195,7 @@ int64_t gg_get_idlocal(gg_ctx* ctx, int32_t id, int32_t box[6], uint32_t* out, i
 }
 
 int gg_grain_count(gg_ctx* ctx) { return ctx ? ctx->grain_count : GG_ERR_INVALID; }
+int gg_domain_size(gg_ctx* ctx) { return ctx ? ctx->N : GG_ERR_INVALID; }
 int gg_loop(gg_ctx* ctx) { return ctx ? ctx->loop : GG_ERR_INVALID; }
 
 int gg_voxel_container(gg_ctx* ctx, uint32_t* labels) {

@@ -148,6 +148,25 @@ inline cudaError_t allow_max_dynamic_smem(K* kernel) {
     return cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, optin - (int)fa.sharedSizeBytes);
 }
 
+// DimensionalBuffer::resizeToCube, dimensionalBuffer.h:139-219
+__host__ __device__ inline Box resize_to_cube(Box b, int maximumLength) {
+    const int grid_size = maximumLength - 1;
+    const unsigned height = b.y1 - b.y0, width = b.x1 - b.x0, depth = b.z1 - b.z0;
+    if (width == height && width == depth) return b;
+    int ref = width > height ? (int)width : (int)height;
+    if (ref < (int)depth) ref = (int)depth;
+    if (ref > (int)width) { const int d = ref - (int)width; b.x0 -= d / 2; b.x1 += d / 2 + d % 2; }
+    if (ref > (int)height) { const int d = ref - (int)height; b.y0 -= d / 2; b.y1 += d / 2 + d % 2; }
+    if (ref > (int)depth) { const int d = ref - (int)depth; b.z0 -= d / 2; b.z1 += d / 2 + d % 2; }
+    if (b.x0 < 0) { const int d = -b.x0; b.x1 += d; b.x0 += d; }
+    else if (b.x1 > grid_size) { const int d = grid_size - b.x1; b.x1 += d; b.x0 += d; }
+    if (b.y0 < 0) { const int d = -b.y0; b.y1 += d; b.y0 += d; }
+    else if (b.y1 > grid_size) { const int d = grid_size - b.y1; b.y1 += d; b.y0 += d; }
+    if (b.z0 < 0) { const int d = -b.z0; b.z1 += d; b.z0 += d; }
+    else if (b.z1 > grid_size) { const int d = grid_size - b.z1; b.z1 += d; b.z0 += d; }
+    return b;
+}
+
 // Runs a set-up action once per CUDA device, on the device current at the call.
 // Kernel attributes such as the dynamic shared-memory opt-in belong to the
 // device (context) they were set on, so a process that drives a second device

@@ -483,7 +483,9 @@ __global__ void __launch_bounds__(kThreads, 4) compare_kernel(CompareArgs<T> a) 
             const T in = s.val[ea * kVS + v];
             const int x = X0 + v % kTX, y = Y0 + (v / kTX) % kTY, z = Z0 + v / (kTX * kTY);
             bool positive = false;
-            if (in != NEG) {  // else the voxel is outside this grain's box
+            // else the voxel is outside this grain's box, or (recalculateIDLocal) the grain
+            // does not exist and executeComparison leaves it alone
+            if (in != NEG && (a.set_comparison || a.exists[s.id[ea]])) {
             // the first listed neighbour among the largest values, ties to the earliest position
             int best = -1;
             unsigned short bpos = kNotListed;
@@ -548,11 +550,12 @@ __global__ void __launch_bounds__(kThreads, 4) compare_kernel(CompareArgs<T> a) 
                     }
             }
             T res;
-            if ((double)fabs(in) < lim) res = T(0.5) * (in - cmpv);
+            if (!a.set_comparison) res = cmpv;
+            else if ((double)fabs(in) < lim) res = T(0.5) * (in - cmpv);
             else res = in;
             a.out.data[s.outoff[ea] + f] = res;
             a.id_new[s.idoff[ea] + f] = idv;
-            positive = res >= 0;
+            positive = a.set_comparison && res >= 0;
             }
             // new bounding box (executeSetComparison, box.cpp:858-877), reduced over the warp
             // first: its 32 lanes hold the same entry (kTV and blockDim are multiples of 64)

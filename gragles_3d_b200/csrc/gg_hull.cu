@@ -15,13 +15,19 @@
 //     as the reference does (including its ID-list quirks), and writes the elements in
 //     search order with their barycenter segments, bounding boxes and an ID -> elements
 //     index.
-//   correction_kernel: a CTA per (grain, z-slice); the voxels with |input| < delta are
-//     grouped by IDLocal neighbour, and a warp takes 32 voxels of one neighbour at a
-//     time.  It scans only the elements whose searched IDs hold that neighbour (from the
-//     index), skipping an element or a chunk of 16 barycenters when the distance to its
-//     bounding box cannot beat any lane's best (an exact bound: no barycenter inside can
-//     win under the strict <).  The energies use CUDA's acos/log/exp/pow: within a few
-//     ULP of the reference's libm, not bit-identical.
+//   correction_kernel: a CTA per grain, with the grain's element index, element boxes
+//     and FP32 barycenters staged in shared memory; slice by slice, the voxels with
+//     |input| < delta are grouped by IDLocal neighbour, and a warp takes 32 voxels of
+//     one neighbour at a time.  The winner of the reference's search is the least (distance, element
+//     index) over the barycenters of the elements holding that neighbour.  The warp
+//     finds it with an FP32 filter -- per barycenter p, q = |p'|^2 - 2 v'.p' (three FMAs
+//     on coordinates relative to an integer origin), minimised per element -- that
+//     proves the winning element whenever the best and second-best elements are more
+//     than twice the filter's error bound apart; otherwise (a near tie) the barycenters
+//     within the band are re-measured with the reference's FP64 distance in the
+//     reference's order.  The result is the reference's element, bit for bit.  The
+//     energies use CUDA's acos/log/exp/pow: within a few ULP of the reference's libm,
+//     not bit-identical.
 #include "gg_kernels.cuh"
 
 namespace gg {
@@ -418,7 +424,8 @@ __global__ void __launch_bounds__(32) elements_kernel(ElementArgs a) {
         __syncwarp();
         for (int k = lane; k < nl; k += 32) S.off[k] = S.cnt[k];
         __syncwarp();
-        if (warp_scan_excl(S.off, nl) > a.el.bary_cap && lane == 0) { atomicOr(a.err, ERR_HULL); atomicOr(a.cap.diag, HULL_TRIANGLES); }
+        const int nbary = warp_scan_excl(S.off, nl);
+        if (nbary > a.el.bary_cap && lane == 0) { atomicOr(a.err, ERR_HULL); atomicOr(a.cap.diag, HULL_TRIANGLES); }
         // 3. barycenters grouped by list, in triangle order (subDivideTrianglesToInterfacialElements):
         //    a record's triangles go after those of the earlier records of its list.  The
         //    warp first places its 32 records, then copies their triangles together.
@@ -633,7 +640,7 @@ __global__ void __launch_bounds__(32) elements_kernel(ElementArgs a) {
             uint32_t* ids = a.el.ids + (long long)g * a.el.id_cap;
             int2* segs = a.el.segs + (long long)g * a.el.seg_cap;
             HullChunk* chunks = a.el.chunks + (long long)g * a.el.chunk_cap;
-            int ne = 0, ni = 0, ns = 0, nch = 0, nd = 0, np = 0;
+            int ne = 0, ni = 0, ns = 0, nch = 0, nd = 0, np = 0, pb = 0;
             bool over = false, over_index = false;
             // IDs from junction j's segment chain (j >= 0), else the nid IDs of id_src
             auto emit = [&](int type, const uint32_t* id_src, int j, int nid, int head, bool chained, double en,
@@ -650,7 +657,7 @@ __global__ void __launch_bounds__(32) elements_kernel(ElementArgs a) {
                     if (ni != id_off + nid) atomicOr(a.err, ERR_BOUNDS);
                     nid = ni - id_off;
                 }
-                int nseg = 0, nchunk = 0;
+                int nseg = 0, nchunk = 0, pcnt = 0;
                 for (int k = head; k >= 0; k = chained ? S.next_key[k] : -1) {
                     if (ns >= a.el.seg_cap) { over = true; break; }
                     if (k >= kLMax || S.off[k] < 0 || S.off[k] + S.cnt[k] > a.el.bary_cap) {
@@ -660,6 +667,7 @@ __global__ void __launch_bounds__(32) elements_kernel(ElementArgs a) {
                     const int off = S.off[k], cnt = S.cnt[k];
                     segs[ns++] = make_int2(off, cnt);
                     nseg++;
+                    pcnt += cnt;
                     for (int c0 = 0; c0 < cnt; c0 += kHullChunk) {
                         if (nch >= a.el.chunk_cap) { over = true; break; }
                         chunks[nch].start = off + c0;
@@ -679,6 +687,13 @@ __global__ void __launch_bounds__(32) elements_kernel(ElementArgs a) {
                 e.energy = en;
                 e.mobility = mo;
                 e.area = 0.0;
+                if (pb + pcnt > a.el.bary_cap) {  // every barycenter belongs to one element
+                    over = true;
+                    pcnt = 0;
+                }
+                e.pbase = pb;
+                e.pcount = pcnt;
+                pb += pcnt;
                 // the IDs projectPointToGrainBoundary compares: all for a high-order
                 // junction, else the first 3 (QJ), 2 (TL), 1 (GB); each element once per ID
                 const int nc = type == 4 ? nid : min(nid, type);
@@ -748,6 +763,7 @@ __global__ void __launch_bounds__(32) elements_kernel(ElementArgs a) {
             if (over) { atomicOr(a.err, ERR_HULL); atomicOr(a.cap.diag, over_index ? HULL_INDEX : HULL_TABLE); }
             a.el.n_elem[g] = ne;
             a.el.n_idx[g] = nd;
+            a.el.n_flat[g] = pb;
             S.ne = ne;
             S.nch = nch;
             S.nd = nd;
@@ -807,6 +823,53 @@ __global__ void __launch_bounds__(32) elements_kernel(ElementArgs a) {
                     el.hi[q] = hi[q];
                 }
             }
+            // the correction's FP32 barycenters, relative to the integer centre of the
+            // elements' boxes (the lane wrote those boxes itself above)
+            double ulo[3] = {1e300, 1e300, 1e300}, uhi[3] = {-1e300, -1e300, -1e300};
+            for (int e = lane; e < ne; e += 32)
+#pragma unroll
+                for (int q = 0; q < 3; q++) {
+                    ulo[q] = fmin(ulo[q], E[e].lo[q]);
+                    uhi[q] = fmax(uhi[q], E[e].hi[q]);
+                }
+#pragma unroll
+            for (int q = 0; q < 3; q++)
+#pragma unroll
+                for (int o = 16; o > 0; o >>= 1) {
+                    ulo[q] = fmin(ulo[q], __shfl_xor_sync(kFull, ulo[q], o));
+                    uhi[q] = fmax(uhi[q], __shfl_xor_sync(kFull, uhi[q], o));
+                }
+            double org[3] = {0, 0, 0};
+            if (ne > 0 && uhi[0] >= ulo[0])
+#pragma unroll
+                for (int q = 0; q < 3; q++) org[q] = floor(0.5 * (ulo[q] + uhi[q]));
+            (void)nbary;
+            float4* pf = a.el.ebf + (long long)g * a.el.bary_cap;
+            int* pidx = a.el.eidx + (long long)g * a.el.bary_cap;
+            const int2* gsegs = a.el.segs + (long long)g * a.el.seg_cap;
+            float r2 = 0.f;
+            for (int e = 0; e < ne; e++) {  // element by element, its segments in order
+                const HullElem& el = E[e];
+                int dst = el.pbase;
+                for (int sgi = 0; sgi < el.nseg; sgi++) {
+                    const int2 sg = gsegs[el.seg_off + sgi];
+                    if (sg.x < 0 || sg.y < 0 || sg.x + sg.y > a.el.bary_cap || dst + sg.y > el.pbase + el.pcount)
+                        break;
+                    for (int i = lane; i < sg.y; i += 32) {
+                        const long long src = sg.x + i;
+                        const double dx = eb[3 * src] - org[0], dy = eb[3 * src + 1] - org[1],
+                                     dz = eb[3 * src + 2] - org[2];
+                        const double w = dx * dx + dy * dy + dz * dz;
+                        pf[dst + i] = make_float4((float)dx, (float)dy, (float)dz, (float)w);
+                        pidx[dst + i] = (int)src;
+                        r2 = fmaxf(r2, (float)w);
+                    }
+                    dst += sg.y;
+                }
+            }
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1) r2 = fmaxf(r2, __shfl_xor_sync(kFull, r2, o));
+            if (lane == 0) a.el.eorg[g] = make_float4((float)org[0], (float)org[1], (float)org[2], r2);
         }
         __syncwarp();
     }
@@ -824,66 +887,123 @@ __device__ __forceinline__ double sqdist3(double x, double y, double z, const do
     return d0 * d0 + (d1 * d1 + d2 * d2);
 }
 
-// Can a barycenter inside [lo, hi], in element e, beat the best (distance, element)
-// so far?  The distance to the clamped point is computed like the barycenter
-// distances, and rounding is monotone, so no barycenter in the box has a computed
-// distance below it.
-__device__ __forceinline__ bool may_beat(double x, double y, double z, const double* lo, const double* hi,
-                                         double best, int e, int win) {
-    const double c[3] = {x < lo[0] ? lo[0] : (x > hi[0] ? hi[0] : x), y < lo[1] ? lo[1] : (y > hi[1] ? hi[1] : y),
-                         z < lo[2] ? lo[2] : (z > hi[2] ? hi[2] : z)};
-    const double lb = sqdist3(x, y, z, c);
-    return lb < best || (lb == best && e < win);
+constexpr int kCThreads = 256;
+constexpr int kCVox = 2048;           // voxels of one pass over a slice (whole rows)
+constexpr unsigned short kNoD = 0xFFFF;
+constexpr float kInf = 3.0e38f;
+constexpr int kSPts = 2048;           // barycenters staged in shared memory (more: read from HBM)
+constexpr int kSElem = 512;           // the element table's capacity per grain
+constexpr int kSPairs = 2048;         // the index's (element, ID) pair capacity per grain
+
+// One grain's search data, staged once per grain, and the slice pass's voxel groups.
+struct CorrSmem {
+    float4 pts[kSPts];            // FP32 barycenters, element by element (ebf)
+    float box[kSElem][6];         // element boxes relative to the origin, rounded outward
+    int2 rng[kSElem];             // element e's barycenters in pts: (first, count)
+    unsigned short pairs[kSPairs];// the index's element lists (search order per ID)
+    uint32_t hkey[kCHash];        // neighbour ID -> dense index d
+    unsigned short hden[kCHash];
+    int2 drng[kIdxMax];           // dense index d -> its elements in pairs
+    int dcnt[kIdxMax], doff[kIdxMax], dcur[kIdxMax], dpk[kIdxMax + 1];
+    unsigned short vd[kCVox];     // dense neighbour index of the pass's voxels, kNoD: no search
+    unsigned short vlist[kCVox];  // pass voxels grouped by neighbour
+};
+
+// q of barycenter p for the voxel whose relative coordinates give (ax, ay, az) = -2 v':
+// |p'|^2 - 2 v'.p' = |v' - p'|^2 - |v'|^2.
+__device__ __forceinline__ float qval(const float4 p, float ax, float ay, float az) {
+    return fmaf(az, p.z, fmaf(ay, p.y, fmaf(ax, p.x, p.w)));
 }
 
-constexpr int kCThreads = 256;
-constexpr int kCVox = 4096;           // voxels of one pass over a slice (whole rows)
-constexpr unsigned short kNoD = 0xFFFF;
+// The least q over n consecutive barycenters.
+__device__ __forceinline__ float run_min(const float4* p, int n, float ax, float ay, float az) {
+    float m0 = kInf, m1 = kInf;
+    int i = 0;
+    for (; i + 4 <= n; i += 4) {
+        const float4 a = p[i], b = p[i + 1], c = p[i + 2], d = p[i + 3];
+        m0 = fminf(m0, qval(a, ax, ay, az));
+        m1 = fminf(m1, qval(b, ax, ay, az));
+        m0 = fminf(m0, qval(c, ax, ay, az));
+        m1 = fminf(m1, qval(d, ax, ay, az));
+    }
+    for (; i < n; i++) m0 = fminf(m0, qval(p[i], ax, ay, az));
+    return fminf(m0, m1);
+}
 
-// projectPointToGrainBoundary (grainHull.cpp:570-660) searches the elements holding id
-// in order and keeps a barycenter only when strictly nearer than every earlier one: the
-// winner is the least (distance, element index) over all candidates, whatever order
-// they are visited in.  A warp searches for 32 voxels with the same IDLocal neighbour
-// at once (a packet): the candidate elements and chunks are the same for all, a box is
-// skipped when no lane's voxel can beat its best through it, and every barycenter load
-// is a broadcast.  (best, win, wb) comes in as any candidate already known, or (1e7,
-// -1, -1), and leaves as the winner and its barycenter.
-__device__ __forceinline__ void project_packet(const HullElem* __restrict__ elem,
-                                               const HullChunk* __restrict__ chunks, const double* __restrict__ eb,
-                                               const unsigned short* __restrict__ pairs, int2 rng, bool active,
-                                               double x, double y, double z, const HullElements& el, int ne,
-                                               double& best, int& win, int& wb, int* err) {
-    for (int c = 0; c < rng.y; c++) {
-        const int e = pairs[rng.x + c];
+// The near-tie case: the barycenters whose q is within the band, measured with the
+// reference's FP64 distance (Vector3d::squaredNorm, c0 + (c1 + c2)) and kept only when
+// strictly nearer, visiting elements in search order and each element's barycenters in
+// order, as projectPointToGrainBoundary does (grainHull.cpp:570-660).  Every barycenter
+// that can be the reference's winner has q <= best + eps2, so the subset has the same
+// winner.
+__device__ int exact_winner(const CorrSmem& S, const float4* pts, int first, int count, int ne,
+                            const int* __restrict__ eidx, const double* __restrict__ eb, double x, double y, double z,
+                            float ax, float ay, float az, float limit) {
+    double bd = 10000000.0;
+    int bw = -1;
+    for (int c = 0; c < count; c++) {
+        const int e = S.pairs[first + c];
+        if (e >= ne) continue;
+        const int2 r = S.rng[e];
+        for (int i = r.x; i < r.x + r.y; i++) {
+            if (qval(pts[i], ax, ay, az) > limit) continue;
+            const double d = sqdist3(x, y, z, eb + 3 * (long long)eidx[i]);
+            if (d < bd) {
+                bd = d;
+                bw = e;
+            }
+        }
+    }
+    return bw;
+}
+
+// The element whose (energy, mobility) the voxel (i, j, k) takes: the reference's
+// winner among the elements S.pairs[first, first + count) (-1: none, weight (1, 1)).
+// All lanes of the warp call it with the same elements (a packet of one neighbour).
+// Each element's least q is compared with the best and second-best so far; when the
+// best element beats every other by more than eps2 (twice the filter's error bound) it
+// is the reference's winner, else the near tie is settled in FP64 (exact_winner).
+// Elements are taken in reverse search order, so the grain boundary (last in search
+// order, and the usual winner) sets a tight best first, and an element is skipped when
+// no lane's voxel can come within the band of its best through the element's box.
+__device__ __forceinline__ int search_packet(const CorrSmem& S, const float4* pts, int first, int count, bool active,
+                                             int i, int j, int k, float4 org, float eps2, int ne,
+                                             const int* __restrict__ eidx, const double* __restrict__ eb, int* err) {
+    const float vx = (float)i - org.x, vy = (float)j - org.y, vz = (float)k - org.z;  // exact
+    const float ax = -2.f * vx, ay = -2.f * vy, az = -2.f * vz;
+    const float vv = vx * vx + vy * vy + vz * vz;  // exact (integers below 2^24)
+    float best = kInf, second = kInf;
+    int beste = -1;
+    for (int c = count - 1; c >= 0; c--) {
+        const int e = S.pairs[first + c];
         if (e >= ne) {
             if ((threadIdx.x & 31) == 0) atomicOr(err, ERR_BOUNDS);
             continue;
         }
-        const HullElem& E = elem[e];
-        if (!__any_sync(kFull, active && may_beat(x, y, z, E.lo, E.hi, best, e, win))) continue;
-        const int c0 = E.chunk_off, c1 = E.chunk_off + E.nchunk;
-        if (c0 < 0 || c1 > el.chunk_cap) {
-            if ((threadIdx.x & 31) == 0) atomicOr(err, ERR_BOUNDS);
-            continue;
+        {   // lower bound of q over the element's box: |v' - box|^2 (FP32, scaled down past its
+            // rounding) - |v'|^2 - eps; the box was rounded outward.  best = kInf never skips.
+            const float* bx = S.box[e];
+            const float dx = vx < bx[0] ? bx[0] - vx : (vx > bx[3] ? vx - bx[3] : 0.f);
+            const float dy = vy < bx[1] ? bx[1] - vy : (vy > bx[4] ? vy - bx[4] : 0.f);
+            const float dz = vz < bx[2] ? bx[2] - vz : (vz > bx[5] ? vz - bx[5] : 0.f);
+            const float d2 = fmaf(dz, dz, fmaf(dy, dy, dx * dx));
+            const float lb = d2 * (1.f - 1.0f / 1048576.f) - vv - 0.5f * eps2;
+            if (!__any_sync(kFull, active && lb <= best + eps2)) continue;
         }
-        for (int ch = c0; ch < c1; ch++) {
-            const HullChunk& C = chunks[ch];
-            if (!__any_sync(kFull, active && may_beat(x, y, z, C.lo, C.hi, best, e, win))) continue;
-            if (C.start < 0 || C.count < 0 || C.start + C.count > el.bary_cap) {
-                if ((threadIdx.x & 31) == 0) atomicOr(err, ERR_BOUNDS);
-                continue;
-            }
-            const double* b = eb + 3 * (long long)C.start;
-            for (int i = 0; i < C.count; i++) {
-                const double d = sqdist3(x, y, z, b + 3 * i);
-                if (d < best || (d == best && e < win)) {
-                    best = d;
-                    win = e;
-                    wb = C.start + i;
-                }
-            }
+        const int2 r = S.rng[e];
+        const float m = run_min(pts + r.x, r.y, ax, ay, az);
+        if (m < best) {
+            second = best;
+            best = m;
+            beste = e;
+        } else {
+            second = fminf(second, m);
         }
     }
+    if (beste < 0) return -1;
+    if (second - best > eps2) return beste;  // proven: every other element is farther
+    return exact_winner(S, pts, first, count, ne, eidx, eb, (double)i, (double)j, (double)k, ax, ay, az,
+                        best + eps2);
 }
 
 // The update of one band voxel, box.cpp:476-533, given the element that won (-1: none).
@@ -903,77 +1023,99 @@ __device__ __forceinline__ void correct_voxel(const CorrectionArgs<T>& a, const 
     *outp = (T)o;
 }
 
-// A CTA per (grain, z-slice): the band voxels of a pass (whole rows, <= kCVox voxels)
-// are grouped by IDLocal neighbour (counting sort in shared memory), then the warps take
-// packets of 32 voxels of one neighbour.
+// A CTA per grain: the grain's element index, element boxes and FP32 barycenters are
+// staged in shared memory once; then, slice by slice, the band voxels of a pass (whole
+// rows, <= kCVox voxels) are grouped by IDLocal neighbour (counting sort in shared
+// memory) and the warps take packets of 32 voxels of one neighbour.
 template <typename T>
-__global__ void __launch_bounds__(kCThreads, 2) correction_kernel(CorrectionArgs<T> a) {
-    __shared__ uint32_t hkey[kCHash];
-    __shared__ unsigned short hden[kCHash];
-    __shared__ int2 drng[kIdxMax];
-    __shared__ int dcnt[kIdxMax], doff[kIdxMax], dcur[kIdxMax], dpk[kIdxMax + 1];
-    __shared__ unsigned short vd[kCVox];     // dense neighbour index of the pass's voxels, kNoD: no search
-    __shared__ unsigned short vlist[kCVox];  // pass voxels grouped by neighbour
+__global__ void __launch_bounds__(kCThreads, 3) correction_kernel(CorrectionArgs<T> a) {
+    extern __shared__ __align__(16) unsigned char corr_smem[];
+    CorrSmem& S = *reinterpret_cast<CorrSmem*>(corr_smem);
     const double delta = a.geo.delta;
     const HullElements& el = a.el;
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
-    int staged = -1;  // grain whose index is in shared memory (the same in every thread)
-    int nd = 0;
     for (TileWalk w(a.toff, a.G, blockIdx.x, gridDim.x); w.valid(); w.next()) {
         const int g = w.g;
-        const int ne = min(max(el.n_elem[g], 0), el.elem_cap);
-        // the winner of this lane's last packet, a first bound for the next one of the
-        // same neighbour (packets of a neighbour follow its voxels in row order)
-        if (staged != g) {  // the grain's neighbour -> elements index in shared memory
-            __syncthreads();
-            for (int q = threadIdx.x; q < kCHash; q += blockDim.x) hkey[q] = kNoId;
-            nd = el.n_idx[g];
-            if (nd < 0 || nd > el.idx_cap || nd > kIdxMax) {
-                if (threadIdx.x == 0) atomicOr(a.err, ERR_BOUNDS);
-                nd = 0;
-            }
-            __syncthreads();
-            for (int d = threadIdx.x; d < nd; d += blockDim.x) {
-                const uint32_t id = el.idx_key[(long long)g * el.idx_cap + d];
-                int2 r = el.idx_rng[(long long)g * el.idx_cap + d];
-                if (r.x < 0 || r.y < 0 || r.x + r.y > el.pair_cap) {
-                    atomicOr(a.err, ERR_BOUNDS);
-                    r = make_int2(0, 0);
-                }
-                drng[d] = r;
-                unsigned hs = (id * 2654435761u) & (kCHash - 1);
-                for (int probe = 0; probe < kCHash; probe++) {
-                    if (atomicCAS(&hkey[hs], kNoId, id) == kNoId) {
-                        hden[hs] = (unsigned short)d;
-                        break;
-                    }
-                    hs = (hs + 1) & (kCHash - 1);
-                }
-            }
-            __syncthreads();
-            staged = g;
+        const int ne = min(max(el.n_elem[g], 0), min(el.elem_cap, kSElem));
+        int nd = el.n_idx[g];
+        if (nd < 0 || nd > el.idx_cap || nd > kIdxMax) {
+            if (threadIdx.x == 0) atomicOr(a.err, ERR_BOUNDS);
+            nd = 0;
         }
+        const int nflat = min(max(el.n_flat[g], 0), el.bary_cap);
+        const int npairs = min(el.pair_cap, kSPairs);
+        const float4 org = el.eorg[g];
+        const float4* gpts = el.ebf + (long long)g * el.bary_cap;
+        __syncthreads();  // the previous grain's packets are done with the shared arrays
+        for (int q = threadIdx.x; q < kCHash; q += blockDim.x) S.hkey[q] = kNoId;
+        for (int q = threadIdx.x; q < npairs; q += blockDim.x)
+            S.pairs[q] = el.idx_elem[(long long)g * el.pair_cap + q];
+        for (int e = threadIdx.x; e < ne; e += blockDim.x) {
+            const HullElem& E = el.elem[(long long)g * el.elem_cap + e];
+            int2 r = make_int2(E.pbase, E.pcount);
+            if (r.x < 0 || r.y < 0 || r.x + r.y > nflat) {
+                atomicOr(a.err, ERR_BOUNDS);
+                r = make_int2(0, 0);
+            }
+            S.rng[e] = r;
+            const float o[3] = {org.x, org.y, org.z};
+#pragma unroll
+            for (int q = 0; q < 3; q++) {
+                S.box[e][q] = __double2float_rd(E.lo[q] - (double)o[q]);
+                S.box[e][q + 3] = __double2float_ru(E.hi[q] - (double)o[q]);
+            }
+        }
+        if (nflat <= kSPts)
+            for (int p = threadIdx.x; p < nflat; p += blockDim.x) S.pts[p] = gpts[p];
+        __syncthreads();
+        for (int d = threadIdx.x; d < nd; d += blockDim.x) {
+            const uint32_t id = el.idx_key[(long long)g * el.idx_cap + d];
+            int2 r = el.idx_rng[(long long)g * el.idx_cap + d];
+            if (r.x < 0 || r.y < 0 || r.x + r.y > npairs) {
+                atomicOr(a.err, ERR_BOUNDS);
+                r = make_int2(0, 0);
+            }
+            S.drng[d] = r;
+            unsigned hs = (id * 2654435761u) & (kCHash - 1);
+            for (int probe = 0; probe < kCHash; probe++) {
+                if (atomicCAS(&S.hkey[hs], kNoId, id) == kNoId) {
+                    S.hden[hs] = (unsigned short)d;
+                    break;
+                }
+                hs = (hs + 1) & (kCHash - 1);
+            }
+        }
+        __syncthreads();
+        const float4* pts = nflat <= kSPts ? S.pts : gpts;
+        const int* eidx = el.eidx + (long long)g * el.bary_cap;
         const Box b = load_box(a.box + 6 * g);
-        const int k = b.z0 + w.local;
         const Box bo = load_box(a.idbox_old + 6 * g);
         const long long old_count = bo.count();
         const T* in = a.in + a.in_off[g];
         T* out = a.out + a.out_off[g];
         const uint32_t* idl = a.id_old + a.idoff_old[g];
         const HullElem* elem = el.elem + (long long)g * el.elem_cap;
-        const HullChunk* chunks = el.chunks + (long long)g * el.chunk_cap;
         const double* eb = el.ebary + 3 * (long long)g * el.bary_cap;
-        const unsigned short* pairs = el.idx_elem + (long long)g * el.pair_cap;
         const int nx = b.nx(), ny = b.ny();
         if (nx > kCVox) {
             if (threadIdx.x == 0) atomicOr(a.err, ERR_BOX);
             continue;
         }
+        // the filter's error bound: q is within 16 R^2 2^-24 of |v' - p'|^2 - |v'|^2 (the
+        // three FMAs, the FP32 rounding of p' and |p'|^2), R^2 the largest |v'|^2 or |p'|^2
+        float r2 = org.w;
+        {
+            const float cx = fmaxf(fabsf((float)b.y0 - org.x), fabsf((float)(b.y1 - 1) - org.x));
+            const float cy = fmaxf(fabsf((float)b.x0 - org.y), fabsf((float)(b.x1 - 1) - org.y));
+            const float cz = fmaxf(fabsf((float)b.z0 - org.z), fabsf((float)(b.z1 - 1) - org.z));
+            r2 = fmaxf(r2, cx * cx + cy * cy + cz * cz);
+        }
+        const float eps2 = fmaxf(2.f * 16.f * r2 * (1.0f / 16777216.f) * 1.0001f, 1e-6f);
         const int R = kCVox / nx;
-        int prev_d = -1, prev_e = -1, prev_b = -1;
+        for (int k = b.z0; k < b.z1; k++)
         for (int yp = 0; yp < ny; yp += R) {
             const int nv = min(R, ny - yp) * nx;
-            for (int d = threadIdx.x; d < nd; d += blockDim.x) dcnt[d] = 0;
+            for (int d = threadIdx.x; d < nd; d += blockDim.x) S.dcnt[d] = 0;
             __syncthreads();
             // band voxels: their neighbour; voxels whose neighbour no element holds get (1, 1)
             // now.  Four voxels per thread at a time: their loads are in flight together.
@@ -1005,15 +1147,15 @@ __global__ void __launch_bounds__(kCThreads, 2) correction_kernel(CorrectionArgs
                         const uint32_t id = ids[u];
                         unsigned hs = (id * 2654435761u) & (kCHash - 1);
                         for (int probe = 0; probe < kCHash; probe++) {
-                            const uint32_t key = hkey[hs];
-                            if (key == id) { dd = hden[hs]; break; }
+                            const uint32_t key = S.hkey[hs];
+                            if (key == id) { dd = S.hden[hs]; break; }
                             if (key == kNoId) break;
                             hs = (hs + 1) & (kCHash - 1);
                         }
-                        if (dd != kNoD) atomicAdd(&dcnt[dd], 1);
+                        if (dd != kNoD) atomicAdd(&S.dcnt[dd], 1);
                         else correct_voxel(a, elem, g, -1, id, vals[u], out + fs[u]);
                     }
-                    vd[q] = dd;
+                    S.vd[q] = dd;
                 }
             }
             __syncthreads();
@@ -1021,7 +1163,7 @@ __global__ void __launch_bounds__(kCThreads, 2) correction_kernel(CorrectionArgs
                 int run = 0, prun = 0;
                 for (int d0 = 0; d0 < nd; d0 += 32) {
                     const int d = d0 + lane;
-                    const int c = d < nd ? dcnt[d] : 0, pk = (c + 31) >> 5;
+                    const int c = d < nd ? S.dcnt[d] : 0, pk = (c + 31) >> 5;
                     int ic = c, ip = pk;
 #pragma unroll
                     for (int o = 1; o < 32; o <<= 1) {
@@ -1029,52 +1171,39 @@ __global__ void __launch_bounds__(kCThreads, 2) correction_kernel(CorrectionArgs
                         if (lane >= o) { ic += u; ip += v; }
                     }
                     if (d < nd) {
-                        doff[d] = dcur[d] = run + ic - c;
-                        dpk[d] = prun + ip - pk;
+                        S.doff[d] = S.dcur[d] = run + ic - c;
+                        S.dpk[d] = prun + ip - pk;
                     }
                     run += __shfl_sync(kFull, ic, 31);
                     prun += __shfl_sync(kFull, ip, 31);
                 }
-                if (lane == 0) dpk[nd] = prun;
+                if (lane == 0) S.dpk[nd] = prun;
             }
             __syncthreads();
             for (int q = threadIdx.x; q < nv; q += blockDim.x) {
-                const unsigned short dd = vd[q];
-                if (dd != kNoD) vlist[atomicAdd(&dcur[dd], 1)] = (unsigned short)q;
+                const unsigned short dd = S.vd[q];
+                if (dd != kNoD) S.vlist[atomicAdd(&S.dcur[dd], 1)] = (unsigned short)q;
             }
             __syncthreads();
-            const int P = dpk[nd];
+            const int P = S.dpk[nd];
             for (int pk = warp; pk < P; pk += nwarps) {
                 int lo = 0, hi = nd - 1;  // the neighbour whose packets hold pk
                 while (lo < hi) {
                     const int mid = (lo + hi + 1) >> 1;
-                    if (dpk[mid] <= pk) lo = mid;
+                    if (S.dpk[mid] <= pk) lo = mid;
                     else hi = mid - 1;
                 }
                 const int d = lo;
-                const int start = doff[d] + ((pk - dpk[d]) << 5);
-                const int cnt = min(32, doff[d] + dcnt[d] - start);
+                const int start = S.doff[d] + ((pk - S.dpk[d]) << 5);
+                const int cnt = min(32, S.doff[d] + S.dcnt[d] - start);
                 const bool active = lane < cnt;
-                const int q = vlist[start + (active ? lane : 0)];
+                const int q = S.vlist[start + (active ? lane : 0)];
                 const int i = b.y0 + yp + q / nx, j = b.x0 + q % nx;
                 const long long f = b.at(i, j, k);
-                double best = 10000000.0;
-                int win = -1, wb = -1;
-                if (d == prev_d && prev_e >= 0 && prev_b >= 0) {
-                    const double s = sqdist3((double)i, (double)j, (double)k, eb + 3 * (long long)prev_b);
-                    if (s < best) {  // the reference keeps only distances below its 1e7 start
-                        best = s;
-                        win = prev_e;
-                        wb = prev_b;
-                    }
-                }
                 // the point is Vector3d(i, j, k), box.cpp:481
-                project_packet(elem, chunks, eb, pairs, drng[d], active, (double)i, (double)j, (double)k, el, ne,
-                               best, win, wb, a.err);
+                const int2 dr = S.drng[d];
+                const int win = search_packet(S, pts, dr.x, dr.y, active, i, j, k, org, eps2, ne, eidx, eb, a.err);
                 if (active) {
-                    prev_d = d;
-                    prev_e = win;
-                    prev_b = wb;
                     const uint32_t id = f < old_count ? idl[f] : 0u;
                     correct_voxel(a, elem, g, win, id, (double)in[f], out + f);
                 }
@@ -1141,7 +1270,9 @@ void launch_elements(const ElementArgs& a, int grid, cudaStream_t s) {
 
 template <typename T>
 void launch_correction(const CorrectionArgs<T>& a, int grid, cudaStream_t s) {
-    correction_kernel<T><<<grid, 128, 0, s>>>(a);
+    static PerDevice configured;
+    configured.once([] { allow_max_dynamic_smem(correction_kernel<T>); });
+    correction_kernel<T><<<grid, kCThreads, sizeof(CorrSmem), s>>>(a);
 }
 
 template void launch_correction<double>(const CorrectionArgs<double>&, int, cudaStream_t);

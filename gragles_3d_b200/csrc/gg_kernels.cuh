@@ -103,6 +103,12 @@ struct CompareArgs {
     int pos_cap;
     int* newbox;              // per grain min/max (pre-initialised)
     int* err;
+    // 1: executeComparison then executeSetComparison (the loop's comparison stage);
+    // 0: executeComparison alone (LSbox::recalculateIDLocal after a grid coarsening,
+    //    box.cpp:2697-2700): out = the largest listed neighbour value, no new box, and
+    //    grains that do not exist are left alone (box.cpp:892-893)
+    int set_comparison;
+    const int* exists;        // read when set_comparison == 0
 };
 template <typename T>
 void launch_compare(const CompareArgs<T>& a, int grid, cudaStream_t s);
@@ -183,7 +189,7 @@ struct HullElem {
     int nids, id_off;         // neighbour IDs in the grain's ID pool
     int seg_off, nseg;        // barycenter segments (start, count) in the grain's segment pool
     int chunk_off, nchunk;    // barycenter chunks (each inside one segment) in the chunk pool
-    int pad;
+    int pbase, pcount;        // its barycenters, contiguous, in the flattened FP32 copy (ebf)
     double energy, mobility;  // m_energy, m_mobility
     double area;              // GrainBoundary::computeArea (InterfacialElement.cpp:81-91); 0 for junctions
     double lo[3], hi[3];      // bounding box of its barycenters
@@ -205,6 +211,13 @@ struct HullElements {
     int2* segs;               // (G + 1) x seg_cap
     double* ebary;            // (G + 1) x bary_cap x 3, barycenters grouped by neighbour list
     double* earea;            // (G + 1) x bary_cap, their triangles' area terms in the same order
+    // The same barycenters for the correction's FP32 filter, element by element in table
+    // order (element e's at [pbase, pbase + pcount)): (p - o, |p - o|^2) in FP32, p - o
+    // and its square taken in FP64 first, with o the grain's integer origin
+    float4* ebf;              // (G + 1) x bary_cap
+    int* eidx;                // (G + 1) x bary_cap: position of each of them in ebary
+    int* n_flat;              // G + 1: barycenters in ebf
+    float4* eorg;             // G + 1: (o.x, o.y, o.z, largest |p - o|^2 of the grain)
     HullChunk* chunks;        // (G + 1) x chunk_cap
     // neighbour ID -> the elements whose searched IDs hold it, in search order
     int* n_idx;               // G + 1: distinct IDs
@@ -248,7 +261,7 @@ template <typename T>
 struct CorrectionArgs {
     int G;
     Geometry geo;
-    const int* toff;          // n tiles per convolved grain (z-slices)
+    const int* toff;          // one tile per convolved grain
     const int* present;
     const int* box;           // current (cubic) boxes
     const T* in;              // input of the convolution
@@ -285,11 +298,57 @@ struct MCArgs {
     int nb_cap;
     HullCapture hull;         // hull.cap = 0: not captured
     int* err;
+    // 1: extractContour after a grid coarsening (grainhdl.cpp:1486-1495): every present
+    // grain's hull is rebuilt (none is deleted) and newbox is the resized grid's box,
+    // taken as it is (then resized to a cube) rather than widened by the border
+    int regrid;
 };
 template <typename T>
 void launch_mc(const MCArgs<T>& a, int grid, int side, cudaStream_t s);
 // Dynamic shared memory of the marching-cubes kernel for boxes up to `side`.
 size_t mc_slab_bytes(int side);
+
+// ---- grid coarsening (gg_coarsen.cu) ----
+// LSbox::resizeGrid's new boxes (box.cpp:2595-2621): each present grain's output box
+// scaled by h_old / h_new (`scaled`, the reference's m_newXMin..), then resized to a cube
+// on the new grid (`new_box`).
+struct RegridBoxArgs {
+    int G;
+    const int* present;
+    const int* old_box;       // m_outputDistance's box on the old grid
+    int* scaled;
+    int* new_box;
+    double ratio;             // h_old / h_new
+    int gb, M_new;
+    int* err;
+};
+void launch_regrid_boxes(const RegridBoxArgs& a, cudaStream_t s);
+// The trilinear re-sampling of resizeGrid (box.cpp:2623-2690) into the new boxes.
+template <typename T>
+struct ResampleArgs {
+    int G;
+    const int* toff;          // z-slices of the new boxes
+    Arena<const T> src;       // m_outputDistance on the old grid
+    Arena<T> dst;             // m_inputDistance on the new grid
+    double ratio_inv;         // h_new / h_old
+    int gb;
+    double delta_new;         // delta of the new grid
+};
+template <typename T>
+void launch_resample(const ResampleArgs<T>& a, int grid, cudaStream_t s);
+// IDLocal of present grains that do not exist, flat-resized onto their new box.
+struct IdResizeArgs {
+    int G;
+    const int* present;
+    const int* exists;
+    const uint32_t* id_old;
+    const int* idbox_old;
+    const long long* idoff_old;
+    uint32_t* id_new;
+    const int* idbox_new;
+    const long long* idoff_new;
+};
+void launch_id_resize(const IdResizeArgs& a, int grid, cudaStream_t s);
 
 // ---- redistancing (gg_redist.cu) ----
 template <typename T>

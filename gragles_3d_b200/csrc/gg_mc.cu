@@ -88,25 +88,6 @@ __device__ __forceinline__ void hash_insert(unsigned* hkey, unsigned* hval, unsi
     atomicOr(err, ERR_NEIGHBORS);
 }
 
-// DimensionalBuffer::resizeToCube, dimensionalBuffer.h:139-219
-__device__ Box resize_to_cube(Box b, int maximumLength) {
-    const int grid_size = maximumLength - 1;
-    const unsigned height = b.y1 - b.y0, width = b.x1 - b.x0, depth = b.z1 - b.z0;
-    if (width == height && width == depth) return b;
-    int ref = width > height ? (int)width : (int)height;
-    if (ref < (int)depth) ref = (int)depth;
-    if (ref > (int)width) { const int d = ref - (int)width; b.x0 -= d / 2; b.x1 += d / 2 + d % 2; }
-    if (ref > (int)height) { const int d = ref - (int)height; b.y0 -= d / 2; b.y1 += d / 2 + d % 2; }
-    if (ref > (int)depth) { const int d = ref - (int)depth; b.z0 -= d / 2; b.z1 += d / 2 + d % 2; }
-    if (b.x0 < 0) { const int d = -b.x0; b.x1 += d; b.x0 += d; }
-    else if (b.x1 > grid_size) { const int d = grid_size - b.x1; b.x1 += d; b.x0 += d; }
-    if (b.y0 < 0) { const int d = -b.y0; b.y1 += d; b.y0 += d; }
-    else if (b.y1 > grid_size) { const int d = grid_size - b.y1; b.y1 += d; b.y0 += d; }
-    if (b.z0 < 0) { const int d = -b.z0; b.z1 += d; b.z0 += d; }
-    else if (b.z1 > grid_size) { const int d = grid_size - b.z1; b.z1 += d; b.z0 += d; }
-    return b;
-}
-
 template <typename T>
 __global__ void __launch_bounds__(kThreads, 3) mc_kernel(MCArgs<T> a, int slab_bytes) {
     __shared__ double vbuf[kThreads * 5];
@@ -120,7 +101,7 @@ __global__ void __launch_bounds__(kThreads, 3) mc_kernel(MCArgs<T> a, int slab_b
     extern __shared__ __align__(16) unsigned char slab_raw[];
     for (TileWalk w(a.toff, a.G, blockIdx.x, gridDim.x); w.valid(); w.next()) {
         const int g = w.g;
-        if (!a.exists[g]) {  // the hull vanished last step: delete, grainhdl.cpp:678-680
+        if (!a.exists[g] && !a.regrid) {  // the hull vanished last step: delete, grainhdl.cpp:678-680
             if (threadIdx.x == 0) a.present[g] = 0;
             continue;
         }
@@ -366,15 +347,17 @@ __global__ void __launch_bounds__(kThreads, 3) mc_kernel(MCArgs<T> a, int slab_b
             if (ex) {
                 // tail of executeSetComparison (box.cpp:858-877), then extractContour's resize
                 const int* nbx = a.newbox + 6 * g;
-                const int gb = a.geo.gb, M = a.geo.M;
+                const int gb = a.regrid ? 0 : a.geo.gb, M = a.geo.M;
                 int x0 = nbx[0] - gb, x1 = nbx[1] + gb, y0 = nbx[2] - gb, y1 = nbx[3] + gb;
                 int z0 = nbx[4] - gb, z1 = nbx[5] + gb;
-                if (x0 < 0) x0 = 0;
-                if (y0 < 0) y0 = 0;
-                if (z0 < 0) z0 = 0;
-                if (x1 >= M) x1 = M - 1;
-                if (y1 >= M) y1 = M - 1;
-                if (z1 >= M) z1 = M - 1;
+                if (!a.regrid) {  // the clamp of executeSetComparison (box.cpp:868-877)
+                    if (x0 < 0) x0 = 0;
+                    if (y0 < 0) y0 = 0;
+                    if (z0 < 0) z0 = 0;
+                    if (x1 >= M) x1 = M - 1;
+                    if (y1 >= M) y1 = M - 1;
+                    if (z1 >= M) z1 = M - 1;
+                }
                 const Box nb = resize_to_cube(Box{x0, x1, y0, y1, z0, z1}, M);
                 if (nb.x0 < 0 || nb.y0 < 0 || nb.z0 < 0 || nb.nx() <= 0) atomicOr(a.err, ERR_BOX);
                 store_box(a.out_box + 6 * g, nb);

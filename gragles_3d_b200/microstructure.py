@@ -179,7 +179,8 @@ def write_parameters(path: str, *, n_grains: int, border: int = 10, steps: int =
                      unique_energies: bool = True, mobility_factor: bool = False,
                      stored_energy: bool = False, triple_line_drag: float = 1e6,
                      analysis_every: int = 1000000, neighbor_tracking: bool = False,
-                     plot_interval: int = 1000000) -> None:
+                     plot_interval: int = 1000000, grid_coarsening: bool = False,
+                     coarsening_gradient: float = 0.95) -> None:
     """A ``parameters.xml`` for the reference (Settings.cpp:81-270) in mode 4.
 
     ``NumberOfParticles`` must already hold the grain count: the reference sizes
@@ -196,7 +197,8 @@ def write_parameters(path: str, *, n_grains: int, border: int = 10, steps: int =
         "UseMobilityFactor": int(mobility_factor), "UseStoredElasticEnergy": int(stored_energy),
         "UseMagneticField": 0, "DisableConvolutionCorrection": int(not correction),
         "UseTexture": 0, "ExecuteInParallel": 1, "MaximumNumberOfThreads": threads,
-        "GridCoarsement": 0, "GridCoarsementGradient": 0.95, "ConvolutionMode": 2,
+        "GridCoarsement": int(grid_coarsening), "GridCoarsementGradient": repr(float(coarsening_gradient)),
+        "ConvolutionMode": 2,
         "UniqueGBEnergies": int(unique_energies), "GrainScheduler": 0, "DecoupleGrains": 0,
         "NeighborTracking": int(neighbor_tracking), "StoreTaskDistribution": 0,
     }

@@ -55,6 +55,10 @@ typedef struct {
     int32_t hull_capacity;      /* triangles kept per hull for the correction (0 = 16 side^2 + 2048) */
     int32_t keep_elements;      /* build the interfacial elements every step even without the
                                    correction (computeSurfaceElements, box.cpp:1175-1180), for gg_get_faces */
+    int32_t grid_coarsening;    /* GridCoarsement (grainhdl::gridCoarsement, grainhdl.cpp:1446-1498) */
+    int32_t points_per_grain;   /* NumberOfPointsPerGrain (0 = the mode-4 reader's rule,
+                                   (int)(N / n_grains^(1/3) + 0.5), grainhdl.cpp:221) */
+    double coarsening_gradient; /* GridCoarsementGradient (0 = 0.95, the Settings default) */
 } gg_params;
 
 /* Per-step report (the reference prints the same stage times, grainhdl.cpp:920-933). */
@@ -90,8 +94,17 @@ int gg_set_lists(gg_ctx* ctx, const int64_t* offsets, const uint32_t* ids);
 /* The same membership (inclusive box overlap) in grain-ID order, built on the device. */
 int gg_default_lists(gg_ctx* ctx);
 
-/* One loop iteration of grainhdl::run_sim (grainhdl.cpp:837-917). */
+/* One loop iteration of grainhdl::run_sim (grainhdl.cpp:837-917).  With grid_coarsening
+ * set, the iteration starts with grainhdl::gridCoarsement (grainhdl.cpp:1446-1498): when
+ * the grain count has fallen below coarsening_gradient of its count at the last
+ * coarsening, the domain is re-gridded to the smaller size the reference computes
+ * (LSbox::resizeGrid trilinear re-sampling, then recalculateIDLocal and extractContour,
+ * box.cpp:2595-2702, 1144-1161) before the convolution. */
 int gg_step(gg_ctx* ctx, gg_step_stats* stats);
+
+/* grainhdl::realDomainSize: the current grid size N (smaller than the initial one after
+ * a grid coarsening). */
+int gg_domain_size(gg_ctx* ctx);
 
 /* The stages of one iteration, for stage-level testing, in the order gg_step runs
  * them.  Each stands in for the grainhdl method named. */

@@ -63,6 +63,7 @@ enum Kind {
 struct Dumper {
     FILE* f = nullptr;
     bool stats = false;
+    bool init = true;  // GG_REF_DUMP_INIT=0: no initial SDF and list records (large domains)
     bool all_grains = false;
     std::set<int> grains;
     bool all_loops = true;
@@ -91,6 +92,8 @@ struct Dumper {
         f = std::fopen(path, "wb");
         const char* st = std::getenv("GG_REF_DUMP_STATS");
         stats = st && st[0] == '1';
+        const char* in = std::getenv("GG_REF_DUMP_INIT");
+        init = !(in && in[0] == '0');
         parse_list(std::getenv("GG_REF_DUMP_GRAINS"), all_grains, grains);
         parse_list(std::getenv("GG_REF_DUMP_LOOPS"), all_loops, loops);
     }
@@ -182,7 +185,7 @@ void __wrap__ZN8grainhdl20initializeSimulationEv(grainhdl* self) {
 
 void __wrap__ZN5LSbox23computeDirectNeighboursERK5RTreeIjiLi3EfLi8ELi4EE(LSbox* self, const void* tree) {
     __real__ZN5LSbox23computeDirectNeighboursERK5RTreeIjiLi3EfLi8ELi4EE(self, tree);
-    if (dumper().f && dumper().stats) {
+    if (dumper().f && dumper().stats && dumper().init) {
         dump_sdf(K_INIT_SDF, -1, (int)self->m_ID, self->m_outputDistance);
         dump_list(K_INIT_LIST, -1, (int)self->m_ID, self->m_secondOrderNeighbours);
     }

@@ -58,7 +58,7 @@ def read_records(path: str) -> Iterator[Record]:
 def run_reference(workdir: str, params: str = "parameters.xml", *, threads: int = 8,
                   dump: Optional[str] = None, stats: bool = True, grains: Optional[str] = None,
                   loops: Optional[str] = None, timeout: float = 3600.0,
-                  binary: str = REF_BINARY) -> subprocess.CompletedProcess:
+                  binary: str = REF_BINARY, init: bool = True) -> subprocess.CompletedProcess:
     """Run the compiled reference in ``workdir`` (it writes its outputs there)."""
     env = dict(os.environ)
     env["OMP_NUM_THREADS"] = str(threads)
@@ -71,18 +71,25 @@ def run_reference(workdir: str, params: str = "parameters.xml", *, threads: int 
             env["GG_REF_DUMP_GRAINS"] = grains
         if loops:
             env["GG_REF_DUMP_LOOPS"] = loops
+        if not init:
+            env["GG_REF_DUMP_INIT"] = "0"
     return subprocess.run([binary, params], cwd=workdir, env=env, capture_output=True,
                           text=True, timeout=timeout)
 
 
 def parse_timers(stdout: str) -> dict:
     """The reference's own stage timers (grainhdl.cpp:920-933, ggLS.cpp:74)."""
-    out = {}
+    out = {"coarsening": []}
     keys = {"Convolution time:": "convolution", "Comparison time:": "comparison",
             "Redistancing time:": "redistancing", "Levelset time:": "levelset",
             "GridCoarse/SwitchBuffer/UpNeigh:": "rest", "Sum parallel regions:": "sum",
             "Elapsed seconds for simulation:": "elapsed"}
     for line in stdout.splitlines():
+        # gridCoarsement's report (grainhdl.cpp:1454-1455): the loop, then the new size
+        if line.startswith("coarsing the current grid in Timestep:"):
+            out["coarsening"].append([int(line.split(":")[-1]), 0])
+        elif line.startswith("newSize :") and out["coarsening"]:
+            out["coarsening"][-1][1] = int(line.split(":")[-1])
         for k, name in keys.items():
             if line.strip().startswith(k):
                 try:
@@ -115,12 +122,12 @@ def collect(records) -> dict:
 
 
 def run_case(ms_dir: str, *, threads: int = 8, grains: Optional[str] = None,
-             loops: Optional[str] = None, timeout: float = 3600.0) -> tuple[dict, dict]:
+             loops: Optional[str] = None, timeout: float = 3600.0, init: bool = True) -> tuple[dict, dict]:
     """Run the reference on a prepared case directory and return (collected dump, timers)."""
     fd, dump = tempfile.mkstemp(suffix=".ggdr", dir=ms_dir)
     os.close(fd)
     proc = run_reference(ms_dir, threads=threads, dump=dump, grains=grains, loops=loops,
-                         timeout=timeout)
+                         timeout=timeout, init=init)
     if proc.returncode != 0:
         raise RuntimeError(f"reference failed ({proc.returncode}): {proc.stderr[-2000:]}")
     res = collect(read_records(dump))

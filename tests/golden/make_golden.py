@@ -9,6 +9,12 @@ The "correction" case turns on the convolution correction (box.cpp:426-535) with
 a mix of low-angle and random orientations, the mobility model, a weak
 triple-line drag and stored elastic energies.
 
+The "coarsen" case turns grid coarsening on (GridCoarsement=1, gradient 0.99), so the
+grid shrinks several times within its 40 steps.
+
+The "c1" case is the plain-method configuration (64^3, 200 grains, 50 timesteps) the
+FP64 device path is pinned on at full length.
+
 The "analysis" case reruns the correction case on one thread with the reference's
 analysis outputs on: Texture and Faces records every loop and the voxel container.
 
@@ -39,7 +45,17 @@ CASES = {
     "tiny": (32, 20, 5, 1032, 6, 14, 2),
     "vanish": (40, 150, 5, 1040, 40, 0, 0),
     "correction": (32, 30, 5, 2032, 8, 0, 0),
+    # the plain-method configuration: 64^3, 200 Voronoi grains, 10-voxel border, 50 timesteps
+    # (51 loop iterations, grainhdl.cpp:837); comparison lists kept for the last loop only
+    "c1": (64, 200, 10, 1001, 50, 0, 0),
+    # grid coarsening on (grainhdl.cpp:1446-1498): the grid shrinks whenever the grain count
+    # falls below 0.99 of its count at the last coarsening
+    "coarsen": (40, 150, 5, 1040, 40, 0, 0),
 }
+# parameters.xml settings of the cases beyond the defaults
+SETTINGS = {"coarsen": dict(grid_coarsening=True, coarsening_gradient=0.99)}
+# cases whose per-loop comparison lists are kept only for the final loop (fixture size)
+LAST_LIST_ONLY = {"c1", "coarsen"}
 
 # physics of the cases that run the convolution correction
 PHYSICS = {
@@ -78,10 +94,15 @@ def make(name, N, G, border, seed, steps, keep_grain, keep_loop):
     with tempfile.TemporaryDirectory() as d:
         msgen.write_mode4(ms, d)
         msgen.write_parameters(os.path.join(d, "parameters.xml"), n_grains=G, border=border, steps=steps,
-                               correction=bool(phys), **(phys or {}))
-        res, _ = refdump.run_case(d, threads=4, grains=str(keep_grain) if keep_grain else None,
-                                  loops=str(keep_loop) if keep_grain else None)
+                               correction=bool(phys), **(phys or {}), **SETTINGS.get(name, {}))
+        res, timers = refdump.run_case(d, threads=4, grains=str(keep_grain) if keep_grain else None,
+                                       loops=str(keep_loop) if keep_grain else None)
     out = {"N": N, "G": G, "border": border, "seed": seed, "steps": steps}
+    for k, v in SETTINGS.get(name, {}).items():
+        out["set_" + k] = v
+    if SETTINGS.get(name, {}).get("grid_coarsening"):
+        ev = np.array(timers["coarsening"], np.int64).reshape(-1, 2)
+        out["coarse_loop"], out["coarse_size"] = ev[:, 0], ev[:, 1]
     if phys:
         out["euler"] = ms.euler.copy()
         out["uds_stored_energy"] = ms.stored_energy.copy()
@@ -102,7 +123,8 @@ def make(name, N, G, border, seed, steps, keep_grain, keep_loop):
             box[s, g] = b
         o, i = ragged(res["neighbors"].get(loop, {}), G)
         nb_off.append(o); nb_ids.append(i)
-        o, i = ragged(res["lists"].get(loop, {}), G)
+        keep = name not in LAST_LIST_ONLY or loop == loops[-1]
+        o, i = ragged(res["lists"].get(loop, {}) if keep else {}, G)
         li_off.append(o); li_ids.append(i)
     out.update(exists=exists, volume=vol, surface=sur, box=box,
                nb_off=np.stack(nb_off), nb_ids=np.concatenate(nb_ids), nb_len=np.array([len(x) for x in nb_ids]),

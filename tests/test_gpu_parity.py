@@ -6,6 +6,8 @@ seconds.  Stage tests check each batched kernel on the GPU's own inputs against 
 oracle's single-box restatement; loop tests run both implementations side by side
 and compare every step.
 """
+import os
+
 import numpy as np
 import pytest
 
@@ -223,3 +225,43 @@ def test_voxel_container_matches_oracle(gpu, oracle, precision):
             assert np.array_equal(got, want), f"step {s}: {(got != want).sum()} voxels differ"
         else:
             assert (got != want).mean() < 1e-3, f"step {s}: {(got != want).sum()} voxels differ"
+
+
+def test_c1_fp64_matches_reference_golden(gpu):
+    """The plain-method configuration at full length: 64^3, 200 Voronoi grains, 10-voxel
+    border, 50 timesteps (51 loop iterations), started from the reference's own R-tree
+    comparison lists (tests/golden/c1.npz, written by the compiled reference).  Every
+    loop: existence, boxes, volumes and surfaces bit for bit, hull neighbours in
+    first-seen order, and the grain-count trajectory; the comparison lists of the last
+    loop in order."""
+    d = dict(np.load(os.path.join(os.path.dirname(__file__), "golden", "c1.npz")))
+    N, G, border = int(d["N"]), int(d["G"]), int(d["border"])
+    ms = msgen.voronoi(N, G, seed=int(d["seed"]))
+    ext, counts = ms.grain_extents()
+    gh = gpu.GrainHandler(N, border, 0.2, G, precision=gpu.PRECISION_FP64)
+    gh.load(ms.labels, ext, counts)
+    gh.set_lists(d["init_list_off"], d["init_list_ids"])
+    nb_base = np.concatenate([[0], np.cumsum(d["nb_len"])])
+    li_base = np.concatenate([[0], np.cumsum(d["list_len"])])
+    loops = d["exists"].shape[0]
+    assert loops == int(d["steps"]) + 1
+    for s in range(loops):
+        gh.step()
+        st = gh.stats()
+        assert int(st.exists[1:].sum()) == int(d["exists"][s, 1:].sum()), f"loop {s}: grain count"
+        nb_ids = d["nb_ids"][nb_base[s]:nb_base[s + 1]]
+        for g in range(1, G + 1):
+            assert bool(st.exists[g]) == bool(d["exists"][s, g]), f"loop {s} grain {g}: exists"
+            if not st.exists[g]:
+                continue
+            assert tuple(st.boxes[g]) == tuple(d["box"][s, g]), f"loop {s} grain {g}: box"
+            assert st.volume[g] == d["volume"][s, g], f"loop {s} grain {g}: volume"
+            assert st.surface[g] == d["surface"][s, g], f"loop {s} grain {g}: surface"
+            want = nb_ids[d["nb_off"][s][g]:d["nb_off"][s][g + 1]]
+            assert np.array_equal(gh.neighbors(g), want), f"loop {s} grain {g}: neighbours"
+    li_ids = d["list_ids"][li_base[loops - 1]:li_base[loops]]
+    for g in range(1, G + 1):
+        want = li_ids[d["list_off"][loops - 1][g]:d["list_off"][loops - 1][g + 1]]
+        if want.size:
+            assert np.array_equal(gh.comparison_list(g), want), f"grain {g}: final comparison list"
+    gh.close()
