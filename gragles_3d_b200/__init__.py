@@ -33,7 +33,7 @@ EXPORTED = [
     "gg_stage_redistancing", "gg_get_grain_stats", "gg_get_neighbors", "gg_get_list", "gg_get_sdf",
     "gg_get_idlocal", "gg_grain_count", "gg_loop", "gg_convolve_boxes_f64", "gg_convolve_boxes_mixed",
     "gg_convolve_boxes_f64_noalloc", "gg_set_orientations", "gg_set_stored_energy", "gg_get_elements",
-    "gg_voxel_container", "gg_get_faces", "gg_domain_size",
+    "gg_voxel_container", "gg_get_faces", "gg_domain_size", "gg_rtree_lists", "gg_rtree_lists_from_boxes",
 ]
 
 
@@ -85,6 +85,9 @@ def load_library(path: str = LIB_PATH):
     L.gg_load_state.argtypes = [vp, vp, vp, vp]
     L.gg_set_lists.argtypes = [vp, vp, vp]
     L.gg_default_lists.argtypes = [vp]
+    L.gg_rtree_lists.argtypes = [vp]
+    L.gg_rtree_lists_from_boxes.argtypes = [i32, vp, vp, vp, vp, i64]
+    L.gg_rtree_lists_from_boxes.restype = i64
     L.gg_step.argtypes = [vp, C.POINTER(StepStats)]
     for s in ("gg_stage_convolution", "gg_stage_update_lists", "gg_stage_comparison", "gg_stage_level_set",
               "gg_stage_redistancing", "gg_grain_count", "gg_loop", "gg_domain_size"):
@@ -234,6 +237,11 @@ class GrainHandler:
     def default_lists(self) -> None:
         self._check(load_library().gg_default_lists(self._h))
 
+    def rtree_lists(self) -> None:
+        """The initial comparison lists in the reference's R-tree search order
+        (find_neighbors, grainhdl.cpp:1029-1054)."""
+        self._check(load_library().gg_rtree_lists(self._h))
+
     def set_orientations(self, euler: np.ndarray) -> None:
         """Bunge angles (G, 3) in radians for grain IDs 1..G."""
         e = np.ascontiguousarray(euler, dtype=np.float64)
@@ -327,6 +335,43 @@ class GrainHandler:
                       int(0 in set(self.neighbors(g).tolist())), 0)
         return out
 
+    def texture_text(self) -> list:
+        """The rows of Texture_<loop>.ori, the text form of save_Texture (grainhdl.cpp:776-805),
+        one per existing grain in ascending ID order: ID, hull neighbour count, boundary
+        flag, volume, surface, m_energy, mean width, triple-line length, triple lines,
+        quadruple points, high-order junctions, stored elastic energy, Bunge angles.
+        m_energy is never assigned by the reference (0); GrainHull::meanWidth and
+        computeTriplelineLength (grainHull.cpp:1211-1329) have no caller in it, so the
+        members it prints for them keep their initial value, 0 here.  The junction counts
+        need the interfacial elements (correction or keep_elements)."""
+        st = self.stats()
+        rows = []
+        for g in range(1, self.G + 1):
+            if not st.exists[g]:
+                continue
+            _, tl, qj, hj = self.elements(g)
+            phi1, PHI, phi2 = quaternion_to_euler(euler_to_quaternion(self._euler[g - 1]))
+            rows.append((g, int(st.n_neighbors[g]), int(0 in set(self.neighbors(g).tolist())), st.volume[g],
+                         st.surface[g], 0.0, 0.0, 0.0, float(tl), float(qj), float(hj), self._see[g - 1], phi1, PHI,
+                         phi2))
+        return rows
+
+    def network_rows(self) -> list:
+        """The rows of Microstructure_<loop>.uds that saveNetworkAsVoxelContainer writes
+        (grainhdl.cpp:1093-1111), one per existing grain in ascending ID order: ID, box
+        centre (integer midpoint times h), Bunge angles, box, volume, stored elastic energy."""
+        st = self.stats()
+        h = 1.0 / self.domain_size
+        rows = []
+        for g in range(1, self.G + 1):
+            if not st.exists[g]:
+                continue
+            x0, x1, y0, y1, z0, z1 = (int(v) for v in st.boxes[g])
+            phi1, PHI, phi2 = quaternion_to_euler(euler_to_quaternion(self._euler[g - 1]))
+            rows.append((g, ((x1 - x0) // 2 + x0) * h, ((y1 - y0) // 2 + y0) * h, ((z1 - z0) // 2 + z0) * h, phi1,
+                         PHI, phi2, x0, x1, y0, y1, z0, z1, st.volume[g], self._see[g - 1]))
+        return rows
+
     def voxel_container(self) -> np.ndarray:
         """The network as an (N, N, N) [z][y][x] array of grain IDs (the reference's
         Container_size_N_t_loop.raw)."""
@@ -354,6 +399,23 @@ def from_microstructure(ms, border: int = 10, time_step: float = 0.2, precision:
     else:
         gh.set_lists(*lists)
     return gh
+
+
+def rtree_lists(boxes: np.ndarray, valid: np.ndarray):
+    """find_neighbors' R-tree search on host boxes ((G + 1) x 6, valid (G + 1) flags):
+    the initial comparison lists as CSR (offsets[G + 2], ids) in the reference's order.
+    Host only: no GPU needed."""
+    L = load_library()
+    b = np.ascontiguousarray(boxes, dtype=np.int32)
+    v = np.ascontiguousarray(valid, dtype=np.uint8)
+    G = b.shape[0] - 1
+    off = np.zeros(G + 2, np.int64)
+    n = L.gg_rtree_lists_from_boxes(G, _p(b), _p(v), _p(off), None, 0)
+    if n < 0:
+        raise GGError(int(n), "gg_rtree_lists_from_boxes failed")
+    ids = np.zeros(max(n, 1), np.uint32)
+    L.gg_rtree_lists_from_boxes(G, _p(b), _p(v), _p(off), _p(ids), n)
+    return off, ids[:n]
 
 
 def convolve_boxes_f64(boxes: list, domain_size: int, time_step: float) -> list:

@@ -21,7 +21,7 @@ CSRC = os.path.join(HERE, "csrc")
 OBJ = os.path.join(HERE, "_build")
 LIB = os.path.join(HERE, "libgg_b200.so")
 SOURCES = ["gg_api.cu", "gg_plan.cu", "gg_conv_f64.cu", "gg_conv_tc.cu", "gg_conv_umma.cu", "gg_lists.cu", "gg_compare.cu",
-           "gg_mc.cu", "gg_redist.cu", "gg_init.cu", "gg_noalloc.cu", "gg_hull.cu", "gg_coarsen.cu"]
+           "gg_mc.cu", "gg_redist.cu", "gg_init.cu", "gg_noalloc.cu", "gg_hull.cu", "gg_coarsen.cu", "gg_rtree.cu"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
 

@@ -63,6 +63,7 @@ struct gg_ctx {
     long long pool_voxels = 0, spec_capacity = 0;
     // tiles
     int *d_toff_n = nullptr, *d_toff_slab = nullptr, *d_toff_one = nullptr, *d_toff_mc = nullptr, *d_toff_red = nullptr;
+    int* d_toff_big = nullptr;  // mixed path: slices of the boxes above the tensor-core side
     // tables
     double2* d_tw = nullptr;
     long long* d_tw_off = nullptr;
@@ -277,6 +278,9 @@ int plan(gg_ctx* ctx, const int* box, int only_existing, long long* off, long lo
     a.toff_slab = toff_slab;
     a.slab = ctx->slab;
     a.row_tile = ctx->fp64 ? 0 : kUmmaRows;
+    // mixed path: boxes up to the tensor-core kernel's side in row tiles, larger ones in slices
+    a.class_side = ctx->fp64 ? 0 : kUmmaMaxSide;
+    a.toff_big = (!ctx->fp64 && toff_slab) ? ctx->d_toff_big : nullptr;
     a.toff_one = toff_one;
     a.total_voxels = total_voxels;
     a.err = ctx->d_err;
@@ -418,38 +422,41 @@ int stage_convolution_t(gg_ctx* ctx) {
         launch_conv_f64(a, ctx->grid, conv_f64_smem_bytes(ctx->side_max), ctx->stream);
         ctx->launches += 3;
     } else {
-        if (umma_supported(ctx->side_max)) {
-            if (!ctx->d_cscr) return fail(ctx, GG_ERR_INVALID, "convolution scratch missing");
-            UmmaConvArgs u{};
-            u.G = ctx->G;
-            u.toff = ctx->d_toff_slab;
-            u.box = ctx->d_box[p];
-            u.in = reinterpret_cast<const float*>(ctx->d_arena[p]);
-            u.in_off = ctx->d_off[p];
-            u.out = reinterpret_cast<float*>(ctx->d_arena[p ^ 1]);
-            u.out_off = ctx->d_off[p ^ 1];
-            u.scratch = ctx->d_cscr;
-            u.bmat = ctx->d_bmat;
-            u.boff = ctx->d_boff;
-            u.err = ctx->d_err;
-            launch_conv_umma(u, ctx->num_sms, ctx->side_max, ctx->stream);
-            ctx->launches += 3;
-            CK(cudaGetLastError());
-            return correct_convolution<T>(ctx);
+        // two size classes in one step: sides up to kUmmaMaxSide on the tensor cores, larger
+        // boxes (when any) on the FP32 SIMT kernels; each launch walks only its class's tiles
+        const int small_side = std::min(ctx->side_max, kUmmaMaxSide);
+        if (!umma_supported(small_side)) return fail(ctx, GG_ERR_UNSUPPORTED, "tensor-core convolution unavailable");
+        if (!ctx->d_cscr) return fail(ctx, GG_ERR_INVALID, "convolution scratch missing");
+        UmmaConvArgs u{};
+        u.G = ctx->G;
+        u.toff = ctx->d_toff_slab;
+        u.box = ctx->d_box[p];
+        u.in = reinterpret_cast<const float*>(ctx->d_arena[p]);
+        u.in_off = ctx->d_off[p];
+        u.out = reinterpret_cast<float*>(ctx->d_arena[p ^ 1]);
+        u.out_off = ctx->d_off[p ^ 1];
+        u.scratch = ctx->d_cscr;
+        u.bmat = ctx->d_bmat;
+        u.boff = ctx->d_boff;
+        u.err = ctx->d_err;
+        launch_conv_umma(u, ctx->num_sms, small_side, ctx->stream);
+        ctx->launches += 3;
+        CK(cudaGetLastError());
+        if (ctx->side_max > kUmmaMaxSide) {
+            ConvTCArgs a{};
+            a.G = ctx->G;
+            a.toff = ctx->d_toff_big;
+            a.in = reinterpret_cast<const float*>(ctx->d_arena[p]);
+            a.box = ctx->d_box[p];
+            a.in_off = ctx->d_off[p];
+            a.out = reinterpret_cast<float*>(ctx->d_arena[p ^ 1]);
+            a.out_off = ctx->d_off[p ^ 1];
+            a.circ = ctx->d_circ;
+            a.circ_off = ctx->d_circ_off;
+            a.err = ctx->d_err;
+            launch_conv_tc(a, ctx->num_sms, ctx->side_max, ctx->stream);
+            ctx->launches += 2;
         }
-        ConvTCArgs a{};
-        a.G = ctx->G;
-        a.toff = ctx->d_toff_n;
-        a.in = reinterpret_cast<const float*>(ctx->d_arena[p]);
-        a.box = ctx->d_box[p];
-        a.in_off = ctx->d_off[p];
-        a.out = reinterpret_cast<float*>(ctx->d_arena[p ^ 1]);
-        a.out_off = ctx->d_off[p ^ 1];
-        a.circ = ctx->d_circ;
-        a.circ_off = ctx->d_circ_off;
-        a.err = ctx->d_err;
-        launch_conv_tc(a, ctx->num_sms, ctx->side_max, ctx->stream);
-        ctx->launches += 2;
     }
     CK(cudaGetLastError());
     return correct_convolution<T>(ctx);
@@ -814,7 +821,7 @@ void free_all(gg_ctx* c) {
                     c->d_son, c->d_ncmp, c->d_nson, c->d_pt, c->d_arena[0], c->d_arena[1], c->d_box[0], c->d_box[1],
                     c->d_off[0], c->d_off[1], c->d_idarena[0], c->d_idarena[1], c->d_idbox[0], c->d_idbox[1],
                     c->d_idoff[0], c->d_idoff[1], c->d_spec, c->d_spec_off, c->d_toff_n, c->d_toff_slab,
-                    c->d_toff_one, c->d_toff_mc, c->d_toff_red, c->d_tw, c->d_tw_off, c->d_gtab, c->d_g_off,
+                    c->d_toff_one, c->d_toff_mc, c->d_toff_red, c->d_toff_big, c->d_tw, c->d_tw_off, c->d_gtab, c->d_g_off,
                     c->d_circ, c->d_circ_off, c->d_bmat, c->d_boff, c->d_cscr, c->d_elscr, c->d_quat, c->d_see,
                     c->hull.rec_list, c->hull.rec_ntri, c->hull.bary, c->hull.tarea, c->hull.diag, c->el.earea, c->el.ebf, c->el.eidx, c->el.n_flat, c->el.eorg, c->hull.n_rec, c->hull.n_tri, c->el.n_elem,
                     c->el.elem, c->el.ids, c->el.segs, c->el.ebary, c->el.chunks, c->el.n_idx, c->el.idx_key, c->el.idx_rng,
@@ -905,6 +912,7 @@ int gg_create(const gg_params* params, gg_ctx** out) {
     CK(dalloc(&ctx->d_toff_one, G1 + 1));
     CK(dalloc(&ctx->d_toff_mc, G1 + 1));
     CK(dalloc(&ctx->d_toff_red, G1 + 1));
+    CK(dalloc(&ctx->d_toff_big, G1 + 1));
     CK(dalloc(&ctx->d_err, 1));
     CK(dalloc(&ctx->d_total_vox, 1));
     CK(dalloc(&ctx->d_count3, 3));
@@ -1086,6 +1094,25 @@ int gg_default_lists(gg_ctx* ctx) {
     ctx->launches += 1;
     CK(cudaGetLastError());
     return check_err(ctx, "gg_default_lists");
+}
+
+int gg_rtree_lists(gg_ctx* ctx) {
+    if (!ctx || !ctx->loaded) return GG_ERR_INVALID;
+    const size_t G1 = (size_t)ctx->G + 1;
+    std::vector<int32_t> boxes(6 * G1);
+    std::vector<int> present(G1), exists(G1);
+    CK(cudaStreamSynchronize(ctx->stream));
+    CK(cudaMemcpy(boxes.data(), ctx->d_box[ctx->p ^ 1], sizeof(int32_t) * 6 * G1, cudaMemcpyDeviceToHost));
+    CK(cudaMemcpy(present.data(), ctx->d_present, sizeof(int) * G1, cudaMemcpyDeviceToHost));
+    CK(cudaMemcpy(exists.data(), ctx->d_exists, sizeof(int) * G1, cudaMemcpyDeviceToHost));
+    std::vector<uint8_t> valid(G1, 0);
+    for (size_t g = 1; g < G1; g++) valid[g] = (uint8_t)(present[g] && exists[g]);
+    std::vector<int64_t> off(G1 + 1, 0);
+    const int64_t total = gg_rtree_lists_from_boxes(ctx->G, boxes.data(), valid.data(), off.data(), nullptr, 0);
+    if (total < 0) return fail(ctx, (int)total, "R-tree lists: invalid boxes");
+    std::vector<uint32_t> ids(total > 0 ? total : 1);
+    gg_rtree_lists_from_boxes(ctx->G, boxes.data(), valid.data(), off.data(), ids.data(), total);
+    return gg_set_lists(ctx, off.data(), ids.data());
 }
 
 int gg_stage_convolution(gg_ctx* ctx) {

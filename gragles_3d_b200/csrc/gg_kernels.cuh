@@ -24,6 +24,10 @@ struct PlanArgs {
                               // ceil(n^2 / row_tile) when row_tile > 0; may be null
     int slab;
     int row_tile;
+    // > 0 (with row_tile): grains with side above it get no row tiles in toff_slab and
+    // their n tiles in toff_big instead (the convolution's two size classes)
+    int class_side;
+    int* toff_big;            // out: n tiles per grain of side > class_side, may be null
     int* toff_one;            // out: tile offsets with one tile per grain, may be null
     int* box_copy;            // out: copy of box (6 per grain), may be null
     long long* off_copy;      // out: copy of off, may be null

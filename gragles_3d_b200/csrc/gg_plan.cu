@@ -18,11 +18,11 @@ constexpr long long kAlign = 32;  // elements; 256 B for FP64, 128 B for FP32
 
 struct Counts {
     long long vox, spec, tot;
-    int tn, ts, t1;
+    int tn, ts, t1, tb;
 };
 
 __device__ __forceinline__ Counts add(const Counts& a, const Counts& b) {
-    return Counts{a.vox + b.vox, a.spec + b.spec, a.tot + b.tot, a.tn + b.tn, a.ts + b.ts, a.t1 + b.t1};
+    return Counts{a.vox + b.vox, a.spec + b.spec, a.tot + b.tot, a.tn + b.tn, a.ts + b.ts, a.t1 + b.t1, a.tb + b.tb};
 }
 
 __device__ __forceinline__ Counts shfl_up(const Counts& c, int o) {
@@ -33,11 +33,12 @@ __device__ __forceinline__ Counts shfl_up(const Counts& c, int o) {
     r.tn = __shfl_up_sync(0xffffffffu, c.tn, o);
     r.ts = __shfl_up_sync(0xffffffffu, c.ts, o);
     r.t1 = __shfl_up_sync(0xffffffffu, c.t1, o);
+    r.tb = __shfl_up_sync(0xffffffffu, c.tb, o);
     return r;
 }
 
 __device__ __forceinline__ Counts grain_counts(const PlanArgs& a, int g) {
-    Counts c{0, 0, 0, 0, 0, 0};
+    Counts c{0, 0, 0, 0, 0, 0, 0};
     if (g < 1 || g > a.G || !a.present[g] || (a.only_existing && !a.exists[g])) return c;
     const Box b = load_box(a.box + 6 * g);
     const long long n = b.nx();
@@ -47,9 +48,11 @@ __device__ __forceinline__ Counts grain_counts(const PlanArgs& a, int g) {
     c.spec = (sp + kAlign - 1) / kAlign * kAlign;
     c.tot = v;
     c.tn = (int)n;
-    c.ts = a.row_tile > 0 ? (int)((n * n + a.row_tile - 1) / a.row_tile)
+    const bool big = a.class_side > 0 && n > a.class_side;
+    c.ts = a.row_tile > 0 ? (big ? 0 : (int)((n * n + a.row_tile - 1) / a.row_tile))
                           : (a.slab > 0 ? (int)((n + a.slab - 1) / a.slab) : 0);
     c.t1 = 1;
+    c.tb = big ? (int)n : 0;
     return c;
 }
 
@@ -58,7 +61,7 @@ __global__ void __launch_bounds__(kPlanThreads) plan_kernel(PlanArgs a) {
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const int per = (a.G + kPlanThreads) / kPlanThreads;  // grains 0..G
     const int g0 = threadIdx.x * per, g1 = min(a.G + 1, g0 + per);
-    Counts mine{0, 0, 0, 0, 0, 0};
+    Counts mine{0, 0, 0, 0, 0, 0, 0};
     for (int g = g0; g < g1; g++) mine = add(mine, grain_counts(a, g));
     // block exclusive scan of `mine`
     Counts incl = mine;
@@ -80,9 +83,9 @@ __global__ void __launch_bounds__(kPlanThreads) plan_kernel(PlanArgs a) {
         warp_tot[lane] = wi;  // inclusive over warps
     }
     __syncthreads();
-    Counts run = warp > 0 ? warp_tot[warp - 1] : Counts{0, 0, 0, 0, 0, 0};
+    Counts run = warp > 0 ? warp_tot[warp - 1] : Counts{0, 0, 0, 0, 0, 0, 0};
     const Counts excl_in_warp = Counts{incl.vox - mine.vox, incl.spec - mine.spec, incl.tot - mine.tot,
-                                       incl.tn - mine.tn, incl.ts - mine.ts, incl.t1 - mine.t1};
+                                       incl.tn - mine.tn, incl.ts - mine.ts, incl.t1 - mine.t1, incl.tb - mine.tb};
     run = add(run, excl_in_warp);
     for (int g = g0; g < g1; g++) {
         const Counts c = grain_counts(a, g);
@@ -91,6 +94,7 @@ __global__ void __launch_bounds__(kPlanThreads) plan_kernel(PlanArgs a) {
         if (a.toff_n) a.toff_n[g] = run.tn;
         if (a.toff_slab) a.toff_slab[g] = run.ts;
         if (a.toff_one) a.toff_one[g] = run.t1;
+        if (a.toff_big) a.toff_big[g] = run.tb;
         if (a.box_copy) {
 #pragma unroll
             for (int q = 0; q < 6; q++) a.box_copy[6 * g + q] = a.box[6 * g + q];
@@ -107,6 +111,7 @@ __global__ void __launch_bounds__(kPlanThreads) plan_kernel(PlanArgs a) {
         if (a.toff_n) a.toff_n[a.G + 1] = over ? 0 : T.tn;
         if (a.toff_slab) a.toff_slab[a.G + 1] = over ? 0 : T.ts;
         if (a.toff_one) a.toff_one[a.G + 1] = over ? 0 : T.t1;
+        if (a.toff_big) a.toff_big[a.G + 1] = over ? 0 : T.tb;
         if (a.total_voxels) *a.total_voxels = T.tot;
     }
 }

@@ -142,6 +142,57 @@ def laguerre(N: int, n_grains: int, seed: int, sigma: float = 0.3) -> Microstruc
                           np.zeros(n_grains), pts)
 
 
+# Settings the reference turns the .uds stored-energy column into m_StoredElasticEnergy
+# with (box.cpp:232-233): DislocEnPerM * column / HAGB_Energy * Physical_Domain_Size.
+DISLOC_EN_PER_M, HAGB_ENERGY, PHYSICAL_DOMAIN_SIZE = 2.5e-10, 1.0, 2.52e-4
+
+
+def stored_energy_of(column: np.ndarray) -> np.ndarray:
+    """m_StoredElasticEnergy of each grain from its .uds column (box.cpp:232-233)."""
+    return DISLOC_EN_PER_M * np.asarray(column, np.float64) / HAGB_ENERGY * PHYSICAL_DOMAIN_SIZE
+
+
+def lognormal_stored_energy(ms: Microstructure, seed: int, sigma: float = 0.5, scale: float = 0.1) -> None:
+    """Per-grain stored elastic energy scale * X, X ~ LogNormal(0, sigma), in units of the
+    high-angle boundary energy (m_StoredElasticEnergy = scale * X * HAGB_Energy), written
+    into the .uds column that the reference scales by DislocEnPerM / HAGB_Energy *
+    Physical_Domain_Size (box.cpp:232-233)."""
+    x = np.exp(sigma * normal(seed, ms.n_grains))
+    ms.stored_energy[:] = scale * x * HAGB_ENERGY * HAGB_ENERGY / (DISLOC_EN_PER_M * PHYSICAL_DOMAIN_SIZE)
+
+
+def with_nuclei(ms: Microstructure, seed: int, fraction: float = 0.05, rmin: float = 2.0,
+                rmax: float = 3.0) -> Microstructure:
+    """The microstructure plus round(fraction * G) spherical nuclei (radius uniform in
+    [rmin, rmax] voxels, centres uniform in the domain, uniformly random orientations,
+    zero stored energy) appended as grains G + 1, G + 2, ...: every voxel whose centre lies
+    within a nucleus's radius takes its ID (later nuclei over earlier ones).  A parent grain
+    the nuclei cover completely owns no voxel and is skipped by the reader."""
+    N, G = ms.n, ms.n_grains
+    K = int(round(fraction * G))
+    centres = uniform01(seed, 3 * K).reshape(K, 3) * N
+    radii = rmin + (rmax - rmin) * uniform01(seed + 1, K)
+    labels = ms.labels.copy()
+    for k in range(K):
+        c, r = centres[k], radii[k]
+        lo = np.maximum(np.floor(c - r - 0.5).astype(int), 0)
+        hi = np.minimum(np.ceil(c + r + 0.5).astype(int), N)
+        z, y, x = np.meshgrid(np.arange(lo[2], hi[2]), np.arange(lo[1], hi[1]), np.arange(lo[0], hi[0]),
+                              indexing="ij")
+        inside = (x + 0.5 - c[0]) ** 2 + (y + 0.5 - c[1]) ** 2 + (z + 0.5 - c[2]) ** 2 <= r * r
+        labels[z[inside], y[inside], x[inside]] = G + 1 + k
+    return Microstructure(labels, np.concatenate([ms.euler, _uniform_orientations(seed + 2, K)]),
+                          np.concatenate([ms.stored_energy, np.zeros(K)]), np.concatenate([ms.seeds, centres]))
+
+
+def c4(N: int = 384, n_grains: int = 100000, seed: int = 1004) -> Microstructure:
+    """The stored-energy configuration: Voronoi grains with lognormal stored energy
+    (sigma 0.5, 0.1 of the boundary energy) plus 5% nuclei of radius 2-3 voxels with none."""
+    ms = voronoi(N, n_grains, seed)
+    lognormal_stored_energy(ms, seed + 3)
+    return with_nuclei(ms, seed + 4)
+
+
 def write_mode4(ms: Microstructure, directory: str, raw_name: str = "Container.raw",
                 uds_name: str = "Microstructure.uds", id_offset: int = 1) -> tuple[str, str]:
     """Write ``Container.raw`` + ``.uds`` in the layout grainhdl.cpp:404-578 reads."""
@@ -230,3 +281,51 @@ def write_faces(directory: str, records: np.ndarray, loop: int) -> str:
     path = os.path.join(directory, f"Faces_{int(loop)}.bin")
     np.ascontiguousarray(records).tofile(path)
     return path
+
+
+def _cxx(v) -> str:
+    """A value as the reference's ostream prints it (default precision: %g, 6 digits)."""
+    if isinstance(v, (int, np.integer)):
+        return str(int(v))
+    return "%g" % float(v)
+
+
+def write_texture_text(directory: str, rows: list, loop: int) -> str:
+    """Texture_<loop>.ori as save_Texture writes it without NeighborTracking (grainhdl.cpp:
+    776-805): tab-separated rows of GrainHandler.texture_text()."""
+    path = os.path.join(directory, f"Texture_{int(loop)}.ori")
+    with open(path, "w") as f:
+        for r in rows:
+            f.write("\t".join(_cxx(v) for v in r) + "\n")
+    return path
+
+
+def write_network(directory: str, loop: int, rows: list, labels: np.ndarray, see=None) -> list:
+    """The saved network of saveNetworkAsVoxelContainer (grainhdl.cpp:1074-1154):
+    Microstructure_<loop>.uds (rows of GrainHandler.network_rows(), no header, as the
+    reference writes it), the voxel container, and ContainerVolumeEnergy_size_<N>_t_<loop>.raw.
+    The energy file holds, for every voxel in [z][y][x] order whose grain is in the network
+    (ID 0 = the boundary grain, stored energy 0), that grain's stored elastic energy as a
+    double; with `see` None (UseStoredElasticEnergy off) it is empty.  The reference opens
+    this file but writes the values to the container's file handle after closing it
+    (grainhdl.cpp:1124-1147); here they go to the file it opened."""
+    lab = np.ascontiguousarray(labels, dtype=np.uint32)
+    n = lab.shape[0]
+    uds = os.path.join(directory, f"Microstructure_{int(loop)}.uds")
+    with open(uds, "w") as f:
+        for r in rows:
+            f.write("\t".join(_cxx(v) for v in r) + "\n")
+    cont = write_container(directory, lab, loop)
+    energy = os.path.join(directory, f"ContainerVolumeEnergy_size_{n}_t_{int(loop)}.raw")
+    if see is None:
+        open(energy, "wb").close()
+    else:
+        in_network = np.zeros(len(see) + 1, bool)
+        in_network[0] = True  # getGrainByID(0) is the boundary grain
+        for r in rows:
+            in_network[int(r[0])] = True
+        energy_of = np.zeros(len(see) + 1)
+        energy_of[1:] = np.asarray(see, np.float64)
+        ids = lab.ravel()
+        np.ascontiguousarray(energy_of[ids[in_network[ids]]], "<f8").tofile(energy)
+    return [uds, cont, energy]

@@ -93,6 +93,18 @@ int gg_load_state(gg_ctx* ctx, const uint32_t* labels, const int32_t* extents, c
 int gg_set_lists(gg_ctx* ctx, const int64_t* offsets, const uint32_t* ids);
 /* The same membership (inclusive box overlap) in grain-ID order, built on the device. */
 int gg_default_lists(gg_ctx* ctx);
+/* The lists in the reference's own order: find_neighbors' R-tree over the loaded boxes
+ * (grainhdl.cpp:1029-1054, box.cpp:2871-2887; RTree.h: quadratic split, 8/4 branches
+ * per node, spherical volumes in float), built on the host from the device's initial
+ * boxes and uploaded as gg_set_lists does.  A run from these lists is bit-exact with the
+ * reference's from its first comparison on. */
+int gg_rtree_lists(gg_ctx* ctx);
+/* The same R-tree search on caller boxes, without a context (host only): boxes =
+ * (n_grains + 1) x 6 in box order, valid[g] != 0 for the grains inserted.  Writes
+ * offsets[n_grains + 2] (CSR by grain ID) and up to cap IDs; returns the total ID count
+ * or a negative GG_ERR_*. */
+int64_t gg_rtree_lists_from_boxes(int32_t n_grains, const int32_t* boxes, const uint8_t* valid, int64_t* offsets,
+                                  uint32_t* ids, int64_t cap);
 
 /* One loop iteration of grainhdl::run_sim (grainhdl.cpp:837-917).  With grid_coarsening
  * set, the iteration starts with grainhdl::gridCoarsement (grainhdl.cpp:1446-1498): when

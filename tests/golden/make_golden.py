@@ -18,6 +18,9 @@ FP64 device path is pinned on at full length.
 The "analysis" case reruns the correction case on one thread with the reference's
 analysis outputs on: Texture and Faces records every loop and the voxel container.
 
+The "text" case keeps the reference's text outputs: Texture_<loop>.ori and the saved
+network's Microstructure_<loop>.uds.
+
 The "wall" case keeps one grain's field where it meets the domain wall (from the
 oracle restatement): the evidence that the reference's hull volume jumps when one
 voxel within 1e-8 of zero changes sign.
@@ -179,6 +182,38 @@ def make_analysis(N=32, G=30, border=5, seed=2032, steps=8, plot_every=2):
     print("analysis ok", {k: v.shape for k, v in out.items() if hasattr(v, "shape")})
 
 
+def make_text(N=32, G=30, border=5, seed=2032, steps=6, plot_every=2):
+    """The reference's text outputs on the isotropic path (bit-exact on the device): the
+    correction case's microstructure and stored energies, NeighborTracking off so that
+    save_Texture writes Texture_<loop>.ori every loop (grainhdl.cpp:776-805), and
+    saveNetworkAsVoxelContainer every plot_every loops (Microstructure_<loop>.uds and the
+    container, grainhdl.cpp:1074-1123).  Stored energy stays off in the loop, so the
+    reference's ContainerVolumeEnergy loop writes nothing."""
+    ms = msgen.voronoi(N, G, seed=seed)
+    textured(ms, seed)
+    with tempfile.TemporaryDirectory() as d:
+        msgen.write_mode4(ms, d)
+        msgen.write_parameters(os.path.join(d, "parameters.xml"), n_grains=G, border=border, steps=steps,
+                               analysis_every=1, neighbor_tracking=False, plot_interval=plot_every)
+        res, _ = refdump.run_case(d, threads=1)
+        out = {"N": N, "G": G, "border": border, "seed": seed, "steps": steps, "plot_every": plot_every,
+               "euler": ms.euler.copy(), "uds_stored_energy": ms.stored_energy.copy()}
+        out["init_list_off"], out["init_list_ids"] = ragged(res["init_list"], G)
+        ori, uds, uds_loops = [], [], []
+        for loop in range(1, steps + 1):
+            with open(os.path.join(d, f"Texture_{loop}.ori")) as f:
+                ori.append(f.read())
+            path = os.path.join(d, f"Microstructure_{loop}.uds")
+            if os.path.exists(path):
+                with open(path) as f:
+                    uds.append(f.read())
+                uds_loops.append(loop)
+                assert os.path.getsize(os.path.join(d, f"ContainerVolumeEnergy_size_{N}_t_{loop}.raw")) == 0
+    out.update(ori=np.array(ori), uds=np.array(uds), uds_loops=np.array(uds_loops))
+    np.savez_compressed(os.path.join(HERE, "text.npz"), **out)
+    print("text ok", len(ori), uds_loops)
+
+
 def make_wall(N=64, G=600, border=10, seed=2064, loops=19, gid=159):
     """One grain's field where it meets the domain wall, from the oracle restatement (bit-
     exact with the reference on the device path's parity cases): Voronoi 64^3 / 600 grains,
@@ -218,5 +253,7 @@ if __name__ == "__main__":
             make(name, *args)
     if not only or "analysis" in only:
         make_analysis()
+    if not only or "text" in only:
+        make_text()
     if not only or "wall" in only:
         make_wall()

@@ -80,3 +80,37 @@ def test_faces_without_the_correction(gpu):
     f = gh.faces()
     assert len(f) > 0 and np.all(f["grainA"] > f["grainB"]) and np.all(f["area"] > 0)
     gh.close()
+
+
+def test_text_texture_and_saved_network_match_reference(gpu, tmp_path):
+    """Texture_<loop>.ori and the saved network's Microstructure_<loop>.uds written from the
+    device state equal the compiled reference's own files byte for byte (tests/golden/
+    text.npz: the isotropic path, bit-exact), and the volume-energy file holds each
+    voxel's grain's stored energy."""
+    d = dict(np.load(os.path.join(os.path.dirname(__file__), "golden", "text.npz")))
+    N, G, border = int(d["N"]), int(d["G"]), int(d["border"])
+    ms = msgen.voronoi(N, G, seed=int(d["seed"]))
+    ext, counts = ms.grain_extents()
+    gh = gpu.GrainHandler(N, border, 0.2, G, precision=gpu.PRECISION_FP64, keep_elements=True)
+    gh.load(ms.labels, ext, counts)
+    gh.set_lists(d["init_list_off"], d["init_list_ids"])
+    gh.set_orientations(d["euler"])
+    see = 2.5e-10 * d["uds_stored_energy"] / 1.0 * 2.52e-4  # box.cpp:232-233
+    gh.set_stored_energy(see)
+    gh.step()  # loop 0 writes no texture (grainhdl.cpp:751)
+    uds_loops = d["uds_loops"].tolist()
+    for loop in range(1, int(d["steps"]) + 1):
+        gh.step()
+        path = msgen.write_texture_text(str(tmp_path), gh.texture_text(), loop)
+        with open(path) as f:
+            assert f.read() == str(d["ori"][loop - 1]), f"Texture_{loop}.ori"
+        if loop in uds_loops:
+            labels = gh.voxel_container()
+            uds, _, energy = msgen.write_network(str(tmp_path), loop, gh.network_rows(), labels, see=see)
+            with open(uds) as f:
+                assert f.read() == str(d["uds"][uds_loops.index(loop)]), f"Microstructure_{loop}.uds"
+            e = np.fromfile(energy, "<f8")
+            assert e.size == labels.size  # every voxel belongs to a grain or to the boundary grain
+            want = np.where(labels.ravel() > 0, np.concatenate([[0.0], see])[labels.ravel()], 0.0)
+            assert np.array_equal(e, want)
+    gh.close()

@@ -10,6 +10,8 @@ import tempfile
 import numpy as np
 import pytest
 
+from gragles_3d_b200 import microstructure as msgen
+
 ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 
 
@@ -180,3 +182,86 @@ def test_ctypes_structs_match_the_c_header(tmp_path):
         assert got[(cname, "size")] == C.sizeof(py), cname
         for field, _ in py._fields_:
             assert got[(cname, field)] == getattr(py, field).offset, (cname, field)
+
+
+def test_stored_energy_and_nuclei_generator():
+    """The stored-energy configuration's generator: lognormal stored energy of 0.1 boundary
+    energy (the .uds column scaled back through box.cpp:232-233), then 5% nuclei of radius
+    2-3 voxels appended as new IDs with none; deterministic for a seed."""
+    a, b = msgen.c4(48, 200, seed=5), msgen.c4(48, 200, seed=5)
+    assert np.array_equal(a.labels, b.labels) and np.array_equal(a.stored_energy, b.stored_energy)
+    G, K = 200, 10
+    assert a.n_grains == G + K and a.labels.max() == G + K
+    see = msgen.stored_energy_of(a.stored_energy)
+    assert np.all(see[G:] == 0) and np.all(see[:G] > 0)
+    assert 0.05 < np.median(see[:G]) < 0.2  # 0.1 * LogNormal(0, 0.5): median 0.1
+    _, counts = a.grain_extents()
+    vol = 4.0 / 3.0 * np.pi
+    assert np.all(counts[G:] >= 0.5 * vol * 2 ** 3) and np.all(counts[G:] <= 1.5 * vol * 3 ** 3)
+
+
+def test_text_writers_print_like_the_reference_ostream(tmp_path):
+    """Texture_<loop>.ori and Microstructure_<loop>.uds rows: tab-separated, integers as
+    they are, doubles as the reference's ostream prints them by default (6 significant
+    digits, %g)."""
+    rows = [(3, 7, 1, 0.0195446123, 0.5, 0.0, 0.0, 0.0, 12.0, 6.0, 1.0, 8.399876e-09, 0.158441, 1e6, 2.0)]
+    path = msgen.write_texture_text(str(tmp_path), rows, 4)
+    assert os.path.basename(path) == "Texture_4.ori"
+    with open(path) as f:
+        assert f.read() == "3\t7\t1\t0.0195446\t0.5\t0\t0\t0\t12\t6\t1\t8.39988e-09\t0.158441\t1e+06\t2\n"
+    labels = np.array([[[1, 2], [0, 2]], [[1, 1], [2, 2]]], np.uint32)
+    out = msgen.write_network(str(tmp_path), 4, [(1, 0.5, 0.5, 0.5, 0.1, 0.2, 0.3, 0, 2, 0, 2, 0, 2, 0.125, 3.0),
+                                                   (2, 0.5, 0.5, 0.5, 0.1, 0.2, 0.3, 0, 2, 0, 2, 0, 2, 0.25, 5.0)],
+                              labels, see=np.array([3.0, 5.0]))
+    assert [os.path.basename(p) for p in out] == ["Microstructure_4.uds", "Container_size_2_t_4.raw",
+                                                  "ContainerVolumeEnergy_size_2_t_4.raw"]
+    e = np.fromfile(out[2], "<f8")
+    assert np.array_equal(e, np.array([3.0, 5.0, 0.0, 5.0, 3.0, 3.0, 5.0, 5.0]))
+
+
+def _resize_to_cube(b, M):
+    """DimensionalBuffer::resizeToCube (dimensionalBuffer.h:139-219)."""
+    x0, x1, y0, y1, z0, z1 = b
+    w, h, d = x1 - x0, y1 - y0, z1 - z0
+    if w == h == d:
+        return [x0, x1, y0, y1, z0, z1]
+    ref = max(w, h, d)
+    if ref > w:
+        x0, x1 = x0 - (ref - w) // 2, x1 + (ref - w) // 2 + (ref - w) % 2
+    if ref > h:
+        y0, y1 = y0 - (ref - h) // 2, y1 + (ref - h) // 2 + (ref - h) % 2
+    if ref > d:
+        z0, z1 = z0 - (ref - d) // 2, z1 + (ref - d) // 2 + (ref - d) % 2
+    out = []
+    for lo, hi in ((x0, x1), (y0, y1), (z0, z1)):
+        if lo < 0:
+            lo, hi = 0, hi - lo
+        elif hi > M - 1:
+            lo, hi = lo + (M - 1 - hi), M - 1
+        out += [lo, hi]
+    return out
+
+
+@pytest.mark.parametrize("name", ["tiny", "vanish", "correction", "c1", "coarsen"])
+def test_rtree_lists_follow_the_reference_order(name):
+    """find_neighbors' R-tree (grainhdl.cpp:1029-1054) restated on the host gives the
+    reference's own initial comparison lists, member for member and in order, from the
+    mode-4 constructor's boxes (box.cpp:239-304, then resizeToCube)."""
+    import gragles_3d_b200 as gg
+
+    d = dict(np.load(os.path.join(ROOT, "tests", "golden", f"{name}.npz")))
+    N, G, gb = int(d["N"]), int(d["G"]), int(d["border"])
+    M = N + 2 * gb
+    ext, counts = msgen.voronoi(N, G, seed=int(d["seed"])).grain_extents()
+    boxes = np.zeros((G + 1, 6), np.int32)
+    valid = np.zeros(G + 1, np.uint8)
+    for g in range(1, G + 1):
+        if counts[g - 1] <= 0:
+            continue
+        x0, x1, y0, y1, z0, z1 = (int(v) for v in ext[g - 1])
+        x1, y1, z1 = min(x1 + 2 * gb, M), min(y1 + 2 * gb, M), min(z1 + 2 * gb, M)
+        boxes[g] = _resize_to_cube([max(x0, 0), x1, max(y0, 0), y1, max(z0, 0), z1], M)
+        valid[g] = 1
+    off, ids = gg.rtree_lists(boxes, valid)
+    assert np.array_equal(off, d["init_list_off"])
+    assert np.array_equal(ids, d["init_list_ids"])
