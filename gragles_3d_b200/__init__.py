@@ -34,6 +34,7 @@ EXPORTED = [
     "gg_get_idlocal", "gg_grain_count", "gg_loop", "gg_convolve_boxes_f64", "gg_convolve_boxes_mixed",
     "gg_convolve_boxes_f64_noalloc", "gg_set_orientations", "gg_set_stored_energy", "gg_get_elements",
     "gg_voxel_container", "gg_get_faces", "gg_domain_size", "gg_rtree_lists", "gg_rtree_lists_from_boxes",
+    "gg_launch_config",
 ]
 
 
@@ -51,6 +52,7 @@ class Params(C.Structure):
         ("unique_gb_energies", C.c_int32), ("mobility_model", C.c_int32), ("use_stored_energy", C.c_int32),
         ("triple_line_drag", C.c_double), ("hull_capacity", C.c_int32), ("keep_elements", C.c_int32),
         ("grid_coarsening", C.c_int32), ("points_per_grain", C.c_int32), ("coarsening_gradient", C.c_double),
+        ("autotune", C.c_int32),
     ]
 
 
@@ -86,6 +88,7 @@ def load_library(path: str = LIB_PATH):
     L.gg_set_lists.argtypes = [vp, vp, vp]
     L.gg_default_lists.argtypes = [vp]
     L.gg_rtree_lists.argtypes = [vp]
+    L.gg_launch_config.argtypes = [vp, vp]
     L.gg_rtree_lists_from_boxes.argtypes = [i32, vp, vp, vp, vp, i64]
     L.gg_rtree_lists_from_boxes.restype = i64
     L.gg_step.argtypes = [vp, C.POINTER(StepStats)]
@@ -183,7 +186,7 @@ class GrainHandler:
                  device: int = 0, correction: bool = False, unique_energies: bool = True,
                  mobility_model: bool = False, stored_energy: bool = False, triple_line_drag: float = 0.0,
                  hull_capacity: int = 0, keep_elements: bool = False, grid_coarsening: bool = False,
-                 points_per_grain: int = 0, coarsening_gradient: float = 0.0):
+                 points_per_grain: int = 0, coarsening_gradient: float = 0.0, autotune: bool = False):
         L = load_library()
         self.G = int(n_grains)
         self.N = int(domain_size)
@@ -193,7 +196,7 @@ class GrainHandler:
         p = Params(domain_size, border, float(time_step), n_grains, precision, int(not correction), list_capacity,
                    pool_voxels, device, int(unique_energies), int(mobility_model), int(stored_energy),
                    float(triple_line_drag), hull_capacity, int(keep_elements), int(grid_coarsening),
-                   int(points_per_grain), float(coarsening_gradient))
+                   int(points_per_grain), float(coarsening_gradient), int(autotune))
         self._euler = np.zeros((self.G, 3))
         self._see = np.zeros(self.G)
         h = C.c_void_p()
@@ -276,6 +279,13 @@ class GrainHandler:
     @property
     def loop(self) -> int:
         return self._check(load_library().gg_loop(self._h))
+
+    def launch_config(self) -> tuple:
+        """(CTAs per SM of each stage's kernels, chosen): the stages are the convolution with
+        the correction, lists, comparison, level set and redistancing."""
+        m = np.zeros(5, np.int32)
+        done = self._check(load_library().gg_launch_config(self._h, _p(m)))
+        return tuple(int(v) for v in m), bool(done)
 
     @property
     def domain_size(self) -> int:

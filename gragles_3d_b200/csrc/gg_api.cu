@@ -104,6 +104,12 @@ struct gg_ctx {
     // grid coarsening (grainhdl::gridCoarsement): ngrains at the last coarsening, and
     // NumberOfPointsPerGrain
     int coarse_ref = 0, points_per_grain = 0;
+    // launch configuration: CTAs per SM of each stage's grid-stride kernels (convolution
+    // with the correction, lists, comparison, level set, redistancing), chosen by the
+    // autotuner when it is on
+    int mult[5] = {8, 8, 4, 8, 8};
+    int tune_next = -1;         // candidate the next tuning step runs, -1: not tuning
+    double tune_cost[5][8] = {};
     // element counts of the N-dependent tables' device buffers (reused when they fit)
     size_t tw_cap = 0, gt_cap = 0, circ_cap = 0, bmat_cap = 0;
     size_t tw_off_cap = 0, g_off_cap = 0, c_off_cap = 0, boff_cap = 0;
@@ -111,6 +117,15 @@ struct gg_ctx {
 };
 
 namespace {
+
+// The autotuner's candidates: CTAs per SM for the grid-stride stage kernels.  Every stage
+// kernel walks its tiles grid-stride and computes each grain's results inside one CTA, so
+// the grid changes only the speed, never the results.
+constexpr int kTuneCand[] = {2, 4, 8, 16, 32};
+constexpr int kNumTune = 5;
+enum Stage { ST_CONV = 0, ST_LISTS, ST_COMPARE, ST_LEVELSET, ST_REDIST };
+
+int stage_grid(const gg_ctx* c, int s);
 
 int fail(gg_ctx* c, int code, const char* fmt, ...) {
     char buf[512];
@@ -316,7 +331,7 @@ int redistance(gg_ctx* ctx, int in_a, int out_a, const int* toff, int side) {
     r.in = arena<T>(ctx, in_a);
     r.out = arena<T>(ctx, out_a);
     r.err = ctx->d_err;
-    launch_redistance<T>(r, ctx->grid, side, ctx->stream);
+    launch_redistance<T>(r, stage_grid(ctx, ST_REDIST), side, ctx->stream);
     ctx->launches += 2;
     CK(cudaGetLastError());
     return GG_OK;
@@ -379,7 +394,7 @@ int correct_convolution(gg_ctx* ctx) {
     c.el = ctx->el;
     c.ph = physics(ctx);
     c.err = ctx->d_err;
-    launch_correction<T>(c, ctx->grid, ctx->stream);
+    launch_correction<T>(c, stage_grid(ctx, ST_CONV), ctx->stream);
     ctx->launches += 1;
     CK(cudaGetLastError());
     return GG_OK;
@@ -419,7 +434,7 @@ int stage_convolution_t(gg_ctx* ctx) {
         a.tw_off = ctx->d_tw_off;
         a.gtab = ctx->d_gtab;
         a.g_off = ctx->d_g_off;
-        launch_conv_f64(a, ctx->grid, conv_f64_smem_bytes(ctx->side_max), ctx->stream);
+        launch_conv_f64(a, stage_grid(ctx, ST_CONV), conv_f64_smem_bytes(ctx->side_max), ctx->stream);
         ctx->launches += 3;
     } else {
         // two size classes in one step: sides up to kUmmaMaxSide on the tensor cores, larger
@@ -475,7 +490,7 @@ int stage_update_lists_t(gg_ctx* ctx) {
     a.n_cmp = ctx->d_ncmp;
     a.list_cap = ctx->list_cap;
     a.err = ctx->d_err;
-    launch_update_lists(a, ctx->grid, ctx->stream);
+    launch_update_lists(a, stage_grid(ctx, ST_LISTS), ctx->stream);
     // m_secondOrderNeighbours = m_comparisonList (box.cpp:895), once every list is rebuilt
     ListCopyArgs sl{};
     sl.G = ctx->G;
@@ -485,7 +500,7 @@ int stage_update_lists_t(gg_ctx* ctx) {
     sl.son = ctx->d_son;
     sl.n_son = ctx->d_nson;
     sl.list_cap = ctx->list_cap;
-    launch_copy_lists(sl, ctx->grid, ctx->stream);
+    launch_copy_lists(sl, stage_grid(ctx, ST_LISTS), ctx->stream);
     ctx->launches += 2;
     CK(cudaGetLastError());
     return GG_OK;
@@ -556,7 +571,7 @@ int compare_t(gg_ctx* ctx, int in_a, int out_a, int set_comparison) {
     a.set_comparison = set_comparison;
     a.exists = ctx->d_exists;
     if (set_comparison) cudaEventRecord(ctx->ev[6], ctx->stream);
-    launch_compare<T>(a, ctx->num_sms * 4, ctx->stream);
+    launch_compare<T>(a, stage_grid(ctx, ST_COMPARE), ctx->stream);
     if (set_comparison) cudaEventRecord(ctx->ev[7], ctx->stream);
     ctx->launches += 1;
     CK(cudaGetLastError());
@@ -597,7 +612,7 @@ int level_set_t(gg_ctx* ctx, int p, int regrid) {
     a.err = ctx->d_err;
     a.regrid = regrid;
     if (ctx->elements) a.hull = ctx->hull;
-    launch_mc<T>(a, ctx->grid, ctx->side_max, ctx->stream);
+    launch_mc<T>(a, stage_grid(ctx, ST_LEVELSET), ctx->side_max, ctx->stream);
     ctx->launches += 1;
     CK(cudaGetLastError());
     if (ctx->elements) {  // computeSurfaceElements, box.cpp:1175-1180
@@ -733,6 +748,10 @@ int stage_redistancing_t(gg_ctx* ctx) {
 template <typename T>
 int step_t(gg_ctx* ctx, gg_step_stats* st) {
     const long long launches0 = ctx->launches;
+    // the autotuner: loops 1 .. kNumTune (loop 0 has no correction) each run one candidate
+    const bool tuning = ctx->tune_next >= 0 && ctx->loop >= 1;
+    if (tuning)
+        for (int s = 0; s < 5; s++) ctx->mult[s] = kTuneCand[ctx->tune_next];
     cudaEventRecord(ctx->ev[0], ctx->stream);
     int rc = stage_convolution_t<T>(ctx);
     if (rc) return rc;
@@ -748,6 +767,23 @@ int step_t(gg_ctx* ctx, gg_step_stats* st) {
     CK(cudaEventSynchronize(ctx->ev[5]));
     rc = check_err(ctx, "gg_step");
     if (rc) return rc;
+    if (tuning) {  // device time per voxel-update of each stage under this candidate
+        const double vox = (double)std::max(1LL, *ctx->h_total_vox);
+        for (int s = 0; s < 5; s++) {
+            float ms = 0;
+            cudaEventElapsedTime(&ms, ctx->ev[s], ctx->ev[s + 1]);
+            ctx->tune_cost[s][ctx->tune_next] = ms / vox;
+        }
+        if (++ctx->tune_next == kNumTune) {
+            for (int s = 0; s < 5; s++) {
+                int best = 0;
+                for (int c = 1; c < kNumTune; c++)
+                    if (ctx->tune_cost[s][c] < ctx->tune_cost[s][best]) best = c;
+                ctx->mult[s] = kTuneCand[best];
+            }
+            ctx->tune_next = -1;
+        }
+    }
     if (st) {
         st->loop = ctx->loop;
         st->grain_count = ctx->grain_count;
@@ -780,6 +816,10 @@ int voxel_container_t(gg_ctx* ctx, uint32_t* d_labels) {
     CK(cudaGetLastError());
     return GG_OK;
 }
+}  // namespace
+
+namespace {
+int stage_grid(const gg_ctx* c, int s) { return c->num_sms * c->mult[s]; }
 }  // namespace
 
 // ===================================================================================
@@ -877,6 +917,7 @@ int gg_create(const gg_params* params, gg_ctx** out) {
     ctx->points_per_grain = P.points_per_grain > 0 ? P.points_per_grain
                                                    : (int)(ctx->N / std::pow(ctx->G, 1 / 3.0) + 0.5);
     ctx->coarse_ref = ctx->G;
+    ctx->tune_next = P.autotune ? 0 : -1;
     *out = ctx;
 #undef CK_RET
     cudaError_t e = cudaSetDevice(P.device);
@@ -1030,7 +1071,7 @@ int gg_load_state(gg_ctx* ctx, const uint32_t* labels, const int32_t* extents, c
         CK(dalloc(&ctx->el.idx_key, (size_t)ctx->el.idx_cap * G1h));
         CK(dalloc(&ctx->el.idx_rng, (size_t)ctx->el.idx_cap * G1h));
         CK(dalloc(&ctx->el.idx_elem, (size_t)ctx->el.pair_cap * G1h));
-        ctx->elscr_ctas = ctx->num_sms * 8;
+        ctx->elscr_ctas = ctx->num_sms * 16;
         CK(dalloc(&ctx->d_elscr, elements_scratch_per_cta() * ctx->elscr_ctas));
         CK(cudaMemset(ctx->el.n_elem, 0, sizeof(int) * G1h));
         CK(cudaMemset(ctx->el.n_idx, 0, sizeof(int) * G1h));
@@ -1223,6 +1264,12 @@ int64_t gg_get_idlocal(gg_ctx* ctx, int32_t id, int32_t box[6], uint32_t* out, i
 
 int gg_grain_count(gg_ctx* ctx) { return ctx ? ctx->grain_count : GG_ERR_INVALID; }
 int gg_domain_size(gg_ctx* ctx) { return ctx ? ctx->N : GG_ERR_INVALID; }
+
+int gg_launch_config(gg_ctx* ctx, int32_t ctas_per_sm[5]) {
+    if (!ctx || !ctas_per_sm) return GG_ERR_INVALID;
+    for (int s = 0; s < 5; s++) ctas_per_sm[s] = ctx->mult[s];
+    return ctx->tune_next >= 0 ? 0 : 1;
+}
 int gg_loop(gg_ctx* ctx) { return ctx ? ctx->loop : GG_ERR_INVALID; }
 
 int gg_voxel_container(gg_ctx* ctx, uint32_t* labels) {

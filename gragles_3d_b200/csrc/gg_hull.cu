@@ -112,10 +112,17 @@ struct JHead {
     double pos[3];
 };
 
-// One CTA's global scratch: the junction IDs and the (mobility, energy) of every
-// misorientation job.  Neither is on a latency-critical path.
-constexpr size_t kJIdBytes = (size_t)kLMax * kJIds * 4;
-constexpr size_t kElemScratch = ((kJIdBytes + sizeof(double2) * kJobMax) + 255) & ~(size_t)255;
+// One CTA's global scratch: the junction IDs and heads, the (mobility, energy) of every
+// misorientation job, and the neighbour -> elements index under construction.  They are
+// used by the junction and table phases, mostly by one lane, and keeping them out of
+// shared memory lets several times more grains' warps share an SM.
+constexpr size_t kAlignUp(size_t b) { return (b + 255) & ~(size_t)255; }
+constexpr size_t kJIdBytes = kAlignUp((size_t)kLMax * kJIds * 4);
+constexpr size_t kJResBytes = kAlignUp(sizeof(double2) * kJobMax);
+constexpr size_t kJHeadBytes = kAlignUp(sizeof(JHead) * kLMax);
+constexpr size_t kIndexBytes = kAlignUp((size_t)kIHash * 4 + (size_t)kIHash * 2 + (size_t)kIdxMax * 4 * 4 +
+                                        (size_t)kPairMax * 2 * 2);
+constexpr size_t kElemScratch = kJIdBytes + kJResBytes + kJHeadBytes + kIndexBytes;
 
 struct ElemSmem {
     uint32_t lists[kLMax][8];
@@ -124,18 +131,19 @@ struct ElemSmem {
     int fill[kLMax];    // barycenters placed so far; then the list's first misorientation job
     int next_key[kLMax];
     double energy[kLMax], mobility[kLMax];
-    JHead jh[kLMax];    // working junctions
     int qlist[kLMax], hlist[kLMax];
     int lslot[kLHash];  // list hash: index into lists, -1 empty
+    // in this CTA's global scratch:
+    JHead* jh;                   // kLMax working junctions
     // neighbour ID -> elements index under construction
-    unsigned ikey[kIHash];
-    short iden[kIHash];          // dense ID index of the slot
-    uint32_t dkey[kIdxMax];
-    int dcnt[kIdxMax], dlast[kIdxMax], doff[kIdxMax];
-    unsigned short pe[kPairMax]; // (element, dense ID) pairs in search order
-    unsigned short pd[kPairMax];
-    uint32_t* jids;              // kLMax x kJIds junction IDs (global scratch)
-    double2* jres;               // kJobMax (mobility, energy) (global scratch)
+    unsigned* ikey;              // kIHash
+    short* iden;                 // kIHash: dense ID index of the slot
+    uint32_t* dkey;              // kIdxMax
+    int *dcnt, *dlast, *doff;    // kIdxMax each
+    unsigned short* pe;          // kPairMax (element, dense ID) pairs in search order
+    unsigned short* pd;
+    uint32_t* jids;              // kLMax x kJIds junction IDs
+    double2* jres;               // kJobMax (mobility, energy)
     int nl, nq, nh, nj, ne, nch, nd, np;
 };
 
@@ -331,6 +339,19 @@ __global__ void __launch_bounds__(32) elements_kernel(ElementArgs a) {
         unsigned char* scr = a.scratch + (long long)blockIdx.x * kElemScratch;
         S.jids = reinterpret_cast<uint32_t*>(scr);
         S.jres = reinterpret_cast<double2*>(scr + kJIdBytes);
+        S.jh = reinterpret_cast<JHead*>(scr + kJIdBytes + kJResBytes);
+        unsigned char* ix = scr + kJIdBytes + kJResBytes + kJHeadBytes;
+        S.ikey = reinterpret_cast<unsigned*>(ix);
+        ix += (size_t)kIHash * 4;
+        S.iden = reinterpret_cast<short*>(ix);
+        ix += (size_t)kIHash * 2;
+        S.dkey = reinterpret_cast<uint32_t*>(ix);
+        S.dcnt = reinterpret_cast<int*>(ix + (size_t)kIdxMax * 4);
+        S.dlast = reinterpret_cast<int*>(ix + (size_t)kIdxMax * 8);
+        S.doff = reinterpret_cast<int*>(ix + (size_t)kIdxMax * 12);
+        ix += (size_t)kIdxMax * 16;
+        S.pe = reinterpret_cast<unsigned short*>(ix);
+        S.pd = reinterpret_cast<unsigned short*>(ix + (size_t)kPairMax * 2);
     }
     __syncwarp();
     for (TileWalk w(a.toff, a.G, blockIdx.x, gridDim.x); w.valid(); w.next()) {

@@ -59,6 +59,9 @@ typedef struct {
     int32_t points_per_grain;   /* NumberOfPointsPerGrain (0 = the mode-4 reader's rule,
                                    (int)(N / n_grains^(1/3) + 0.5), grainhdl.cpp:221) */
     double coarsening_gradient; /* GridCoarsementGradient (0 = 0.95, the Settings default) */
+    int32_t autotune;           /* 1: loops 1..5 each time one launch configuration (2, 4, 8, 16 and 32
+                                   CTAs per SM for the grid-stride kernels of every stage) and the
+                                   rest run each stage with its fastest; results do not depend on it */
 } gg_params;
 
 /* Per-step report (the reference prints the same stage times, grainhdl.cpp:920-933). */
@@ -117,6 +120,12 @@ int gg_step(gg_ctx* ctx, gg_step_stats* stats);
 /* grainhdl::realDomainSize: the current grid size N (smaller than the initial one after
  * a grid coarsening). */
 int gg_domain_size(gg_ctx* ctx);
+
+/* The launch configuration in use: CTAs per SM of the grid-stride kernels of each stage
+ * (convolution with the correction, lists, comparison, level set, redistancing).  No
+ * counterpart in the reference (its parallel loops are OpenMP over grains).  Returns 1
+ * once the autotuner has chosen them (or when it is off), 0 while it is still trying. */
+int gg_launch_config(gg_ctx* ctx, int32_t ctas_per_sm[5]);
 
 /* The stages of one iteration, for stage-level testing, in the order gg_step runs
  * them.  Each stands in for the grainhdl method named. */

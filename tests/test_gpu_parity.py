@@ -229,8 +229,9 @@ def test_voxel_container_matches_oracle(gpu, oracle, precision):
 
 def test_c1_fp64_matches_reference_golden(gpu):
     """The plain-method configuration at full length: 64^3, 200 Voronoi grains, 10-voxel
-    border, 50 timesteps (51 loop iterations), started from the reference's own R-tree
-    comparison lists (tests/golden/c1.npz, written by the compiled reference).  Every
+    border, 50 timesteps (51 loop iterations), started from the library's R-tree lists
+    (gg_rtree_lists), which must equal the reference's own (tests/golden/c1.npz, written by
+    the compiled reference).  Every
     loop: existence, boxes, volumes and surfaces bit for bit, hull neighbours in
     first-seen order, and the grain-count trajectory; the comparison lists of the last
     loop in order."""
@@ -240,7 +241,11 @@ def test_c1_fp64_matches_reference_golden(gpu):
     ext, counts = ms.grain_extents()
     gh = gpu.GrainHandler(N, border, 0.2, G, precision=gpu.PRECISION_FP64)
     gh.load(ms.labels, ext, counts)
-    gh.set_lists(d["init_list_off"], d["init_list_ids"])
+    # the library's own R-tree lists are the reference's initial lists, in order
+    gh.rtree_lists()
+    for g in range(1, G + 1):
+        want = d["init_list_ids"][d["init_list_off"][g]:d["init_list_off"][g + 1]]
+        assert np.array_equal(gh.comparison_list(g), want), f"grain {g}: initial list"
     nb_base = np.concatenate([[0], np.cumsum(d["nb_len"])])
     li_base = np.concatenate([[0], np.cumsum(d["list_len"])])
     loops = d["exists"].shape[0]
@@ -265,3 +270,30 @@ def test_c1_fp64_matches_reference_golden(gpu):
         if want.size:
             assert np.array_equal(gh.comparison_list(g), want), f"grain {g}: final comparison list"
     gh.close()
+
+
+def test_autotuned_launches_give_the_same_bits(gpu, oracle):
+    """The autotuner (gg_params.autotune) times five launch configurations on loops 1-5 and
+    keeps each stage's fastest; every stage kernel's results are independent of its grid,
+    so the FP64 run stays bit-identical to an untuned one (and the oracle's)."""
+    N, G, border = 40, 150, 5
+    ms = msgen.voronoi(N, G, seed=1040)
+    ext, counts = ms.grain_extents()
+    runs = []
+    for tune in (False, True):
+        gh = gpu.GrainHandler(N, border, 0.2, G, precision=gpu.PRECISION_FP64, autotune=tune)
+        gh.load(ms.labels, ext, counts)
+        gh.rtree_lists()
+        hist = []
+        for _ in range(9):
+            gh.step()
+            st = gh.stats()
+            hist.append((st.exists.copy(), st.volume.copy(), st.boxes.copy()))
+        cfg, done = gh.launch_config()
+        assert done
+        if tune:
+            assert all(c in (2, 4, 8, 16, 32) for c in cfg), cfg
+        runs.append(hist)
+        gh.close()
+    for (ea, va, ba), (eb, vb, bb) in zip(*runs):
+        assert np.array_equal(ea, eb) and np.array_equal(va, vb) and np.array_equal(ba, bb)
