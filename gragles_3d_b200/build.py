@@ -20,6 +20,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, "csrc")
 OBJ = os.path.join(HERE, "_build")
 LIB = os.path.join(HERE, "libgg_b200.so")
+RUNNER = os.path.join(HERE, "gg_run")
 SOURCES = ["gg_api.cu", "gg_plan.cu", "gg_conv_f64.cu", "gg_conv_tc.cu", "gg_conv_umma.cu", "gg_lists.cu", "gg_compare.cu",
            "gg_mc.cu", "gg_redist.cu", "gg_init.cu", "gg_noalloc.cu", "gg_hull.cu", "gg_coarsen.cu", "gg_rtree.cu"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
@@ -69,6 +70,12 @@ def build(verbose: bool = False) -> str:
     objs = [os.path.join(OBJ, s.replace(".cu", ".o")) for s in SOURCES]
     if jobs or not os.path.exists(LIB):
         run([cc] + ARCH + ["-shared", "-o", LIB] + objs + ["-lcudart"])
+    # the C++ host driver (gg_run): the reference's mode-4 run through the C ABI
+    host_src = os.path.join(HERE, "host", "gg_run.cpp")
+    if not os.path.exists(RUNNER) or os.path.getmtime(RUNNER) < max(os.path.getmtime(host_src), os.path.getmtime(LIB)):
+        run(["g++", "-O2", "-std=c++17", "-ffp-contract=off", host_src, "-I",
+             os.path.join(os.path.dirname(HERE), "include"), "-L", HERE, "-lgg_b200", "-Wl,-rpath,$ORIGIN",
+             "-o", RUNNER])
     return LIB
 
 

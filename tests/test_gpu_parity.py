@@ -297,3 +297,30 @@ def test_autotuned_launches_give_the_same_bits(gpu, oracle):
         gh.close()
     for (ea, va, ba), (eb, vb, bb) in zip(*runs):
         assert np.array_equal(ea, eb) and np.array_equal(va, vb) and np.array_equal(ba, bb)
+
+
+def test_cpp_host_runs_the_reference_mode4_case(gpu, tmp_path):
+    """The C++ host (gragles_3d_b200/gg_run, the reference's mode-4 main over the C ABI) reads
+    the reference's own input files and parameters.xml and reproduces the compiled
+    reference's run of the plain-method configuration: every loop's sum of the existing
+    grains' volumes, summed in grain order, equals the reference's bit for bit."""
+    import subprocess
+
+    d = dict(np.load(os.path.join(os.path.dirname(__file__), "golden", "c1.npz")))
+    N, G, border, steps = int(d["N"]), int(d["G"]), int(d["border"]), int(d["steps"])
+    ms = msgen.voronoi(N, G, seed=int(d["seed"]))
+    msgen.write_mode4(ms, str(tmp_path))
+    params = os.path.join(str(tmp_path), "parameters.xml")
+    msgen.write_parameters(params, n_grains=G, border=border, steps=steps)
+    runner = os.path.join(os.path.dirname(gpu.LIB_PATH), "gg_run")
+    stats = os.path.join(str(tmp_path), "stats.txt")
+    proc = subprocess.run([runner, params, "--stats", stats], capture_output=True, text=True, timeout=600)
+    assert proc.returncode == 0, proc.stderr
+    rows = [line.split("\t") for line in open(stats).read().splitlines()]
+    assert len(rows) == steps + 1
+    for s, r in enumerate(rows):
+        want = 0.0
+        for g in range(1, G + 1):
+            if d["exists"][s, g]:
+                want += d["volume"][s, g]
+        assert int(r[0]) == s and float(r[3]) == want, f"loop {s}: {r[3]} vs {want!r}"
