@@ -16,9 +16,9 @@
 //     search order with their barycenter segments, bounding boxes and an ID -> elements
 //     index.
 //   correction_kernel: a CTA per grain, with the grain's element index, element boxes
-//     and FP32 barycenters staged in shared memory; slice by slice, the voxels with
-//     |input| < delta are grouped by IDLocal neighbour, and a warp takes 32 voxels of
-//     one neighbour at a time.  The winner of the reference's search is the least (distance, element
+//     and FP32 barycenters staged in shared memory; pass by pass over runs of the box's
+//     voxels, those with |input| < delta are grouped by IDLocal neighbour, and a warp
+//     takes 32 voxels of one neighbour at a time.  The winner of the reference's search is the least (distance, element
 //     index) over the barycenters of the elements holding that neighbour.  The warp
 //     finds it with an FP32 filter -- per barycenter p, q = |p'|^2 - 2 v'.p' (three FMAs
 //     on coordinates relative to an integer origin), minimised per element -- that
@@ -112,17 +112,14 @@ struct JHead {
     double pos[3];
 };
 
-// One CTA's global scratch: the junction IDs and heads, the (mobility, energy) of every
-// misorientation job, and the neighbour -> elements index under construction.  They are
-// used by the junction and table phases, mostly by one lane, and keeping them out of
-// shared memory lets several times more grains' warps share an SM.
+// One CTA's global scratch: the junction IDs and heads and the (mobility, energy) of
+// every misorientation job.  They are used by the junction phase, and keeping them out of
+// shared memory lets more grains' warps share an SM.
 constexpr size_t kAlignUp(size_t b) { return (b + 255) & ~(size_t)255; }
 constexpr size_t kJIdBytes = kAlignUp((size_t)kLMax * kJIds * 4);
 constexpr size_t kJResBytes = kAlignUp(sizeof(double2) * kJobMax);
 constexpr size_t kJHeadBytes = kAlignUp(sizeof(JHead) * kLMax);
-constexpr size_t kIndexBytes = kAlignUp((size_t)kIHash * 4 + (size_t)kIHash * 2 + (size_t)kIdxMax * 4 * 4 +
-                                        (size_t)kPairMax * 2 * 2);
-constexpr size_t kElemScratch = kJIdBytes + kJResBytes + kJHeadBytes + kIndexBytes;
+constexpr size_t kElemScratch = kJIdBytes + kJResBytes + kJHeadBytes;
 
 struct ElemSmem {
     uint32_t lists[kLMax][8];
@@ -133,18 +130,19 @@ struct ElemSmem {
     double energy[kLMax], mobility[kLMax];
     int qlist[kLMax], hlist[kLMax];
     int lslot[kLHash];  // list hash: index into lists, -1 empty
+    int lflat[kLMax];   // first position of each list's barycenters in the flattened FP32 copy
+    // neighbour ID -> elements index under construction
+    unsigned ikey[kIHash];
+    short iden[kIHash];          // dense ID index of the slot
+    uint32_t dkey[kIdxMax];
+    int dcnt[kIdxMax], dlast[kIdxMax], doff[kIdxMax];
+    unsigned short pe[kPairMax]; // (element, dense ID) pairs in search order
+    unsigned short pd[kPairMax];
     // in this CTA's global scratch:
     JHead* jh;                   // kLMax working junctions
-    // neighbour ID -> elements index under construction
-    unsigned* ikey;              // kIHash
-    short* iden;                 // kIHash: dense ID index of the slot
-    uint32_t* dkey;              // kIdxMax
-    int *dcnt, *dlast, *doff;    // kIdxMax each
-    unsigned short* pe;          // kPairMax (element, dense ID) pairs in search order
-    unsigned short* pd;
     uint32_t* jids;              // kLMax x kJIds junction IDs
     double2* jres;               // kJobMax (mobility, energy)
-    int nl, nq, nh, nj, ne, nch, nd, np;
+    int nl, nq, nh, nj, ne, nch, nd, np, np_flat;
 };
 
 // FNV-1a over the eight IDs of a cube's sorted list
@@ -340,18 +338,6 @@ __global__ void __launch_bounds__(32) elements_kernel(ElementArgs a) {
         S.jids = reinterpret_cast<uint32_t*>(scr);
         S.jres = reinterpret_cast<double2*>(scr + kJIdBytes);
         S.jh = reinterpret_cast<JHead*>(scr + kJIdBytes + kJResBytes);
-        unsigned char* ix = scr + kJIdBytes + kJResBytes + kJHeadBytes;
-        S.ikey = reinterpret_cast<unsigned*>(ix);
-        ix += (size_t)kIHash * 4;
-        S.iden = reinterpret_cast<short*>(ix);
-        ix += (size_t)kIHash * 2;
-        S.dkey = reinterpret_cast<uint32_t*>(ix);
-        S.dcnt = reinterpret_cast<int*>(ix + (size_t)kIdxMax * 4);
-        S.dlast = reinterpret_cast<int*>(ix + (size_t)kIdxMax * 8);
-        S.doff = reinterpret_cast<int*>(ix + (size_t)kIdxMax * 12);
-        ix += (size_t)kIdxMax * 16;
-        S.pe = reinterpret_cast<unsigned short*>(ix);
-        S.pd = reinterpret_cast<unsigned short*>(ix + (size_t)kPairMax * 2);
     }
     __syncwarp();
     for (TileWalk w(a.toff, a.G, blockIdx.x, gridDim.x); w.valid(); w.next()) {
@@ -439,6 +425,7 @@ __global__ void __launch_bounds__(32) elements_kernel(ElementArgs a) {
             S.cnt[k] = 0;
             S.fill[k] = 0;
             S.next_key[k] = -1;
+            S.lflat[k] = -1;
         }
         __syncwarp();
         for (int r = lane; r < nrec; r += 32) atomicAdd(&S.cnt[rec_ntri[r] >> 8], rec_ntri[r] & 0xFF);
@@ -688,6 +675,7 @@ __global__ void __launch_bounds__(32) elements_kernel(ElementArgs a) {
                     const int off = S.off[k], cnt = S.cnt[k];
                     segs[ns++] = make_int2(off, cnt);
                     nseg++;
+                    S.lflat[k] = pb + pcnt;
                     pcnt += cnt;
                     for (int c0 = 0; c0 < cnt; c0 += kHullChunk) {
                         if (nch >= a.el.chunk_cap) { over = true; break; }
@@ -785,6 +773,7 @@ __global__ void __launch_bounds__(32) elements_kernel(ElementArgs a) {
             a.el.n_elem[g] = ne;
             a.el.n_idx[g] = nd;
             a.el.n_flat[g] = pb;
+            S.np_flat = pb;
             S.ne = ne;
             S.nch = nch;
             S.nd = nd;
@@ -826,7 +815,15 @@ __global__ void __launch_bounds__(32) elements_kernel(ElementArgs a) {
                 const int2 sg = a.el.segs[(long long)g * a.el.seg_cap + el.seg_off];
                 if (sg.x < 0 || sg.y < 0 || sg.x + sg.y > a.el.bary_cap) continue;
                 double surface = 0;
-                for (int i = 0; i < sg.y; i++) surface += ea[sg.x + i];
+                int i = 0;
+                for (; i + 4 <= sg.y; i += 4) {  // the loads run ahead of the sums, which stay in order
+                    const double t0 = ea[sg.x + i], t1 = ea[sg.x + i + 1], t2 = ea[sg.x + i + 2], t3 = ea[sg.x + i + 3];
+                    surface += t0;
+                    surface += t1;
+                    surface += t2;
+                    surface += t3;
+                }
+                for (; i < sg.y; i++) surface += ea[sg.x + i];
                 el.area = surface * a.ph.ds * a.ph.ds;  // ds = h = 1 / realDomainSize
             }
             for (int e = lane; e < ne; e += 32) {
@@ -864,29 +861,29 @@ __global__ void __launch_bounds__(32) elements_kernel(ElementArgs a) {
             if (ne > 0 && uhi[0] >= ulo[0])
 #pragma unroll
                 for (int q = 0; q < 3; q++) org[q] = floor(0.5 * (ulo[q] + uhi[q]));
-            (void)nbary;
+            // every barycenter to its element's run: lane-parallel over the grouped array,
+            // barycenter i of list k (the last list whose first barycenter is <= i) going to
+            // lflat[k] + (i - off[k])
             float4* pf = a.el.ebf + (long long)g * a.el.bary_cap;
             int* pidx = a.el.eidx + (long long)g * a.el.bary_cap;
-            const int2* gsegs = a.el.segs + (long long)g * a.el.seg_cap;
+            const int nl = S.nl, total = min(nbary, a.el.bary_cap), nflat = min(S.np_flat, a.el.bary_cap);
             float r2 = 0.f;
-            for (int e = 0; e < ne; e++) {  // element by element, its segments in order
-                const HullElem& el = E[e];
-                int dst = el.pbase;
-                for (int sgi = 0; sgi < el.nseg; sgi++) {
-                    const int2 sg = gsegs[el.seg_off + sgi];
-                    if (sg.x < 0 || sg.y < 0 || sg.x + sg.y > a.el.bary_cap || dst + sg.y > el.pbase + el.pcount)
-                        break;
-                    for (int i = lane; i < sg.y; i += 32) {
-                        const long long src = sg.x + i;
-                        const double dx = eb[3 * src] - org[0], dy = eb[3 * src + 1] - org[1],
-                                     dz = eb[3 * src + 2] - org[2];
-                        const double w = dx * dx + dy * dy + dz * dz;
-                        pf[dst + i] = make_float4((float)dx, (float)dy, (float)dz, (float)w);
-                        pidx[dst + i] = (int)src;
-                        r2 = fmaxf(r2, (float)w);
-                    }
-                    dst += sg.y;
+            for (int i = lane; i < total; i += 32) {
+                int lo = 0, hi = nl - 1;
+                while (lo < hi) {
+                    const int mid = (lo + hi + 1) >> 1;
+                    if (S.off[mid] <= i) lo = mid;
+                    else hi = mid - 1;
                 }
+                const int base = nl > 0 ? S.lflat[lo] : -1;
+                const int dst = base < 0 ? -1 : base + (i - S.off[lo]);
+                if (dst < 0 || dst >= nflat) continue;  // a list no element holds
+                const double dx = eb[3 * (long long)i] - org[0], dy = eb[3 * (long long)i + 1] - org[1],
+                             dz = eb[3 * (long long)i + 2] - org[2];
+                const double w = dx * dx + dy * dy + dz * dz;
+                pf[dst] = make_float4((float)dx, (float)dy, (float)dz, (float)w);
+                pidx[dst] = i;
+                r2 = fmaxf(r2, (float)w);
             }
 #pragma unroll
             for (int o = 16; o > 0; o >>= 1) r2 = fmaxf(r2, __shfl_xor_sync(kFull, r2, o));
@@ -909,10 +906,10 @@ __device__ __forceinline__ double sqdist3(double x, double y, double z, const do
 }
 
 constexpr int kCThreads = 256;
-constexpr int kCVox = 2048;           // voxels of one pass over a slice (whole rows)
+constexpr int kCVox = 4096;           // voxels of one pass: a run of the box in [z][y][x] order
 constexpr unsigned short kNoD = 0xFFFF;
 constexpr float kInf = 3.0e38f;
-constexpr int kSPts = 2048;           // barycenters staged in shared memory (more: read from HBM)
+constexpr int kSPts = 1536;           // barycenters staged in shared memory (more: read from HBM)
 constexpr int kSElem = 512;           // the element table's capacity per grain
 constexpr int kSPairs = 2048;         // the index's (element, ID) pair capacity per grain
 
@@ -1045,8 +1042,8 @@ __device__ __forceinline__ void correct_voxel(const CorrectionArgs<T>& a, const 
 }
 
 // A CTA per grain: the grain's element index, element boxes and FP32 barycenters are
-// staged in shared memory once; then, slice by slice, the band voxels of a pass (whole
-// rows, <= kCVox voxels) are grouped by IDLocal neighbour (counting sort in shared
+// staged in shared memory once; then, pass by pass over runs of kCVox consecutive voxels
+// of the box, the band voxels are grouped by IDLocal neighbour (counting sort in shared
 // memory) and the warps take packets of 32 voxels of one neighbour.
 template <typename T>
 __global__ void __launch_bounds__(kCThreads, 3) correction_kernel(CorrectionArgs<T> a) {
@@ -1118,10 +1115,8 @@ __global__ void __launch_bounds__(kCThreads, 3) correction_kernel(CorrectionArgs
         const HullElem* elem = el.elem + (long long)g * el.elem_cap;
         const double* eb = el.ebary + 3 * (long long)g * el.bary_cap;
         const int nx = b.nx(), ny = b.ny();
-        if (nx > kCVox) {
-            if (threadIdx.x == 0) atomicOr(a.err, ERR_BOX);
-            continue;
-        }
+        const int nxy = nx * ny;
+        const long long nvox = (long long)nxy * b.nz();
         // the filter's error bound: q is within 16 R^2 2^-24 of |v' - p'|^2 - |v'|^2 (the
         // three FMAs, the FP32 rounding of p' and |p'|^2), R^2 the largest |v'|^2 or |p'|^2
         float r2 = org.w;
@@ -1132,10 +1127,10 @@ __global__ void __launch_bounds__(kCThreads, 3) correction_kernel(CorrectionArgs
             r2 = fmaxf(r2, cx * cx + cy * cy + cz * cz);
         }
         const float eps2 = fmaxf(2.f * 16.f * r2 * (1.0f / 16777216.f) * 1.0001f, 1e-6f);
-        const int R = kCVox / nx;
-        for (int k = b.z0; k < b.z1; k++)
-        for (int yp = 0; yp < ny; yp += R) {
-            const int nv = min(R, ny - yp) * nx;
+        // passes over consecutive runs of kCVox voxels of the box, across rows and slices,
+        // so that a pass holds many packets and few barriers are paid per voxel
+        for (long long v0 = 0; v0 < nvox; v0 += kCVox) {
+            const int nv = (int)min((long long)kCVox, nvox - v0);
             for (int d = threadIdx.x; d < nd; d += blockDim.x) S.dcnt[d] = 0;
             __syncthreads();
             // band voxels: their neighbour; voxels whose neighbour no element holds get (1, 1)
@@ -1152,8 +1147,7 @@ __global__ void __launch_bounds__(kCThreads, 3) correction_kernel(CorrectionArgs
                     vals[u] = delta;  // outside the band
                     ids[u] = 0u;
                     if (q < nv) {
-                        const int i = b.y0 + yp + q / nx, j = b.x0 + q % nx;
-                        fs[u] = b.at(i, j, k);
+                        fs[u] = v0 + q;  // the box's flat [z][y][x] index
                         vals[u] = (double)in[fs[u]];
                         // IDLocal flat-resized onto the box (dimensionalBuffer.h:120-131)
                         ids[u] = fs[u] < old_count ? idl[fs[u]] : 0u;
@@ -1219,8 +1213,9 @@ __global__ void __launch_bounds__(kCThreads, 3) correction_kernel(CorrectionArgs
                 const int cnt = min(32, S.doff[d] + S.dcnt[d] - start);
                 const bool active = lane < cnt;
                 const int q = S.vlist[start + (active ? lane : 0)];
-                const int i = b.y0 + yp + q / nx, j = b.x0 + q % nx;
-                const long long f = b.at(i, j, k);
+                const long long f = v0 + q;
+                const int k = b.z0 + (int)(f / nxy), rem = (int)(f % nxy);
+                const int i = b.y0 + rem / nx, j = b.x0 + rem % nx;
                 // the point is Vector3d(i, j, k), box.cpp:481
                 const int2 dr = S.drng[d];
                 const int win = search_packet(S, pts, dr.x, dr.y, active, i, j, k, org, eps2, ne, eidx, eb, a.err);
