@@ -888,6 +888,25 @@ __global__ void __launch_bounds__(32) elements_kernel(ElementArgs a) {
 #pragma unroll
             for (int o = 16; o > 0; o >>= 1) r2 = fmaxf(r2, __shfl_xor_sync(kFull, r2, o));
             if (lane == 0) a.el.eorg[g] = make_float4((float)org[0], (float)org[1], (float)org[2], r2);
+            // every chunk's FP32 box relative to the origin (rounded outward) and its run in
+            // the flattened copy: the chunk lies in one list, whose run starts at lflat
+            float4* cb = a.el.ecb + 2 * (long long)g * a.el.chunk_cap;
+            for (int c = lane; c < nch && c < a.el.chunk_cap; c += 32) {
+                const HullChunk& C = chunks[c];
+                int lo = 0, hi = nl - 1;
+                while (lo < hi) {
+                    const int mid = (lo + hi + 1) >> 1;
+                    if (S.off[mid] <= C.start) lo = mid;
+                    else hi = mid - 1;
+                }
+                const int base = nl > 0 ? S.lflat[lo] : -1;
+                int first = base < 0 ? 0 : base + (C.start - S.off[lo]), count = base < 0 ? 0 : C.count;
+                if (first < 0 || count < 0 || first + count > nflat) first = count = 0;
+                cb[2 * c] = make_float4(__double2float_rd(C.lo[0] - org[0]), __double2float_rd(C.lo[1] - org[1]),
+                                        __double2float_rd(C.lo[2] - org[2]), __int_as_float(first));
+                cb[2 * c + 1] = make_float4(__double2float_ru(C.hi[0] - org[0]), __double2float_ru(C.hi[1] - org[1]),
+                                            __double2float_ru(C.hi[2] - org[2]), __int_as_float(count));
+            }
         }
         __syncwarp();
     }
@@ -906,18 +925,20 @@ __device__ __forceinline__ double sqdist3(double x, double y, double z, const do
 }
 
 constexpr int kCThreads = 256;
-constexpr int kCVox = 4096;           // voxels of one pass: a run of the box in [z][y][x] order
+constexpr int kCVox = 2048;           // voxels of one pass: a run of the box in [z][y][x] order
 constexpr unsigned short kNoD = 0xFFFF;
 constexpr float kInf = 3.0e38f;
 constexpr int kSPts = 1536;           // barycenters staged in shared memory (more: read from HBM)
 constexpr int kSElem = 512;           // the element table's capacity per grain
+constexpr int kSChunk = 384;          // chunk boxes staged in shared memory (more: read from HBM)
 constexpr int kSPairs = 2048;         // the index's (element, ID) pair capacity per grain
 
 // One grain's search data, staged once per grain, and the slice pass's voxel groups.
 struct CorrSmem {
     float4 pts[kSPts];            // FP32 barycenters, element by element (ebf)
+    float4 cb[2 * kSChunk];       // chunk boxes and runs (ecb)
     float box[kSElem][6];         // element boxes relative to the origin, rounded outward
-    int2 rng[kSElem];             // element e's barycenters in pts: (first, count)
+    int2 crng[kSElem];            // element e's chunks: (first, count)
     unsigned short pairs[kSPairs];// the index's element lists (search order per ID)
     uint32_t hkey[kCHash];        // neighbour ID -> dense index d
     unsigned short hden[kCHash];
@@ -925,6 +946,7 @@ struct CorrSmem {
     int dcnt[kIdxMax], doff[kIdxMax], dcur[kIdxMax], dpk[kIdxMax + 1];
     unsigned short vd[kCVox];     // dense neighbour index of the pass's voxels, kNoD: no search
     unsigned short vlist[kCVox];  // pass voxels grouped by neighbour
+    int nch;                      // the grain's chunks
 };
 
 // q of barycenter p for the voxel whose relative coordinates give (ax, ay, az) = -2 v':
@@ -954,7 +976,7 @@ __device__ __forceinline__ float run_min(const float4* p, int n, float ax, float
 // order, as projectPointToGrainBoundary does (grainHull.cpp:570-660).  Every barycenter
 // that can be the reference's winner has q <= best + eps2, so the subset has the same
 // winner.
-__device__ int exact_winner(const CorrSmem& S, const float4* pts, int first, int count, int ne,
+__device__ int exact_winner(const CorrSmem& S, const float4* pts, const float4* cb, int first, int count, int ne,
                             const int* __restrict__ eidx, const double* __restrict__ eb, double x, double y, double z,
                             float ax, float ay, float az, float limit) {
     double bd = 10000000.0;
@@ -962,17 +984,31 @@ __device__ int exact_winner(const CorrSmem& S, const float4* pts, int first, int
     for (int c = 0; c < count; c++) {
         const int e = S.pairs[first + c];
         if (e >= ne) continue;
-        const int2 r = S.rng[e];
-        for (int i = r.x; i < r.x + r.y; i++) {
-            if (qval(pts[i], ax, ay, az) > limit) continue;
-            const double d = sqdist3(x, y, z, eb + 3 * (long long)eidx[i]);
-            if (d < bd) {
-                bd = d;
-                bw = e;
+        const int2 cr = S.crng[e];
+        for (int ch = cr.x; ch < cr.x + cr.y; ch++) {  // the element's chunks cover its barycenters in order
+            const int p0 = __float_as_int(cb[2 * ch].w), pn = __float_as_int(cb[2 * ch + 1].w);
+            for (int i = p0; i < p0 + pn; i++) {
+                if (qval(pts[i], ax, ay, az) > limit) continue;
+                const double d = sqdist3(x, y, z, eb + 3 * (long long)eidx[i]);
+                if (d < bd) {
+                    bd = d;
+                    bw = e;
+                }
             }
         }
     }
     return bw;
+}
+
+// Lower bound of q over a box [lo, hi] (relative, rounded outward) for the voxel v':
+// |v' - box|^2 in FP32, scaled down past its rounding, - |v'|^2 - eps.
+__device__ __forceinline__ float box_bound(float vx, float vy, float vz, float vv, float lx, float ly, float lz,
+                                           float hx, float hy, float hz, float eps) {
+    const float dx = vx < lx ? lx - vx : (vx > hx ? vx - hx : 0.f);
+    const float dy = vy < ly ? ly - vy : (vy > hy ? vy - hy : 0.f);
+    const float dz = vz < lz ? lz - vz : (vz > hz ? vz - hz : 0.f);
+    const float d2 = fmaf(dz, dz, fmaf(dy, dy, dx * dx));
+    return d2 * (1.f - 1.0f / 1048576.f) - vv - eps;
 }
 
 // The element whose (energy, mobility) the voxel (i, j, k) takes: the reference's
@@ -984,12 +1020,14 @@ __device__ int exact_winner(const CorrSmem& S, const float4* pts, int first, int
 // Elements are taken in reverse search order, so the grain boundary (last in search
 // order, and the usual winner) sets a tight best first, and an element is skipped when
 // no lane's voxel can come within the band of its best through the element's box.
-__device__ __forceinline__ int search_packet(const CorrSmem& S, const float4* pts, int first, int count, bool active,
-                                             int i, int j, int k, float4 org, float eps2, int ne,
-                                             const int* __restrict__ eidx, const double* __restrict__ eb, int* err) {
+__device__ __forceinline__ int search_packet(const CorrSmem& S, const float4* pts, const float4* cb, int first,
+                                             int count, bool active, int i, int j, int k, float4 org, float eps2,
+                                             int ne, const int* __restrict__ eidx, const double* __restrict__ eb,
+                                             int* err) {
     const float vx = (float)i - org.x, vy = (float)j - org.y, vz = (float)k - org.z;  // exact
     const float ax = -2.f * vx, ay = -2.f * vy, az = -2.f * vz;
     const float vv = vx * vx + vy * vy + vz * vz;  // exact (integers below 2^24)
+    const float eps = 0.5f * eps2;
     float best = kInf, second = kInf;
     int beste = -1;
     for (int c = count - 1; c >= 0; c--) {
@@ -998,18 +1036,22 @@ __device__ __forceinline__ int search_packet(const CorrSmem& S, const float4* pt
             if ((threadIdx.x & 31) == 0) atomicOr(err, ERR_BOUNDS);
             continue;
         }
-        {   // lower bound of q over the element's box: |v' - box|^2 (FP32, scaled down past its
-            // rounding) - |v'|^2 - eps; the box was rounded outward.  best = kInf never skips.
-            const float* bx = S.box[e];
-            const float dx = vx < bx[0] ? bx[0] - vx : (vx > bx[3] ? vx - bx[3] : 0.f);
-            const float dy = vy < bx[1] ? bx[1] - vy : (vy > bx[4] ? vy - bx[4] : 0.f);
-            const float dz = vz < bx[2] ? bx[2] - vz : (vz > bx[5] ? vz - bx[5] : 0.f);
-            const float d2 = fmaf(dz, dz, fmaf(dy, dy, dx * dx));
-            const float lb = d2 * (1.f - 1.0f / 1048576.f) - vv - 0.5f * eps2;
-            if (!__any_sync(kFull, active && lb <= best + eps2)) continue;
+        // an element, then each of its chunks, is skipped when no lane's voxel can come
+        // within the band of its best through the box (best = kInf: never skipped)
+        const float* bx = S.box[e];
+        if (!__any_sync(kFull, active && box_bound(vx, vy, vz, vv, bx[0], bx[1], bx[2], bx[3], bx[4], bx[5], eps) <=
+                                             best + eps2))
+            continue;
+        const int2 cr = S.crng[e];
+        float m = kInf;
+        for (int ch = cr.x; ch < cr.x + cr.y; ch++) {
+            const float4 l = cb[2 * ch], h = cb[2 * ch + 1];
+            // the element's own best so far bounds it too: min(best, m) is what a chunk must beat
+            const float lim = fminf(best, m) + eps2;
+            if (!__any_sync(kFull, active && box_bound(vx, vy, vz, vv, l.x, l.y, l.z, h.x, h.y, h.z, eps) <= lim))
+                continue;
+            m = fminf(m, run_min(pts + __float_as_int(l.w), __float_as_int(h.w), ax, ay, az));
         }
-        const int2 r = S.rng[e];
-        const float m = run_min(pts + r.x, r.y, ax, ay, az);
         if (m < best) {
             second = best;
             best = m;
@@ -1020,7 +1062,7 @@ __device__ __forceinline__ int search_packet(const CorrSmem& S, const float4* pt
     }
     if (beste < 0) return -1;
     if (second - best > eps2) return beste;  // proven: every other element is farther
-    return exact_winner(S, pts, first, count, ne, eidx, eb, (double)i, (double)j, (double)k, ax, ay, az,
+    return exact_winner(S, pts, cb, first, count, ne, eidx, eb, (double)i, (double)j, (double)k, ax, ay, az,
                         best + eps2);
 }
 
@@ -1064,18 +1106,21 @@ __global__ void __launch_bounds__(kCThreads, 3) correction_kernel(CorrectionArgs
         const int npairs = min(el.pair_cap, kSPairs);
         const float4 org = el.eorg[g];
         const float4* gpts = el.ebf + (long long)g * el.bary_cap;
+        const float4* gcb = el.ecb + 2 * (long long)g * el.chunk_cap;
         __syncthreads();  // the previous grain's packets are done with the shared arrays
+        if (threadIdx.x == 0) S.nch = 0;
         for (int q = threadIdx.x; q < kCHash; q += blockDim.x) S.hkey[q] = kNoId;
         for (int q = threadIdx.x; q < npairs; q += blockDim.x)
             S.pairs[q] = el.idx_elem[(long long)g * el.pair_cap + q];
         for (int e = threadIdx.x; e < ne; e += blockDim.x) {
             const HullElem& E = el.elem[(long long)g * el.elem_cap + e];
-            int2 r = make_int2(E.pbase, E.pcount);
-            if (r.x < 0 || r.y < 0 || r.x + r.y > nflat) {
+            int2 r = make_int2(E.chunk_off, E.nchunk);
+            if (r.x < 0 || r.y < 0 || r.x + r.y > el.chunk_cap) {
                 atomicOr(a.err, ERR_BOUNDS);
                 r = make_int2(0, 0);
             }
-            S.rng[e] = r;
+            S.crng[e] = r;
+            atomicMax(&S.nch, r.x + r.y);
             const float o[3] = {org.x, org.y, org.z};
 #pragma unroll
             for (int q = 0; q < 3; q++) {
@@ -1086,6 +1131,9 @@ __global__ void __launch_bounds__(kCThreads, 3) correction_kernel(CorrectionArgs
         if (nflat <= kSPts)
             for (int p = threadIdx.x; p < nflat; p += blockDim.x) S.pts[p] = gpts[p];
         __syncthreads();
+        const int nch = S.nch;
+        if (nch <= kSChunk)
+            for (int c = threadIdx.x; c < 2 * nch; c += blockDim.x) S.cb[c] = gcb[c];
         for (int d = threadIdx.x; d < nd; d += blockDim.x) {
             const uint32_t id = el.idx_key[(long long)g * el.idx_cap + d];
             int2 r = el.idx_rng[(long long)g * el.idx_cap + d];
@@ -1105,6 +1153,7 @@ __global__ void __launch_bounds__(kCThreads, 3) correction_kernel(CorrectionArgs
         }
         __syncthreads();
         const float4* pts = nflat <= kSPts ? S.pts : gpts;
+        const float4* cb = nch <= kSChunk ? S.cb : gcb;
         const int* eidx = el.eidx + (long long)g * el.bary_cap;
         const Box b = load_box(a.box + 6 * g);
         const Box bo = load_box(a.idbox_old + 6 * g);
@@ -1218,7 +1267,7 @@ __global__ void __launch_bounds__(kCThreads, 3) correction_kernel(CorrectionArgs
                 const int i = b.y0 + rem / nx, j = b.x0 + rem % nx;
                 // the point is Vector3d(i, j, k), box.cpp:481
                 const int2 dr = S.drng[d];
-                const int win = search_packet(S, pts, dr.x, dr.y, active, i, j, k, org, eps2, ne, eidx, eb, a.err);
+                const int win = search_packet(S, pts, cb, dr.x, dr.y, active, i, j, k, org, eps2, ne, eidx, eb, a.err);
                 if (active) {
                     const uint32_t id = f < old_count ? idl[f] : 0u;
                     correct_voxel(a, elem, g, win, id, (double)in[f], out + f);

@@ -220,6 +220,9 @@ struct HullElements {
     // and its square taken in FP64 first, with o the grain's integer origin
     float4* ebf;              // (G + 1) x bary_cap
     int* eidx;                // (G + 1) x bary_cap: position of each of them in ebary
+    // each chunk's box relative to the origin, rounded outward to FP32, and its run in
+    // ebf: (lo.x, lo.y, lo.z, first as int bits), (hi.x, hi.y, hi.z, count as int bits)
+    float4* ecb;              // (G + 1) x chunk_cap x 2
     int* n_flat;              // G + 1: barycenters in ebf
     float4* eorg;             // G + 1: (o.x, o.y, o.z, largest |p - o|^2 of the grain)
     HullChunk* chunks;        // (G + 1) x chunk_cap
