@@ -64,6 +64,7 @@ struct gg_ctx {
     // tiles
     int *d_toff_n = nullptr, *d_toff_slab = nullptr, *d_toff_one = nullptr, *d_toff_mc = nullptr, *d_toff_red = nullptr;
     int* d_toff_big = nullptr;  // mixed path: slices of the boxes above the tensor-core side
+    WorkOrder work{};           // largest-first order of the per-grain kernels
     // tables
     double2* d_tw = nullptr;
     long long* d_tw_off = nullptr;
@@ -394,8 +395,11 @@ int correct_convolution(gg_ctx* ctx) {
     c.el = ctx->el;
     c.ph = physics(ctx);
     c.err = ctx->d_err;
+    launch_work_order(ctx->work, ctx->G, ctx->d_toff_one, ctx->d_box[p], ctx->stream);
+    c.order = ctx->work.order;
+    c.queue = ctx->work.queue;
     launch_correction<T>(c, stage_grid(ctx, ST_CONV), ctx->stream);
-    ctx->launches += 1;
+    ctx->launches += 3;
     CK(cudaGetLastError());
     return GG_OK;
 }
@@ -865,7 +869,8 @@ void free_all(gg_ctx* c) {
                     c->d_circ, c->d_circ_off, c->d_bmat, c->d_boff, c->d_cscr, c->d_elscr, c->d_quat, c->d_see,
                     c->hull.rec_list, c->hull.rec_ntri, c->hull.bary, c->hull.tarea, c->hull.diag, c->el.earea, c->el.ebf, c->el.ecb, c->el.eidx, c->el.n_flat, c->el.eorg, c->hull.n_rec, c->hull.n_tri, c->el.n_elem,
                     c->el.elem, c->el.ids, c->el.segs, c->el.ebary, c->el.chunks, c->el.n_idx, c->el.idx_key, c->el.idx_rng,
-                    c->el.idx_elem, c->d_err, c->d_total_vox, c->d_count3, c->bins.count,
+                    c->el.idx_elem, c->d_err, c->d_total_vox, c->d_count3, c->bins.count, c->work.keys,
+                    c->work.keys_out, c->work.vals, c->work.order, c->work.temp, c->work.queue,
                     c->bins.off, c->bins.cursor, c->bins.entries, c->bins.max_count};
     for (void* p : ptrs)
         if (p) cudaFree(p);
@@ -954,6 +959,13 @@ int gg_create(const gg_params* params, gg_ctx** out) {
     CK(dalloc(&ctx->d_toff_mc, G1 + 1));
     CK(dalloc(&ctx->d_toff_red, G1 + 1));
     CK(dalloc(&ctx->d_toff_big, G1 + 1));
+    CK(dalloc(&ctx->work.keys, G1));
+    CK(dalloc(&ctx->work.keys_out, G1));
+    CK(dalloc(&ctx->work.vals, G1));
+    CK(dalloc(&ctx->work.order, G1));
+    CK(dalloc(&ctx->work.queue, kQueues));
+    ctx->work.temp_bytes = work_order_temp_bytes(ctx->G);
+    CK(cudaMalloc(&ctx->work.temp, ctx->work.temp_bytes ? ctx->work.temp_bytes : 1));
     CK(dalloc(&ctx->d_err, 1));
     CK(dalloc(&ctx->d_total_vox, 1));
     CK(dalloc(&ctx->d_count3, 3));

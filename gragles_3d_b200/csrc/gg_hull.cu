@@ -928,17 +928,18 @@ constexpr int kCThreads = 256;
 constexpr int kCVox = 2048;           // voxels of one pass: a run of the box in [z][y][x] order
 constexpr unsigned short kNoD = 0xFFFF;
 constexpr float kInf = 3.0e38f;
-constexpr int kSPts = 1536;           // barycenters staged in shared memory (more: read from HBM)
-constexpr int kSElem = 512;           // the element table's capacity per grain
-constexpr int kSChunk = 384;          // chunk boxes staged in shared memory (more: read from HBM)
-constexpr int kSPairs = 2048;         // the index's (element, ID) pair capacity per grain
+constexpr int kSPts = 2560;           // barycenters staged in shared memory (more: read from HBM)
+constexpr int kSElem = kLMax;         // elements per grain: one per distinct list at most
+constexpr int kSPairs = kPairMax;     // the index's (element, ID) pairs per grain
+static_assert(kSElem <= 0xFFFF && kSPairs <= 0xFFFF, "16-bit element and pair indices");
 
 // One grain's search data, staged once per grain, and the slice pass's voxel groups.
 struct CorrSmem {
     float4 pts[kSPts];            // FP32 barycenters, element by element (ebf)
-    float4 cb[2 * kSChunk];       // chunk boxes and runs (ecb)
     float box[kSElem][6];         // element boxes relative to the origin, rounded outward
     int2 crng[kSElem];            // element e's chunks: (first, count)
+    int2 erun[kSElem];            // element e's barycenters as one run (first, count), or x = -1:
+                                  // several runs (a merged junction), taken chunk by chunk
     unsigned short pairs[kSPairs];// the index's element lists (search order per ID)
     uint32_t hkey[kCHash];        // neighbour ID -> dense index d
     unsigned short hden[kCHash];
@@ -946,7 +947,7 @@ struct CorrSmem {
     int dcnt[kIdxMax], doff[kIdxMax], dcur[kIdxMax], dpk[kIdxMax + 1];
     unsigned short vd[kCVox];     // dense neighbour index of the pass's voxels, kNoD: no search
     unsigned short vlist[kCVox];  // pass voxels grouped by neighbour
-    int nch;                      // the grain's chunks
+    int next;                     // the work-order position this CTA fetched
 };
 
 // q of barycenter p for the voxel whose relative coordinates give (ax, ay, az) = -2 v':
@@ -970,13 +971,25 @@ __device__ __forceinline__ float run_min(const float4* p, int n, float ax, float
     return fminf(m0, m1);
 }
 
+// The least q over element e's barycenters: its run, or its chunks' runs.
+__device__ __forceinline__ float element_min(const CorrSmem& S, const float4* pts, const float4* gcb, int e,
+                                             float ax, float ay, float az) {
+    const int2 r = S.erun[e];
+    if (r.x >= 0) return run_min(pts + r.x, r.y, ax, ay, az);
+    const int2 cr = S.crng[e];
+    float m = kInf;
+    for (int ch = cr.x; ch < cr.x + cr.y; ch++)
+        m = fminf(m, run_min(pts + __float_as_int(gcb[2 * ch].w), __float_as_int(gcb[2 * ch + 1].w), ax, ay, az));
+    return m;
+}
+
 // The near-tie case: the barycenters whose q is within the band, measured with the
 // reference's FP64 distance (Vector3d::squaredNorm, c0 + (c1 + c2)) and kept only when
 // strictly nearer, visiting elements in search order and each element's barycenters in
 // order, as projectPointToGrainBoundary does (grainHull.cpp:570-660).  Every barycenter
 // that can be the reference's winner has q <= best + eps2, so the subset has the same
 // winner.
-__device__ int exact_winner(const CorrSmem& S, const float4* pts, const float4* cb, int first, int count, int ne,
+__device__ int exact_winner(const CorrSmem& S, const float4* pts, const float4* gcb, int first, int count, int ne,
                             const int* __restrict__ eidx, const double* __restrict__ eb, double x, double y, double z,
                             float ax, float ay, float az, float limit) {
     double bd = 10000000.0;
@@ -984,9 +997,12 @@ __device__ int exact_winner(const CorrSmem& S, const float4* pts, const float4* 
     for (int c = 0; c < count; c++) {
         const int e = S.pairs[first + c];
         if (e >= ne) continue;
-        const int2 cr = S.crng[e];
-        for (int ch = cr.x; ch < cr.x + cr.y; ch++) {  // the element's chunks cover its barycenters in order
-            const int p0 = __float_as_int(cb[2 * ch].w), pn = __float_as_int(cb[2 * ch + 1].w);
+        // the element's run, or its chunks: either covers its barycenters in order
+        const int2 r = S.erun[e], cr = S.crng[e];
+        const int nrun = r.x >= 0 ? 1 : cr.y;
+        for (int u = 0; u < nrun; u++) {
+            const int p0 = r.x >= 0 ? r.x : __float_as_int(gcb[2 * (cr.x + u)].w);
+            const int pn = r.x >= 0 ? r.y : __float_as_int(gcb[2 * (cr.x + u) + 1].w);
             for (int i = p0; i < p0 + pn; i++) {
                 if (qval(pts[i], ax, ay, az) > limit) continue;
                 const double d = sqdist3(x, y, z, eb + 3 * (long long)eidx[i]);
@@ -1020,7 +1036,7 @@ __device__ __forceinline__ float box_bound(float vx, float vy, float vz, float v
 // Elements are taken in reverse search order, so the grain boundary (last in search
 // order, and the usual winner) sets a tight best first, and an element is skipped when
 // no lane's voxel can come within the band of its best through the element's box.
-__device__ __forceinline__ int search_packet(const CorrSmem& S, const float4* pts, const float4* cb, int first,
+__device__ __forceinline__ int search_packet(const CorrSmem& S, const float4* pts, const float4* gcb, int first,
                                              int count, bool active, int i, int j, int k, float4 org, float eps2,
                                              int ne, const int* __restrict__ eidx, const double* __restrict__ eb,
                                              int* err) {
@@ -1042,16 +1058,7 @@ __device__ __forceinline__ int search_packet(const CorrSmem& S, const float4* pt
         if (!__any_sync(kFull, active && box_bound(vx, vy, vz, vv, bx[0], bx[1], bx[2], bx[3], bx[4], bx[5], eps) <=
                                              best + eps2))
             continue;
-        const int2 cr = S.crng[e];
-        float m = kInf;
-        for (int ch = cr.x; ch < cr.x + cr.y; ch++) {
-            const float4 l = cb[2 * ch], h = cb[2 * ch + 1];
-            // the element's own best so far bounds it too: min(best, m) is what a chunk must beat
-            const float lim = fminf(best, m) + eps2;
-            if (!__any_sync(kFull, active && box_bound(vx, vy, vz, vv, l.x, l.y, l.z, h.x, h.y, h.z, eps) <= lim))
-                continue;
-            m = fminf(m, run_min(pts + __float_as_int(l.w), __float_as_int(h.w), ax, ay, az));
-        }
+        const float m = element_min(S, pts, gcb, e, ax, ay, az);
         if (m < best) {
             second = best;
             best = m;
@@ -1062,7 +1069,7 @@ __device__ __forceinline__ int search_packet(const CorrSmem& S, const float4* pt
     }
     if (beste < 0) return -1;
     if (second - best > eps2) return beste;  // proven: every other element is farther
-    return exact_winner(S, pts, cb, first, count, ne, eidx, eb, (double)i, (double)j, (double)k, ax, ay, az,
+    return exact_winner(S, pts, gcb, first, count, ne, eidx, eb, (double)i, (double)j, (double)k, ax, ay, az,
                         best + eps2);
 }
 
@@ -1094,8 +1101,18 @@ __global__ void __launch_bounds__(kCThreads, 3) correction_kernel(CorrectionArgs
     const double delta = a.geo.delta;
     const HullElements& el = a.el;
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
-    for (TileWalk w(a.toff, a.G, blockIdx.x, gridDim.x); w.valid(); w.next()) {
-        const int g = w.g;
+    const int n_work = a.toff[a.G + 1];  // grains with a tile (0 when the plan overflowed)
+    for (;;) {
+        __syncthreads();  // the previous grain's packets are done with the shared arrays
+        if (threadIdx.x == 0) S.next = atomicAdd(a.queue, 1);
+        __syncthreads();
+        const int t = S.next;
+        if (t >= n_work) break;
+        const int g = a.order[t];
+        if (g < 1 || g > a.G) {
+            if (threadIdx.x == 0) atomicOr(a.err, ERR_BOUNDS);
+            continue;
+        }
         const int ne = min(max(el.n_elem[g], 0), min(el.elem_cap, kSElem));
         int nd = el.n_idx[g];
         if (nd < 0 || nd > el.idx_cap || nd > kIdxMax) {
@@ -1107,8 +1124,6 @@ __global__ void __launch_bounds__(kCThreads, 3) correction_kernel(CorrectionArgs
         const float4 org = el.eorg[g];
         const float4* gpts = el.ebf + (long long)g * el.bary_cap;
         const float4* gcb = el.ecb + 2 * (long long)g * el.chunk_cap;
-        __syncthreads();  // the previous grain's packets are done with the shared arrays
-        if (threadIdx.x == 0) S.nch = 0;
         for (int q = threadIdx.x; q < kCHash; q += blockDim.x) S.hkey[q] = kNoId;
         for (int q = threadIdx.x; q < npairs; q += blockDim.x)
             S.pairs[q] = el.idx_elem[(long long)g * el.pair_cap + q];
@@ -1120,7 +1135,22 @@ __global__ void __launch_bounds__(kCThreads, 3) correction_kernel(CorrectionArgs
                 r = make_int2(0, 0);
             }
             S.crng[e] = r;
-            atomicMax(&S.nch, r.x + r.y);
+            // one run when the chunks follow one another in the flattened copy
+            int2 run = make_int2(-1, 0);
+            if (r.y > 0) {
+                const int f0 = __float_as_int(gcb[2 * r.x].w);
+                int end = f0;
+                bool one = f0 >= 0;
+                for (int ch = r.x; ch < r.x + r.y && one; ch++) {
+                    const int f = __float_as_int(gcb[2 * ch].w), n = __float_as_int(gcb[2 * ch + 1].w);
+                    one = f == end && n >= 0;
+                    end = f + n;
+                }
+                if (one && end <= nflat) run = make_int2(f0, end - f0);
+            } else {
+                run = make_int2(0, 0);
+            }
+            S.erun[e] = run;
             const float o[3] = {org.x, org.y, org.z};
 #pragma unroll
             for (int q = 0; q < 3; q++) {
@@ -1130,10 +1160,7 @@ __global__ void __launch_bounds__(kCThreads, 3) correction_kernel(CorrectionArgs
         }
         if (nflat <= kSPts)
             for (int p = threadIdx.x; p < nflat; p += blockDim.x) S.pts[p] = gpts[p];
-        __syncthreads();
-        const int nch = S.nch;
-        if (nch <= kSChunk)
-            for (int c = threadIdx.x; c < 2 * nch; c += blockDim.x) S.cb[c] = gcb[c];
+        __syncthreads();  // the hash is cleared
         for (int d = threadIdx.x; d < nd; d += blockDim.x) {
             const uint32_t id = el.idx_key[(long long)g * el.idx_cap + d];
             int2 r = el.idx_rng[(long long)g * el.idx_cap + d];
@@ -1153,7 +1180,6 @@ __global__ void __launch_bounds__(kCThreads, 3) correction_kernel(CorrectionArgs
         }
         __syncthreads();
         const float4* pts = nflat <= kSPts ? S.pts : gpts;
-        const float4* cb = nch <= kSChunk ? S.cb : gcb;
         const int* eidx = el.eidx + (long long)g * el.bary_cap;
         const Box b = load_box(a.box + 6 * g);
         const Box bo = load_box(a.idbox_old + 6 * g);
@@ -1267,7 +1293,7 @@ __global__ void __launch_bounds__(kCThreads, 3) correction_kernel(CorrectionArgs
                 const int i = b.y0 + rem / nx, j = b.x0 + rem % nx;
                 // the point is Vector3d(i, j, k), box.cpp:481
                 const int2 dr = S.drng[d];
-                const int win = search_packet(S, pts, cb, dr.x, dr.y, active, i, j, k, org, eps2, ne, eidx, eb, a.err);
+                const int win = search_packet(S, pts, gcb, dr.x, dr.y, active, i, j, k, org, eps2, ne, eidx, eb, a.err);
                 if (active) {
                     const uint32_t id = f < old_count ? idl[f] : 0u;
                     correct_voxel(a, elem, g, win, id, (double)in[f], out + f);

@@ -36,6 +36,23 @@ struct PlanArgs {
 };
 void launch_plan(const PlanArgs& a, cudaStream_t s);
 
+// ---- largest-first work order for the per-grain kernels (gg_plan.cu) ----
+// order[0, toff[G + 1]) = the grains with a tile in `toff` (one tile per grain), by
+// decreasing box voxels; the kernels that take it fetch positions from a counter
+// (*queue, zeroed here) so that the largest grains start first and the rest fill in.
+struct WorkOrder {
+    int* keys;               // G + 1 scratch keys
+    int* keys_out;           // G + 1
+    int* vals;               // G + 1 (grain IDs)
+    int* order;              // G + 1 (out)
+    void* temp;              // radix-sort scratch
+    size_t temp_bytes;
+    int* queue;              // kQueues counters (out: zeroed)
+};
+constexpr int kQueues = 4;
+size_t work_order_temp_bytes(int G);
+void launch_work_order(const WorkOrder& w, int G, const int* toff_one, const int* box, cudaStream_t s);
+
 // Copy box + offsets of every present grain from one layout to another.
 void launch_copy_layout(int G, const int* present, const int* box_src, const long long* off_src, int* box_dst,
                         long long* off_dst, cudaStream_t s);
@@ -280,6 +297,8 @@ struct CorrectionArgs {
     const long long* idoff_old;
     HullElements el;
     HullPhysics ph;
+    const int* order;         // grains by decreasing box (WorkOrder), fetched through *queue
+    int* queue;
     int* err;
 };
 template <typename T>

@@ -9,6 +9,10 @@
 // timestep can be launched without synchronisation.
 #include "gg_kernels.cuh"
 
+#include <cub/device/device_radix_sort.cuh>
+
+#include <climits>
+
 namespace gg {
 
 namespace {
@@ -133,6 +137,37 @@ void launch_plan(const PlanArgs& a, cudaStream_t s) { plan_kernel<<<1, kPlanThre
 void launch_copy_layout(int G, const int* present, const int* box_src, const long long* off_src, int* box_dst,
                         long long* off_dst, cudaStream_t s) {
     copy_layout_kernel<<<(G + 256) / 256, 256, 0, s>>>(G, present, box_src, off_src, box_dst, off_dst);
+}
+
+
+namespace {
+// Sort keys of the work order: box voxels + 1 for the grains with a tile, 0 for the rest.
+__global__ void order_keys_kernel(int G, const int* toff_one, const int* box, int* keys, int* vals) {
+    for (int g = blockIdx.x * blockDim.x + threadIdx.x; g <= G; g += gridDim.x * blockDim.x) {
+        int key = 0;
+        if (g >= 1 && toff_one[g + 1] - toff_one[g] > 0) {
+            const Box b = load_box(box + 6 * g);
+            key = (int)min(b.count() + 1, (long long)INT_MAX);
+        }
+        keys[g] = key;
+        vals[g] = g;
+    }
+}
+}  // namespace
+
+size_t work_order_temp_bytes(int G) {
+    size_t bytes = 0;
+    cub::DeviceRadixSort::SortPairsDescending(nullptr, bytes, (const int*)nullptr, (int*)nullptr,
+                                              (const int*)nullptr, (int*)nullptr, G + 1);
+    return bytes;
+}
+
+void launch_work_order(const WorkOrder& w, int G, const int* toff_one, const int* box, cudaStream_t s) {
+    order_keys_kernel<<<(G + 256) / 256, 256, 0, s>>>(G, toff_one, box, w.keys, w.vals);
+    size_t bytes = w.temp_bytes;
+    cub::DeviceRadixSort::SortPairsDescending(w.temp, bytes, w.keys, w.keys_out, w.vals, w.order, G + 1, 0,
+                                              31, s);
+    cudaMemsetAsync(w.queue, 0, sizeof(int) * kQueues, s);
 }
 
 }  // namespace gg
