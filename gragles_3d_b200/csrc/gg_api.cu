@@ -395,11 +395,12 @@ int correct_convolution(gg_ctx* ctx) {
     c.el = ctx->el;
     c.ph = physics(ctx);
     c.err = ctx->d_err;
-    launch_work_order(ctx->work, ctx->G, ctx->d_toff_one, ctx->d_box[p], ctx->stream);
+    launch_work_order(ctx->work, ctx->G, ctx->d_toff_one, ctx->d_box[p], correction_item_voxels(), ctx->stream);
     c.order = ctx->work.order;
+    c.item_off = ctx->work.item_off;
     c.queue = ctx->work.queue;
     launch_correction<T>(c, stage_grid(ctx, ST_CONV), ctx->stream);
-    ctx->launches += 3;
+    ctx->launches += 5;
     CK(cudaGetLastError());
     return GG_OK;
 }
@@ -870,7 +871,7 @@ void free_all(gg_ctx* c) {
                     c->hull.rec_list, c->hull.rec_ntri, c->hull.bary, c->hull.tarea, c->hull.diag, c->el.earea, c->el.ebf, c->el.ecb, c->el.eidx, c->el.n_flat, c->el.eorg, c->hull.n_rec, c->hull.n_tri, c->el.n_elem,
                     c->el.elem, c->el.ids, c->el.segs, c->el.ebary, c->el.chunks, c->el.n_idx, c->el.idx_key, c->el.idx_rng,
                     c->el.idx_elem, c->d_err, c->d_total_vox, c->d_count3, c->bins.count, c->work.keys,
-                    c->work.keys_out, c->work.vals, c->work.order, c->work.temp, c->work.queue,
+                    c->work.keys_out, c->work.vals, c->work.order, c->work.item_off, c->work.temp, c->work.queue,
                     c->bins.off, c->bins.cursor, c->bins.entries, c->bins.max_count};
     for (void* p : ptrs)
         if (p) cudaFree(p);
@@ -963,6 +964,7 @@ int gg_create(const gg_params* params, gg_ctx** out) {
     CK(dalloc(&ctx->work.keys_out, G1));
     CK(dalloc(&ctx->work.vals, G1));
     CK(dalloc(&ctx->work.order, G1));
+    CK(dalloc(&ctx->work.item_off, G1 + 1));
     CK(dalloc(&ctx->work.queue, kQueues));
     ctx->work.temp_bytes = work_order_temp_bytes(ctx->G);
     CK(cudaMalloc(&ctx->work.temp, ctx->work.temp_bytes ? ctx->work.temp_bytes : 1));
@@ -1069,8 +1071,9 @@ int gg_load_state(gg_ctx* ctx, const uint32_t* labels, const int32_t* extents, c
         CK(dalloc(&ctx->el.segs, (size_t)ctx->el.seg_cap * G1h));
         CK(dalloc(&ctx->el.ebary, 3 * cap * G1h));
         CK(dalloc(&ctx->el.earea, cap * G1h));
-        CK(dalloc(&ctx->el.ebf, cap * G1h));
-        CK(dalloc(&ctx->el.eidx, cap * G1h));
+        ctx->el.flat_cap = (int)((cap + ctx->el.elem_cap + 1) & ~1LL);
+        CK(dalloc(&ctx->el.ebf, (size_t)ctx->el.flat_cap * G1h));
+        CK(dalloc(&ctx->el.eidx, (size_t)ctx->el.flat_cap * G1h));
         CK(dalloc(&ctx->el.n_flat, G1h));
         CK(cudaMemset(ctx->el.n_flat, 0, sizeof(int) * G1h));
         CK(dalloc(&ctx->el.eorg, G1h));

@@ -43,6 +43,7 @@ constexpr unsigned kFull = 0xFFFFFFFFu;
 constexpr int kIdxMax = 256;       // distinct neighbour IDs the elements of one hull search
 constexpr int kIHash = 2 * kIdxMax;
 constexpr int kPairMax = 1024;     // (element, searched ID) pairs of one hull
+constexpr float kPadQ = 3.0e38f;   // |p|^2 of a padding barycenter: its q is never a minimum
 constexpr int kJobMax = 9 * kLMax; // misorientations of one hull's elements (9 per QJ list)
 
 // ---------------------------------------------------------------------------------
@@ -696,13 +697,15 @@ __global__ void __launch_bounds__(32) elements_kernel(ElementArgs a) {
                 e.energy = en;
                 e.mobility = mo;
                 e.area = 0.0;
-                if (pb + pcnt > a.el.bary_cap) {  // every barycenter belongs to one element
+                // every barycenter belongs to one element; each element's run starts on a
+                // pair boundary and an odd run gets one padding entry (ebf's pair layout)
+                if (pb + pcnt + (pcnt & 1) > a.el.flat_cap) {
                     over = true;
                     pcnt = 0;
                 }
                 e.pbase = pb;
                 e.pcount = pcnt;
-                pb += pcnt;
+                pb += pcnt + (pcnt & 1);
                 // the IDs projectPointToGrainBoundary compares: all for a high-order
                 // junction, else the first 3 (QJ), 2 (TL), 1 (GB); each element once per ID
                 const int nc = type == 4 ? nid : min(nid, type);
@@ -864,9 +867,9 @@ __global__ void __launch_bounds__(32) elements_kernel(ElementArgs a) {
             // every barycenter to its element's run: lane-parallel over the grouped array,
             // barycenter i of list k (the last list whose first barycenter is <= i) going to
             // lflat[k] + (i - off[k])
-            float4* pf = a.el.ebf + (long long)g * a.el.bary_cap;
-            int* pidx = a.el.eidx + (long long)g * a.el.bary_cap;
-            const int nl = S.nl, total = min(nbary, a.el.bary_cap), nflat = min(S.np_flat, a.el.bary_cap);
+            float* pf = reinterpret_cast<float*>(a.el.ebf + (long long)g * a.el.flat_cap);
+            int* pidx = a.el.eidx + (long long)g * a.el.flat_cap;
+            const int nl = S.nl, total = min(nbary, a.el.bary_cap), nflat = min(S.np_flat, a.el.flat_cap);
             float r2 = 0.f;
             for (int i = lane; i < total; i += 32) {
                 int lo = 0, hi = nl - 1;
@@ -881,9 +884,28 @@ __global__ void __launch_bounds__(32) elements_kernel(ElementArgs a) {
                 const double dx = eb[3 * (long long)i] - org[0], dy = eb[3 * (long long)i + 1] - org[1],
                              dz = eb[3 * (long long)i + 2] - org[2];
                 const double w = dx * dx + dy * dy + dz * dz;
-                pf[dst] = make_float4((float)dx, (float)dy, (float)dz, (float)w);
+                float* pp = pf + 8 * (dst >> 1) + (dst & 1);  // pair layout: x0 x1 y0 y1 z0 z1 w0 w1
+                pp[0] = (float)dx;
+                pp[2] = (float)dy;
+                pp[4] = (float)dz;
+                pp[6] = (float)w;
                 pidx[dst] = i;
                 r2 = fmaxf(r2, (float)w);
+            }
+            // the padding entry of every odd run: at the origin with q = kInf, never a minimum
+            {
+                const HullElem* E = a.el.elem + (long long)g * a.el.elem_cap;
+                for (int e = lane; e < S.ne; e += 32) {
+                    const int n = E[e].pcount, dst = E[e].pbase + n;
+                    if ((n & 1) && dst >= 0 && dst < nflat) {
+                        float* pp = pf + 8 * (dst >> 1) + (dst & 1);
+                        pp[0] = 0.f;
+                        pp[2] = 0.f;
+                        pp[4] = 0.f;
+                        pp[6] = kPadQ;
+                        pidx[dst] = -1;
+                    }
+                }
             }
 #pragma unroll
             for (int o = 16; o > 0; o >>= 1) r2 = fmaxf(r2, __shfl_xor_sync(kFull, r2, o));
@@ -925,21 +947,20 @@ __device__ __forceinline__ double sqdist3(double x, double y, double z, const do
 }
 
 constexpr int kCThreads = 256;
-constexpr int kCVox = 2048;           // voxels of one pass: a run of the box in [z][y][x] order
+constexpr int kCVox = 4096;           // voxels of one pass: a run of the box in [z][y][x] order
+constexpr int kCItem = 4 * kCVox;     // voxels of one work item: a grain's box is cut into runs of these
 constexpr unsigned short kNoD = 0xFFFF;
 constexpr float kInf = 3.0e38f;
-constexpr int kSPts = 2560;           // barycenters staged in shared memory (more: read from HBM)
+constexpr int kSPts = 2304;           // barycenters staged in shared memory (more: read from HBM)
 constexpr int kSElem = kLMax;         // elements per grain: one per distinct list at most
 constexpr int kSPairs = kPairMax;     // the index's (element, ID) pairs per grain
 static_assert(kSElem <= 0xFFFF && kSPairs <= 0xFFFF, "16-bit element and pair indices");
 
 // One grain's search data, staged once per grain, and the slice pass's voxel groups.
 struct CorrSmem {
-    float4 pts[kSPts];            // FP32 barycenters, element by element (ebf)
+    float4 pts[kSPts];            // FP32 barycenters, element by element, in pairs (ebf)
     float box[kSElem][6];         // element boxes relative to the origin, rounded outward
-    int2 crng[kSElem];            // element e's chunks: (first, count)
-    int2 erun[kSElem];            // element e's barycenters as one run (first, count), or x = -1:
-                                  // several runs (a merged junction), taken chunk by chunk
+    int2 erun[kSElem];            // element e's run in ebf: (first, count), both even
     unsigned short pairs[kSPairs];// the index's element lists (search order per ID)
     uint32_t hkey[kCHash];        // neighbour ID -> dense index d
     unsigned short hden[kCHash];
@@ -947,7 +968,8 @@ struct CorrSmem {
     int dcnt[kIdxMax], doff[kIdxMax], dcur[kIdxMax], dpk[kIdxMax + 1];
     unsigned short vd[kCVox];     // dense neighbour index of the pass's voxels, kNoD: no search
     unsigned short vlist[kCVox];  // pass voxels grouped by neighbour
-    int next;                     // the work-order position this CTA fetched
+    int next;                     // the work item this CTA fetched
+    int pk_next;                  // the pass's next unclaimed packet
 };
 
 // q of barycenter p for the voxel whose relative coordinates give (ax, ay, az) = -2 v':
@@ -956,31 +978,53 @@ __device__ __forceinline__ float qval(const float4 p, float ax, float ay, float 
     return fmaf(az, p.z, fmaf(ay, p.y, fmaf(ax, p.x, p.w)));
 }
 
-// The least q over n consecutive barycenters.
-__device__ __forceinline__ float run_min(const float4* p, int n, float ax, float ay, float az) {
-    float m0 = kInf, m1 = kInf;
-    int i = 0;
-    for (; i + 4 <= n; i += 4) {
-        const float4 a = p[i], b = p[i + 1], c = p[i + 2], d = p[i + 3];
-        m0 = fminf(m0, qval(a, ax, ay, az));
-        m1 = fminf(m1, qval(b, ax, ay, az));
-        m0 = fminf(m0, qval(c, ax, ay, az));
-        m1 = fminf(m1, qval(d, ax, ay, az));
-    }
-    for (; i < n; i++) m0 = fminf(m0, qval(p[i], ax, ay, az));
-    return fminf(m0, m1);
+// Barycenter i of the pair layout (x0 x1 y0 y1 | z0 z1 w0 w1 per pair) as (x, y, z, w).
+__device__ __forceinline__ float4 pt_at(const float4* pts, int i) {
+    const float* f = reinterpret_cast<const float*>(pts + 2 * (i >> 1)) + (i & 1);
+    return make_float4(f[0], f[2], f[4], f[6]);
 }
 
-// The least q over element e's barycenters: its run, or its chunks' runs.
-__device__ __forceinline__ float element_min(const CorrSmem& S, const float4* pts, const float4* gcb, int e,
-                                             float ax, float ay, float az) {
-    const int2 r = S.erun[e];
-    if (r.x >= 0) return run_min(pts + r.x, r.y, ax, ay, az);
-    const int2 cr = S.crng[e];
-    float m = kInf;
-    for (int ch = cr.x; ch < cr.x + cr.y; ch++)
-        m = fminf(m, run_min(pts + __float_as_int(gcb[2 * ch].w), __float_as_int(gcb[2 * ch + 1].w), ax, ay, az));
-    return m;
+// Two FP32 lanes packed in 64 bits: the operands of the packed FMA.
+__device__ __forceinline__ unsigned long long pack2(float lo, float hi) {
+    unsigned long long r;
+    asm("mov.b64 %0, {%1, %2};" : "=l"(r) : "f"(lo), "f"(hi));
+    return r;
+}
+
+// fma.rn per lane: each half rounds exactly as fmaf does.
+__device__ __forceinline__ unsigned long long fma2(unsigned long long a, unsigned long long b,
+                                                   unsigned long long c) {
+    unsigned long long d;
+    asm("fma.rn.f32x2 %0, %1, %2, %3;" : "=l"(d) : "l"(a), "l"(b), "l"(c));
+    return d;
+}
+
+// min(m, both halves of r).
+__device__ __forceinline__ float min_of(float m, unsigned long long r) {
+    float lo, hi, d;
+    asm("mov.b64 {%0, %1}, %2;" : "=f"(lo), "=f"(hi) : "l"(r));
+    asm("min.f32 %0, %1, %2, %3;" : "=f"(d) : "f"(m), "f"(lo), "f"(hi));
+    return d;
+}
+
+// The least q over the n (even) barycenters of a run starting at pair boundary `first`:
+// two barycenters per packed FMA chain, the same three roundings per barycenter as qval.
+__device__ __forceinline__ float run_min(const float4* pts, int first, int n, unsigned long long A2,
+                                         unsigned long long B2, unsigned long long C2) {
+    const ulonglong2* p = reinterpret_cast<const ulonglong2*>(pts + first);  // 2 per pair
+    const int np = n >> 1;
+    float m0 = kInf, m1 = kInf;
+    int i = 0;
+    for (; i + 2 <= np; i += 2) {
+        const ulonglong2 xy0 = p[2 * i], zw0 = p[2 * i + 1], xy1 = p[2 * i + 2], zw1 = p[2 * i + 3];
+        m0 = min_of(m0, fma2(C2, zw0.x, fma2(B2, xy0.y, fma2(A2, xy0.x, zw0.y))));
+        m1 = min_of(m1, fma2(C2, zw1.x, fma2(B2, xy1.y, fma2(A2, xy1.x, zw1.y))));
+    }
+    if (i < np) {
+        const ulonglong2 xy0 = p[2 * i], zw0 = p[2 * i + 1];
+        m0 = min_of(m0, fma2(C2, zw0.x, fma2(B2, xy0.y, fma2(A2, xy0.x, zw0.y))));
+    }
+    return fminf(m0, m1);
 }
 
 // The near-tie case: the barycenters whose q is within the band, measured with the
@@ -989,7 +1033,7 @@ __device__ __forceinline__ float element_min(const CorrSmem& S, const float4* pt
 // order, as projectPointToGrainBoundary does (grainHull.cpp:570-660).  Every barycenter
 // that can be the reference's winner has q <= best + eps2, so the subset has the same
 // winner.
-__device__ int exact_winner(const CorrSmem& S, const float4* pts, const float4* gcb, int first, int count, int ne,
+__device__ int exact_winner(const CorrSmem& S, const float4* pts, int first, int count, int ne,
                             const int* __restrict__ eidx, const double* __restrict__ eb, double x, double y, double z,
                             float ax, float ay, float az, float limit) {
     double bd = 10000000.0;
@@ -997,19 +1041,15 @@ __device__ int exact_winner(const CorrSmem& S, const float4* pts, const float4* 
     for (int c = 0; c < count; c++) {
         const int e = S.pairs[first + c];
         if (e >= ne) continue;
-        // the element's run, or its chunks: either covers its barycenters in order
-        const int2 r = S.erun[e], cr = S.crng[e];
-        const int nrun = r.x >= 0 ? 1 : cr.y;
-        for (int u = 0; u < nrun; u++) {
-            const int p0 = r.x >= 0 ? r.x : __float_as_int(gcb[2 * (cr.x + u)].w);
-            const int pn = r.x >= 0 ? r.y : __float_as_int(gcb[2 * (cr.x + u) + 1].w);
-            for (int i = p0; i < p0 + pn; i++) {
-                if (qval(pts[i], ax, ay, az) > limit) continue;
-                const double d = sqdist3(x, y, z, eb + 3 * (long long)eidx[i]);
-                if (d < bd) {
-                    bd = d;
-                    bw = e;
-                }
+        const int2 r = S.erun[e];  // the element's barycenters in order (a padding entry: q = kInf)
+        for (int i = r.x; i < r.x + r.y; i++) {
+            if (qval(pt_at(pts, i), ax, ay, az) > limit) continue;
+            const int src = eidx[i];
+            if (src < 0) continue;
+            const double d = sqdist3(x, y, z, eb + 3 * (long long)src);
+            if (d < bd) {
+                bd = d;
+                bw = e;
             }
         }
     }
@@ -1036,12 +1076,12 @@ __device__ __forceinline__ float box_bound(float vx, float vy, float vz, float v
 // Elements are taken in reverse search order, so the grain boundary (last in search
 // order, and the usual winner) sets a tight best first, and an element is skipped when
 // no lane's voxel can come within the band of its best through the element's box.
-__device__ __forceinline__ int search_packet(const CorrSmem& S, const float4* pts, const float4* gcb, int first,
-                                             int count, bool active, int i, int j, int k, float4 org, float eps2,
-                                             int ne, const int* __restrict__ eidx, const double* __restrict__ eb,
-                                             int* err) {
+__device__ __forceinline__ int search_packet(const CorrSmem& S, const float4* pts, int first, int count, bool active,
+                                             int i, int j, int k, float4 org, float eps2, int ne,
+                                             const int* __restrict__ eidx, const double* __restrict__ eb, int* err) {
     const float vx = (float)i - org.x, vy = (float)j - org.y, vz = (float)k - org.z;  // exact
     const float ax = -2.f * vx, ay = -2.f * vy, az = -2.f * vz;
+    const unsigned long long A2 = pack2(ax, ax), B2 = pack2(ay, ay), C2 = pack2(az, az);
     const float vv = vx * vx + vy * vy + vz * vz;  // exact (integers below 2^24)
     const float eps = 0.5f * eps2;
     float best = kInf, second = kInf;
@@ -1058,7 +1098,8 @@ __device__ __forceinline__ int search_packet(const CorrSmem& S, const float4* pt
         if (!__any_sync(kFull, active && box_bound(vx, vy, vz, vv, bx[0], bx[1], bx[2], bx[3], bx[4], bx[5], eps) <=
                                              best + eps2))
             continue;
-        const float m = element_min(S, pts, gcb, e, ax, ay, az);
+        const int2 r = S.erun[e];
+        const float m = run_min(pts, r.x, r.y, A2, B2, C2);
         if (m < best) {
             second = best;
             best = m;
@@ -1069,7 +1110,7 @@ __device__ __forceinline__ int search_packet(const CorrSmem& S, const float4* pt
     }
     if (beste < 0) return -1;
     if (second - best > eps2) return beste;  // proven: every other element is farther
-    return exact_winner(S, pts, gcb, first, count, ne, eidx, eb, (double)i, (double)j, (double)k, ax, ay, az,
+    return exact_winner(S, pts, first, count, ne, eidx, eb, (double)i, (double)j, (double)k, ax, ay, az,
                         best + eps2);
 }
 
@@ -1101,14 +1142,16 @@ __global__ void __launch_bounds__(kCThreads, 3) correction_kernel(CorrectionArgs
     const double delta = a.geo.delta;
     const HullElements& el = a.el;
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
-    const int n_work = a.toff[a.G + 1];  // grains with a tile (0 when the plan overflowed)
+    const int n_items = a.item_off[a.G + 1];
     for (;;) {
-        __syncthreads();  // the previous grain's packets are done with the shared arrays
+        __syncthreads();  // the previous item's packets are done with the shared arrays
         if (threadIdx.x == 0) S.next = atomicAdd(a.queue, 1);
         __syncthreads();
         const int t = S.next;
-        if (t >= n_work) break;
-        const int g = a.order[t];
+        if (t >= n_items) break;
+        const int pos = work_position(a.item_off, a.G, t);
+        const int g = a.order[pos];
+        const long long item = t - a.item_off[pos];  // the run of box voxels this CTA takes
         if (g < 1 || g > a.G) {
             if (threadIdx.x == 0) atomicOr(a.err, ERR_BOUNDS);
             continue;
@@ -1119,35 +1162,18 @@ __global__ void __launch_bounds__(kCThreads, 3) correction_kernel(CorrectionArgs
             if (threadIdx.x == 0) atomicOr(a.err, ERR_BOUNDS);
             nd = 0;
         }
-        const int nflat = min(max(el.n_flat[g], 0), el.bary_cap);
+        const int nflat = min(max(el.n_flat[g], 0), el.flat_cap) & ~1;
         const int npairs = min(el.pair_cap, kSPairs);
         const float4 org = el.eorg[g];
-        const float4* gpts = el.ebf + (long long)g * el.bary_cap;
-        const float4* gcb = el.ecb + 2 * (long long)g * el.chunk_cap;
+        const float4* gpts = el.ebf + (long long)g * el.flat_cap;
         for (int q = threadIdx.x; q < kCHash; q += blockDim.x) S.hkey[q] = kNoId;
         for (int q = threadIdx.x; q < npairs; q += blockDim.x)
             S.pairs[q] = el.idx_elem[(long long)g * el.pair_cap + q];
         for (int e = threadIdx.x; e < ne; e += blockDim.x) {
             const HullElem& E = el.elem[(long long)g * el.elem_cap + e];
-            int2 r = make_int2(E.chunk_off, E.nchunk);
-            if (r.x < 0 || r.y < 0 || r.x + r.y > el.chunk_cap) {
+            int2 run = make_int2(E.pbase, E.pcount + (E.pcount & 1));  // with its padding entry
+            if (run.x < 0 || (run.x & 1) || run.y < 0 || run.x + run.y > nflat) {
                 atomicOr(a.err, ERR_BOUNDS);
-                r = make_int2(0, 0);
-            }
-            S.crng[e] = r;
-            // one run when the chunks follow one another in the flattened copy
-            int2 run = make_int2(-1, 0);
-            if (r.y > 0) {
-                const int f0 = __float_as_int(gcb[2 * r.x].w);
-                int end = f0;
-                bool one = f0 >= 0;
-                for (int ch = r.x; ch < r.x + r.y && one; ch++) {
-                    const int f = __float_as_int(gcb[2 * ch].w), n = __float_as_int(gcb[2 * ch + 1].w);
-                    one = f == end && n >= 0;
-                    end = f + n;
-                }
-                if (one && end <= nflat) run = make_int2(f0, end - f0);
-            } else {
                 run = make_int2(0, 0);
             }
             S.erun[e] = run;
@@ -1180,7 +1206,7 @@ __global__ void __launch_bounds__(kCThreads, 3) correction_kernel(CorrectionArgs
         }
         __syncthreads();
         const float4* pts = nflat <= kSPts ? S.pts : gpts;
-        const int* eidx = el.eidx + (long long)g * el.bary_cap;
+        const int* eidx = el.eidx + (long long)g * el.flat_cap;
         const Box b = load_box(a.box + 6 * g);
         const Box bo = load_box(a.idbox_old + 6 * g);
         const long long old_count = bo.count();
@@ -1204,9 +1230,11 @@ __global__ void __launch_bounds__(kCThreads, 3) correction_kernel(CorrectionArgs
         const float eps2 = fmaxf(2.f * 16.f * r2 * (1.0f / 16777216.f) * 1.0001f, 1e-6f);
         // passes over consecutive runs of kCVox voxels of the box, across rows and slices,
         // so that a pass holds many packets and few barriers are paid per voxel
-        for (long long v0 = 0; v0 < nvox; v0 += kCVox) {
-            const int nv = (int)min((long long)kCVox, nvox - v0);
+        const long long v_end = min(nvox, (item + 1) * kCItem);
+        for (long long v0 = item * kCItem; v0 < v_end; v0 += kCVox) {
+            const int nv = (int)min((long long)kCVox, v_end - v0);
             for (int d = threadIdx.x; d < nd; d += blockDim.x) S.dcnt[d] = 0;
+            if (threadIdx.x == 0) S.pk_next = nwarps;  // packet w goes to warp w, the rest on demand
             __syncthreads();
             // band voxels: their neighbour; voxels whose neighbour no element holds get (1, 1)
             // now.  Four voxels per thread at a time: their loads are in flight together.
@@ -1276,7 +1304,7 @@ __global__ void __launch_bounds__(kCThreads, 3) correction_kernel(CorrectionArgs
             }
             __syncthreads();
             const int P = S.dpk[nd];
-            for (int pk = warp; pk < P; pk += nwarps) {
+            for (int pk = warp; pk < P;) {
                 int lo = 0, hi = nd - 1;  // the neighbour whose packets hold pk
                 while (lo < hi) {
                     const int mid = (lo + hi + 1) >> 1;
@@ -1293,11 +1321,14 @@ __global__ void __launch_bounds__(kCThreads, 3) correction_kernel(CorrectionArgs
                 const int i = b.y0 + rem / nx, j = b.x0 + rem % nx;
                 // the point is Vector3d(i, j, k), box.cpp:481
                 const int2 dr = S.drng[d];
-                const int win = search_packet(S, pts, gcb, dr.x, dr.y, active, i, j, k, org, eps2, ne, eidx, eb, a.err);
+                const int win = search_packet(S, pts, dr.x, dr.y, active, i, j, k, org, eps2, ne, eidx, eb, a.err);
                 if (active) {
                     const uint32_t id = f < old_count ? idl[f] : 0u;
                     correct_voxel(a, elem, g, win, id, (double)in[f], out + f);
                 }
+                int nxt = 0;
+                if (lane == 0) nxt = atomicAdd(&S.pk_next, 1);
+                pk = __shfl_sync(kFull, nxt, 0);
             }
             __syncthreads();
         }
@@ -1307,6 +1338,7 @@ __global__ void __launch_bounds__(kCThreads, 3) correction_kernel(CorrectionArgs
 }  // namespace
 
 size_t elements_scratch_per_cta() { return kElemScratch; }
+int correction_item_voxels() { return kCItem; }
 
 namespace {
 __global__ void faces_kernel(int G, const int* exists, HullElements el, const long long* off, int* count,

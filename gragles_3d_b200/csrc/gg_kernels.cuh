@@ -36,22 +36,36 @@ struct PlanArgs {
 };
 void launch_plan(const PlanArgs& a, cudaStream_t s);
 
-// ---- largest-first work order for the per-grain kernels (gg_plan.cu) ----
-// order[0, toff[G + 1]) = the grains with a tile in `toff` (one tile per grain), by
-// decreasing box voxels; the kernels that take it fetch positions from a counter
-// (*queue, zeroed here) so that the largest grains start first and the rest fill in.
+// ---- largest-first work items for the per-grain kernels (gg_plan.cu) ----
+// order[0, n) = the grains with a tile in `toff_one`, by decreasing box voxels; grain
+// order[i] is cut into items of item_vox box voxels (the last one shorter), numbered
+// from item_off[i] on (item_off[G + 1] = all items).  The kernels that take it fetch
+// item numbers from a counter (*queue, zeroed here), so that the largest grains start
+// first, the rest fill in, and no grain is longer than one item on one CTA.
 struct WorkOrder {
     int* keys;               // G + 1 scratch keys
-    int* keys_out;           // G + 1
+    int* keys_out;           // G + 1: box voxels + 1 in order, 0 for grains without a tile
     int* vals;               // G + 1 (grain IDs)
     int* order;              // G + 1 (out)
-    void* temp;              // radix-sort scratch
+    int* item_off;           // G + 2 (out)
+    void* temp;              // radix-sort and scan scratch
     size_t temp_bytes;
     int* queue;              // kQueues counters (out: zeroed)
 };
 constexpr int kQueues = 4;
 size_t work_order_temp_bytes(int G);
-void launch_work_order(const WorkOrder& w, int G, const int* toff_one, const int* box, cudaStream_t s);
+void launch_work_order(const WorkOrder& w, int G, const int* toff_one, const int* box, int item_vox,
+                       cudaStream_t s);
+
+// The position i of work item t in the order: the last i in [0, G] with item_off[i] <= t.
+__device__ __forceinline__ int work_position(const int* __restrict__ item_off, int G, int t) {
+    int lo = 0, hi = G + 1;
+    while (hi - lo > 1) {
+        const int mid = (lo + hi) >> 1;
+        if (__ldg(item_off + mid) <= t) lo = mid; else hi = mid;
+    }
+    return lo;
+}
 
 // Copy box + offsets of every present grain from one layout to another.
 void launch_copy_layout(int G, const int* present, const int* box_src, const long long* off_src, int* box_dst,
@@ -226,6 +240,7 @@ struct HullChunk {
 
 struct HullElements {
     int elem_cap, id_cap, seg_cap, bary_cap, chunk_cap, idx_cap, pair_cap;
+    int flat_cap;             // entries of ebf / eidx per grain: bary_cap + one padding per element
     int* n_elem;              // G + 1
     HullElem* elem;           // (G + 1) x elem_cap
     uint32_t* ids;            // (G + 1) x id_cap
@@ -233,10 +248,12 @@ struct HullElements {
     double* ebary;            // (G + 1) x bary_cap x 3, barycenters grouped by neighbour list
     double* earea;            // (G + 1) x bary_cap, their triangles' area terms in the same order
     // The same barycenters for the correction's FP32 filter, element by element in table
-    // order (element e's at [pbase, pbase + pcount)): (p - o, |p - o|^2) in FP32, p - o
-    // and its square taken in FP64 first, with o the grain's integer origin
-    float4* ebf;              // (G + 1) x bary_cap
-    int* eidx;                // (G + 1) x bary_cap: position of each of them in ebary
+    // order (element e's at [pbase, pbase + pcount), pbase even, an odd run padded by one
+    // entry with |p - o|^2 = 3e38): (p - o, |p - o|^2) in FP32, p - o and its square taken
+    // in FP64 first, with o the grain's integer origin.  Pairs of entries are interleaved
+    // as (x0, x1, y0, y1), (z0, z1, w0, w1) for the packed FMA.
+    float4* ebf;              // (G + 1) x flat_cap
+    int* eidx;                // (G + 1) x flat_cap: position of each of them in ebary (-1: padding)
     // each chunk's box relative to the origin, rounded outward to FP32, and its run in
     // ebf: (lo.x, lo.y, lo.z, first as int bits), (hi.x, hi.y, hi.z, count as int bits)
     float4* ecb;              // (G + 1) x chunk_cap x 2
@@ -297,10 +314,12 @@ struct CorrectionArgs {
     const long long* idoff_old;
     HullElements el;
     HullPhysics ph;
-    const int* order;         // grains by decreasing box (WorkOrder), fetched through *queue
+    const int* order;         // grains by decreasing box (WorkOrder) and their work items,
+    const int* item_off;      // fetched through *queue
     int* queue;
     int* err;
 };
+int correction_item_voxels();  // box voxels of one work item of the correction
 template <typename T>
 void launch_correction(const CorrectionArgs<T>& a, int grid, cudaStream_t s);
 

@@ -10,6 +10,7 @@
 #include "gg_kernels.cuh"
 
 #include <cub/device/device_radix_sort.cuh>
+#include <cub/device/device_scan.cuh>
 
 #include <climits>
 
@@ -141,11 +142,13 @@ void launch_copy_layout(int G, const int* present, const int* box_src, const lon
 
 
 namespace {
-// Sort keys of the work order: box voxels + 1 for the grains with a tile, 0 for the rest.
+// Sort keys of the work order: box voxels + 1 for the grains with a tile, 0 for the rest
+// (all of them when the plan overflowed and gave no tiles).
 __global__ void order_keys_kernel(int G, const int* toff_one, const int* box, int* keys, int* vals) {
+    const bool none = toff_one[G + 1] == 0;
     for (int g = blockIdx.x * blockDim.x + threadIdx.x; g <= G; g += gridDim.x * blockDim.x) {
         int key = 0;
-        if (g >= 1 && toff_one[g + 1] - toff_one[g] > 0) {
+        if (g >= 1 && !none && toff_one[g + 1] - toff_one[g] > 0) {
             const Box b = load_box(box + 6 * g);
             key = (int)min(b.count() + 1, (long long)INT_MAX);
         }
@@ -153,20 +156,33 @@ __global__ void order_keys_kernel(int G, const int* toff_one, const int* box, in
         vals[g] = g;
     }
 }
+// Items per grain in order (item_off[i + 1]; item_off[0] = 0), summed afterwards.
+__global__ void item_count_kernel(int G, const int* keys_out, int item_vox, int* item_off) {
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i <= G; i += gridDim.x * blockDim.x) {
+        const long long v = (long long)keys_out[i] - 1;  // box voxels, -1: no tile
+        item_off[i + 1] = v < 0 ? 0 : (item_vox > 0 ? (int)((v + item_vox - 1) / item_vox) : 1);
+        if (i == 0) item_off[0] = 0;
+    }
+}
 }  // namespace
 
 size_t work_order_temp_bytes(int G) {
-    size_t bytes = 0;
-    cub::DeviceRadixSort::SortPairsDescending(nullptr, bytes, (const int*)nullptr, (int*)nullptr,
+    size_t sort = 0, scan = 0;
+    cub::DeviceRadixSort::SortPairsDescending(nullptr, sort, (const int*)nullptr, (int*)nullptr,
                                               (const int*)nullptr, (int*)nullptr, G + 1);
-    return bytes;
+    cub::DeviceScan::InclusiveSum(nullptr, scan, (const int*)nullptr, (int*)nullptr, G + 1);
+    return sort > scan ? sort : scan;
 }
 
-void launch_work_order(const WorkOrder& w, int G, const int* toff_one, const int* box, cudaStream_t s) {
+void launch_work_order(const WorkOrder& w, int G, const int* toff_one, const int* box, int item_vox,
+                       cudaStream_t s) {
     order_keys_kernel<<<(G + 256) / 256, 256, 0, s>>>(G, toff_one, box, w.keys, w.vals);
     size_t bytes = w.temp_bytes;
     cub::DeviceRadixSort::SortPairsDescending(w.temp, bytes, w.keys, w.keys_out, w.vals, w.order, G + 1, 0,
                                               31, s);
+    item_count_kernel<<<(G + 256) / 256, 256, 0, s>>>(G, w.keys_out, item_vox, w.item_off);
+    bytes = w.temp_bytes;
+    cub::DeviceScan::InclusiveSum(w.temp, bytes, w.item_off + 1, w.item_off + 1, G + 1, s);
     cudaMemsetAsync(w.queue, 0, sizeof(int) * kQueues, s);
 }
 
