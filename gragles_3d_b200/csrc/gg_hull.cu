@@ -949,6 +949,8 @@ __device__ __forceinline__ double sqdist3(double x, double y, double z, const do
 constexpr int kCThreads = 256;
 constexpr int kCVox = 4096;           // voxels of one pass: a run of the box in [z][y][x] order
 constexpr int kCItem = 4 * kCVox;     // voxels of one work item: a grain's box is cut into runs of these
+constexpr int kLV = 2;                // voxels per lane: a packet is 32 kLV voxels of one neighbour
+constexpr int kPacket = 32 * kLV;
 constexpr unsigned short kNoD = 0xFFFF;
 constexpr float kInf = 3.0e38f;
 constexpr int kSPts = 2304;           // barycenters staged in shared memory (more: read from HBM)
@@ -1007,24 +1009,23 @@ __device__ __forceinline__ float min_of(float m, unsigned long long r) {
     return d;
 }
 
-// The least q over the n (even) barycenters of a run starting at pair boundary `first`:
-// two barycenters per packed FMA chain, the same three roundings per barycenter as qval.
-__device__ __forceinline__ float run_min(const float4* pts, int first, int n, unsigned long long A2,
-                                         unsigned long long B2, unsigned long long C2) {
+// The least q, for each of a lane's V voxels, over the n (even) barycenters of a run
+// starting at pair boundary `first`: two barycenters per packed FMA chain, the same
+// three roundings per barycenter as qval.  Each loaded pair serves all V voxels.
+template <int V>
+__device__ __forceinline__ void run_min(const float4* pts, int first, int n, const unsigned long long (&A2)[V],
+                                        const unsigned long long (&B2)[V], const unsigned long long (&C2)[V],
+                                        float (&m)[V]) {
     const ulonglong2* p = reinterpret_cast<const ulonglong2*>(pts + first);  // 2 per pair
     const int np = n >> 1;
-    float m0 = kInf, m1 = kInf;
-    int i = 0;
-    for (; i + 2 <= np; i += 2) {
-        const ulonglong2 xy0 = p[2 * i], zw0 = p[2 * i + 1], xy1 = p[2 * i + 2], zw1 = p[2 * i + 3];
-        m0 = min_of(m0, fma2(C2, zw0.x, fma2(B2, xy0.y, fma2(A2, xy0.x, zw0.y))));
-        m1 = min_of(m1, fma2(C2, zw1.x, fma2(B2, xy1.y, fma2(A2, xy1.x, zw1.y))));
+#pragma unroll
+    for (int u = 0; u < V; u++) m[u] = kInf;
+#pragma unroll 2
+    for (int i = 0; i < np; i++) {
+        const ulonglong2 xy = p[2 * i], zw = p[2 * i + 1];
+#pragma unroll
+        for (int u = 0; u < V; u++) m[u] = min_of(m[u], fma2(C2[u], zw.x, fma2(B2[u], xy.y, fma2(A2[u], xy.x, zw.y))));
     }
-    if (i < np) {
-        const ulonglong2 xy0 = p[2 * i], zw0 = p[2 * i + 1];
-        m0 = min_of(m0, fma2(C2, zw0.x, fma2(B2, xy0.y, fma2(A2, xy0.x, zw0.y))));
-    }
-    return fminf(m0, m1);
 }
 
 // The near-tie case: the barycenters whose q is within the band, measured with the
@@ -1067,62 +1068,87 @@ __device__ __forceinline__ float box_bound(float vx, float vy, float vz, float v
     return d2 * (1.f - 1.0f / 1048576.f) - vv - eps;
 }
 
-// The element whose (energy, mobility) the voxel (i, j, k) takes: the reference's
-// winner among the elements S.pairs[first, first + count) (-1: none, weight (1, 1)).
-// All lanes of the warp call it with the same elements (a packet of one neighbour).
-// Each element's least q is compared with the best and second-best so far; when the
-// best element beats every other by more than eps2 (twice the filter's error bound) it
-// is the reference's winner, else the near tie is settled in FP64 (exact_winner).
-// Elements are taken in reverse search order, so the grain boundary (last in search
-// order, and the usual winner) sets a tight best first, and an element is skipped when
-// no lane's voxel can come within the band of its best through the element's box.
-__device__ __forceinline__ int search_packet(const CorrSmem& S, const float4* pts, int first, int count, bool active,
-                                             int i, int j, int k, float4 org, float eps2, int ne,
-                                             const int* __restrict__ eidx, const double* __restrict__ eb, int* err) {
-    const float vx = (float)i - org.x, vy = (float)j - org.y, vz = (float)k - org.z;  // exact
-    const float ax = -2.f * vx, ay = -2.f * vy, az = -2.f * vz;
-    const unsigned long long A2 = pack2(ax, ax), B2 = pack2(ay, ay), C2 = pack2(az, az);
-    const float vv = vx * vx + vy * vy + vz * vz;  // exact (integers below 2^24)
+// The elements whose (energy, mobility) a lane's V voxels (i, j, k) take: the
+// reference's winner among the elements S.pairs[first, first + count) (-1: none,
+// weight (1, 1)).  All lanes of the warp call it with the same elements (a packet of one
+// neighbour).  Per voxel, each element's least q is compared with the best and
+// second-best so far; when the best element beats every other by more than eps2 (twice
+// the filter's error bound) it is the reference's winner, else the near tie is settled
+// in FP64 (exact_winner).  Elements are taken in reverse search order, so the grain
+// boundary (last in search order, and the usual winner) sets a tight best first, and an
+// element is skipped when no voxel of the warp can come within the band of its best
+// through the element's box.
+template <int V>
+__device__ __forceinline__ void search_packet(const CorrSmem& S, const float4* pts, int first, int count,
+                                              const bool (&active)[V], const int (&ii)[V], const int (&jj)[V],
+                                              const int (&kk)[V], float4 org, float eps2, int ne,
+                                              const int* __restrict__ eidx, const double* __restrict__ eb, int* err,
+                                              int (&win)[V]) {
+    float vx[V], vy[V], vz[V], vv[V], best[V], second[V];
+    unsigned long long A2[V], B2[V], C2[V];
+    int beste[V];
+#pragma unroll
+    for (int u = 0; u < V; u++) {
+        vx[u] = (float)ii[u] - org.x;  // exact
+        vy[u] = (float)jj[u] - org.y;
+        vz[u] = (float)kk[u] - org.z;
+        vv[u] = vx[u] * vx[u] + vy[u] * vy[u] + vz[u] * vz[u];  // exact (integers below 2^24)
+        A2[u] = pack2(-2.f * vx[u], -2.f * vx[u]);
+        B2[u] = pack2(-2.f * vy[u], -2.f * vy[u]);
+        C2[u] = pack2(-2.f * vz[u], -2.f * vz[u]);
+        best[u] = second[u] = kInf;
+        beste[u] = -1;
+    }
     const float eps = 0.5f * eps2;
-    float best = kInf, second = kInf;
-    int beste = -1;
     for (int c = count - 1; c >= 0; c--) {
         const int e = S.pairs[first + c];
         if (e >= ne) {
             if ((threadIdx.x & 31) == 0) atomicOr(err, ERR_BOUNDS);
             continue;
         }
-        // an element, then each of its chunks, is skipped when no lane's voxel can come
-        // within the band of its best through the box (best = kInf: never skipped)
+        // skipped when no voxel can come within the band of its best through the
+        // element's box (best = kInf: never skipped)
         const float* bx = S.box[e];
-        if (!__any_sync(kFull, active && box_bound(vx, vy, vz, vv, bx[0], bx[1], bx[2], bx[3], bx[4], bx[5], eps) <=
-                                             best + eps2))
-            continue;
+        const float lx = bx[0], ly = bx[1], lz = bx[2], hx = bx[3], hy = bx[4], hz = bx[5];
+        bool need = false;
+#pragma unroll
+        for (int u = 0; u < V; u++)
+            need = need || (active[u] && box_bound(vx[u], vy[u], vz[u], vv[u], lx, ly, lz, hx, hy, hz, eps) <=
+                                             best[u] + eps2);
+        if (!__any_sync(kFull, need)) continue;
         const int2 r = S.erun[e];
-        const float m = run_min(pts, r.x, r.y, A2, B2, C2);
-        if (m < best) {
-            second = best;
-            best = m;
-            beste = e;
-        } else {
-            second = fminf(second, m);
+        float m[V];
+        run_min<V>(pts, r.x, r.y, A2, B2, C2, m);
+#pragma unroll
+        for (int u = 0; u < V; u++) {
+            if (m[u] < best[u]) {
+                second[u] = best[u];
+                best[u] = m[u];
+                beste[u] = e;
+            } else {
+                second[u] = fminf(second[u], m[u]);
+            }
         }
     }
-    if (beste < 0) return -1;
-    if (second - best > eps2) return beste;  // proven: every other element is farther
-    return exact_winner(S, pts, first, count, ne, eidx, eb, (double)i, (double)j, (double)k, ax, ay, az,
-                        best + eps2);
+#pragma unroll
+    for (int u = 0; u < V; u++) {
+        win[u] = beste[u];
+        // proven when every other element is farther by more than the band
+        if (beste[u] >= 0 && !(second[u] - best[u] > eps2))
+            win[u] = exact_winner(S, pts, first, count, ne, eidx, eb, (double)ii[u], (double)jj[u], (double)kk[u],
+                                  -2.f * vx[u], -2.f * vy[u], -2.f * vz[u], best[u] + eps2);
+    }
 }
 
 // The update of one band voxel, box.cpp:476-533, given the element that won (-1: none).
 template <typename T>
 __device__ __forceinline__ void correct_voxel(const CorrectionArgs<T>& a, const HullElem* elem, int g, int win,
-                                              uint32_t id, double val, T* outp) {
+                                              uint32_t id, double val, double conv, T* outp) {
     const double ts = 1 / 1.21;  // TimeSlope, grainhdl.cpp:1432
     const double E = win >= 0 ? elem[win].energy : 1.0, M = win >= 0 ? elem[win].mobility : 1.0;
     // GBInfo(m_energy, m_mobility) fills (mobility, energy): field energy = M, field mobility = E
     const double fe = M, fm = E;
-    double o = val + ((double)*outp - val) * fe * fm * 1.0;
+    double o = val + (conv - val) * fe * fm * 1.0;
     if (a.ph.use_see) {
         const bool alive = id == 0 || (id <= (uint32_t)a.G && a.present[id]);
         const double fs = alive ? (a.ph.see[g] - a.ph.see[id]) * fm * a.ph.dt / (ts * ts) : 0.0;
@@ -1271,7 +1297,7 @@ __global__ void __launch_bounds__(kCThreads, 3) correction_kernel(CorrectionArgs
                             hs = (hs + 1) & (kCHash - 1);
                         }
                         if (dd != kNoD) atomicAdd(&S.dcnt[dd], 1);
-                        else correct_voxel(a, elem, g, -1, id, vals[u], out + fs[u]);
+                        else correct_voxel(a, elem, g, -1, id, vals[u], (double)out[fs[u]], out + fs[u]);
                     }
                     S.vd[q] = dd;
                 }
@@ -1281,7 +1307,7 @@ __global__ void __launch_bounds__(kCThreads, 3) correction_kernel(CorrectionArgs
                 int run = 0, prun = 0;
                 for (int d0 = 0; d0 < nd; d0 += 32) {
                     const int d = d0 + lane;
-                    const int c = d < nd ? S.dcnt[d] : 0, pk = (c + 31) >> 5;
+                    const int c = d < nd ? S.dcnt[d] : 0, pk = (c + kPacket - 1) / kPacket;
                     int ic = c, ip = pk;
 #pragma unroll
                     for (int o = 1; o < 32; o <<= 1) {
@@ -1312,20 +1338,39 @@ __global__ void __launch_bounds__(kCThreads, 3) correction_kernel(CorrectionArgs
                     else hi = mid - 1;
                 }
                 const int d = lo;
-                const int start = S.doff[d] + ((pk - S.dpk[d]) << 5);
-                const int cnt = min(32, S.doff[d] + S.dcnt[d] - start);
-                const bool active = lane < cnt;
-                const int q = S.vlist[start + (active ? lane : 0)];
-                const long long f = v0 + q;
-                const int k = b.z0 + (int)(f / nxy), rem = (int)(f % nxy);
-                const int i = b.y0 + rem / nx, j = b.x0 + rem % nx;
-                // the point is Vector3d(i, j, k), box.cpp:481
-                const int2 dr = S.drng[d];
-                const int win = search_packet(S, pts, dr.x, dr.y, active, i, j, k, org, eps2, ne, eidx, eb, a.err);
-                if (active) {
-                    const uint32_t id = f < old_count ? idl[f] : 0u;
-                    correct_voxel(a, elem, g, win, id, (double)in[f], out + f);
+                const int start = S.doff[d] + (pk - S.dpk[d]) * kPacket;
+                const int cnt = min(kPacket, S.doff[d] + S.dcnt[d] - start);
+                bool active[kLV];
+                int ii[kLV], jj[kLV], kk[kLV], win[kLV];
+                long long f[kLV];
+                T vin[kLV], vconv[kLV];
+                uint32_t id[kLV];
+#pragma unroll
+                for (int u = 0; u < kLV; u++) {
+                    const int slot = lane + 32 * u;
+                    active[u] = slot < cnt;
+                    const int q = S.vlist[start + (active[u] ? slot : 0)];
+                    f[u] = v0 + q;
+                    const int rem = (int)(f[u] % nxy);
+                    // the point is Vector3d(i, j, k), box.cpp:481
+                    kk[u] = b.z0 + (int)(f[u] / nxy);
+                    ii[u] = b.y0 + rem / nx;
+                    jj[u] = b.x0 + rem % nx;
+                    // the voxel's input, convolved value and IDLocal, loaded while the search runs
+                    vin[u] = T(0);
+                    vconv[u] = T(0);
+                    id[u] = 0u;
+                    if (active[u]) {
+                        vin[u] = in[f[u]];
+                        vconv[u] = out[f[u]];
+                        id[u] = f[u] < old_count ? idl[f[u]] : 0u;
+                    }
                 }
+                const int2 dr = S.drng[d];
+                search_packet<kLV>(S, pts, dr.x, dr.y, active, ii, jj, kk, org, eps2, ne, eidx, eb, a.err, win);
+#pragma unroll
+                for (int u = 0; u < kLV; u++)
+                    if (active[u]) correct_voxel(a, elem, g, win[u], id[u], (double)vin[u], (double)vconv[u], out + f[u]);
                 int nxt = 0;
                 if (lane == 0) nxt = atomicAdd(&S.pk_next, 1);
                 pk = __shfl_sync(kFull, nxt, 0);
