@@ -134,6 +134,11 @@ __device__ __forceinline__ void cp_async_elem(T* dst_smem, const T* src) {
     asm volatile("cp.async.ca.shared.global [%0], [%1], %2;\n" ::"r"(d), "l"(src), "n"(sizeof(T)) : "memory");
 }
 __device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;\n" ::: "memory"); }
+// Asynchronous 16-byte global -> shared copy through L2 (both addresses 16-byte aligned).
+__device__ __forceinline__ void cp_async16(void* dst_smem, const void* src) {
+    const unsigned d = (unsigned)__cvta_generic_to_shared(dst_smem);
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(d), "l"(src) : "memory");
+}
 
 // Opt a kernel into the largest dynamic shared memory the device allows next to
 // its static shared memory.

@@ -957,13 +957,14 @@ constexpr int kSPts = 2304;           // barycenters staged in shared memory (mo
 constexpr int kSElem = kLMax;         // elements per grain: one per distinct list at most
 constexpr int kSPairs = kPairMax;     // the index's (element, ID) pairs per grain
 static_assert(kSElem <= 0xFFFF && kSPairs <= 0xFFFF, "16-bit element and pair indices");
+static_assert(kSPairs % 8 == 0, "pair lists are copied 16 bytes at a time");
 
 // One grain's search data, staged once per grain, and the slice pass's voxel groups.
 struct CorrSmem {
     float4 pts[kSPts];            // FP32 barycenters, element by element, in pairs (ebf)
     float box[kSElem][6];         // element boxes relative to the origin, rounded outward
     int2 erun[kSElem];            // element e's run in ebf: (first, count), both even
-    unsigned short pairs[kSPairs];// the index's element lists (search order per ID)
+    alignas(16) unsigned short pairs[kSPairs];  // the index's element lists (search order per ID)
     uint32_t hkey[kCHash];        // neighbour ID -> dense index d
     unsigned short hden[kCHash];
     int2 drng[kIdxMax];           // dense index d -> its elements in pairs
@@ -1193,8 +1194,13 @@ __global__ void __launch_bounds__(kCThreads, 3) correction_kernel(CorrectionArgs
         const float4 org = el.eorg[g];
         const float4* gpts = el.ebf + (long long)g * el.flat_cap;
         for (int q = threadIdx.x; q < kCHash; q += blockDim.x) S.hkey[q] = kNoId;
-        for (int q = threadIdx.x; q < npairs; q += blockDim.x)
-            S.pairs[q] = el.idx_elem[(long long)g * el.pair_cap + q];
+        {  // the pair lists and the barycenters, copied asynchronously (waited for below)
+            const uint4* src = reinterpret_cast<const uint4*>(el.idx_elem + (long long)g * el.pair_cap);
+            uint4* dst = reinterpret_cast<uint4*>(S.pairs);
+            for (int q = threadIdx.x; q < npairs / 8; q += blockDim.x) cp_async16(dst + q, src + q);
+            if (nflat <= kSPts)
+                for (int q = threadIdx.x; q < nflat; q += blockDim.x) cp_async16(S.pts + q, gpts + q);
+        }
         for (int e = threadIdx.x; e < ne; e += blockDim.x) {
             const HullElem& E = el.elem[(long long)g * el.elem_cap + e];
             int2 run = make_int2(E.pbase, E.pcount + (E.pcount & 1));  // with its padding entry
@@ -1210,9 +1216,8 @@ __global__ void __launch_bounds__(kCThreads, 3) correction_kernel(CorrectionArgs
                 S.box[e][q + 3] = __double2float_ru(E.hi[q] - (double)o[q]);
             }
         }
-        if (nflat <= kSPts)
-            for (int p = threadIdx.x; p < nflat; p += blockDim.x) S.pts[p] = gpts[p];
-        __syncthreads();  // the hash is cleared
+        cp_async_wait_all();
+        __syncthreads();  // the hash is cleared, the copies have landed
         for (int d = threadIdx.x; d < nd; d += blockDim.x) {
             const uint32_t id = el.idx_key[(long long)g * el.idx_cap + d];
             int2 r = el.idx_rng[(long long)g * el.idx_cap + d];
@@ -1263,31 +1268,30 @@ __global__ void __launch_bounds__(kCThreads, 3) correction_kernel(CorrectionArgs
             if (threadIdx.x == 0) S.pk_next = nwarps;  // packet w goes to warp w, the rest on demand
             __syncthreads();
             // band voxels: their neighbour; voxels whose neighbour no element holds get (1, 1)
-            // now.  Four voxels per thread at a time: their loads are in flight together.
-            constexpr int kBatch = 4;
+            // now.  A batch of voxels per thread: their loads are in flight together.
+            constexpr int kBatch = sizeof(T) == 4 ? 16 : 8;
             for (int q0 = threadIdx.x; q0 < nv; q0 += kBatch * blockDim.x) {
-                double vals[kBatch];
+                T vals[kBatch];
                 uint32_t ids[kBatch];
-                long long fs[kBatch];
 #pragma unroll
                 for (int u = 0; u < kBatch; u++) {
                     const int q = q0 + u * blockDim.x;
-                    fs[u] = 0;
-                    vals[u] = delta;  // outside the band
+                    const long long f = v0 + q;  // the box's flat [z][y][x] index
+                    vals[u] = T(0);
                     ids[u] = 0u;
                     if (q < nv) {
-                        fs[u] = v0 + q;  // the box's flat [z][y][x] index
-                        vals[u] = (double)in[fs[u]];
+                        vals[u] = in[f];
                         // IDLocal flat-resized onto the box (dimensionalBuffer.h:120-131)
-                        ids[u] = fs[u] < old_count ? idl[fs[u]] : 0u;
+                        ids[u] = f < old_count ? idl[f] : 0u;
                     }
                 }
 #pragma unroll
                 for (int u = 0; u < kBatch; u++) {
                     const int q = q0 + u * blockDim.x;
                     if (q >= nv) continue;
+                    const long long fq = v0 + q;
                     unsigned short dd = kNoD;
-                    if (fabs(vals[u]) < delta) {
+                    if (fabs((double)vals[u]) < delta) {
                         const uint32_t id = ids[u];
                         unsigned hs = (id * 2654435761u) & (kCHash - 1);
                         for (int probe = 0; probe < kCHash; probe++) {
@@ -1297,7 +1301,7 @@ __global__ void __launch_bounds__(kCThreads, 3) correction_kernel(CorrectionArgs
                             hs = (hs + 1) & (kCHash - 1);
                         }
                         if (dd != kNoD) atomicAdd(&S.dcnt[dd], 1);
-                        else correct_voxel(a, elem, g, -1, id, vals[u], (double)out[fs[u]], out + fs[u]);
+                        else correct_voxel(a, elem, g, -1, id, (double)vals[u], (double)out[fq], out + fq);
                     }
                     S.vd[q] = dd;
                 }
