@@ -617,8 +617,12 @@ int level_set_t(gg_ctx* ctx, int p, int regrid) {
     a.err = ctx->d_err;
     a.regrid = regrid;
     if (ctx->elements) a.hull = ctx->hull;
+    launch_work_order(ctx->work, ctx->G, ctx->d_toff_mc, ctx->d_box[p], 0, ctx->stream);
+    a.order = ctx->work.order;
+    a.item_off = ctx->work.item_off;
+    a.queue = ctx->work.queue;
     launch_mc<T>(a, stage_grid(ctx, ST_LEVELSET), ctx->side_max, ctx->stream);
-    ctx->launches += 1;
+    ctx->launches += 5;
     CK(cudaGetLastError());
     if (ctx->elements) {  // computeSurfaceElements, box.cpp:1175-1180
         ElementArgs e{};
@@ -630,6 +634,9 @@ int level_set_t(gg_ctx* ctx, int p, int regrid) {
         e.ph = physics(ctx);
         e.scratch = ctx->d_elscr;
         e.scratch_ctas = ctx->elscr_ctas;
+        e.order = ctx->work.order;
+        e.item_off = ctx->work.item_off;
+        e.queue = ctx->work.queue + 1;
         e.err = ctx->d_err;
         launch_elements(e, ctx->elscr_ctas, ctx->stream);
         ctx->launches += 1;

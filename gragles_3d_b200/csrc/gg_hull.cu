@@ -144,6 +144,7 @@ struct ElemSmem {
     uint32_t* jids;              // kLMax x kJIds junction IDs
     double2* jres;               // kJobMax (mobility, energy)
     int nl, nq, nh, nj, ne, nch, nd, np, np_flat;
+    int next;  // the work item this warp fetched
 };
 
 // FNV-1a over the eight IDs of a cube's sorted list
@@ -341,9 +342,15 @@ __global__ void __launch_bounds__(32) elements_kernel(ElementArgs a) {
         S.jh = reinterpret_cast<JHead*>(scr + kJIdBytes + kJResBytes);
     }
     __syncwarp();
-    for (TileWalk w(a.toff, a.G, blockIdx.x, gridDim.x); w.valid(); w.next()) {
-        const int g = w.g;
-        if (!a.exists[g]) continue;
+    const int n_items = a.item_off[a.G + 1];
+    for (;;) {  // grains largest first, fetched on demand
+        if (lane == 0) S.next = atomicAdd(a.queue, 1);
+        __syncwarp();
+        const int t = S.next;
+        __syncwarp();
+        if (t >= n_items) break;
+        const int g = a.order[work_position(a.item_off, a.G, t)];
+        if (g < 1 || g > a.G || !a.exists[g]) continue;
         const long long cb = (long long)g * a.cap.cap;
         const int nrec = a.cap.n_rec[g], ntri = a.cap.n_tri[g];
         uint32_t* rec_list = a.cap.rec_list + 8 * cb;

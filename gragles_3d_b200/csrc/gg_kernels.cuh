@@ -287,6 +287,9 @@ struct ElementArgs {
     HullPhysics ph;
     unsigned char* scratch;   // scratch_ctas x elements_scratch_per_cta() bytes
     int scratch_ctas;         // the launch uses at most this many CTAs
+    const int* order;         // the grains of toff by decreasing box (WorkOrder, one item
+    const int* item_off;      // each), fetched through *queue
+    int* queue;
     int* err;
 };
 size_t elements_scratch_per_cta();
@@ -347,6 +350,9 @@ struct MCArgs {
     // grain's hull is rebuilt (none is deleted) and newbox is the resized grid's box,
     // taken as it is (then resized to a cube) rather than widened by the border
     int regrid;
+    const int* order;         // the grains of toff by decreasing box (WorkOrder, one item
+    const int* item_off;      // each), fetched through *queue
+    int* queue;
 };
 template <typename T>
 void launch_mc(const MCArgs<T>& a, int grid, int side, cudaStream_t s);

@@ -98,9 +98,17 @@ __global__ void __launch_bounds__(kThreads, 3) mc_kernel(MCArgs<T> a, int slab_b
     __shared__ unsigned nb_id[kHash];
     __shared__ unsigned nb_key[kHash];
     __shared__ int n_found;
+    __shared__ int next_item;
     extern __shared__ __align__(16) unsigned char slab_raw[];
-    for (TileWalk w(a.toff, a.G, blockIdx.x, gridDim.x); w.valid(); w.next()) {
-        const int g = w.g;
+    const int n_items = a.item_off[a.G + 1];
+    for (;;) {  // grains largest first, fetched on demand
+        __syncthreads();
+        if (threadIdx.x == 0) next_item = atomicAdd(a.queue, 1);
+        __syncthreads();
+        const int t = next_item;
+        if (t >= n_items) break;
+        const int g = a.order[work_position(a.item_off, a.G, t)];
+        if (g < 1 || g > a.G) continue;
         if (!a.exists[g] && !a.regrid) {  // the hull vanished last step: delete, grainhdl.cpp:678-680
             if (threadIdx.x == 0) a.present[g] = 0;
             continue;
