@@ -420,7 +420,10 @@ def main():
             keys = ["ms_convolution", "ms_lists", "ms_comparison", "ms_levelset", "ms_redistancing", "ms_total"]
             print(json.dumps({"profile_run": args.paths, "config": dict(WORKLOAD), "value": vox / (ms_e / 1e3),
                               "unit": UNIT, "ms_per_step": ms_e / args.steps, "clocks": clk,
-                              "stage_ms": {k: float(np.mean([r[k] for r in reps])) for k in keys}}))
+                              "stage_ms": {k: float(np.mean([r[k] for r in reps])) for k in keys},
+                              # per timed step: what a captured comparison launch processed
+                              "compare_voxels": [int(r["compare_voxels"]) for r in reps],
+                              "ms_compare_kernel": [float(r["ms_compare_kernel"]) for r in reps]}))
         if dist:
             dist.barrier()
             dist.destroy_process_group()
