@@ -65,6 +65,8 @@ struct gg_ctx {
     int *d_toff_n = nullptr, *d_toff_slab = nullptr, *d_toff_one = nullptr, *d_toff_mc = nullptr, *d_toff_red = nullptr;
     int* d_toff_big = nullptr;  // mixed path: slices of the boxes above the tensor-core side
     WorkOrder work{};           // largest-first order of the per-grain kernels
+    TileBins lbins{};           // the list update's candidate cells
+    int lbins_cells = 0;        // cells the count arrays hold
     // tables
     double2* d_tw = nullptr;
     long long* d_tw_off = nullptr;
@@ -482,8 +484,38 @@ int stage_convolution_t(gg_ctx* ctx) {
     return correct_convolution<T>(ctx);
 }
 
+// Make room for the list update's cell entries of the current layout.
+int ensure_list_bins(gg_ctx* ctx) {
+    const int n = ctx->M / kListCell + 1;
+    if ((long long)n * n * n > ctx->lbins_cells) return fail(ctx, GG_ERR_INVALID, "list cells exceed their arrays");
+    ctx->lbins.ntx = ctx->lbins.nty = ctx->lbins.ntz = n;
+    const long long need = list_bin_capacity(ctx->G, ctx->side_max);
+    if (need <= ctx->lbins.capacity) return GG_OK;
+    CK(cudaStreamSynchronize(ctx->stream));
+    if (ctx->lbins.entries) CK(cudaFree(ctx->lbins.entries));
+    ctx->lbins.capacity = need + need / 4;
+    CK(dalloc(&ctx->lbins.entries, ctx->lbins.capacity));
+    return GG_OK;
+}
+
 int stage_update_lists_t(gg_ctx* ctx) {
     ctx->p ^= 1;  // switchDistancebuffer, grainhdl.cpp:852
+    int rc = ensure_list_bins(ctx);
+    if (rc) return rc;
+    // position tables of the previous lists (every present grain: the lists of grains
+    // whose hull vanished last step are walked too), and the candidate cells
+    PosTableArgs pt{};
+    pt.G = ctx->G;
+    pt.present = ctx->d_present;
+    pt.cmp = ctx->d_son;
+    pt.n_cmp = ctx->d_nson;
+    pt.list_cap = ctx->list_cap;
+    pt.table = ctx->d_pt;
+    pt.pos_cap = ctx->pos_cap;
+    pt.err = ctx->d_err;
+    launch_pos_tables(pt, ctx->grid, ctx->stream);
+    launch_list_bins(ctx->lbins, ctx->G, ctx->d_exists, ctx->d_box[ctx->p], ctx->d_err, ctx->stream);
+    ctx->launches += 4;
     ListArgs a{};
     a.G = ctx->G;
     a.toff = ctx->d_toff_one;
@@ -494,6 +526,9 @@ int stage_update_lists_t(gg_ctx* ctx) {
     a.cmp = ctx->d_cmp;
     a.n_cmp = ctx->d_ncmp;
     a.list_cap = ctx->list_cap;
+    a.cells = ctx->lbins;
+    a.pos = ctx->d_pt;
+    a.pos_cap = ctx->pos_cap;
     a.err = ctx->d_err;
     launch_update_lists(a, stage_grid(ctx, ST_LISTS), ctx->stream);
     // m_secondOrderNeighbours = m_comparisonList (box.cpp:895), once every list is rebuilt
@@ -879,7 +914,8 @@ void free_all(gg_ctx* c) {
                     c->el.elem, c->el.ids, c->el.segs, c->el.ebary, c->el.chunks, c->el.n_idx, c->el.idx_key, c->el.idx_rng,
                     c->el.idx_elem, c->d_err, c->d_total_vox, c->d_count3, c->bins.count, c->work.keys,
                     c->work.keys_out, c->work.vals, c->work.order, c->work.item_off, c->work.temp, c->work.queue,
-                    c->bins.off, c->bins.cursor, c->bins.entries, c->bins.max_count};
+                    c->bins.off, c->bins.cursor, c->bins.entries, c->bins.max_count, c->lbins.count,
+                    c->lbins.off, c->lbins.cursor, c->lbins.entries};
     for (void* p : ptrs)
         if (p) cudaFree(p);
     if (c->h_maxcount) cudaFreeHost(c->h_maxcount);
@@ -995,6 +1031,13 @@ int gg_create(const gg_params* params, gg_ctx** out) {
     CK(dalloc(&ctx->bins.off, n_tiles + 1));
     CK(dalloc(&ctx->bins.cursor, n_tiles + 1));
     CK(dalloc(&ctx->bins.max_count, 1));
+    {
+        const int n = ctx->M / kListCell + 1;
+        ctx->lbins_cells = n * n * n;
+        CK(dalloc(&ctx->lbins.count, (size_t)ctx->lbins_cells + 1));
+        CK(dalloc(&ctx->lbins.off, (size_t)ctx->lbins_cells + 1));
+        CK(dalloc(&ctx->lbins.cursor, (size_t)ctx->lbins_cells + 1));
+    }
     CK(cudaMallocHost((void**)&ctx->h_maxcount, sizeof(int)));
     CK(cudaMallocHost((void**)&ctx->h_count3, 3 * sizeof(int)));
     CK(cudaMallocHost((void**)&ctx->h_total_vox, sizeof(long long)));

@@ -161,20 +161,29 @@ struct ListArgs {
     uint32_t* cmp;
     int* n_cmp;
     int list_cap;
+    TileBins cells;           // existing grains by the kListCell^3 domain cells their boxes touch
+    const unsigned long long* pos;  // position tables of the son lists (PosTableArgs)
+    int pos_cap;
     int* err;
 };
-// Shared memory of the list update: two bitmaps over the IDs 0..G, a 4096-slot hash
-// of new IDs with their first positions, and 2048 selected (position, ID) pairs.
+// Shared memory of the list update: two bitmaps over the IDs 0..G and 2048 selected
+// (position, ID) pairs.
 __host__ __device__ inline int list_bitmap_words(int G) { return (G + 32) >> 5; }
-inline size_t list_smem_bytes(int G) { return (size_t)list_bitmap_words(G) * 8 + 4096 * 8 + 2048 * 8; }
+inline size_t list_smem_bytes(int G) { return (size_t)list_bitmap_words(G) * 8 + 2048 * 8; }
 void launch_update_lists(const ListArgs& a, int grid, cudaStream_t s);
+// The candidate cells of the list update: every existing grain under each cell of
+// kListCell^3 voxels that its inclusive box [x0, x1] x [y0, y1] x [z0, z1] reaches.
+constexpr int kListCell = 16;
+void launch_list_bins(const TileBins& tb, int G, const int* exists, const int* box, int* err, cudaStream_t s);
+long long list_bin_capacity(int G, int side);
 
 // Per grain an open-addressing table (ID << 32 | list position) of the comparison list,
 // pos_cap slots per grain of which pos_table_size(K) are used; built once per step
 // and probed by every comparison tile the grain's box reaches.
 struct PosTableArgs {
     int G;
-    const int* toff;          // one tile per existing grain
+    const int* toff;          // one tile per existing grain; null: every present grain
+    const int* present;
     const uint32_t* cmp;
     const int* n_cmp;
     int list_cap;
