@@ -1042,12 +1042,16 @@ __device__ __forceinline__ void run_min(const float4* pts, int first, int n, con
 // order, as projectPointToGrainBoundary does (grainHull.cpp:570-660).  Every barycenter
 // that can be the reference's winner has q <= best + eps2, so the subset has the same
 // winner.
+// `band` marks (bit c, when count <= 32) the candidates whose least q came within the band
+// of the best so far when they were scanned: a superset of those within the final band,
+// the only ones that can hold such a barycenter; the rest are not visited.
 __device__ int exact_winner(const CorrSmem& S, const float4* pts, int first, int count, int ne,
                             const int* __restrict__ eidx, const double* __restrict__ eb, double x, double y, double z,
-                            float ax, float ay, float az, float limit) {
+                            float ax, float ay, float az, float limit, unsigned band) {
     double bd = 10000000.0;
     int bw = -1;
     for (int c = 0; c < count; c++) {
+        if (count <= 32 && !((band >> c) & 1u)) continue;
         const int e = S.pairs[first + c];
         if (e >= ne) continue;
         const int2 r = S.erun[e];  // the element's barycenters in order (a padding entry: q = kInf)
@@ -1095,6 +1099,7 @@ __device__ __forceinline__ void search_packet(const CorrSmem& S, const float4* p
     float vx[V], vy[V], vz[V], vv[V], best[V], second[V];
     unsigned long long A2[V], B2[V], C2[V];
     int beste[V];
+    unsigned band[V];  // candidates within the band of the best when scanned (count <= 32)
 #pragma unroll
     for (int u = 0; u < V; u++) {
         vx[u] = (float)ii[u] - org.x;  // exact
@@ -1106,6 +1111,7 @@ __device__ __forceinline__ void search_packet(const CorrSmem& S, const float4* p
         C2[u] = pack2(-2.f * vz[u], -2.f * vz[u]);
         best[u] = second[u] = kInf;
         beste[u] = -1;
+        band[u] = 0u;
     }
     const float eps = 0.5f * eps2;
     for (int c = count - 1; c >= 0; c--) {
@@ -1136,6 +1142,7 @@ __device__ __forceinline__ void search_packet(const CorrSmem& S, const float4* p
             } else {
                 second[u] = fminf(second[u], m[u]);
             }
+            if (m[u] <= best[u] + eps2) band[u] |= 1u << (c & 31);
         }
     }
 #pragma unroll
@@ -1144,7 +1151,7 @@ __device__ __forceinline__ void search_packet(const CorrSmem& S, const float4* p
         // proven when every other element is farther by more than the band
         if (beste[u] >= 0 && !(second[u] - best[u] > eps2))
             win[u] = exact_winner(S, pts, first, count, ne, eidx, eb, (double)ii[u], (double)jj[u], (double)kk[u],
-                                  -2.f * vx[u], -2.f * vy[u], -2.f * vz[u], best[u] + eps2);
+                                  -2.f * vx[u], -2.f * vy[u], -2.f * vz[u], best[u] + eps2, band[u]);
     }
 }
 
