@@ -76,7 +76,8 @@ struct gg_ctx {
     long long* d_circ_off = nullptr;
     uint16_t* d_bmat = nullptr;       // the same, split FP16 hi/lo in the tensor-core operand layout
     long long* d_boff = nullptr;
-    float* d_cscr = nullptr;          // mixed-path convolution scratch (out's layout)
+    float* d_cscr = nullptr;          // mixed-path convolution scratch (out's layout); without the
+                                      // correction the input arena serves, once read
     unsigned char* d_elscr = nullptr; // element build: per-CTA junction and pair scratch
     bool elements = false;            // interfacial elements built every step (correction or keep_elements)
     int elscr_ctas = 0;
@@ -448,23 +449,16 @@ int stage_convolution_t(gg_ctx* ctx) {
         // boxes (when any) on the FP32 SIMT kernels; each launch walks only its class's tiles
         const int small_side = std::min(ctx->side_max, kUmmaMaxSide);
         if (!umma_supported(small_side)) return fail(ctx, GG_ERR_UNSUPPORTED, "tensor-core convolution unavailable");
-        if (!ctx->d_cscr) return fail(ctx, GG_ERR_INVALID, "convolution scratch missing");
-        UmmaConvArgs u{};
-        u.G = ctx->G;
-        u.toff = ctx->d_toff_slab;
-        u.box = ctx->d_box[p];
-        u.in = reinterpret_cast<const float*>(ctx->d_arena[p]);
-        u.in_off = ctx->d_off[p];
-        u.out = reinterpret_cast<float*>(ctx->d_arena[p ^ 1]);
-        u.out_off = ctx->d_off[p ^ 1];
-        u.scratch = ctx->d_cscr;
-        u.bmat = ctx->d_bmat;
-        u.boff = ctx->d_boff;
-        u.err = ctx->d_err;
-        launch_conv_umma(u, ctx->num_sms, small_side, ctx->stream);
-        ctx->launches += 3;
-        CK(cudaGetLastError());
-        if (ctx->side_max > kUmmaMaxSide) {
+        // The middle pass needs a buffer in out's layout.  Without the correction nothing
+        // reads the input after the convolution (the comparison overwrites its arena), so
+        // the input arena serves, and the large boxes, which read the input, go first.
+        float* scratch = ctx->d_cscr;
+        if (!scratch) {
+            if (ctx->correction) return fail(ctx, GG_ERR_INVALID, "convolution scratch missing");
+            scratch = reinterpret_cast<float*>(ctx->d_arena[p]);
+        }
+        const bool big = ctx->side_max > kUmmaMaxSide;
+        auto large_boxes = [&]() {
             ConvTCArgs a{};
             a.G = ctx->G;
             a.toff = ctx->d_toff_big;
@@ -478,7 +472,23 @@ int stage_convolution_t(gg_ctx* ctx) {
             a.err = ctx->d_err;
             launch_conv_tc(a, ctx->num_sms, ctx->side_max, ctx->stream);
             ctx->launches += 2;
-        }
+        };
+        if (big) large_boxes();
+        UmmaConvArgs u{};
+        u.G = ctx->G;
+        u.toff = ctx->d_toff_slab;
+        u.box = ctx->d_box[p];
+        u.in = reinterpret_cast<const float*>(ctx->d_arena[p]);
+        u.in_off = ctx->d_off[p];
+        u.out = reinterpret_cast<float*>(ctx->d_arena[p ^ 1]);
+        u.out_off = ctx->d_off[p ^ 1];
+        u.scratch = scratch;
+        u.bmat = ctx->d_bmat;
+        u.boff = ctx->d_boff;
+        u.err = ctx->d_err;
+        launch_conv_umma(u, ctx->num_sms, small_side, ctx->stream);
+        ctx->launches += 3;
+        CK(cudaGetLastError());
     }
     CK(cudaGetLastError());
     return correct_convolution<T>(ctx);
@@ -1098,7 +1108,7 @@ int gg_load_state(gg_ctx* ctx, const uint32_t* labels, const int32_t* extents, c
         CK(dalloc(&ctx->d_idarena[a], ctx->pool_voxels));
     }
     if (ctx->fp64) CK(dalloc(&ctx->d_spec, ctx->spec_capacity));
-    else CK(dalloc(&ctx->d_cscr, ctx->pool_voxels));
+    else if (ctx->correction) CK(dalloc(&ctx->d_cscr, ctx->pool_voxels));
     if (ctx->elements) {
         const long long cap = ctx->P.hull_capacity > 0 ? ctx->P.hull_capacity : 16LL * side * side + 2048;
         const size_t G1h = (size_t)G + 1;
