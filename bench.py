@@ -49,6 +49,16 @@ WORKLOADS = {
                              hull_capacity=HULL_CAPACITY)),
     "voronoi-128": (dict(workload="voronoi-128^3-2000-grains-isotropic", domain=128, grains=2000, border=10,
                          time_step=0.2, seed=1002), {}),
+    # the larger configurations: one path at a time (--paths mixed), the pool sized to
+    # the initial boxes times pool_factor so that the state fits the 180 GB of HBM
+    "stored-energy-384": (dict(workload="voronoi-384^3-100000-grains-lognormal-stored-energy-5pct-nuclei",
+                               domain=384, grains=100000, border=10, time_step=0.2, seed=1004, generator="c4",
+                               pool_factor=1.3),
+                          dict(correction=True, unique_energies=False, mobility_model=True, stored_energy=True,
+                               hull_capacity=4000)),
+    "laguerre-512": (dict(workload="laguerre-512^3-250000-grains-lognormal-radii-isotropic", domain=512,
+                          grains=250000, border=10, time_step=0.2, seed=1005, generator="laguerre",
+                          pool_factor=1.03), dict(correction=False)),
 }
 WORKLOAD = dict(WORKLOADS["anisotropic-256"][0])
 PHYSICS = dict(WORKLOADS["anisotropic-256"][1])  # GrainHandler physics keywords of the workload
@@ -60,9 +70,39 @@ PHYSICS = dict(WORKLOADS["anisotropic-256"][1])  # GrainHandler physics keywords
 def microstructure():
     from gragles_3d_b200 import microstructure as msgen
 
-    ms = msgen.voronoi(WORKLOAD["domain"], WORKLOAD["grains"], seed=WORKLOAD["seed"])
+    gen = WORKLOAD.get("generator", "voronoi")
+    if gen == "c4":
+        ms = msgen.c4(WORKLOAD["domain"], WORKLOAD["grains"], seed=WORKLOAD["seed"])
+    elif gen == "laguerre":
+        ms = msgen.laguerre(WORKLOAD["domain"], WORKLOAD["grains"], seed=WORKLOAD["seed"])
+    else:
+        ms = msgen.voronoi(WORKLOAD["domain"], WORKLOAD["grains"], seed=WORKLOAD["seed"])
     ext, counts = ms.grain_extents()
     return ms, ext, counts
+
+
+def handler(gg, ms, ext, counts, precision, device):
+    """A GrainHandler of the workload (its physics and, for the large configurations, a
+    pool of pool_factor times the initial boxes' voxels)."""
+    from gragles_3d_b200 import microstructure as msgen
+
+    extra = {}
+    if "pool_factor" in WORKLOAD:
+        e6 = np.asarray(ext).reshape(-1, 6).astype(np.int64)
+        side = np.maximum.reduce([e6[:, 1] - e6[:, 0], e6[:, 3] - e6[:, 2], e6[:, 5] - e6[:, 4]]) + 1 \
+            + 2 * WORKLOAD["border"]
+        need = int(((side ** 3 + 31) // 32 * 32)[np.asarray(counts) > 0].sum())
+        extra["pool_voxels"] = int(WORKLOAD["pool_factor"] * need)
+    gh = gg.GrainHandler(WORKLOAD["domain"], WORKLOAD["border"], WORKLOAD["time_step"], ms.n_grains,
+                         precision=precision, device=device, **PHYSICS, **extra)
+    return gh, (lambda: _prepare(gh, ms, msgen))
+
+
+def _prepare(gh, ms, msgen):
+    if PHYSICS.get("correction"):
+        gh.set_orientations(ms.euler)
+    if PHYSICS.get("stored_energy"):
+        gh.set_stored_energy(msgen.stored_energy_of(ms.stored_energy))
 
 
 def read_peaks():
@@ -165,12 +205,10 @@ def run_device(gg, precision, ms, ext, counts, steps, warmup, device, dist, keep
     """Device-resident run: state loaded before the timed region."""
     import torch
 
-    gh = gg.GrainHandler(WORKLOAD["domain"], WORKLOAD["border"], WORKLOAD["time_step"], WORKLOAD["grains"],
-                         precision=precision, device=device, **PHYSICS)
+    gh, prepare = handler(gg, ms, ext, counts, precision, device)
     gh.load(ms.labels, ext, counts)
     gh.default_lists()
-    if PHYSICS:
-        gh.set_orientations(ms.euler)
+    prepare()
     for _ in range(warmup):
         gh.step()
     reps = []
@@ -249,16 +287,14 @@ def run_e2e(gg, precision, ms, ext, counts, steps, warmup, device):
     labels = pinned.numpy()
 
     def one_pass(n, timed):
-        gh = gg.GrainHandler(WORKLOAD["domain"], WORKLOAD["border"], WORKLOAD["time_step"], WORKLOAD["grains"],
-                             precision=precision, device=device, **PHYSICS)
+        gh, prepare = handler(gg, ms, ext, counts, precision, device)
         torch.cuda.synchronize()
         ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         ev0.record()
         t0 = time.perf_counter()
         gh.load(labels, ext, counts)
         gh.default_lists()
-        if PHYSICS:
-            gh.set_orientations(ms.euler)
+        prepare()
         t_setup = time.perf_counter() - t0
         vox = 0
         for _ in range(n):
@@ -274,10 +310,12 @@ def run_e2e(gg, precision, ms, ext, counts, steps, warmup, device):
     # allocations of gg_load_state, whose time varies with the driver's memory state
     passes = sorted((one_pass(steps, True) for _ in range(3)), key=lambda r: r[1])
     vox, ms_elapsed, ms_setup = passes[1]
-    G1 = WORKLOAD["grains"] + 1
+    G1 = ms.n_grains + 1
     h2d = labels.nbytes + ext.astype(np.int32).nbytes + counts.astype(np.int64).nbytes
-    if PHYSICS:
+    if PHYSICS.get("correction"):
         h2d += ms.euler.astype(np.float64).nbytes
+    if PHYSICS.get("stored_energy"):
+        h2d += ms.n_grains * 8
     d2h = G1 * (1 + 8 + 8 + 24 + 4)
     return {"value": vox / (ms_elapsed / 1e3), "unit": UNIT, "h2d_bytes_per_step": int(h2d // steps),
             "d2h_bytes_per_step": int(d2h), "ms": ms_elapsed, "ms_setup": ms_setup}
@@ -381,7 +419,9 @@ def main():
     ap.add_argument("--grains", type=int, default=None, help="profiling aid: grain count for --domain")
     ap.add_argument("--workload", default="anisotropic-256", choices=sorted(WORKLOADS),
                     help="anisotropic-256 (default): the 256^3 / 20,000-grain anisotropic workload with the "
-                         "correction; voronoi-128: the isotropic 128^3 / 2,000-grain workload")
+                         "correction; voronoi-128: the isotropic 128^3 / 2,000-grain workload; "
+                         "stored-energy-384 (384^3, 100,000 grains + 5%% nuclei, stored energy) and laguerre-512 "
+                         "(512^3, 250,000 Laguerre grains): with --paths mixed")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
     WORKLOAD.clear()
