@@ -65,6 +65,7 @@ struct gg_ctx {
     int *d_toff_n = nullptr, *d_toff_slab = nullptr, *d_toff_one = nullptr, *d_toff_mc = nullptr, *d_toff_red = nullptr;
     int* d_toff_big = nullptr;  // mixed path: slices of the boxes above the tensor-core side
     WorkOrder work{};           // largest-first order of the per-grain kernels
+    int* d_toff_rcls = nullptr; // redistancing size classes: kRedistClasses x (G + 2)
     TileBins lbins{};           // the list update's candidate cells
     int lbins_cells = 0;        // cells the count arrays hold
     // tables
@@ -326,7 +327,7 @@ int side_check(gg_ctx* ctx, int side) {
 }
 
 template <typename T>
-int redistance(gg_ctx* ctx, int in_a, int out_a, const int* toff, int side) {
+int redistance(gg_ctx* ctx, int in_a, int out_a, const int* toff, int side, bool classes = false) {
     RedistArgs<T> r{};
     r.G = ctx->G;
     r.geo = ctx->geo;
@@ -335,8 +336,16 @@ int redistance(gg_ctx* ctx, int in_a, int out_a, const int* toff, int side) {
     r.in = arena<T>(ctx, in_a);
     r.out = arena<T>(ctx, out_a);
     r.err = ctx->d_err;
-    launch_redistance<T>(r, stage_grid(ctx, ST_REDIST), side, ctx->stream);
-    ctx->launches += 2;
+    if (classes) {  // per size class of the output boxes (their tiles from toff)
+        launch_redist_classes(ctx->G, toff, ctx->d_box[out_a], ctx->d_toff_rcls, ctx->stream);
+        launch_redistance<T>(r, stage_grid(ctx, ST_REDIST), side, ctx->d_toff_rcls, ctx->stream);
+        int nc = 0;
+        for (int c = 0; c < kRedistClasses && (c == 0 || redist_side(c - 1) < side); c++) nc++;
+        ctx->launches += 1 + 2 * nc;
+    } else {
+        launch_redistance<T>(r, stage_grid(ctx, ST_REDIST), side, nullptr, ctx->stream);
+        ctx->launches += 2;
+    }
     CK(cudaGetLastError());
     return GG_OK;
 }
@@ -792,7 +801,7 @@ int stage_redistancing_t(gg_ctx* ctx) {
     if (rc) return rc;
     rc = check_err(ctx, "redistancing plan");
     if (rc) return rc;
-    rc = redistance<T>(ctx, p, p ^ 1, ctx->d_toff_red, std::max(side_new, ctx->side_max));
+    rc = redistance<T>(ctx, p, p ^ 1, ctx->d_toff_red, std::max(side_new, ctx->side_max), true);
     if (rc) return rc;
     // in.resize(out dims), box.cpp:2581-2584
     launch_copy_layout(ctx->G, ctx->d_present, ctx->d_box[p ^ 1], ctx->d_off[p ^ 1], ctx->d_box[p], ctx->d_off[p],
@@ -923,7 +932,7 @@ void free_all(gg_ctx* c) {
                     c->hull.rec_list, c->hull.rec_ntri, c->hull.bary, c->hull.tarea, c->hull.diag, c->el.earea, c->el.ebf, c->el.ecb, c->el.eidx, c->el.n_flat, c->el.eorg, c->hull.n_rec, c->hull.n_tri, c->el.n_elem,
                     c->el.elem, c->el.ids, c->el.segs, c->el.ebary, c->el.chunks, c->el.n_idx, c->el.idx_key, c->el.idx_rng,
                     c->el.idx_elem, c->d_err, c->d_total_vox, c->d_count3, c->bins.count, c->work.keys,
-                    c->work.keys_out, c->work.vals, c->work.order, c->work.item_off, c->work.temp, c->work.queue,
+                    c->d_toff_rcls, c->work.keys_out, c->work.vals, c->work.order, c->work.item_off, c->work.temp, c->work.queue,
                     c->bins.off, c->bins.cursor, c->bins.entries, c->bins.max_count, c->lbins.count,
                     c->lbins.off, c->lbins.cursor, c->lbins.entries};
     for (void* p : ptrs)
@@ -1013,6 +1022,7 @@ int gg_create(const gg_params* params, gg_ctx** out) {
     CK(dalloc(&ctx->d_toff_mc, G1 + 1));
     CK(dalloc(&ctx->d_toff_red, G1 + 1));
     CK(dalloc(&ctx->d_toff_big, G1 + 1));
+    CK(dalloc(&ctx->d_toff_rcls, (size_t)kRedistClasses * (G1 + 1)));
     CK(dalloc(&ctx->work.keys, G1));
     CK(dalloc(&ctx->work.keys_out, G1));
     CK(dalloc(&ctx->work.vals, G1));

@@ -421,8 +421,18 @@ struct RedistArgs {
     Arena<T> out;
     int* err;
 };
+// Size classes of the redistancing: grains whose output box side n falls in class c
+// (n <= redist_side(c), above the previous bound) run in launches whose block size and
+// shared memory fit that side, so that small boxes do not pay for the largest one.
+constexpr int kRedistClasses = 5;
+__host__ __device__ constexpr int redist_side(int c) {
+    return c <= 0 ? 32 : (c == 1 ? 40 : (c == 2 ? 48 : (c == 3 ? 64 : (1 << 30))));
+}
+// class_toff: kRedistClasses tile tables of stride G + 2 (n tiles per grain of the class),
+// from launch_redist_classes; null: one launch over `a.toff` sized for `side`.
 template <typename T>
-void launch_redistance(const RedistArgs<T>& a, int grid, int side, cudaStream_t s);
+void launch_redistance(const RedistArgs<T>& a, int grid, int side, const int* class_toff, cudaStream_t s);
+void launch_redist_classes(int G, const int* toff_all, const int* box, int* class_toff, cudaStream_t s);
 // Shared memory of one unit (one warp) at box side nmax; must fit one CTA.
 size_t redist_smem_bytes(int nmax, bool fp64);
 

@@ -281,21 +281,109 @@ size_t redist_smem_bytes(int nmax, bool fp64) {
     return 2 * (xy > z ? xy : z) * e;
 }
 
+namespace {
+// Per class c, the exclusive scan over grains of n (the output box side) for the grains
+// of toff_all (n tiles each) whose n is in class c; one CTA, as plan_kernel.
+__global__ void __launch_bounds__(1024) redist_class_kernel(int G, const int* toff_all, const int* box,
+                                                            int* class_toff) {
+    __shared__ int warp_tot[32][kRedistClasses];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int stride = G + 2;
+    const bool none = toff_all[G + 1] == 0;  // the plan overflowed: no tiles at all
+    const int per = (G + blockDim.x) / blockDim.x;  // grains 0..G
+    const int g0 = threadIdx.x * per, g1 = min(G + 1, g0 + per);
+    auto count = [&](int g, int c) {
+        if (none || g < 1 || g > G || toff_all[g + 1] - toff_all[g] <= 0) return 0;
+        const int n = load_box(box + 6 * g).nx();
+        const int lo = c == 0 ? 0 : redist_side(c - 1);
+        return (n > lo && n <= redist_side(c)) ? n : 0;
+    };
+    int mine[kRedistClasses], incl[kRedistClasses];
+#pragma unroll
+    for (int c = 0; c < kRedistClasses; c++) {
+        mine[c] = 0;
+        for (int g = g0; g < g1; g++) mine[c] += count(g, c);
+        incl[c] = mine[c];
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const int u = __shfl_up_sync(0xffffffffu, incl[c], o);
+            if (lane >= o) incl[c] += u;
+        }
+        if (lane == 31) warp_tot[warp][c] = incl[c];
+    }
+    __syncthreads();
+    if (warp == 0) {
+#pragma unroll
+        for (int c = 0; c < kRedistClasses; c++) {
+            const int w = warp_tot[lane][c];
+            int wi = w;
+#pragma unroll
+            for (int o = 1; o < 32; o <<= 1) {
+                const int u = __shfl_up_sync(0xffffffffu, wi, o);
+                if (lane >= o) wi += u;
+            }
+            warp_tot[lane][c] = wi;  // inclusive over warps
+        }
+    }
+    __syncthreads();
+#pragma unroll
+    for (int c = 0; c < kRedistClasses; c++) {
+        int run = (warp > 0 ? warp_tot[warp - 1][c] : 0) + incl[c] - mine[c];
+        int* t = class_toff + (long long)c * stride;
+        for (int g = g0; g < g1; g++) {
+            t[g] = run;
+            run += count(g, c);
+        }
+        if (threadIdx.x == blockDim.x - 1) t[G + 1] = warp_tot[31][c];
+    }
+}
+
+// CTAs of kernel k with `threads` threads and `smem` bytes that fit the device at once.
+template <typename K>
+int resident_ctas(K kernel, int threads, size_t smem) {
+    int dev = 0, sms = 0, per_sm = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, threads, smem);
+    return sms * (per_sm > 0 ? per_sm : 1);
+}
+}  // namespace
+
+void launch_redist_classes(int G, const int* toff_all, const int* box, int* class_toff, cudaStream_t s) {
+    redist_class_kernel<<<1, 1024, 0, s>>>(G, toff_all, box, class_toff);
+}
+
 template <typename T>
-void launch_redistance(const RedistArgs<T>& a, int grid, int side, cudaStream_t s) {
+void launch_redistance(const RedistArgs<T>& a, int grid, int side, const int* class_toff, cudaStream_t s) {
     static PerDevice configured;
     configured.once([] {
         allow_max_dynamic_smem(redist_xy_kernel<T>);
         allow_max_dynamic_smem(redist_z_kernel<T>);
     });
-    const size_t smem = redist_smem_bytes(side, sizeof(T) == 8);
-    int threads = (side + 31) / 32 * 32;
-    threads = threads > kMaxThreads ? kMaxThreads : threads;
-    redist_xy_kernel<T><<<grid * 2, threads, smem, s>>>(a);
-    redist_z_kernel<T><<<grid * 2, threads, smem, s>>>(a);
+    if (!class_toff) {
+        const size_t smem = redist_smem_bytes(side, sizeof(T) == 8);
+        int threads = (side + 31) / 32 * 32;
+        threads = threads > kMaxThreads ? kMaxThreads : threads;
+        redist_xy_kernel<T><<<grid * 2, threads, smem, s>>>(a);
+        redist_z_kernel<T><<<grid * 2, threads, smem, s>>>(a);
+        return;
+    }
+    // one pair of launches per size class up to the largest side, each sized for its
+    // class's largest side and filling the device with its own CTAs
+    for (int c = 0; c < kRedistClasses; c++) {
+        const int lo = c == 0 ? 0 : redist_side(c - 1);
+        if (lo >= side) break;
+        const int n = std::min(redist_side(c), side);
+        const size_t smem = redist_smem_bytes(n, sizeof(T) == 8);
+        const int threads = std::min((n + 31) / 32 * 32, kMaxThreads);
+        RedistArgs<T> ac = a;
+        ac.toff = class_toff + (long long)c * (a.G + 2);
+        redist_xy_kernel<T><<<resident_ctas(redist_xy_kernel<T>, threads, smem), threads, smem, s>>>(ac);
+        redist_z_kernel<T><<<resident_ctas(redist_z_kernel<T>, threads, smem), threads, smem, s>>>(ac);
+    }
 }
 
-template void launch_redistance<double>(const RedistArgs<double>&, int, int, cudaStream_t);
-template void launch_redistance<float>(const RedistArgs<float>&, int, int, cudaStream_t);
+template void launch_redistance<double>(const RedistArgs<double>&, int, int, const int*, cudaStream_t);
+template void launch_redistance<float>(const RedistArgs<float>&, int, int, const int*, cudaStream_t);
 
 }  // namespace gg
