@@ -268,7 +268,7 @@ int check_err(gg_ctx* ctx, const char* where) {
                            : (d & HULL_JUNCTIONS)    ? "more than 256 junctions on one hull"
                            : (d & HULL_JOBS)         ? "more misorientations on one hull than the element build holds"
                            : (d & HULL_INDEX)        ? "a hull's neighbour -> elements index beyond its capacity"
-                           : (d & HULL_TABLE)        ? "a hull's element, ID, segment or chunk table beyond its capacity"
+                           : (d & HULL_TABLE)        ? "a hull's element, ID or segment table beyond its capacity"
                                                      : "hull or interfacial-element capacity exceeded";
         return fail(ctx, GG_ERR_POOL_EXHAUSTED, "%s: %s (diag %d)", where, what, d);
     }
@@ -929,8 +929,8 @@ void free_all(gg_ctx* c) {
                     c->d_idoff[0], c->d_idoff[1], c->d_spec, c->d_spec_off, c->d_toff_n, c->d_toff_slab,
                     c->d_toff_one, c->d_toff_mc, c->d_toff_red, c->d_toff_big, c->d_tw, c->d_tw_off, c->d_gtab, c->d_g_off,
                     c->d_circ, c->d_circ_off, c->d_bmat, c->d_boff, c->d_cscr, c->d_elscr, c->d_quat, c->d_see,
-                    c->hull.rec_list, c->hull.rec_ntri, c->hull.bary, c->hull.tarea, c->hull.diag, c->el.earea, c->el.ebf, c->el.ecb, c->el.eidx, c->el.n_flat, c->el.eorg, c->hull.n_rec, c->hull.n_tri, c->el.n_elem,
-                    c->el.elem, c->el.ids, c->el.segs, c->el.ebary, c->el.chunks, c->el.n_idx, c->el.idx_key, c->el.idx_rng,
+                    c->hull.rec_list, c->hull.rec_ntri, c->hull.bary, c->hull.tarea, c->hull.diag, c->el.earea, c->el.ebf, c->el.eidx, c->el.n_flat, c->el.eorg, c->hull.n_rec, c->hull.n_tri, c->el.n_elem,
+                    c->el.elem, c->el.ids, c->el.segs, c->el.ebary, c->el.n_idx, c->el.idx_key, c->el.idx_rng,
                     c->el.idx_elem, c->d_err, c->d_total_vox, c->d_count3, c->bins.count, c->work.keys,
                     c->d_toff_rcls, c->work.keys_out, c->work.vals, c->work.order, c->work.item_off, c->work.temp, c->work.queue,
                     c->bins.off, c->bins.cursor, c->bins.entries, c->bins.max_count, c->lbins.count,
@@ -1148,11 +1148,8 @@ int gg_load_state(gg_ctx* ctx, const uint32_t* labels, const int32_t* extents, c
         CK(cudaMemset(ctx->el.n_flat, 0, sizeof(int) * G1h));
         CK(dalloc(&ctx->el.eorg, G1h));
         CK(cudaMemset(ctx->el.eorg, 0, sizeof(float4) * G1h));
-        ctx->el.chunk_cap = (int)(cap / kHullChunk) + ctx->el.seg_cap;
         ctx->el.idx_cap = 256;
         ctx->el.pair_cap = 2048;
-        CK(dalloc(&ctx->el.chunks, (size_t)ctx->el.chunk_cap * G1h));
-        CK(dalloc(&ctx->el.ecb, 2 * (size_t)ctx->el.chunk_cap * G1h));
         CK(dalloc(&ctx->el.n_idx, G1h));
         CK(dalloc(&ctx->el.idx_key, (size_t)ctx->el.idx_cap * G1h));
         CK(dalloc(&ctx->el.idx_rng, (size_t)ctx->el.idx_cap * G1h));

@@ -143,7 +143,7 @@ struct ElemSmem {
     JHead* jh;                   // kLMax working junctions
     uint32_t* jids;              // kLMax x kJIds junction IDs
     double2* jres;               // kJobMax (mobility, energy)
-    int nl, nq, nh, nj, ne, nch, nd, np, np_flat;
+    int nl, nq, nh, nj, ne, nd, np, np_flat;
     int next;  // the work item this warp fetched
 };
 
@@ -249,6 +249,13 @@ __device__ __forceinline__ void chain(ElemSmem& S, JHead& A, const JHead& B, int
     A.id_tail = B.id_tail;
     A.nids += B.nids;
 }
+
+// A float as an int whose signed order is the float's order (and back).
+__device__ __forceinline__ int order_key(float f) {
+    const int b = __float_as_int(f);
+    return b >= 0 ? b : b ^ 0x7FFFFFFF;
+}
+__device__ __forceinline__ float key_float(int k) { return __int_as_float(k >= 0 ? k : k ^ 0x7FFFFFFF); }
 
 // Warp-wide exclusive scan of v[0, n) in place (n <= kLMax); returns the total.
 __device__ int warp_scan_excl(int* v, int n) {
@@ -648,21 +655,20 @@ __global__ void __launch_bounds__(32) elements_kernel(ElementArgs a) {
         }
         __syncwarp();
         // 6. the element table in search order: HJ, QJ, TL, GB, with its barycenter
-        //    segments cut into chunks, and the (element, searched ID) pairs
+        //    segments, and the (element, searched ID) pairs
         for (int q = lane; q < kIHash; q += 32) S.ikey[q] = kNoId;
         __syncwarp();
         if (lane == 0) {
             HullElem* E = a.el.elem + (long long)g * a.el.elem_cap;
             uint32_t* ids = a.el.ids + (long long)g * a.el.id_cap;
             int2* segs = a.el.segs + (long long)g * a.el.seg_cap;
-            HullChunk* chunks = a.el.chunks + (long long)g * a.el.chunk_cap;
-            int ne = 0, ni = 0, ns = 0, nch = 0, nd = 0, np = 0, pb = 0;
+            int ne = 0, ni = 0, ns = 0, nd = 0, np = 0, pb = 0;
             bool over = false, over_index = false;
             // IDs from junction j's segment chain (j >= 0), else the nid IDs of id_src
             auto emit = [&](int type, const uint32_t* id_src, int j, int nid, int head, bool chained, double en,
                             double mo) {
                 if (ne >= a.el.elem_cap || ni + nid > a.el.id_cap) { over = true; return; }
-                const int id_off = ni, seg_off = ns, chunk_off = nch;
+                const int id_off = ni, seg_off = ns;
                 if (j < 0) {
                     for (int q = 0; q < nid; q++) ids[ni++] = id_src[q];
                 } else {
@@ -673,7 +679,7 @@ __global__ void __launch_bounds__(32) elements_kernel(ElementArgs a) {
                     if (ni != id_off + nid) atomicOr(a.err, ERR_BOUNDS);
                     nid = ni - id_off;
                 }
-                int nseg = 0, nchunk = 0, pcnt = 0;
+                int nseg = 0, pcnt = 0;
                 for (int k = head; k >= 0; k = chained ? S.next_key[k] : -1) {
                     if (ns >= a.el.seg_cap) { over = true; break; }
                     if (k >= kLMax || S.off[k] < 0 || S.off[k] + S.cnt[k] > a.el.bary_cap) {
@@ -684,14 +690,8 @@ __global__ void __launch_bounds__(32) elements_kernel(ElementArgs a) {
                     segs[ns++] = make_int2(off, cnt);
                     nseg++;
                     S.lflat[k] = pb + pcnt;
+                    S.fill[k] = ne;  // fill is free after the jobs: the list's element
                     pcnt += cnt;
-                    for (int c0 = 0; c0 < cnt; c0 += kHullChunk) {
-                        if (nch >= a.el.chunk_cap) { over = true; break; }
-                        chunks[nch].start = off + c0;
-                        chunks[nch].count = min(kHullChunk, cnt - c0);
-                        nch++;
-                        nchunk++;
-                    }
                 }
                 HullElem& e = E[ne];
                 e.type = type;
@@ -699,8 +699,6 @@ __global__ void __launch_bounds__(32) elements_kernel(ElementArgs a) {
                 e.nids = nid;
                 e.seg_off = seg_off;
                 e.nseg = nseg;
-                e.chunk_off = chunk_off;
-                e.nchunk = nchunk;
                 e.energy = en;
                 e.mobility = mo;
                 e.area = 0.0;
@@ -785,38 +783,18 @@ __global__ void __launch_bounds__(32) elements_kernel(ElementArgs a) {
             a.el.n_flat[g] = pb;
             S.np_flat = pb;
             S.ne = ne;
-            S.nch = nch;
             S.nd = nd;
         }
         __syncwarp();
         {
-            const int ne = S.ne, nch = S.nch, nd = S.nd;
+            const int ne = S.ne, nd = S.nd;
             HullElem* E = a.el.elem + (long long)g * a.el.elem_cap;
-            HullChunk* chunks = a.el.chunks + (long long)g * a.el.chunk_cap;
             uint32_t* ikey = a.el.idx_key + (long long)g * a.el.idx_cap;
             int2* irng = a.el.idx_rng + (long long)g * a.el.idx_cap;
             for (int d = lane; d < nd && d < a.el.idx_cap; d += 32) {
                 ikey[d] = S.dkey[d];
                 irng[d] = make_int2(S.doff[d], S.dcnt[d]);
             }
-            // chunk bounding boxes, then element boxes from their chunks (min/max: exact in any order)
-            for (int c = lane; c < nch; c += 32) {
-                HullChunk& C = chunks[c];
-                double lo[3] = {1e300, 1e300, 1e300}, hi[3] = {-1e300, -1e300, -1e300};
-                const double* b = eb + 3 * (long long)C.start;
-                for (int i = 0; i < C.count; i++)
-#pragma unroll
-                    for (int q = 0; q < 3; q++) {
-                        lo[q] = fmin(lo[q], b[3 * i + q]);
-                        hi[q] = fmax(hi[q], b[3 * i + q]);
-                    }
-#pragma unroll
-                for (int q = 0; q < 3; q++) {
-                    C.lo[q] = lo[q];
-                    C.hi[q] = hi[q];
-                }
-            }
-            __syncwarp();
             // GrainBoundary::computeArea (InterfacialElement.cpp:81-91): its triangles'
             // terms summed in triangle order, times h^2
             for (int e = lane; e < ne; e += 32) {
@@ -836,29 +814,15 @@ __global__ void __launch_bounds__(32) elements_kernel(ElementArgs a) {
                 for (; i < sg.y; i++) surface += ea[sg.x + i];
                 el.area = surface * a.ph.ds * a.ph.ds;  // ds = h = 1 / realDomainSize
             }
-            for (int e = lane; e < ne; e += 32) {
-                HullElem& el = E[e];
-                double lo[3] = {1e300, 1e300, 1e300}, hi[3] = {-1e300, -1e300, -1e300};
-                for (int c = el.chunk_off; c < el.chunk_off + el.nchunk; c++)
-#pragma unroll
-                    for (int q = 0; q < 3; q++) {
-                        lo[q] = fmin(lo[q], chunks[c].lo[q]);
-                        hi[q] = fmax(hi[q], chunks[c].hi[q]);
-                    }
-#pragma unroll
-                for (int q = 0; q < 3; q++) {
-                    el.lo[q] = lo[q];
-                    el.hi[q] = hi[q];
-                }
-            }
-            // the correction's FP32 barycenters, relative to the integer centre of the
-            // elements' boxes (the lane wrote those boxes itself above)
+            // the correction's FP32 barycenters, relative to the integer centre of the box
+            // of the grain's barycenters (min/max: exact in any order)
+            const int nl = S.nl, total = min(nbary, a.el.bary_cap), nflat = min(S.np_flat, a.el.flat_cap);
             double ulo[3] = {1e300, 1e300, 1e300}, uhi[3] = {-1e300, -1e300, -1e300};
-            for (int e = lane; e < ne; e += 32)
+            for (int i = lane; i < total; i += 32)
 #pragma unroll
                 for (int q = 0; q < 3; q++) {
-                    ulo[q] = fmin(ulo[q], E[e].lo[q]);
-                    uhi[q] = fmax(uhi[q], E[e].hi[q]);
+                    ulo[q] = fmin(ulo[q], eb[3 * (long long)i + q]);
+                    uhi[q] = fmax(uhi[q], eb[3 * (long long)i + q]);
                 }
 #pragma unroll
             for (int q = 0; q < 3; q++)
@@ -871,12 +835,20 @@ __global__ void __launch_bounds__(32) elements_kernel(ElementArgs a) {
             if (ne > 0 && uhi[0] >= ulo[0])
 #pragma unroll
                 for (int q = 0; q < 3; q++) org[q] = floor(0.5 * (ulo[q] + uhi[q]));
+            // element boxes relative to the origin, rounded outward to FP32, as orderable
+            // integer keys in the index arrays' shared memory (dead by now): 6 per element
+            int* bkey = reinterpret_cast<int*>(S.ikey);
+            static_assert(sizeof(unsigned) * kIHash + sizeof(short) * kIHash + sizeof(uint32_t) * kIdxMax +
+                                  3 * sizeof(int) * kIdxMax + 2 * sizeof(unsigned short) * kPairMax >=
+                              6 * sizeof(int) * kLMax,
+                          "the index arrays hold the element-box keys");
+            for (int q = lane; q < 6 * min(ne, kLMax); q += 32) bkey[q] = (q % 6) < 3 ? INT_MAX : INT_MIN;
+            __syncwarp();
             // every barycenter to its element's run: lane-parallel over the grouped array,
             // barycenter i of list k (the last list whose first barycenter is <= i) going to
             // lflat[k] + (i - off[k])
             float* pf = reinterpret_cast<float*>(a.el.ebf + (long long)g * a.el.flat_cap);
             int* pidx = a.el.eidx + (long long)g * a.el.flat_cap;
-            const int nl = S.nl, total = min(nbary, a.el.bary_cap), nflat = min(S.np_flat, a.el.flat_cap);
             float r2 = 0.f;
             for (int i = lane; i < total; i += 32) {
                 int lo = 0, hi = nl - 1;
@@ -898,10 +870,31 @@ __global__ void __launch_bounds__(32) elements_kernel(ElementArgs a) {
                 pp[6] = (float)w;
                 pidx[dst] = i;
                 r2 = fmaxf(r2, (float)w);
+                const int e = S.fill[lo];  // the element list lo went to (emit)
+                if (e >= 0 && e < ne && e < kLMax) {
+                    int* bk = bkey + 6 * e;
+                    atomicMin(bk + 0, order_key(__double2float_rd(dx)));
+                    atomicMin(bk + 1, order_key(__double2float_rd(dy)));
+                    atomicMin(bk + 2, order_key(__double2float_rd(dz)));
+                    atomicMax(bk + 3, order_key(__double2float_ru(dx)));
+                    atomicMax(bk + 4, order_key(__double2float_ru(dy)));
+                    atomicMax(bk + 5, order_key(__double2float_ru(dz)));
+                }
+            }
+            __syncwarp();
+            // the element boxes, stored as origin + the FP32 bound (exact in FP64), so that
+            // the correction's outward rounding of (box - origin) gives the bound back
+            for (int e = lane; e < min(ne, kLMax); e += 32) {
+                HullElem& el = E[e];
+                const int* bk = bkey + 6 * e;
+#pragma unroll
+                for (int q = 0; q < 3; q++) {
+                    el.lo[q] = bk[q] == INT_MAX ? 1e300 : org[q] + (double)key_float(bk[q]);
+                    el.hi[q] = bk[q + 3] == INT_MIN ? -1e300 : org[q] + (double)key_float(bk[q + 3]);
+                }
             }
             // the padding entry of every odd run: at the origin with q = kInf, never a minimum
             {
-                const HullElem* E = a.el.elem + (long long)g * a.el.elem_cap;
                 for (int e = lane; e < S.ne; e += 32) {
                     const int n = E[e].pcount, dst = E[e].pbase + n;
                     if ((n & 1) && dst >= 0 && dst < nflat) {
@@ -917,25 +910,6 @@ __global__ void __launch_bounds__(32) elements_kernel(ElementArgs a) {
 #pragma unroll
             for (int o = 16; o > 0; o >>= 1) r2 = fmaxf(r2, __shfl_xor_sync(kFull, r2, o));
             if (lane == 0) a.el.eorg[g] = make_float4((float)org[0], (float)org[1], (float)org[2], r2);
-            // every chunk's FP32 box relative to the origin (rounded outward) and its run in
-            // the flattened copy: the chunk lies in one list, whose run starts at lflat
-            float4* cb = a.el.ecb + 2 * (long long)g * a.el.chunk_cap;
-            for (int c = lane; c < nch && c < a.el.chunk_cap; c += 32) {
-                const HullChunk& C = chunks[c];
-                int lo = 0, hi = nl - 1;
-                while (lo < hi) {
-                    const int mid = (lo + hi + 1) >> 1;
-                    if (S.off[mid] <= C.start) lo = mid;
-                    else hi = mid - 1;
-                }
-                const int base = nl > 0 ? S.lflat[lo] : -1;
-                int first = base < 0 ? 0 : base + (C.start - S.off[lo]), count = base < 0 ? 0 : C.count;
-                if (first < 0 || count < 0 || first + count > nflat) first = count = 0;
-                cb[2 * c] = make_float4(__double2float_rd(C.lo[0] - org[0]), __double2float_rd(C.lo[1] - org[1]),
-                                        __double2float_rd(C.lo[2] - org[2]), __int_as_float(first));
-                cb[2 * c + 1] = make_float4(__double2float_ru(C.hi[0] - org[0]), __double2float_ru(C.hi[1] - org[1]),
-                                            __double2float_ru(C.hi[2] - org[2]), __int_as_float(count));
-            }
         }
         __syncwarp();
     }

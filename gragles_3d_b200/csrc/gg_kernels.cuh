@@ -232,23 +232,14 @@ struct HullElem {
     int type;                 // 1 GB, 2 TL, 3 QJ, 4 HJ
     int nids, id_off;         // neighbour IDs in the grain's ID pool
     int seg_off, nseg;        // barycenter segments (start, count) in the grain's segment pool
-    int chunk_off, nchunk;    // barycenter chunks (each inside one segment) in the chunk pool
     int pbase, pcount;        // its barycenters, contiguous, in the flattened FP32 copy (ebf)
     double energy, mobility;  // m_energy, m_mobility
     double area;              // GrainBoundary::computeArea (InterfacialElement.cpp:81-91); 0 for junctions
     double lo[3], hi[3];      // bounding box of its barycenters
 };
 
-// At most kHullChunk consecutive barycenters of one segment with their bounding box:
-// the correction skips a chunk whose box is no nearer than the best barycenter so far.
-constexpr int kHullChunk = 16;
-struct HullChunk {
-    double lo[3], hi[3];
-    int start, count;         // barycenters [start, start + count) of the grouped array
-};
-
 struct HullElements {
-    int elem_cap, id_cap, seg_cap, bary_cap, chunk_cap, idx_cap, pair_cap;
+    int elem_cap, id_cap, seg_cap, bary_cap, idx_cap, pair_cap;
     int flat_cap;             // entries of ebf / eidx per grain: bary_cap + one padding per element
     int* n_elem;              // G + 1
     HullElem* elem;           // (G + 1) x elem_cap
@@ -263,12 +254,8 @@ struct HullElements {
     // as (x0, x1, y0, y1), (z0, z1, w0, w1) for the packed FMA.
     float4* ebf;              // (G + 1) x flat_cap
     int* eidx;                // (G + 1) x flat_cap: position of each of them in ebary (-1: padding)
-    // each chunk's box relative to the origin, rounded outward to FP32, and its run in
-    // ebf: (lo.x, lo.y, lo.z, first as int bits), (hi.x, hi.y, hi.z, count as int bits)
-    float4* ecb;              // (G + 1) x chunk_cap x 2
     int* n_flat;              // G + 1: barycenters in ebf
     float4* eorg;             // G + 1: (o.x, o.y, o.z, largest |p - o|^2 of the grain)
-    HullChunk* chunks;        // (G + 1) x chunk_cap
     // neighbour ID -> the elements whose searched IDs hold it, in search order
     int* n_idx;               // G + 1: distinct IDs
     uint32_t* idx_key;        // (G + 1) x idx_cap
