@@ -1129,6 +1129,18 @@ __device__ __forceinline__ void search_packet(const CorrSmem& S, const float4* p
     }
 }
 
+// q = n / d and r = n % d for 0 <= n < 2^24 and d >= 1, from rcp = RN(1 / d): the float
+// quotient is within 2 of n / d (two roundings of relative size 2^-24 on a value below
+// 2^24), and two correction steps each way make it exact.
+__device__ __forceinline__ void divmod24(int n, int d, float rcp, int& q, int& r) {
+    q = __float2int_rz((float)n * rcp);
+    r = n - q * d;
+    if (r < 0) { q--; r += d; }
+    if (r < 0) { q--; r += d; }
+    if (r >= d) { q++; r -= d; }
+    if (r >= d) { q++; r -= d; }
+}
+
 // The update of one band voxel, box.cpp:476-533, given the element that won (-1: none).
 template <typename T>
 __device__ __forceinline__ void correct_voxel(const CorrectionArgs<T>& a, const HullElem* elem, int g, int win,
@@ -1237,6 +1249,9 @@ __global__ void __launch_bounds__(kCThreads, 3) correction_kernel(CorrectionArgs
         const int nx = b.nx(), ny = b.ny();
         const int nxy = nx * ny;
         const long long nvox = (long long)nxy * b.nz();
+        // a packet voxel's (z, y, x) from its flat index without 64-bit division
+        const bool fastdiv = nvox < (1LL << 24) && nx > 0;
+        const float rnxy = fastdiv ? __frcp_rn((float)nxy) : 0.f, rnx = fastdiv ? __frcp_rn((float)nx) : 0.f;
         // the filter's error bound: q is within 16 R^2 2^-24 of |v' - p'|^2 - |v'|^2 (the
         // three FMAs, the FP32 rounding of p' and |p'|^2), R^2 the largest |v'|^2 or |p'|^2
         float r2 = org.w;
@@ -1343,11 +1358,20 @@ __global__ void __launch_bounds__(kCThreads, 3) correction_kernel(CorrectionArgs
                     active[u] = slot < cnt;
                     const int q = S.vlist[start + (active[u] ? slot : 0)];
                     f[u] = v0 + q;
-                    const int rem = (int)(f[u] % nxy);
+                    int qz, rem, qy, qx;
+                    if (fastdiv) {
+                        divmod24((int)f[u], nxy, rnxy, qz, rem);
+                        divmod24(rem, nx, rnx, qy, qx);
+                    } else {
+                        qz = (int)(f[u] / nxy);
+                        rem = (int)(f[u] % nxy);
+                        qy = rem / nx;
+                        qx = rem % nx;
+                    }
                     // the point is Vector3d(i, j, k), box.cpp:481
-                    kk[u] = b.z0 + (int)(f[u] / nxy);
-                    ii[u] = b.y0 + rem / nx;
-                    jj[u] = b.x0 + rem % nx;
+                    kk[u] = b.z0 + qz;
+                    ii[u] = b.y0 + qy;
+                    jj[u] = b.x0 + qx;
                     // the voxel's input, convolved value and IDLocal, loaded while the search runs
                     vin[u] = T(0);
                     vconv[u] = T(0);
