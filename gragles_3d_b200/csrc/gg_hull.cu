@@ -144,6 +144,7 @@ struct ElemSmem {
     uint32_t* jids;              // kLMax x kJIds junction IDs
     double2* jres;               // kJobMax (mobility, energy)
     int nl, nq, nh, nj, ne, nd, np, np_flat;
+    double ubox[6];  // box of the grain's barycenters (lo, hi)
     int next;  // the work item this warp fetched
 };
 
@@ -451,7 +452,9 @@ __global__ void __launch_bounds__(32) elements_kernel(ElementArgs a) {
         if (nbary > a.el.bary_cap && lane == 0) { atomicOr(a.err, ERR_HULL); atomicOr(a.cap.diag, HULL_TRIANGLES); }
         // 3. barycenters grouped by list, in triangle order (subDivideTrianglesToInterfacialElements):
         //    a record's triangles go after those of the earlier records of its list.  The
-        //    warp first places its 32 records, then copies their triangles together.
+        //    warp first places its 32 records, then copies their triangles together,
+        //    taking the box of all barycenters on the way (the correction's origin).
+        double ulo0 = 1e300, ulo1 = 1e300, ulo2 = 1e300, uhi0 = -1e300, uhi1 = -1e300, uhi2 = -1e300;
         for (int base = 0, tbase = 0; base < nrec; base += 32) {
             const int r = base + lane;
             const bool valid = r < nrec;
@@ -495,10 +498,25 @@ __global__ void __launch_bounds__(32) elements_kernel(ElementArgs a) {
                     eb[3 * (long long)pos + 1] = b1;
                     eb[3 * (long long)pos + 2] = b2;
                     ea[pos] = ta;
+                    ulo0 = fmin(ulo0, b0); ulo1 = fmin(ulo1, b1); ulo2 = fmin(ulo2, b2);
+                    uhi0 = fmax(uhi0, b0); uhi1 = fmax(uhi1, b1); uhi2 = fmax(uhi2, b2);
                 }
             }
             tbase += total;
             __syncwarp();
+        }
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) {
+            ulo0 = fmin(ulo0, __shfl_xor_sync(kFull, ulo0, o));
+            ulo1 = fmin(ulo1, __shfl_xor_sync(kFull, ulo1, o));
+            ulo2 = fmin(ulo2, __shfl_xor_sync(kFull, ulo2, o));
+            uhi0 = fmax(uhi0, __shfl_xor_sync(kFull, uhi0, o));
+            uhi1 = fmax(uhi1, __shfl_xor_sync(kFull, uhi1, o));
+            uhi2 = fmax(uhi2, __shfl_xor_sync(kFull, uhi2, o));
+        }
+        if (lane == 0) {
+            S.ubox[0] = ulo0; S.ubox[1] = ulo1; S.ubox[2] = ulo2;
+            S.ubox[3] = uhi0; S.ubox[4] = uhi1; S.ubox[5] = uhi2;
         }
         // 4. one element per list: energy and mobility (computeGrainBoundaryElements).
         //    Every misorientation a list needs is a job; the warp runs the jobs of all
@@ -815,26 +833,12 @@ __global__ void __launch_bounds__(32) elements_kernel(ElementArgs a) {
                 el.area = surface * a.ph.ds * a.ph.ds;  // ds = h = 1 / realDomainSize
             }
             // the correction's FP32 barycenters, relative to the integer centre of the box
-            // of the grain's barycenters (min/max: exact in any order)
+            // of the grain's barycenters (taken while they were grouped)
             const int nl = S.nl, total = min(nbary, a.el.bary_cap), nflat = min(S.np_flat, a.el.flat_cap);
-            double ulo[3] = {1e300, 1e300, 1e300}, uhi[3] = {-1e300, -1e300, -1e300};
-            for (int i = lane; i < total; i += 32)
-#pragma unroll
-                for (int q = 0; q < 3; q++) {
-                    ulo[q] = fmin(ulo[q], eb[3 * (long long)i + q]);
-                    uhi[q] = fmax(uhi[q], eb[3 * (long long)i + q]);
-                }
-#pragma unroll
-            for (int q = 0; q < 3; q++)
-#pragma unroll
-                for (int o = 16; o > 0; o >>= 1) {
-                    ulo[q] = fmin(ulo[q], __shfl_xor_sync(kFull, ulo[q], o));
-                    uhi[q] = fmax(uhi[q], __shfl_xor_sync(kFull, uhi[q], o));
-                }
             double org[3] = {0, 0, 0};
-            if (ne > 0 && uhi[0] >= ulo[0])
+            if (ne > 0 && S.ubox[3] >= S.ubox[0])
 #pragma unroll
-                for (int q = 0; q < 3; q++) org[q] = floor(0.5 * (ulo[q] + uhi[q]));
+                for (int q = 0; q < 3; q++) org[q] = floor(0.5 * (S.ubox[q] + S.ubox[q + 3]));
             // element boxes relative to the origin, rounded outward to FP32, as orderable
             // integer keys in the index arrays' shared memory (dead by now): 6 per element
             int* bkey = reinterpret_cast<int*>(S.ikey);
