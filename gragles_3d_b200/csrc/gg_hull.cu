@@ -608,68 +608,109 @@ __global__ void __launch_bounds__(32) elements_kernel(ElementArgs a) {
             }
             __syncwarp();
         }
-        if (lane == 0) {
+        // The merges below are sequential, as the reference's: each scan takes the first
+        // pair closer than 2 in the reference's order and restarts from there.  The warp
+        // tests 32 candidates of a scan at a time; one lane merges.
+        {
             // quadruple points closer than 2: a new high-order junction from the pair
-            for (int i = 0; i < S.nq; i++) {
-                for (int j = i + 1; j < S.nq; j++) {
+            int i = 0;
+            while (i < S.nq) {
+                const double* ap = S.jh[S.qlist[i]].pos;
+                int found = -1;
+                for (int j0 = i + 1; j0 < S.nq && found < 0; j0 += 32) {
+                    const int j = j0 + lane;
+                    const bool hit = j < S.nq && sqrt(sqdist(ap, S.jh[S.qlist[j]].pos)) < 2;
+                    const unsigned m = __ballot_sync(kFull, hit);
+                    if (m) found = j0 + __ffs(m) - 1;
+                }
+                if (found < 0) {
+                    i++;
+                    continue;
+                }
+                if (S.nj >= kLMax) {
+                    if (lane == 0) { atomicOr(a.err, ERR_HULL); atomicOr(a.cap.diag, HULL_JUNCTIONS); }
+                    i++;
+                    continue;
+                }
+                if (lane == 0) {
+                    const int j = found;
                     JHead& A = S.jh[S.qlist[i]];
                     JHead& B = S.jh[S.qlist[j]];
-                    if (sqrt(sqdist(A.pos, B.pos)) < 2) {
-                        if (S.nj >= kLMax) { atomicOr(a.err, ERR_HULL); atomicOr(a.cap.diag, HULL_JUNCTIONS); break; }
-                        const uint32_t* aid = S.jids + (long long)S.qlist[i] * kJIds;
-                        const uint32_t* bid = S.jids + (long long)S.qlist[j] * kJIds;
-                        const uint32_t a0 = aid[0], a1 = aid[1], a2 = aid[2], b0 = bid[0], b1 = bid[1], b2 = bid[2];
-                        JHead& H = S.jh[S.nj];
-                        uint32_t* hid = S.jids + (long long)S.nj * kJIds;
-                        H.type = 4;
-                        start_ids(H, S.nj);
-                        push_id(H, hid, a0, a.err, a.cap.diag);
-                        push_id(H, hid, a1, a.err, a.cap.diag);
-                        push_id(H, hid, a2, a.err, a.cap.diag);
-                        const uint32_t bq[3] = {b0, b1, b2};
-                        for (int q = 0; q < 3; q++)  // B's IDs that A already has (sic)
-                            if (bq[q] == a0 || bq[q] == a1 || bq[q] == a2) push_id(H, hid, bq[q], a.err, a.cap.diag);
-                        H.head = A.head;
-                        H.tail = A.tail;
-                        S.next_key[H.tail] = B.head;  // the lists of A, then of B; IDs as above
-                        H.tail = B.tail;
-                        junction_position(H, S, eb, a.el.bary_cap, a.err);
-                        // erase i and j (j - 1 after the first erase), then append H
-                        for (int u = j; u < S.nq - 1; u++) S.qlist[u] = S.qlist[u + 1];
-                        for (int u = i; u < S.nq - 2; u++) S.qlist[u] = S.qlist[u + 1];
-                        S.nq -= 2;
-                        S.hlist[S.nh++] = S.nj++;
-                        i--;
-                        break;
+                    const uint32_t* aid = S.jids + (long long)S.qlist[i] * kJIds;
+                    const uint32_t* bid = S.jids + (long long)S.qlist[j] * kJIds;
+                    const uint32_t a0 = aid[0], a1 = aid[1], a2 = aid[2], b0 = bid[0], b1 = bid[1], b2 = bid[2];
+                    JHead& H = S.jh[S.nj];
+                    uint32_t* hid = S.jids + (long long)S.nj * kJIds;
+                    H.type = 4;
+                    start_ids(H, S.nj);
+                    push_id(H, hid, a0, a.err, a.cap.diag);
+                    push_id(H, hid, a1, a.err, a.cap.diag);
+                    push_id(H, hid, a2, a.err, a.cap.diag);
+                    const uint32_t bq[3] = {b0, b1, b2};
+                    for (int q = 0; q < 3; q++)  // B's IDs that A already has (sic)
+                        if (bq[q] == a0 || bq[q] == a1 || bq[q] == a2) push_id(H, hid, bq[q], a.err, a.cap.diag);
+                    H.head = A.head;
+                    H.tail = A.tail;
+                    S.next_key[H.tail] = B.head;  // the lists of A, then of B; IDs as above
+                    H.tail = B.tail;
+                    junction_position(H, S, eb, a.el.bary_cap, a.err);
+                    // erase i and j (j - 1 after the first erase), then append H
+                    for (int u = j; u < S.nq - 1; u++) S.qlist[u] = S.qlist[u + 1];
+                    for (int u = i; u < S.nq - 2; u++) S.qlist[u] = S.qlist[u + 1];
+                    S.nq -= 2;
+                    S.hlist[S.nh++] = S.nj++;
+                }
+                __syncwarp();  // i again: the next quadruple point moved into it
+            }
+            // quadruple points closer than 2 to a high-order junction join it (its
+            // position moves with every join)
+            for (int k = 0; k < S.nh; k++) {
+                int i = 0;
+                for (;;) {
+                    const double* hp = S.jh[S.hlist[k]].pos;
+                    int found = -1;
+                    for (int i0 = i; i0 < S.nq && found < 0; i0 += 32) {
+                        const int ii = i0 + lane;
+                        const bool hit = ii < S.nq && sqrt(sqdist(S.jh[S.qlist[ii]].pos, hp)) < 2;
+                        const unsigned m = __ballot_sync(kFull, hit);
+                        if (m) found = i0 + __ffs(m) - 1;
                     }
+                    if (found < 0) break;
+                    if (lane == 0) {
+                        JHead& H = S.jh[S.hlist[k]];
+                        chain(S, H, S.jh[S.qlist[found]], S.qlist[found]);
+                        junction_position(H, S, eb, a.el.bary_cap, a.err);
+                        for (int u = found; u < S.nq - 1; u++) S.qlist[u] = S.qlist[u + 1];
+                        S.nq--;
+                    }
+                    __syncwarp();
+                    i = found;
                 }
             }
-            // quadruple points closer than 2 to a high-order junction join it
-            for (int k = 0; k < S.nh; k++)
-                for (int i = 0; i < S.nq; i++) {
-                    JHead& H = S.jh[S.hlist[k]];
-                    JHead& Q = S.jh[S.qlist[i]];
-                    if (sqrt(sqdist(Q.pos, H.pos)) < 2) {
-                        chain(S, H, Q, S.qlist[i]);
-                        junction_position(H, S, eb, a.el.bary_cap, a.err);
-                        for (int u = i; u < S.nq - 1; u++) S.qlist[u] = S.qlist[u + 1];
-                        S.nq--;
-                        i--;
-                    }
-                }
             // high-order junctions closer than 2 merge
-            for (int i = 0; i < S.nh; i++)
-                for (int k = i + 1; k < S.nh; k++) {
-                    JHead& A = S.jh[S.hlist[i]];
-                    JHead& B = S.jh[S.hlist[k]];
-                    if (sqrt(sqdist(A.pos, B.pos)) < 2) {
-                        chain(S, A, B, S.hlist[k]);
-                        junction_position(A, S, eb, a.el.bary_cap, a.err);
-                        for (int u = k; u < S.nh - 1; u++) S.hlist[u] = S.hlist[u + 1];
-                        S.nh--;
-                        k--;
+            for (int i = 0; i < S.nh; i++) {
+                int k = i + 1;
+                for (;;) {
+                    const double* ap = S.jh[S.hlist[i]].pos;
+                    int found = -1;
+                    for (int k0 = k; k0 < S.nh && found < 0; k0 += 32) {
+                        const int kk = k0 + lane;
+                        const bool hit = kk < S.nh && sqrt(sqdist(ap, S.jh[S.hlist[kk]].pos)) < 2;
+                        const unsigned m = __ballot_sync(kFull, hit);
+                        if (m) found = k0 + __ffs(m) - 1;
                     }
+                    if (found < 0) break;
+                    if (lane == 0) {
+                        JHead& A = S.jh[S.hlist[i]];
+                        chain(S, A, S.jh[S.hlist[found]], S.hlist[found]);
+                        junction_position(A, S, eb, a.el.bary_cap, a.err);
+                        for (int u = found; u < S.nh - 1; u++) S.hlist[u] = S.hlist[u + 1];
+                        S.nh--;
+                    }
+                    __syncwarp();
+                    k = found;
                 }
+            }
         }
         __syncwarp();
         // 6. the element table in search order: HJ, QJ, TL, GB, with its barycenter
