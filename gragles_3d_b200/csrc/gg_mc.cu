@@ -158,15 +158,16 @@ __global__ void __launch_bounds__(kThreads, 3) mc_kernel(MCArgs<T> a, int slab_b
           {
               const T* src = sdf + (long long)zc0 * plane;
               const int nv = (lz + 1) * plane;
-              for (int v0 = 0; v0 < nv; v0 += 8 * kThreads) {
-                  T r[8];
+              constexpr int kMB = sizeof(T) == 4 ? 16 : 8;  // loads in flight per thread
+              for (int v0 = 0; v0 < nv; v0 += kMB * kThreads) {
+                  T r[kMB];
 #pragma unroll
-                  for (int u = 0; u < 8; u++) {
+                  for (int u = 0; u < kMB; u++) {
                       const int v = v0 + u * kThreads + threadIdx.x;
                       r[u] = v < nv ? src[v] : T(-1);
                   }
 #pragma unroll
-                  for (int u = 0; u < 8; u++) {
+                  for (int u = 0; u < kMB; u++) {
                       const int v = v0 + u * kThreads + threadIdx.x;
                       if (v < nv) sgn[v] = r[u] >= T(0);
                   }
