@@ -977,6 +977,7 @@ constexpr int kCVox = 4096;           // voxels of one pass: a run of the box in
 constexpr int kCItem = 4 * kCVox;     // voxels of one work item: a grain's box is cut into runs of these
 constexpr int kLV = 2;                // voxels per lane: a packet is 32 kLV voxels of one neighbour
 constexpr int kPacket = 32 * kLV;
+constexpr int kWarpTies = 8;          // near ties a packet settles voxel by voxel with the whole warp
 constexpr unsigned short kNoD = 0xFFFF;
 constexpr float kInf = 3.0e38f;
 constexpr int kSPts = 2304;           // barycenters staged in shared memory (more: read from HBM)
@@ -1088,6 +1089,46 @@ __device__ int exact_winner(const CorrSmem& S, const float4* pts, int first, int
     return bw;
 }
 
+// exact_winner for one voxel with the whole warp: lane l takes barycenters l, l + 32, ...
+// of each element the band holds, keeping the least FP64 distance and, among equal
+// ones, the first in its own order; the warp then reduces on (distance, element position
+// c, barycenter) -- the first in search order among the least, as the sequential walk.
+__device__ int exact_winner_warp(const CorrSmem& S, const float4* pts, int first, int count, int ne,
+                                 const int* __restrict__ eidx, const double* __restrict__ eb, int i, int j, int k,
+                                 float4 org, float limit, unsigned band) {
+    const int lane = threadIdx.x & 31;
+    const float ax = -2.f * ((float)i - org.x), ay = -2.f * ((float)j - org.y), az = -2.f * ((float)k - org.z);
+    const double x = (double)i, y = (double)j, z = (double)k;
+    double bd = 10000000.0;
+    int bkey = 0x7FFFFFFF;  // (c << 20) | barycenter position in the element's run
+    for (int c = 0; c < count; c++) {
+        if (count <= 32 && !((band >> c) & 1u)) continue;
+        const int e = S.pairs[first + c];
+        if (e >= ne) continue;
+        const int2 r = S.erun[e];
+        for (int t = lane; t < r.y; t += 32) {
+            if (qval(pt_at(pts, r.x + t), ax, ay, az) > limit) continue;
+            const int src = eidx[r.x + t];
+            if (src < 0) continue;
+            const double d = sqdist3(x, y, z, eb + 3 * (long long)src);
+            if (d < bd) {
+                bd = d;
+                bkey = (c << 20) | t;
+            }
+        }
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        const double od = __shfl_xor_sync(kFull, bd, o);
+        const int ok = __shfl_xor_sync(kFull, bkey, o);
+        if (od < bd || (od == bd && ok < bkey)) {
+            bd = od;
+            bkey = ok;
+        }
+    }
+    return bkey == 0x7FFFFFFF ? -1 : S.pairs[first + (bkey >> 20)];
+}
+
 // Lower bound of q over a box [lo, hi] (relative, rounded outward) for the voxel v':
 // |v' - box|^2 in FP32, scaled down past its rounding, - |v'|^2 - eps.
 __device__ __forceinline__ float box_bound(float vx, float vy, float vz, float vv, float lx, float ly, float lz,
@@ -1164,13 +1205,37 @@ __device__ __forceinline__ void search_packet(const CorrSmem& S, const float4* p
             if (m[u] <= best[u] + eps2) band[u] |= 1u << (c & 31);
         }
     }
+    // proven when every other element is farther by more than the band; a few near ties
+    // are settled one voxel at a time by the whole warp, many by each lane for its own
+    unsigned tie[V];
+    int nties = 0;
 #pragma unroll
     for (int u = 0; u < V; u++) {
         win[u] = beste[u];
-        // proven when every other element is farther by more than the band
-        if (beste[u] >= 0 && !(second[u] - best[u] > eps2))
-            win[u] = exact_winner(S, pts, first, count, ne, eidx, eb, (double)ii[u], (double)jj[u], (double)kk[u],
-                                  -2.f * vx[u], -2.f * vy[u], -2.f * vz[u], best[u] + eps2, band[u]);
+        tie[u] = __ballot_sync(kFull, active[u] && beste[u] >= 0 && !(second[u] - best[u] > eps2));
+        nties += __popc(tie[u]);
+    }
+    if (nties == 0) return;
+    const int lane = threadIdx.x & 31;
+    if (nties <= kWarpTies) {
+#pragma unroll
+        for (int u = 0; u < V; u++)
+            for (unsigned m = tie[u]; m; m &= m - 1) {
+                const int src = __ffs(m) - 1;
+                const int si = __shfl_sync(kFull, ii[u], src), sj = __shfl_sync(kFull, jj[u], src),
+                          sk = __shfl_sync(kFull, kk[u], src);
+                const float lim = __shfl_sync(kFull, best[u] + eps2, src);
+                const unsigned bnd = __shfl_sync(kFull, band[u], src);
+                const int w = exact_winner_warp(S, pts, first, count, ne, eidx, eb, si, sj, sk, org, lim, bnd);
+                if (lane == src) win[u] = w;
+            }
+    } else {
+#pragma unroll
+        for (int u = 0; u < V; u++)
+            if ((tie[u] >> lane) & 1u)
+                win[u] = exact_winner(S, pts, first, count, ne, eidx, eb, (double)ii[u], (double)jj[u],
+                                      (double)kk[u], -2.f * vx[u], -2.f * vy[u], -2.f * vz[u], best[u] + eps2,
+                                      band[u]);
     }
 }
 
