@@ -225,6 +225,8 @@ struct TileSmem {
     unsigned char* ulist;  // those entries, ascending
     unsigned char* ucol;   // per entry: its column of pos (the first kUCap of ulist), 0xFF: none
     int* nu;            // their count
+    unsigned char* bnd;    // per entry: its box reaches the boundary grain's zone
+    unsigned char* deep;   // per voxel: at least gb from every face of that zone
 };
 
 template <typename T>
@@ -246,9 +248,16 @@ __device__ TileSmem<T> carve(unsigned char* base, int mcap) {
     s.pos = reinterpret_cast<unsigned short*>(p); p += 2 * (size_t)mcap * kUCap;
     s.ulist = p; p += 256;
     s.ucol = p; p += 256;
-    s.topi = p;
+    s.topi = p; p += kTV * kTop;
+    s.deep = p; p += kTV;
+    s.bnd = p;
     return s;
 }
+
+// |in| < lim, lim in FP64, as (double)fabs(in) < lim: for FP32 values against the FP32
+// bound rounded up (a float is below a double exactly when it is below that bound).
+__device__ __forceinline__ bool in_band(double in, double lim) { return fabs(in) < lim; }
+__device__ __forceinline__ bool in_band(float in, double lim) { return fabsf(in) < __double2float_ru(lim); }
 
 template <typename T>
 __device__ __forceinline__ T neg_inf();
@@ -317,6 +326,8 @@ __global__ void __launch_bounds__(kThreads, 4) compare_kernel(CompareArgs<T> a) 
             s.outoff[e] = a.out.off[g];
             s.idoff[e] = a.idoff_new[g];
             s.tsize[e] = pos_table_size(a.n_cmp[g], a.pos_cap);
+            s.bnd[e] = !(bb[0] > a.geo.gb && bb[1] < a.geo.M - a.geo.gb && bb[2] > a.geo.gb &&
+                         bb[3] < a.geo.M - a.geo.gb && bb[4] > a.geo.gb && bb[5] < a.geo.M - a.geo.gb);
             s.bbox[6 * e + 0] = INT_MAX; s.bbox[6 * e + 1] = INT_MIN;
             s.bbox[6 * e + 2] = INT_MAX; s.bbox[6 * e + 3] = INT_MIN;
             s.bbox[6 * e + 4] = INT_MAX; s.bbox[6 * e + 5] = INT_MIN;
@@ -406,6 +417,11 @@ __global__ void __launch_bounds__(kThreads, 4) compare_kernel(CompareArgs<T> a) 
                     if (ti[k] != 0xFF) atomicOr(s.umask + (ti[k] >> 5), 1u << (ti[k] & 31));
                 }
                 s.ncand[v] = nc;
+                // A voxel at least gb from every face of the boundary grain's zone gets an
+                // all-negative distance <= -gb from bc_assign, which changes nothing.
+                const int x = X0 + v % kTX, y = Y0 + (v / kTX) % kTY, z = Z0 + v / (kTX * kTY);
+                const int lo_in = 2 * a.geo.gb - 1, hi_in = a.geo.M - 1 - 2 * a.geo.gb;
+                s.deep[v] = x >= lo_in && x <= hi_in && y >= lo_in && y <= hi_in && z >= lo_in && z <= hi_in;
             }
         }
         __syncthreads();
@@ -535,13 +551,7 @@ __global__ void __launch_bounds__(kThreads, 4) compare_kernel(CompareArgs<T> a) 
                 const Box Bold = load_box(a.idbox_old + 6 * ga);
                 idv = f < Bold.count() ? a.id_old[a.idoff_old[ga] + f] : 0u;
             }
-            const bool boundary = !(A.x0 > a.geo.gb && A.x1 < a.geo.M - a.geo.gb && A.y0 > a.geo.gb &&
-                                    A.y1 < a.geo.M - a.geo.gb && A.z0 > a.geo.gb && A.z1 < a.geo.M - a.geo.gb);
-            // A voxel at least gb from every face of the boundary grain's zone gets an
-            // all-negative distance <= -gb from bc_assign, which changes nothing: skip it.
-            const int lo_in = 2 * a.geo.gb - 1, hi_in = a.geo.M - 1 - 2 * a.geo.gb;
-            const bool deep = x >= lo_in && x <= hi_in && y >= lo_in && y <= hi_in && z >= lo_in && z <= hi_in;
-            if (boundary && !deep) {
+            if (s.bnd[ea] && !s.deep[v]) {  // the boundary condition near the zone's faces
                 const double d = bc_dist(A, y, x, z, a.geo.M, a.geo.gb);
                 if (d > -a.geo.gb)
                     if (d * a.geo.h > (double)cmpv) {
@@ -551,7 +561,7 @@ __global__ void __launch_bounds__(kThreads, 4) compare_kernel(CompareArgs<T> a) 
             }
             T res;
             if (!a.set_comparison) res = cmpv;
-            else if ((double)fabs(in) < lim) res = T(0.5) * (in - cmpv);
+            else if (in_band(in, lim)) res = T(0.5) * (in - cmpv);
             else res = in;
             a.out.data[s.outoff[ea] + f] = res;
             a.id_new[s.idoff[ea] + f] = idv;
@@ -603,7 +613,7 @@ size_t compare_smem_bytes(int mcap, bool fp64) {
     const size_t e = fp64 ? 8 : 4;
     return 24 * (size_t)mcap + e * (size_t)mcap * kVS + e * kTV * kTop + 4 * (size_t)mcap +
            48 * (size_t)mcap + 4 * (size_t)mcap + 4 * kTV + 48 + 2 * (size_t)mcap * kUCap + 512 +
-           kTV * kTop + 64;
+           kTV * kTop + kTV + (size_t)mcap + 64;
 }
 
 long long bin_capacity(int G, int side) {
