@@ -409,13 +409,19 @@ struct RedistArgs {
     int* err;
 };
 // Size classes of the redistancing: grains whose output box side n falls in class c
-// (n <= redist_side(c), above the previous bound) run in launches whose block size and
-// shared memory fit that side, so that small boxes do not pay for the largest one.
-constexpr int kRedistClasses = 5;
+// (n <= redist_side(c), above the previous bound) run in launches whose block size,
+// strides and shared memory fit that side, so that small boxes do not pay for the
+// largest one; a CTA of class c runs redist_units(c) slices (or rows) of one grain side
+// by side so that its lanes stay busy.
+constexpr int kRedistClasses = 7;
 __host__ __device__ constexpr int redist_side(int c) {
-    return c <= 0 ? 32 : (c == 1 ? 40 : (c == 2 ? 48 : (c == 3 ? 64 : (1 << 30))));
+    return c <= 0 ? 24 : (c == 1 ? 32 : (c == 2 ? 40 : (c == 3 ? 48 : (c == 4 ? 56 : (c == 5 ? 64 : (1 << 30))))));
 }
-// class_toff: kRedistClasses tile tables of stride G + 2 (n tiles per grain of the class),
+__host__ __device__ constexpr int redist_units(int c) {
+    return c <= 0 ? 5 : (c == 1 ? 4 : (c == 2 ? 3 : (c == 3 ? 2 : 1)));
+}
+// class_toff: kRedistClasses tile tables of stride G + 2 (ceil(n / redist_units(c)) tiles
+// per grain of class c),
 // from launch_redist_classes; null: one launch over `a.toff` sized for `side`.
 template <typename T>
 void launch_redistance(const RedistArgs<T>& a, int grid, int side, const int* class_toff, cudaStream_t s);

@@ -26,15 +26,27 @@ constexpr int kThreads = 256;
 constexpr int kHash = 1024;  // distinct neighbour IDs per grain (power of two)
 constexpr int kSlabBytes = 36 * 1024;  // shared memory for a slab's sign bytes and cube lists
 
-// cubeindex bit b <-> corner offset (dx, dy, dz), marchingCubes.cpp:376-385
-__constant__ int c_corner[8][3] = {{0, 0, 1}, {1, 0, 1}, {1, 0, 0}, {0, 0, 0},
-                                   {0, 1, 1}, {1, 1, 1}, {1, 1, 0}, {0, 1, 0}};
-// edge e joins corners (a, b) in VertexInterp argument order, marchingCubes.cpp:392-469
-__constant__ int c_edge[12][2] = {{0, 1}, {1, 2}, {2, 3}, {3, 0}, {4, 5}, {5, 6},
-                                  {6, 7}, {7, 4}, {0, 4}, {1, 5}, {2, 6}, {3, 7}};
-// neighbour-list corner order, marchingCubes.cpp:505-553
-__constant__ int c_nbc[8][3] = {{0, 0, 0}, {1, 0, 0}, {1, 1, 0}, {0, 1, 0},
-                                {0, 0, 1}, {1, 0, 1}, {1, 1, 1}, {0, 1, 1}};
+// cubeindex bit q <-> corner offset (dx, dy, dz), marchingCubes.cpp:376-385:
+// (0,0,1) (1,0,1) (1,0,0) (0,0,0) (0,1,1) (1,1,1) (1,1,0) (0,1,0); compile-time
+// functions, so that every unrolled corner offset folds into the address.
+__host__ __device__ constexpr int corner_dx(int q) { return ((q & 3) == 1 || (q & 3) == 2) ? 1 : 0; }
+__host__ __device__ constexpr int corner_dy(int q) { return q >> 2; }
+__host__ __device__ constexpr int corner_dz(int q) { return (q & 3) < 2 ? 1 : 0; }
+// edge e joins corners (edge_a(e), edge_b(e)) in VertexInterp argument order,
+// marchingCubes.cpp:392-469: (0,1) (1,2) (2,3) (3,0) (4,5) (5,6) (6,7) (7,4) (0,4) (1,5) (2,6) (3,7)
+__host__ __device__ constexpr int edge_a(int e) { return e < 8 ? e : e - 8; }
+__host__ __device__ constexpr int edge_b(int e) { return e < 8 ? ((e & 4) | ((e + 1) & 3)) : e - 4; }
+// neighbour-list corner order, marchingCubes.cpp:505-553:
+// (0,0,0) (1,0,0) (1,1,0) (0,1,0) (0,0,1) (1,0,1) (1,1,1) (0,1,1)
+__host__ __device__ constexpr int nbc_dx(int k) { return ((k & 3) == 1 || (k & 3) == 2) ? 1 : 0; }
+__host__ __device__ constexpr int nbc_dy(int k) { return (k & 3) >= 2 ? 1 : 0; }
+__host__ __device__ constexpr int nbc_dz(int k) { return k >> 2; }
+static_assert(corner_dx(1) == 1 && corner_dz(2) == 0 && corner_dy(7) == 1 && corner_dz(4) == 1, "corner table");
+static_assert(edge_b(3) == 0 && edge_b(7) == 4 && edge_b(6) == 7 && edge_a(11) == 3 && edge_b(11) == 7, "edge table");
+static_assert(nbc_dx(2) == 1 && nbc_dy(3) == 1 && nbc_dx(3) == 0 && nbc_dz(5) == 1, "neighbour corner table");
+// a cube crosses the zero level unless its 8 corners agree: the edge table is 0 exactly
+// for cube indices 0 and 255
+__device__ __forceinline__ bool cube_active(int ci) { return ci != 0 && ci != 255; }
 
 struct V3 { double x, y, z; };
 
@@ -129,7 +141,9 @@ __global__ void __launch_bounds__(kThreads, 3) mc_kernel(MCArgs<T> a, int slab_b
         // Slabs of LZ cube layers: the sign bytes of their LZ + 1 voxel layers are staged
         // with one coalesced load per voxel, then every cube is classified from shared
         // memory; a cube-index byte and an active-list entry per cube.
-        int LZ = ncplane > 0 ? (slab_bytes - plane - 2) / (plane + 3 * ncplane) : 0;
+        // per cube layer: a sign byte per voxel, a cube-index byte and a 2-byte list entry
+        // per cube, an active-cube bit per cube (in 32-bit words)
+        int LZ = ncplane > 0 ? (slab_bytes - plane - 16) / (plane + 3 * ncplane + ncplane / 8 + 1) : 0;
         if (ncplane > 0 && LZ > 65535 / ncplane) LZ = 65535 / ncplane;
         if (LZ > ncz) LZ = ncz;
         if (ncplane > 0 && LZ < 1) {  // a single layer does not fit the shared memory
@@ -141,6 +155,8 @@ __global__ void __launch_bounds__(kThreads, 3) mc_kernel(MCArgs<T> a, int slab_b
         // 2-byte entries at an even offset from the (16-byte aligned) buffer start
         const int act_off = ((LZ + 1) * plane + LZ * ncplane + 1) & ~1;
         unsigned short* act = reinterpret_cast<unsigned short*>(slab_raw + act_off);
+        // one word per 32 consecutive cubes of the slab, bit = the cube is active
+        unsigned* amask = reinterpret_cast<unsigned*>(slab_raw + ((act_off + 2 * LZ * ncplane + 3) & ~3));
         // cube (lx, ly, lz) of a slab is lz * ncplane + ly * ncx + lx; a step of kThreads
         // cubes is (sz, sy, sx) in that mixed radix, so coordinates advance without divisions
         int sx = 0, sy = 0, sz = 0;
@@ -175,16 +191,23 @@ __global__ void __launch_bounds__(kThreads, 3) mc_kernel(MCArgs<T> a, int slab_b
           }
           __syncthreads();
           {
+              // cubes base + threadIdx.x, a whole warp on 32 consecutive cubes (a multiple
+              // of 32 from the slab start): the warp's ballot is that word of amask
               const int q0 = threadIdx.x / ncx;
               int cx = threadIdx.x - q0 * ncx, cz = q0 / ncy;
               int cy = q0 - cz * ncy;
-              for (int cl = threadIdx.x; cl < ncs; cl += kThreads) {
-                  const unsigned char* p = sgn + cz * plane + cy * nxb + cx;
+              for (int cl0 = 0; cl0 < ncs; cl0 += kThreads) {
+                  const int cl = cl0 + threadIdx.x;
                   int ci = 0;
+                  if (cl < ncs) {
+                      const unsigned char* p = sgn + cz * plane + cy * nxb + cx;
 #pragma unroll
-                  for (int q = 0; q < 8; q++)
-                      ci |= (int)p[c_corner[q][2] * plane + c_corner[q][1] * nxb + c_corner[q][0]] << q;
-                  cidx[cl] = (unsigned char)ci;
+                      for (int q = 0; q < 8; q++)
+                          ci |= (int)p[corner_dz(q) * plane + corner_dy(q) * nxb + corner_dx(q)] << q;
+                      cidx[cl] = (unsigned char)ci;
+                  }
+                  const unsigned m = __ballot_sync(0xffffffffu, cube_active(ci));
+                  if ((threadIdx.x & 31) == 0 && cl < ncs) amask[cl >> 5] = m;
                   cx += sx;
                   cy += sy;
                   cz += sz;
@@ -193,15 +216,17 @@ __global__ void __launch_bounds__(kThreads, 3) mc_kernel(MCArgs<T> a, int slab_b
               }
           }
           __syncthreads();
-          // active cubes of the slab, in cube order: thread t scans cubes [t seg, (t + 1) seg)
-          const int seg = (ncs + kThreads - 1) / kThreads;
-          const int s0 = threadIdx.x * seg, s1 = min(s0 + seg, ncs);
+          // active cubes of the slab, in cube order: thread t takes words [t seg, (t + 1) seg)
+          const int nmask = (ncs + 31) >> 5;
+          const int seg = (nmask + kThreads - 1) / kThreads;
+          const int s0 = threadIdx.x * seg, s1 = min(s0 + seg, nmask);
           int nloc = 0;
-          for (int lc = s0; lc < s1; lc++) nloc += gg_mc_edge_table[cidx[lc]] != 0;
+          for (int m = s0; m < s1; m++) nloc += __popc(amask[m]);
           int n_act;
           int w = block_exclusive_scan(nloc, warp_sums, n_act);
-          for (int lc = s0; lc < s1; lc++)
-              if (gg_mc_edge_table[cidx[lc]] != 0) act[w++] = (unsigned short)lc;
+          for (int m = s0; m < s1; m++)
+              for (unsigned bits = amask[m]; bits; bits &= bits - 1)
+                  act[w++] = (unsigned short)(m * 32 + __ffs(bits) - 1);
           __syncthreads();
           for (int ab = 0; ab < n_act; ab += kThreads) {
             const int ia = ab + threadIdx.x;
@@ -221,7 +246,7 @@ __global__ void __launch_bounds__(kThreads, 3) mc_kernel(MCArgs<T> a, int slab_b
                 base = lzz * plane + ly * nxb + lx;
 #pragma unroll
                 for (int k = 0; k < 8; k++)
-                    val[k] = (double)sdf[base + c_corner[k][2] * plane + c_corner[k][1] * nxb + c_corner[k][0]];
+                    val[k] = (double)sdf[base + corner_dz(k) * plane + corner_dy(k) * nxb + corner_dx(k)];
                 while (gg_mc_tri_table[ci][3 * nt] != -1) nt++;
             }
             int chunk_total;
@@ -232,9 +257,9 @@ __global__ void __launch_bounds__(kThreads, 3) mc_kernel(MCArgs<T> a, int slab_b
 #pragma unroll
                 for (int e = 0; e < 12; e++) {
                     if (!(et & (1 << e))) continue;
-                    const int ka = c_edge[e][0], kb = c_edge[e][1];
-                    const V3 p1{(double)(x + c_corner[ka][0]), (double)(y + c_corner[ka][1]), (double)(z + c_corner[ka][2])};
-                    const V3 p2{(double)(x + c_corner[kb][0]), (double)(y + c_corner[kb][1]), (double)(z + c_corner[kb][2])};
+                    const int ka = edge_a(e), kb = edge_b(e);
+                    const V3 p1{(double)(x + corner_dx(ka)), (double)(y + corner_dy(ka)), (double)(z + corner_dz(ka))};
+                    const V3 p2{(double)(x + corner_dx(kb)), (double)(y + corner_dy(kb)), (double)(z + corner_dz(kb))};
                     vl[e] = vinterp(p1, p2, val[ka], val[kb]);
                 }
                 for (int q = 0; q < nt; q++) {
@@ -272,7 +297,7 @@ __global__ void __launch_bounds__(kThreads, 3) mc_kernel(MCArgs<T> a, int slab_b
                 int cnt = 0;
 #pragma unroll
                 for (int k = 0; k < 8; k++) {
-                    const int at = base + c_nbc[k][2] * plane + c_nbc[k][1] * nxb + c_nbc[k][0];
+                    const int at = base + nbc_dz(k) * plane + nbc_dy(k) * nxb + nbc_dx(k);
                     // inside = value >= 0: the staged sign byte of the corner (slab-relative)
                     const int sat = at - zc0 * plane;
                     unsigned id = sgn[sat] ? (unsigned)g : idl[at];
@@ -404,7 +429,7 @@ __global__ void count_kernel(int G, const int* present, const int* exists, const
 size_t mc_slab_bytes(int side) {
     // at least one cube layer: two voxel layers of sign bytes, a byte and a list entry per cube
     const size_t n = side > 1 ? side : 2;
-    const size_t one_layer = 2 * n * n + 3 * (n - 1) * (n - 1) + 2;
+    const size_t one_layer = 2 * n * n + 3 * (n - 1) * (n - 1) + (n - 1) * (n - 1) / 8 + 1 + 16;
     return one_layer > kSlabBytes ? one_layer : kSlabBytes;
 }
 

@@ -40,11 +40,19 @@ struct Intersect {
     }
 };
 
-// x + isgn(s) * h of the reference, without the int -> T conversion and product:
-// isgn(s) * h is exactly h, -h or +0.
+// isgn(s) * h of the reference: h, -h or +0 (isgn is 0 for +-0 and NaN), as a sign copy.
+__device__ __forceinline__ float copysign_t(float h, float s) { return copysignf(h, s); }
+__device__ __forceinline__ double copysign_t(double h, double s) { return copysign(h, s); }
 template <typename T>
-__device__ __forceinline__ T add_sgn(T x, T s, T h) {
-    return x + (s > T(0) ? h : (s < T(0) ? -h : T(0)));  // x - h is x + (-h) in IEEE arithmetic
+__device__ __forceinline__ T sgn_h(T s, T h) {
+    return fabs(s) > T(0) ? copysign_t(h, s) : T(0);
+}
+
+// The propagation step: out_next takes out_here + isgn(src) * h when that is closer to 0.
+template <typename T>
+__device__ __forceinline__ void step_prop(T src, T out_here, T& out_next, T h) {
+    const T candidate = out_here + sgn_h(src, h);
+    if (fabs(candidate) < fabs(out_next)) out_next = candidate;
 }
 
 // The interpolation step at a sign change between a (here) and b (next), then the
@@ -56,217 +64,266 @@ __device__ __forceinline__ void step_in(T a, T b, T& out_here, T& out_next, T h)
         const T distToZero = -a / i_slope;
         if (fabs(out_here) > fabs(distToZero)) out_here = -distToZero * isgn(i_slope);
     }
-    const T candidate = add_sgn(out_here, b, h);
-    if (fabs(candidate) < fabs(out_next)) out_next = candidate;
-}
-template <typename T>
-__device__ __forceinline__ void step_prop(T sgn_src, T out_here, T& out_next, T h) {
-    const T candidate = add_sgn(out_here, sgn_src, h);
-    if (fabs(candidate) < fabs(out_next)) out_next = candidate;
+    step_prop(b, out_here, out_next, h);
 }
 
-// Forward sweep over positions p0 .. p_end - 1 of a line: o[p * so] is the output at
-// p, in[p * si] the input, valid for p in [p0, p_in_end) when `inside`.  The
-// reference's x/y/z forward loops (box.cpp:2367-2401, 2437-2472, 2501-2538) take
-// step_in while p < p_in_end - 1 (and inside), else step_prop: a prefix, so the loop
-// is split in two.
+// `count` steps along one line from op = &o[p] (cur = o[p]), moving s elements a step
+// (s < 0 backwards); the input value at a position sits d elements after the output's.
+// Each step stores o[p] and carries the updated o[p + s].  MODE 0 propagates with the
+// sign of o[p + s] itself, MODE 1 with the sign of in[p + s], MODE 2 is step_in between
+// in[p] and in[p + s].  Steps run four at a time with their loads issued first; in
+// MODE 2 a group without a sign change in the input (nearly all of them) takes the
+// propagation alone, which is what step_in does there, with one sign for the group.
+// s and d are compile-time constants for the fixed-pitch classes, so every address is a
+// register plus an offset.
+template <typename T, int MODE>
+__device__ __forceinline__ T* line_steps(T* op, T& cur, int count, int s, int d, T h) {
+    int k = 0;
+    if (MODE == 2) {
+        if (count <= 0) return op;
+        T a = op[d];
+        for (; k + 4 <= count; k += 4, op += 4 * s) {
+            T nx[4], b[4];
+#pragma unroll
+            for (int j = 0; j < 4; j++) {
+                nx[j] = op[(j + 1) * s];
+                b[j] = op[d + (j + 1) * s];
+            }
+            const bool change = (a * b[0] <= T(0)) | (b[0] * b[1] <= T(0)) | (b[1] * b[2] <= T(0)) |
+                                (b[2] * b[3] <= T(0));
+            if (change) {
+#pragma unroll
+                for (int j = 0; j < 4; j++) {
+                    step_in(j ? b[j - 1] : a, b[j], cur, nx[j], h);
+                    op[j * s] = cur;
+                    cur = nx[j];
+                }
+            } else {
+                // a * b > 0 at every step: a and the four b share one sign and none is
+                // 0, so isgn(b) * h is the same for the four steps
+                const T inc = copysign_t(h, a);
+#pragma unroll
+                for (int j = 0; j < 4; j++) {
+                    const T candidate = cur + inc;
+                    if (fabs(candidate) < fabs(nx[j])) nx[j] = candidate;
+                    op[j * s] = cur;
+                    cur = nx[j];
+                }
+            }
+            a = b[3];
+        }
+        for (; k < count; k++, op += s) {
+            T nx = op[s];
+            const T b = op[d + s];
+            step_in(a, b, cur, nx, h);
+            *op = cur;
+            cur = nx;
+            a = b;
+        }
+        return op;
+    }
+    for (; k + 4 <= count; k += 4, op += 4 * s) {
+        T nx[4], src[4];
+#pragma unroll
+        for (int j = 0; j < 4; j++) {
+            nx[j] = op[(j + 1) * s];
+            src[j] = MODE == 1 ? op[d + (j + 1) * s] : nx[j];
+        }
+#pragma unroll
+        for (int j = 0; j < 4; j++) {
+            step_prop(src[j], cur, nx[j], h);
+            op[j * s] = cur;
+            cur = nx[j];
+        }
+    }
+    for (; k < count; k++, op += s) {
+        T nx = op[s];
+        step_prop(MODE == 1 ? op[d + s] : nx, cur, nx, h);
+        *op = cur;
+        cur = nx;
+    }
+    return op;
+}
+
+// Forward sweep over positions p0 .. p_end - 1 of a line with stride so, the input d
+// elements after the output.  The reference's x/y/z forward loops (box.cpp:2367-2401,
+// 2437-2472, 2501-2538) take step_in while p < p_in_end - 1 (and inside), else the
+// propagation with the output's own sign: a prefix, so the loop is split in two.
 template <typename T>
-__device__ __forceinline__ void sweep_forward(T* o, int so, const T* in, int si, int p0, int p_end, int p_in_end,
-                                              bool inside, T h) {
+__device__ __forceinline__ void sweep_forward(T* o, int so, int d, int p0, int p_end, int p_in_end, bool inside,
+                                              T h) {
     if (p0 >= p_end - 1) return;
     T* op = o + p0 * so;
     T cur = *op;
-    int p = p0;
     const int pin = inside ? min(p_in_end - 1, p_end - 1) : p0;
-    if (p < pin) {
-        const T* ip = in + p0 * si;
-        T icur = *ip;
-#pragma unroll 4
-        for (; p < pin; p++, op += so, ip += si) {
-            T nxt = op[so];
-            const T inx = ip[si];
-            step_in(icur, inx, cur, nxt, h);
-            *op = cur;
-            cur = nxt;
-            icur = inx;
-        }
-    }
-#pragma unroll 4
-    for (; p < p_end - 1; p++, op += so) {
-        T nxt = op[so];
-        step_prop(nxt, cur, nxt, h);
-        *op = cur;
-        cur = nxt;
-    }
+    const int nin = pin > p0 ? pin - p0 : 0;
+    op = line_steps<T, 2>(op, cur, nin, so, d, h);
+    op = line_steps<T, 0>(op, cur, p_end - 1 - p0 - nin, so, d, h);
     *op = cur;
 }
 
 // Backward propagation from p_start down to p_lo + 1 (box.cpp:2403-2435, 2474-2496):
-// step_prop with the sign of in(p - 1) while p > p_in_lo (and inside), else of the
-// output itself.  out_here is never modified.
+// the sign of in(p - 1) while p > p_in_lo (and inside), else of the output itself.
+// out(p_start) is never modified (storing it back leaves it as it was).
 template <typename T>
-__device__ __forceinline__ void sweep_backward_prop(T* o, int so, const T* in, int si, int p_start, int p_lo,
-                                                    int p_in_lo, bool inside, T h) {
+__device__ __forceinline__ void sweep_backward_prop(T* o, int so, int d, int p_start, int p_lo, int p_in_lo,
+                                                    bool inside, T h) {
     if (p_start <= p_lo) return;
     T* op = o + p_start * so;
     T cur = *op;
-    int p = p_start;
-    if (inside) {
-        const int plim = max(p_in_lo, p_lo);
-        const T* ip = in + (p_start - 1) * si;
-#pragma unroll 4
-        for (; p > plim; p--, op -= so, ip -= si) {
-            T nxt = op[-so];
-            step_prop(*ip, cur, nxt, h);
-            op[-so] = nxt;
-            cur = nxt;
-        }
-    }
-#pragma unroll 4
-    for (; p > p_lo; p--, op -= so) {
-        T nxt = op[-so];
-        step_prop(nxt, cur, nxt, h);
-        op[-so] = nxt;
-        cur = nxt;
-    }
-}
-
-// Backward sweep with interpolation (the z backward loop, box.cpp:2539-2576): step_in
-// while p > p_in_lo (and inside), else step_prop; step_in may change o(p) as well.
-template <typename T>
-__device__ __forceinline__ void sweep_backward_in(T* o, int so, const T* in, int si, int p_start, int p_lo,
-                                                  int p_in_lo, bool inside, T h) {
-    if (p_start <= p_lo) return;
-    T* op = o + p_start * so;
-    T cur = *op;
-    int p = p_start;
     const int plim = max(p_in_lo, p_lo);
-    if (inside && p > plim) {
-        const T* ip = in + p_start * si;
-        T icur = *ip;
-#pragma unroll 4
-        for (; p > plim; p--, op -= so, ip -= si) {
-            T nxt = op[-so];
-            const T inx = ip[-si];
-            step_in(icur, inx, cur, nxt, h);
-            *op = cur;
-            cur = nxt;
-            icur = inx;
-        }
-    }
-#pragma unroll 4
-    for (; p > p_lo; p--, op -= so) {
-        T nxt = op[-so];
-        step_prop(nxt, cur, nxt, h);
-        *op = cur;
-        cur = nxt;
-    }
+    const int nin = inside && p_start > plim ? p_start - plim : 0;
+    op = line_steps<T, 1>(op, cur, nin, -so, d, h);
+    op = line_steps<T, 0>(op, cur, p_start - nin - p_lo, -so, d, h);
     *op = cur;
 }
 
+// Backward sweep with interpolation (the z backward loop, box.cpp:2539-2576): step_in
+// while p > p_in_lo (and inside), else the propagation with the output's own sign.
 template <typename T>
+__device__ __forceinline__ void sweep_backward_in(T* o, int so, int d, int p_start, int p_lo, int p_in_lo,
+                                                  bool inside, T h) {
+    if (p_start <= p_lo) return;
+    T* op = o + p_start * so;
+    T cur = *op;
+    const int plim = max(p_in_lo, p_lo);
+    const int nin = inside && p_start > plim ? p_start - plim : 0;
+    op = line_steps<T, 2>(op, cur, nin, -so, d, h);
+    op = line_steps<T, 0>(op, cur, p_start - nin - p_lo, -so, d, h);
+    *op = cur;
+}
+
+// Shared-memory layout of a fixed-pitch class of largest side S (even, a multiple of 8):
+// one unit's output plane and input plane of S rows of pitch S + 1 (xy) or S x S (z),
+// units spaced so that lane t of the CTA, unit t / S, line t % S, reads bank t mod 32 in
+// every sweep (the unit stride is congruent to S modulo 32, as S (S + 1) is).
+__host__ __device__ constexpr int xy_unit_stride(int S) { return 2 * S * (S + 1) + (32 - S % 32) % 32; }
+__host__ __device__ constexpr int z_unit_stride(int S) { return 2 * S * S + S % 32; }
+__host__ __device__ constexpr int class_threads(int S, int U) { return S ? (U * S + 31) / 32 * 32 : kMaxThreads; }
+
+// Kernel xy: a CTA per (grain, U consecutive output z-slices); unit u of the CTA owns
+// slice ob.z0 + U * tile + u, its threads run its rows for the x sweeps and its columns
+// for the y sweeps.  S = 0: one unit of runtime pitch (sides above the fixed classes).
+template <typename T, int S, int U>
 __global__ void __launch_bounds__(kMaxThreads) redist_xy_kernel(RedistArgs<T> a) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
-    const int tid = threadIdx.x, nt = blockDim.x;
-    T* O = reinterpret_cast<T*>(smem_raw);  // out slice, [y][x] with pitch P, then in values
+    const int tid = threadIdx.x;
+    const int u = S ? tid / S : 0;
+    const int line = S ? tid - u * S : tid;
+    const int lstride = S ? S : blockDim.x;
     const T h = (T)a.geo.h;
     for (TileWalk w(a.toff, a.G, blockIdx.x, gridDim.x); w.valid(); w.next()) {
         const int g = w.g;
         const Box ob = a.out.grain_box(g);
         const Box ib = a.in.grain_box(g);
-        const int k = ob.z0 + w.local;
+        const int k = ob.z0 + w.local * U + u;
+        const bool unit = u < U && k < ob.z1;
         const Intersect I(ib, ob);
         const int nx = ob.nx(), ny = ob.ny();
+        const int P = S ? S + 1 : (nx | 1);
+        const int PL = S ? S * (S + 1) : ny * P;  // the input plane follows the output plane
+        T* O = reinterpret_cast<T*>(smem_raw) + (S ? u * xy_unit_stride(S) : 0);
+        T* In = O + PL;
         T* outg = a.out.grain_ptr(g) + (long long)(k - ob.z0) * nx * ny;
-        if (!(k >= I.zmin && k < I.zmax - 1)) {  // no xy sweep reaches this slice
-            for (int q = tid; q < nx * ny; q += nt) outg[q] = T(-1);
-            continue;  // uniform across the CTA
-        }
-        const int P = nx | 1;
-        T* In = O + ny * P;  // IN(i, j) at the same position as OUT(i, j), on the intersection
-        for (int q = tid; q < ny * P; q += nt) O[q] = T(-1);
-        {
+        const bool sweeps = unit && k >= I.zmin && k < I.zmax - 1;
+        if (unit && !sweeps)  // no xy sweep reaches this slice
+            for (int q = line; q < nx * ny; q += lstride) outg[q] = T(-1);
+        if (sweeps) {
+            for (int q = line; q < ny * P; q += lstride) O[q] = T(-1);
             // rows of the intersection, x-adjacent threads on x-adjacent words
-            const int w = I.xmax - I.xmin;
+            const int wd = I.xmax - I.xmin;
             const T* src = a.in.grain_ptr(g) + ib.at(I.ymin, I.xmin, k);
             T* dst = In + (I.ymin - ob.y0) * P + (I.xmin - ob.x0);
             for (int yy = 0; yy < I.ymax - I.ymin; yy++, src += ib.nx(), dst += P)
-                for (int xx = tid; xx < w; xx += nt) cp_async_elem(dst + xx, src + xx);
+                for (int xx = line; xx < wd; xx += lstride) cp_async_elem(dst + xx, src + xx);
         }
         cp_async_wait_all();
         __syncthreads();
-        T* O0 = O - (long long)ob.y0 * P - ob.x0;  // O0[i * P + j] = OUT(i, j)
-        const T* in_k = In - (long long)ob.y0 * P - ob.x0;  // in_k[i * P + j] = IN(i, j)
-        const int inx = P;
-        for (int i = I.ymin + tid; i < ob.y1; i += nt)  // x forward, box.cpp:2367-2401
-            sweep_forward(O0 + (long long)i * P, 1, in_k + (long long)i * inx, 1, I.xmin, ob.x1, I.xmax, i < I.ymax, h);
+        T* O0 = O - (long long)ob.y0 * P - ob.x0;  // O0[i * P + j] = OUT(i, j), IN(i, j) PL further
+        if (sweeps)
+            for (int i = I.ymin + line; i < ob.y1; i += lstride)  // x forward, box.cpp:2367-2401
+                sweep_forward(O0 + (long long)i * P, 1, PL, I.xmin, ob.x1, I.xmax, i < I.ymax, h);
         __syncthreads();
-        for (int i = I.ymin + tid; i < ob.y1; i += nt)  // x backward, box.cpp:2403-2435
-            sweep_backward_prop(O0 + (long long)i * P, 1, in_k + (long long)i * inx, 1, I.xmax - 1, ob.x0, I.xmin,
-                                i < I.ymax, h);
+        if (sweeps)
+            for (int i = I.ymin + line; i < ob.y1; i += lstride)  // x backward, box.cpp:2403-2435
+                sweep_backward_prop(O0 + (long long)i * P, 1, PL, I.xmax - 1, ob.x0, I.xmin, i < I.ymax, h);
         __syncthreads();
-        for (int j = I.xmin + tid; j < ob.x1; j += nt)  // y forward, box.cpp:2437-2472
-            sweep_forward(O0 + j, P, in_k + j, inx, I.ymin, ob.y1, I.ymax, j < I.xmax, h);
+        if (sweeps)
+            for (int j = I.xmin + line; j < ob.x1; j += lstride)  // y forward, box.cpp:2437-2472
+                sweep_forward(O0 + j, P, PL, I.ymin, ob.y1, I.ymax, j < I.xmax, h);
         __syncthreads();
-        for (int j = I.xmin + tid; j < ob.x1; j += nt)  // y backward, box.cpp:2474-2496
-            sweep_backward_prop(O0 + j, P, in_k + j, inx, I.ymax - 1, ob.y0, I.ymin, j < I.xmax, h);
+        if (sweeps) {
+            for (int j = I.xmin + line; j < ob.x1; j += lstride)  // y backward, box.cpp:2474-2496
+                sweep_backward_prop(O0 + j, P, PL, I.ymax - 1, ob.y0, I.ymin, j < I.xmax, h);
+        }
         __syncthreads();
-        for (int yy = 0; yy < ny; yy++)
-            for (int xx = tid; xx < nx; xx += nt) outg[yy * nx + xx] = O[yy * P + xx];
+        if (sweeps)
+            for (int yy = 0; yy < ny; yy++)
+                for (int xx = line; xx < nx; xx += lstride) outg[yy * nx + xx] = O[yy * P + xx];
         __syncthreads();
     }
 }
 
-template <typename T>
+// Kernel z: a CTA per (grain, U consecutive output y-rows); unit u owns row
+// ob.y0 + U * tile + u, whose [z][x] plane sits in shared memory, and its threads run
+// the z recurrences of one column each (x-adjacent threads touch adjacent words).
+template <typename T, int S, int U>
 __global__ void __launch_bounds__(kMaxThreads) redist_z_kernel(RedistArgs<T> a) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
-    const int tid = threadIdx.x, nt = blockDim.x;
-    T* Z = reinterpret_cast<T*>(smem_raw);  // [k][x] of this row, then the in values
+    const int tid = threadIdx.x;
+    const int u = S ? tid / S : 0;
+    const int line = S ? tid - u * S : tid;
+    const int lstride = S ? S : blockDim.x;
     const T h = (T)a.geo.h;
     const T delta = (T)a.geo.delta;
     for (TileWalk w(a.toff, a.G, blockIdx.x, gridDim.x); w.valid(); w.next()) {
         const int g = w.g;
         const Box ob = a.out.grain_box(g);
         const Box ib = a.in.grain_box(g);
-        const int i = ob.y0 + w.local;
+        const int i = ob.y0 + w.local * U + u;
+        const bool unit = u < U && i < ob.y1;
         const Intersect I(ib, ob);
         const int nx = ob.nx(), nz = ob.nz();
+        const int PZ = S ? S : nx;                // z stride in shared memory
+        const int PLZ = S ? S * S : nx * nz;      // the input plane follows the output plane
         const long long zs = (long long)nx * ob.ny();  // z stride of the output box
+        T* Z = reinterpret_cast<T*>(smem_raw) + (S ? u * z_unit_stride(S) : 0);
+        T* Zin = Z + PLZ;
         T* outr = a.out.grain_ptr(g) + (long long)(i - ob.y0) * nx;  // OUT(i, x0, z0)
-        T* Zin = Z + nx * nz;  // IN(i, j, k) at the position of OUT(i, j, k), on the intersection
-        for (int kk = 0; kk < nz; kk++)
-            for (int xx = tid; xx < nx; xx += nt) cp_async_elem(Z + kk * nx + xx, outr + kk * zs + xx);
-        if (i >= I.ymin && i < I.ymax) {
-            const int w = I.xmax - I.xmin;
-            const long long izs = (long long)ib.nx() * ib.ny();
-            const T* src = a.in.grain_ptr(g) + ib.at(i, I.xmin, I.zmin);
-            T* dst = Zin + (I.zmin - ob.z0) * nx + (I.xmin - ob.x0);
-            for (int k = I.zmin; k < I.zmax; k++, src += izs, dst += nx)
-                for (int xx = tid; xx < w; xx += nt) cp_async_elem(dst + xx, src + xx);
+        if (unit) {
+            for (int kk = 0; kk < nz; kk++)
+                for (int xx = line; xx < nx; xx += lstride) cp_async_elem(Z + kk * PZ + xx, outr + kk * zs + xx);
+            if (i >= I.ymin && i < I.ymax) {
+                const int wd = I.xmax - I.xmin;
+                const long long izs = (long long)ib.nx() * ib.ny();
+                const T* src = a.in.grain_ptr(g) + ib.at(i, I.xmin, I.zmin);
+                T* dst = Zin + (I.zmin - ob.z0) * PZ + (I.xmin - ob.x0);
+                for (int k = I.zmin; k < I.zmax; k++, src += izs, dst += PZ)
+                    for (int xx = line; xx < wd; xx += lstride) cp_async_elem(dst + xx, src + xx);
+            }
         }
         cp_async_wait_all();
         __syncthreads();
-        if (i >= I.ymin) {
-            const int izs = nx;
-            T* Z0 = Z - (long long)ob.z0 * nx - ob.x0;  // Z0[k * nx + j] = OUT(i, j, k)
-            const T* in_i = Zin - (long long)ob.z0 * nx - ob.x0;  // in_i[k * nx + j] = IN(i, j, k)
-            for (int j = I.xmin + tid; j < ob.x1; j += nt) {
+        if (unit && i >= I.ymin) {
+            T* Z0 = Z - (long long)ob.z0 * PZ - ob.x0;  // Z0[k * PZ + j] = OUT(i, j, k), IN PLZ further
+            for (int j = I.xmin + line; j < ob.x1; j += lstride) {
                 const bool inside = i < I.ymax && j < I.xmax;
                 // z forward, box.cpp:2501-2538
-                sweep_forward(Z0 + j, nx, in_i + j, izs, I.zmin, ob.z1, I.zmax, inside, h);
+                sweep_forward(Z0 + j, PZ, PLZ, I.zmin, ob.z1, I.zmax, inside, h);
                 // z backward, box.cpp:2539-2576
-                sweep_backward_in(Z0 + j, nx, in_i + j, izs, I.zmax - 1, ob.z0, I.zmin, inside, h);
+                sweep_backward_in(Z0 + j, PZ, PLZ, I.zmax - 1, ob.z0, I.zmin, inside, h);
             }
         }
         __syncthreads();
         // clampValues(-delta, delta), dimensionalBufferReal.h:44-57
-        for (int kk = 0; kk < nz; kk++)
-            for (int xx = tid; xx < nx; xx += nt) {
-                T v = Z[kk * nx + xx];
-                if (v < -delta) v = -delta;
-                else if (v > delta) v = delta;
-                outr[kk * zs + xx] = v;
-            }
+        if (unit)
+            for (int kk = 0; kk < nz; kk++)
+                for (int xx = line; xx < nx; xx += lstride) {
+                    T v = Z[kk * PZ + xx];
+                    if (v < -delta) v = -delta;
+                    else if (v > delta) v = delta;
+                    outr[kk * zs + xx] = v;
+                }
         __syncthreads();
     }
 }
@@ -282,8 +339,9 @@ size_t redist_smem_bytes(int nmax, bool fp64) {
 }
 
 namespace {
-// Per class c, the exclusive scan over grains of n (the output box side) for the grains
-// of toff_all (n tiles each) whose n is in class c; one CTA, as plan_kernel.
+// Per class c, the exclusive scan over grains of ceil(n / redist_units(c)) (n the output
+// box side) for the grains of toff_all (n tiles each) whose n is in class c; one CTA, as
+// plan_kernel.
 __global__ void __launch_bounds__(1024) redist_class_kernel(int G, const int* toff_all, const int* box,
                                                             int* class_toff) {
     __shared__ int warp_tot[32][kRedistClasses];
@@ -294,9 +352,10 @@ __global__ void __launch_bounds__(1024) redist_class_kernel(int G, const int* to
     const int g0 = threadIdx.x * per, g1 = min(G + 1, g0 + per);
     auto count = [&](int g, int c) {
         if (none || g < 1 || g > G || toff_all[g + 1] - toff_all[g] <= 0) return 0;
-        const int n = load_box(box + 6 * g).nx();
+        const Box b = load_box(box + 6 * g);  // cubes; the largest side bounds every stride
+        const int n = max(b.nx(), max(b.ny(), b.nz()));
         const int lo = c == 0 ? 0 : redist_side(c - 1);
-        return (n > lo && n <= redist_side(c)) ? n : 0;
+        return (n > lo && n <= redist_side(c)) ? (n + redist_units(c) - 1) / redist_units(c) : 0;
     };
     int mine[kRedistClasses], incl[kRedistClasses];
 #pragma unroll
@@ -353,33 +412,55 @@ void launch_redist_classes(int G, const int* toff_all, const int* box, int* clas
     redist_class_kernel<<<1, 1024, 0, s>>>(G, toff_all, box, class_toff);
 }
 
-template <typename T>
-void launch_redistance(const RedistArgs<T>& a, int grid, int side, const int* class_toff, cudaStream_t s) {
+namespace {
+template <typename T, int S, int U>
+void launch_class(const RedistArgs<T>& a, int n, cudaStream_t s) {
+    static_assert(S % 8 == 0 && U * S <= kMaxThreads, "fixed-pitch classes: sides a multiple of 8");
     static PerDevice configured;
     configured.once([] {
-        allow_max_dynamic_smem(redist_xy_kernel<T>);
-        allow_max_dynamic_smem(redist_z_kernel<T>);
+        allow_max_dynamic_smem(redist_xy_kernel<T, S, U>);
+        allow_max_dynamic_smem(redist_z_kernel<T, S, U>);
     });
-    if (!class_toff) {
+    const int threads = S ? class_threads(S, U) : std::min((n + 31) / 32 * 32, kMaxThreads);
+    const size_t e = sizeof(T);
+    const size_t sxy = S ? (size_t)U * xy_unit_stride(S) * e : redist_smem_bytes(n, e == 8);
+    const size_t sz = S ? (size_t)U * z_unit_stride(S) * e : redist_smem_bytes(n, e == 8);
+    redist_xy_kernel<T, S, U><<<resident_ctas(redist_xy_kernel<T, S, U>, threads, sxy), threads, sxy, s>>>(a);
+    redist_z_kernel<T, S, U><<<resident_ctas(redist_z_kernel<T, S, U>, threads, sz), threads, sz, s>>>(a);
+}
+}  // namespace
+
+template <typename T>
+void launch_redistance(const RedistArgs<T>& a, int grid, int side, const int* class_toff, cudaStream_t s) {
+    if (!class_toff) {  // one unit per CTA of runtime pitch, over a.toff (n tiles a grain)
+        static PerDevice configured;
+        configured.once([] {
+            allow_max_dynamic_smem(redist_xy_kernel<T, 0, 1>);
+            allow_max_dynamic_smem(redist_z_kernel<T, 0, 1>);
+        });
         const size_t smem = redist_smem_bytes(side, sizeof(T) == 8);
         int threads = (side + 31) / 32 * 32;
         threads = threads > kMaxThreads ? kMaxThreads : threads;
-        redist_xy_kernel<T><<<grid * 2, threads, smem, s>>>(a);
-        redist_z_kernel<T><<<grid * 2, threads, smem, s>>>(a);
+        redist_xy_kernel<T, 0, 1><<<grid * 2, threads, smem, s>>>(a);
+        redist_z_kernel<T, 0, 1><<<grid * 2, threads, smem, s>>>(a);
         return;
     }
-    // one pair of launches per size class up to the largest side, each sized for its
-    // class's largest side and filling the device with its own CTAs
+    // one pair of launches per size class up to the largest side, each filling the
+    // device with its own CTAs
     for (int c = 0; c < kRedistClasses; c++) {
         const int lo = c == 0 ? 0 : redist_side(c - 1);
         if (lo >= side) break;
-        const int n = std::min(redist_side(c), side);
-        const size_t smem = redist_smem_bytes(n, sizeof(T) == 8);
-        const int threads = std::min((n + 31) / 32 * 32, kMaxThreads);
         RedistArgs<T> ac = a;
         ac.toff = class_toff + (long long)c * (a.G + 2);
-        redist_xy_kernel<T><<<resident_ctas(redist_xy_kernel<T>, threads, smem), threads, smem, s>>>(ac);
-        redist_z_kernel<T><<<resident_ctas(redist_z_kernel<T>, threads, smem), threads, smem, s>>>(ac);
+        switch (c) {
+            case 0: launch_class<T, redist_side(0), redist_units(0)>(ac, 0, s); break;
+            case 1: launch_class<T, redist_side(1), redist_units(1)>(ac, 0, s); break;
+            case 2: launch_class<T, redist_side(2), redist_units(2)>(ac, 0, s); break;
+            case 3: launch_class<T, redist_side(3), redist_units(3)>(ac, 0, s); break;
+            case 4: launch_class<T, redist_side(4), redist_units(4)>(ac, 0, s); break;
+            case 5: launch_class<T, redist_side(5), redist_units(5)>(ac, 0, s); break;
+            default: launch_class<T, 0, 1>(ac, side, s); break;
+        }
     }
 }
 
