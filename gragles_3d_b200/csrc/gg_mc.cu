@@ -138,39 +138,27 @@ __global__ void __launch_bounds__(kThreads, 3) mc_kernel(MCArgs<T> a, int slab_b
         const bool capture = a.hull.cap > 0;
         const long long hbase = (long long)g * a.hull.cap;
         const int nxb = b.nx(), plane = b.nx() * b.ny();
-        // Slabs of LZ cube layers: the sign bytes of their LZ + 1 voxel layers are staged
-        // with one coalesced load per voxel, then every cube is classified from shared
-        // memory; a cube-index byte and an active-list entry per cube.
-        // per cube layer: a sign byte per voxel, a cube-index byte and a 2-byte list entry
-        // per cube, an active-cube bit per cube (in 32-bit words)
-        int LZ = ncplane > 0 ? (slab_bytes - plane - 16) / (plane + 3 * ncplane + ncplane / 8 + 1) : 0;
+        // Slabs of LZ cube layers.  The signs of their LZ + 1 voxel layers are staged as
+        // bits (one coalesced load per voxel, a warp ballot per 32 voxels in x, y, z
+        // order); a row of 32 cubes is active where its 8 corner bit vectors disagree,
+        // found with a few word operations; the active cubes are listed in cube order.
+        const int wr = (ncx + 31) >> 5;          // active-mask words per cube row
+        const int pw = (plane + 31) >> 5;        // sign words per voxel layer (bound)
+        int LZ = ncplane > 0 ? (slab_bytes - 4 * pw - 16) / (4 * pw + 4 * ncy * wr + 2 * ncplane + 4) : 0;
         if (ncplane > 0 && LZ > 65535 / ncplane) LZ = 65535 / ncplane;
         if (LZ > ncz) LZ = ncz;
         if (ncplane > 0 && LZ < 1) {  // a single layer does not fit the shared memory
             if (threadIdx.x == 0) atomicOr(a.err, ERR_BOX);
             LZ = 0;
         }
-        unsigned char* sgn = slab_raw;
-        unsigned char* cidx = sgn + (LZ + 1) * plane;
-        // 2-byte entries at an even offset from the (16-byte aligned) buffer start
-        const int act_off = ((LZ + 1) * plane + LZ * ncplane + 1) & ~1;
-        unsigned short* act = reinterpret_cast<unsigned short*>(slab_raw + act_off);
-        // one word per 32 consecutive cubes of the slab, bit = the cube is active
-        unsigned* amask = reinterpret_cast<unsigned*>(slab_raw + ((act_off + 2 * LZ * ncplane + 3) & ~3));
-        // cube (lx, ly, lz) of a slab is lz * ncplane + ly * ncx + lx; a step of kThreads
-        // cubes is (sz, sy, sx) in that mixed radix, so coordinates advance without divisions
-        int sx = 0, sy = 0, sz = 0;
-        if (ncplane > 0) {
-            const int st = kThreads / ncx;
-            sx = kThreads - st * ncx;
-            sz = st / ncy;
-            sy = st - sz * ncy;
-        }
+        unsigned* sb = reinterpret_cast<unsigned*>(slab_raw);  // sign bits of the slab's voxels
+        const int sbw = ((LZ + 1) * plane + 31) / 32 + 1;      // + 1: 32-bit reads at any bit
+        unsigned* am = sb + sbw;                                // active bits, wr words per cube row
+        unsigned short* act = reinterpret_cast<unsigned short*>(am + LZ * ncy * wr);
         __syncthreads();
         for (int zc0 = 0; LZ > 0 && zc0 < ncz; zc0 += LZ) {
           const int lz = min(LZ, ncz - zc0);
-          const int ncs = lz * ncplane;
-          // sign bytes of voxel layers zc0 .. zc0 + lz (inside = value >= 0, marchingCubes.cpp:12-15)
+          // sign bits of voxel layers zc0 .. zc0 + lz (inside = value >= 0, marchingCubes.cpp:12-15)
           {
               const T* src = sdf + (long long)zc0 * plane;
               const int nv = (lz + 1) * plane;
@@ -184,49 +172,44 @@ __global__ void __launch_bounds__(kThreads, 3) mc_kernel(MCArgs<T> a, int slab_b
                   }
 #pragma unroll
                   for (int u = 0; u < kMB; u++) {
-                      const int v = v0 + u * kThreads + threadIdx.x;
-                      if (v < nv) sgn[v] = r[u] >= T(0);
+                      const unsigned m = __ballot_sync(0xffffffffu, r[u] >= T(0));
+                      const int w0 = v0 + u * kThreads + (threadIdx.x & ~31);  // a multiple of 32
+                      if ((threadIdx.x & 31) == 0 && w0 < nv) sb[w0 >> 5] = m;
                   }
               }
           }
           __syncthreads();
-          {
-              // cubes base + threadIdx.x, a whole warp on 32 consecutive cubes (a multiple
-              // of 32 from the slab start): the warp's ballot is that word of amask
-              const int q0 = threadIdx.x / ncx;
-              int cx = threadIdx.x - q0 * ncx, cz = q0 / ncy;
-              int cy = q0 - cz * ncy;
-              for (int cl0 = 0; cl0 < ncs; cl0 += kThreads) {
-                  const int cl = cl0 + threadIdx.x;
-                  int ci = 0;
-                  if (cl < ncs) {
-                      const unsigned char* p = sgn + cz * plane + cy * nxb + cx;
+          // active bits: word j of cube row (cz, cy) covers cubes x = 32 j .. 32 j + 31
+          const int nrow = lz * ncy, nw = nrow * wr;
+          for (int q = threadIdx.x; q < nw; q += kThreads) {
+              const int row = q / wr, j = q - row * wr;
+              const int cz = row / ncy, cy = row - cz * ncy;
+              const int v0 = (cz * ncy + cy + cz) * nxb + 32 * j;  // voxel (32 j, cy, cz): (cz ny + cy) nx
+              unsigned all = 0xffffffffu, any = 0u;
 #pragma unroll
-                      for (int q = 0; q < 8; q++)
-                          ci |= (int)p[corner_dz(q) * plane + corner_dy(q) * nxb + corner_dx(q)] << q;
-                      cidx[cl] = (unsigned char)ci;
-                  }
-                  const unsigned m = __ballot_sync(0xffffffffu, cube_active(ci));
-                  if ((threadIdx.x & 31) == 0 && cl < ncs) amask[cl >> 5] = m;
-                  cx += sx;
-                  cy += sy;
-                  cz += sz;
-                  if (cx >= ncx) { cx -= ncx; cy++; }
-                  if (cy >= ncy) { cy -= ncy; cz++; }
+              for (int c = 0; c < 8; c++) {
+                  const int v = v0 + corner_dz(c) * plane + corner_dy(c) * nxb + corner_dx(c);
+                  const unsigned bits = __funnelshift_r(sb[v >> 5], sb[(v >> 5) + 1], v & 31);
+                  all &= bits;
+                  any |= bits;
               }
+              const int left = ncx - 32 * j;
+              const unsigned valid = left >= 32 ? 0xffffffffu : (1u << left) - 1u;
+              am[q] = any & ~all & valid;
           }
           __syncthreads();
-          // active cubes of the slab, in cube order: thread t takes words [t seg, (t + 1) seg)
-          const int nmask = (ncs + 31) >> 5;
-          const int seg = (nmask + kThreads - 1) / kThreads;
-          const int s0 = threadIdx.x * seg, s1 = min(s0 + seg, nmask);
+          // the active cubes in cube order: thread t takes words [t seg, (t + 1) seg)
+          const int seg = (nw + kThreads - 1) / kThreads;
+          const int s0 = threadIdx.x * seg, s1 = min(s0 + seg, nw);
           int nloc = 0;
-          for (int m = s0; m < s1; m++) nloc += __popc(amask[m]);
+          for (int m = s0; m < s1; m++) nloc += __popc(am[m]);
           int n_act;
           int w = block_exclusive_scan(nloc, warp_sums, n_act);
-          for (int m = s0; m < s1; m++)
-              for (unsigned bits = amask[m]; bits; bits &= bits - 1)
-                  act[w++] = (unsigned short)(m * 32 + __ffs(bits) - 1);
+          for (int m = s0; m < s1; m++) {
+              const int row = m / wr, x0 = 32 * (m - row * wr);
+              for (unsigned bits = am[m]; bits; bits &= bits - 1)
+                  act[w++] = (unsigned short)(row * ncx + x0 + __ffs(bits) - 1);
+          }
           __syncthreads();
           for (int ab = 0; ab < n_act; ab += kThreads) {
             const int ia = ab + threadIdx.x;
@@ -237,9 +220,14 @@ __global__ void __launch_bounds__(kThreads, 3) mc_kernel(MCArgs<T> a, int slab_b
             if (ia < n_act) {
                 const int cl = act[ia];
                 c = zc0 * ncplane + cl;  // cube index in the reference's z, y, x order
-                ci = cidx[cl];
                 const int lzl = cl / ncplane, rem = cl - lzl * ncplane;
                 const int ly = rem / ncx, lx = rem - ly * ncx, lzz = zc0 + lzl;
+                const int sv = (lzl * ncy + ly + lzl) * nxb + lx;  // slab-relative voxel of the cube
+#pragma unroll
+                for (int q = 0; q < 8; q++) {
+                    const int v = sv + corner_dz(q) * plane + corner_dy(q) * nxb + corner_dx(q);
+                    ci |= (int)((sb[v >> 5] >> (v & 31)) & 1u) << q;
+                }
                 x = b.x0 + lx;
                 y = b.y0 + ly;
                 z = b.z0 + lzz;
@@ -300,7 +288,7 @@ __global__ void __launch_bounds__(kThreads, 3) mc_kernel(MCArgs<T> a, int slab_b
                     const int at = base + nbc_dz(k) * plane + nbc_dy(k) * nxb + nbc_dx(k);
                     // inside = value >= 0: the staged sign byte of the corner (slab-relative)
                     const int sat = at - zc0 * plane;
-                    unsigned id = sgn[sat] ? (unsigned)g : idl[at];
+                    unsigned id = ((sb[sat >> 5] >> (sat & 31)) & 1u) ? (unsigned)g : idl[at];
                     bool found = false;
                     for (int q = 0; q < cnt; q++) found |= (lst[q] == id);
                     if (!found) {
@@ -427,9 +415,11 @@ __global__ void count_kernel(int G, const int* present, const int* exists, const
 }  // namespace
 
 size_t mc_slab_bytes(int side) {
-    // at least one cube layer: two voxel layers of sign bytes, a byte and a list entry per cube
+    // at least one cube layer: two voxel layers of sign bits, the cube layer's active bits
+    // and a list entry per cube
     const size_t n = side > 1 ? side : 2;
-    const size_t one_layer = 2 * n * n + 3 * (n - 1) * (n - 1) + (n - 1) * (n - 1) / 8 + 1 + 16;
+    const size_t pw = (n * n + 31) / 32, wr = (n - 1 + 31) / 32;
+    const size_t one_layer = 8 * pw + 16 + 4 * (n - 1) * wr + 2 * (n - 1) * (n - 1) + 4;
     return one_layer > kSlabBytes ? one_layer : kSlabBytes;
 }
 
