@@ -24,6 +24,7 @@ namespace {
 
 constexpr int kThreads = 256;
 constexpr int kHash = 1024;  // distinct neighbour IDs per grain (power of two)
+static_assert(kThreads * 5 * sizeof(double) >= 2 * kHash * sizeof(unsigned), "ID collection aliases the volume buffer");
 constexpr int kSlabBytes = 36 * 1024;  // shared memory for a slab's sign bytes and cube lists
 
 // cubeindex bit q <-> corner offset (dx, dy, dz), marchingCubes.cpp:376-385:
@@ -107,12 +108,25 @@ __global__ void __launch_bounds__(kThreads, 3) mc_kernel(MCArgs<T> a, int slab_b
     __shared__ int warp_sums[33];
     __shared__ unsigned hkey[kHash];
     __shared__ unsigned hval[kHash];
-    __shared__ unsigned nb_id[kHash];
-    __shared__ unsigned nb_key[kHash];
+    // the cube tables, read per active cube with scattered indices: triangle edges as
+    // nibbles with the triangle count in bits 60-63, and the edge masks
+    __shared__ unsigned long long s_tri[256];
+    __shared__ unsigned short s_edge[256];
+    __shared__ unsigned g_key;  // the grain's own ID: its smallest key (first active cube)
     __shared__ int n_found;
     __shared__ int next_item;
     extern __shared__ __align__(16) unsigned char slab_raw[];
     const int n_items = a.item_off[a.G + 1];
+    for (int ci = threadIdx.x; ci < 256; ci += blockDim.x) {
+        unsigned long long t = 0;
+        int k = 0;
+        while (k < 15 && gg_mc_tri_table[ci][k] != -1) {
+            t |= (unsigned long long)gg_mc_tri_table[ci][k] << (4 * k);
+            k++;
+        }
+        s_tri[ci] = t | ((unsigned long long)(k / 3) << 60);
+        s_edge[ci] = (unsigned short)gg_mc_edge_table[ci];
+    }
     for (;;) {  // grains largest first, fetched on demand
         __syncthreads();
         if (threadIdx.x == 0) next_item = atomicAdd(a.queue, 1);
@@ -129,7 +143,10 @@ __global__ void __launch_bounds__(kThreads, 3) mc_kernel(MCArgs<T> a, int slab_b
         const T* sdf = a.in.grain_ptr(g);
         const uint32_t* idl = a.idl + a.idoff[g];
         for (int q = threadIdx.x; q < kHash; q += blockDim.x) { hkey[q] = 0xFFFFFFFFu; hval[q] = 0xFFFFFFFFu; }
-        if (threadIdx.x == 0) n_found = 0;
+        if (threadIdx.x == 0) {
+            n_found = 0;
+            g_key = 0xFFFFFFFFu;
+        }
         const int ncx = b.nx() - 1, ncy = b.ny() - 1, ncz = b.nz() - 1;
         const int ncplane = (ncx > 0 && ncy > 0 && ncz > 0) ? ncx * ncy : 0;
         double vol = 0.0, area = 0.0;
@@ -235,12 +252,15 @@ __global__ void __launch_bounds__(kThreads, 3) mc_kernel(MCArgs<T> a, int slab_b
 #pragma unroll
                 for (int k = 0; k < 8; k++)
                     val[k] = (double)sdf[base + corner_dz(k) * plane + corner_dy(k) * nxb + corner_dx(k)];
-                while (gg_mc_tri_table[ci][3 * nt] != -1) nt++;
+                nt = (int)(s_tri[ci] >> 60);
             }
             int chunk_total;
             const int off = block_exclusive_scan(nt, warp_sums, chunk_total);
+            unsigned lst[8];
+            int cnt = 0;
             if (nt > 0) {
-                const int et = gg_mc_edge_table[ci];
+                const int et = s_edge[ci];
+                const unsigned long long tri = s_tri[ci];
                 V3 vl[12];
 #pragma unroll
                 for (int e = 0; e < 12; e++) {
@@ -251,9 +271,9 @@ __global__ void __launch_bounds__(kThreads, 3) mc_kernel(MCArgs<T> a, int slab_b
                     vl[e] = vinterp(p1, p2, val[ka], val[kb]);
                 }
                 for (int q = 0; q < nt; q++) {
-                    const V3 p0 = vl[gg_mc_tri_table[ci][3 * q]];
-                    const V3 p1 = vl[gg_mc_tri_table[ci][3 * q + 1]];
-                    const V3 p2 = vl[gg_mc_tri_table[ci][3 * q + 2]];
+                    const V3 p0 = vl[(tri >> (12 * q)) & 15];
+                    const V3 p1 = vl[(tri >> (12 * q + 4)) & 15];
+                    const V3 p2 = vl[(tri >> (12 * q + 8)) & 15];
                     if (capture) {  // Triangle::computeBarycenter, triangle.h:12-18
                         const long long ti = ntri + off + q;
                         if (ti < a.hull.cap) {
@@ -281,24 +301,37 @@ __global__ void __launch_bounds__(kThreads, 3) mc_kernel(MCArgs<T> a, int slab_b
                     if (capture && ntri + off + q < a.hull.cap) a.hull.tarea[hbase + ntri + off + q] = abuf[off + q];
                 }
                 // generateAdditionalInformation: sorted distinct corner IDs, marchingCubes.cpp:501-583
-                unsigned lst[8];
-                int cnt = 0;
+                // (the eight IDs loaded first, then an insertion sort in registers)
+                unsigned ids[8];
 #pragma unroll
                 for (int k = 0; k < 8; k++) {
                     const int at = base + nbc_dz(k) * plane + nbc_dy(k) * nxb + nbc_dx(k);
-                    // inside = value >= 0: the staged sign byte of the corner (slab-relative)
+                    // inside = value >= 0: the staged sign bit of the corner (slab-relative)
                     const int sat = at - zc0 * plane;
-                    unsigned id = ((sb[sat >> 5] >> (sat & 31)) & 1u) ? (unsigned)g : idl[at];
+                    const unsigned outside_id = idl[at];
+                    ids[k] = ((sb[sat >> 5] >> (sat & 31)) & 1u) ? (unsigned)g : outside_id;
+                }
+#pragma unroll
+                for (int k = 0; k < 8; k++) {
+                    unsigned id = ids[k];
                     bool found = false;
-                    for (int q = 0; q < cnt; q++) found |= (lst[q] == id);
+#pragma unroll
+                    for (int q = 0; q < k; q++) found |= q < cnt && lst[q] == id;
                     if (!found) {
-                        for (int q = 0; q < cnt; q++)
-                            if (id < lst[q]) { const unsigned tmp = lst[q]; lst[q] = id; id = tmp; }
-                        lst[cnt++] = id;
+#pragma unroll
+                        for (int q = 0; q < k; q++)
+                            if (q < cnt && id < lst[q]) { const unsigned tmp = lst[q]; lst[q] = id; id = tmp; }
+#pragma unroll
+                        for (int q = 0; q <= k; q++)
+                            if (q == cnt) lst[q] = id;
+                        cnt++;
                     }
                 }
-                const unsigned ck = (unsigned)c << 3;
-                for (int q = 0; q < cnt; q++) hash_insert(hkey, hval, lst[q], ck | q, a.err);
+                if (threadIdx.x == 0) {  // the chunk's first cube; the first chunk's is the grain's first
+#pragma unroll
+                    for (int q = 0; q < 8; q++)
+                        if (q < cnt && lst[q] == (unsigned)g) g_key = min(g_key, ((unsigned)c << 3) | q);
+                }
                 if (capture) {  // the cube's list, in cube order, for the interfacial elements
                     const int ri = nrec + ia;
                     if (ri < a.hull.cap) {
@@ -309,6 +342,24 @@ __global__ void __launch_bounds__(kThreads, 3) mc_kernel(MCArgs<T> a, int slab_b
                     } else {
                         { atomicOr(a.err, ERR_HULL); atomicOr(a.hull.diag, HULL_RECORDS); }
                     }
+                }
+            }
+            {
+                // the IDs other than g into the hash, key (cube << 3 | rank): one insert per
+                // distinct ID per warp and round, with the warp's smallest key for it
+                const int lane = threadIdx.x & 31;
+                const unsigned ck = (unsigned)c << 3;
+                const int rounds = __reduce_max_sync(0xffffffffu, cnt);
+                for (int r = 0; r < rounds; r++) {
+                    unsigned id = 0xFFFFFFFFu;
+#pragma unroll
+                    for (int k = 0; k < 8; k++)
+                        if (k == r && k < cnt) id = lst[k];
+                    if (id == (unsigned)g) id = 0xFFFFFFFFu;
+                    const unsigned key = id != 0xFFFFFFFFu ? (ck | (unsigned)r) : 0xFFFFFFFFu;
+                    const unsigned grp = __match_any_sync(0xffffffffu, id);
+                    const unsigned kmin = __reduce_min_sync(grp, key);
+                    if (id != 0xFFFFFFFFu && lane == __ffs(grp) - 1) hash_insert(hkey, hval, id, kmin, a.err);
                 }
             }
             __syncthreads();
@@ -337,7 +388,11 @@ __global__ void __launch_bounds__(kThreads, 3) mc_kernel(MCArgs<T> a, int slab_b
           }
           nrec += n_act;
         }
-        // collect the distinct IDs and order them by first appearance
+        // collect the distinct IDs and order them by first appearance (g with its key first)
+        if (threadIdx.x == 0 && g_key != 0xFFFFFFFFu) hash_insert(hkey, hval, (unsigned)g, g_key, a.err);
+        __syncthreads();
+        unsigned* nb_id = reinterpret_cast<unsigned*>(vbuf);  // the chunk buffers are done with
+        unsigned* nb_key = nb_id + kHash;
         for (int q = threadIdx.x; q < kHash; q += blockDim.x) {
             if (hkey[q] != 0xFFFFFFFFu) {
                 const int slot = atomicAdd(&n_found, 1);
