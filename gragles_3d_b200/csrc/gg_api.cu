@@ -601,7 +601,7 @@ int compare_t(gg_ctx* ctx, int in_a, int out_a, int set_comparison) {
     ctx->launches += 1;
     launch_bin(ctx->bins, ctx->G, set_comparison ? ctx->d_exists : ctx->d_present, ctx->d_box[in_a], ctx->d_err,
                ctx->stream);
-    ctx->launches += 4;
+    ctx->launches += 5;
     CK(cudaMemcpyAsync(ctx->h_maxcount, ctx->bins.max_count, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
     CK(cudaStreamSynchronize(ctx->stream));
     rc = check_err(ctx, "comparison binning");  // nothing may read past the tile entries
@@ -933,7 +933,7 @@ void free_all(gg_ctx* c) {
                     c->el.elem, c->el.ids, c->el.segs, c->el.ebary, c->el.n_idx, c->el.idx_key, c->el.idx_rng,
                     c->el.idx_elem, c->d_err, c->d_total_vox, c->d_count3, c->bins.count, c->work.keys,
                     c->d_toff_rcls, c->work.keys_out, c->work.vals, c->work.order, c->work.item_off, c->work.temp, c->work.queue,
-                    c->bins.off, c->bins.cursor, c->bins.entries, c->bins.max_count, c->lbins.count,
+                    c->bins.off, c->bins.cursor, c->bins.entries, c->bins.max_count, c->bins.temp, c->lbins.count,
                     c->lbins.off, c->lbins.cursor, c->lbins.entries};
     for (void* p : ptrs)
         if (p) cudaFree(p);
@@ -1051,6 +1051,8 @@ int gg_create(const gg_params* params, gg_ctx** out) {
     CK(dalloc(&ctx->bins.off, n_tiles + 1));
     CK(dalloc(&ctx->bins.cursor, n_tiles + 1));
     CK(dalloc(&ctx->bins.max_count, 1));
+    ctx->bins.temp_bytes = exclusive_scan_temp_bytes((int)n_tiles + 1);
+    CK(cudaMalloc(&ctx->bins.temp, ctx->bins.temp_bytes ? ctx->bins.temp_bytes : 1));
     {
         const int n = ctx->M / kListCell + 1;
         ctx->lbins_cells = n * n * n;

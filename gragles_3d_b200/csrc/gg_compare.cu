@@ -143,12 +143,24 @@ __global__ void bin_kernel(TileBins tb, int G, const int* exists, const int* box
             if (!FILL) {
                 atomicAdd(tb.count + t, 1);
             } else {
-                const long long slot = tb.off[t] + atomicAdd(tb.cursor + t, 1);
-                if (slot < tb.capacity) tb.entries[slot] = (uint32_t)g;
+                const long long slot = (long long)tb.off[t] + atomicAdd(tb.cursor + t, 1);
+                if (slot >= 0 && slot < tb.capacity) tb.entries[slot] = (uint32_t)g;
                 else atomicOr(err, ERR_POOL);
             }
         }
     }
+}
+
+// After the device-wide exclusive scan of the tile counts: the largest count and the
+// capacity check (off[n_tiles] is the total, count[n_tiles] being 0).
+__global__ void bin_check_kernel(TileBins tb, int n_tiles, int* err) {
+    int m = 0;
+    for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < n_tiles; t += gridDim.x * blockDim.x) m = max(m, tb.count[t]);
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) m = max(m, __shfl_xor_sync(0xffffffffu, m, o));
+    if ((threadIdx.x & 31) == 0 && m > 0) atomicMax(tb.max_count, m);
+    if (blockIdx.x == 0 && threadIdx.x == 0 && ((long long)tb.off[n_tiles] > tb.capacity || tb.off[n_tiles] < 0))
+        atomicOr(err, ERR_POOL);
 }
 
 // Exclusive scan of the tile counts (one CTA), largest count, capacity check.
@@ -631,7 +643,13 @@ void launch_bin(const TileBins& tb, int G, const int* exists, const int* box, in
     cudaMemsetAsync(tb.cursor, 0, sizeof(int) * (n_tiles + 1), s);
     const int grid = (G + 4) / 4;  // one warp per grain, 4 warps per block
     bin_kernel<false><<<grid, 128, 0, s>>>(tb, G, exists, box, err);
-    bin_scan_kernel<<<1, 1024, 0, s>>>(tb, n_tiles, err);
+    if (tb.temp) {  // device-wide: the one-CTA scan below walks the tiles serially
+        launch_exclusive_scan(tb.temp, tb.temp_bytes, tb.count, tb.off, n_tiles + 1, s);
+        cudaMemsetAsync(tb.max_count, 0, sizeof(int), s);
+        bin_check_kernel<<<(n_tiles + 255) / 256 < 1184 ? (n_tiles + 255) / 256 : 1184, 256, 0, s>>>(tb, n_tiles, err);
+    } else {
+        bin_scan_kernel<<<1, 1024, 0, s>>>(tb, n_tiles, err);
+    }
     bin_kernel<true><<<grid, 128, 0, s>>>(tb, G, exists, box, err);
 }
 

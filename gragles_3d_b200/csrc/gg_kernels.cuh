@@ -83,7 +83,13 @@ struct TileBins {
     uint32_t* entries;        // grain IDs
     long long capacity;
     int* max_count;           // device scalar: most grains reaching one tile
+    void* temp;               // device-wide scan scratch (domain tiles), temp_bytes
+    size_t temp_bytes;
 };
+// Scratch bytes of launch_exclusive_scan over n ints; the scan writes out[i] = sum of
+// in[0 .. i - 1] for i < n.
+size_t exclusive_scan_temp_bytes(int n);
+void launch_exclusive_scan(void* temp, size_t temp_bytes, const int* in, int* out, int n, cudaStream_t s);
 void launch_bin(const TileBins& tb, int G, const int* exists, const int* box, int* err, cudaStream_t s);
 long long bin_capacity(int G, int side);
 

@@ -3,7 +3,8 @@
 // The reference allocates every box with std::vector and resizes it every step
 // (dimensionalBuffer.h:120-131, jemalloc underneath).  Here the boxes of all grains
 // are packed into one arena per buffer role; after every change of box sizes one
-// CTA re-plans the packing (exclusive scan of the aligned n^3 over grains), the
+// CTA re-plans the packing (exclusive scan of the aligned n^3 over grains, a chunk of
+// consecutive grains at a time), the
 // half-spectrum scratch, and the tile offsets that the batched stage kernels use
 // to map their CTAs to (grain, tile).  Nothing goes back to the host, so a whole
 // timestep can be launched without synchronisation.
@@ -61,54 +62,57 @@ __device__ __forceinline__ Counts grain_counts(const PlanArgs& a, int g) {
     return c;
 }
 
+// Grains 0..G in chunks of kPlanThreads consecutive IDs (coalesced loads and stores):
+// a block exclusive scan per chunk on top of the running total of the earlier chunks.
 __global__ void __launch_bounds__(kPlanThreads) plan_kernel(PlanArgs a) {
     __shared__ Counts warp_tot[32];
+    __shared__ Counts carry_s;
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    const int per = (a.G + kPlanThreads) / kPlanThreads;  // grains 0..G
-    const int g0 = threadIdx.x * per, g1 = min(a.G + 1, g0 + per);
-    Counts mine{0, 0, 0, 0, 0, 0, 0};
-    for (int g = g0; g < g1; g++) mine = add(mine, grain_counts(a, g));
-    // block exclusive scan of `mine`
-    Counts incl = mine;
-#pragma unroll
-    for (int o = 1; o < 32; o <<= 1) {
-        const Counts u = shfl_up(incl, o);
-        if (lane >= o) incl = add(incl, u);
-    }
-    if (lane == 31) warp_tot[warp] = incl;
-    __syncthreads();
-    if (warp == 0) {
-        Counts w = warp_tot[lane];
-        Counts wi = w;
+    Counts carry{0, 0, 0, 0, 0, 0, 0};
+    for (int g0 = 0; g0 <= a.G; g0 += kPlanThreads) {
+        const int g = g0 + threadIdx.x;
+        const Counts mine = g <= a.G ? grain_counts(a, g) : Counts{0, 0, 0, 0, 0, 0, 0};
+        Counts incl = mine;
 #pragma unroll
         for (int o = 1; o < 32; o <<= 1) {
-            const Counts u = shfl_up(wi, o);
-            if (lane >= o) wi = add(wi, u);
+            const Counts u = shfl_up(incl, o);
+            if (lane >= o) incl = add(incl, u);
         }
-        warp_tot[lane] = wi;  // inclusive over warps
-    }
-    __syncthreads();
-    Counts run = warp > 0 ? warp_tot[warp - 1] : Counts{0, 0, 0, 0, 0, 0, 0};
-    const Counts excl_in_warp = Counts{incl.vox - mine.vox, incl.spec - mine.spec, incl.tot - mine.tot,
-                                       incl.tn - mine.tn, incl.ts - mine.ts, incl.t1 - mine.t1, incl.tb - mine.tb};
-    run = add(run, excl_in_warp);
-    for (int g = g0; g < g1; g++) {
-        const Counts c = grain_counts(a, g);
-        if (a.off) a.off[g] = run.vox;
-        if (a.spec_off) a.spec_off[g] = run.spec;
-        if (a.toff_n) a.toff_n[g] = run.tn;
-        if (a.toff_slab) a.toff_slab[g] = run.ts;
-        if (a.toff_one) a.toff_one[g] = run.t1;
-        if (a.toff_big) a.toff_big[g] = run.tb;
-        if (a.box_copy) {
+        if (lane == 31) warp_tot[warp] = incl;
+        __syncthreads();
+        if (warp == 0) {
+            Counts wi = warp_tot[lane];
 #pragma unroll
-            for (int q = 0; q < 6; q++) a.box_copy[6 * g + q] = a.box[6 * g + q];
+            for (int o = 1; o < 32; o <<= 1) {
+                const Counts u = shfl_up(wi, o);
+                if (lane >= o) wi = add(wi, u);
+            }
+            warp_tot[lane] = wi;  // inclusive over warps
         }
-        if (a.off_copy && a.off) a.off_copy[g] = run.vox;
-        run = add(run, c);
+        __syncthreads();
+        Counts run = add(carry, warp > 0 ? warp_tot[warp - 1] : Counts{0, 0, 0, 0, 0, 0, 0});
+        run = add(run, Counts{incl.vox - mine.vox, incl.spec - mine.spec, incl.tot - mine.tot, incl.tn - mine.tn,
+                              incl.ts - mine.ts, incl.t1 - mine.t1, incl.tb - mine.tb});
+        if (g <= a.G) {
+            if (a.off) a.off[g] = run.vox;
+            if (a.spec_off) a.spec_off[g] = run.spec;
+            if (a.toff_n) a.toff_n[g] = run.tn;
+            if (a.toff_slab) a.toff_slab[g] = run.ts;
+            if (a.toff_one) a.toff_one[g] = run.t1;
+            if (a.toff_big) a.toff_big[g] = run.tb;
+            if (a.box_copy) {
+#pragma unroll
+                for (int q = 0; q < 6; q++) a.box_copy[6 * g + q] = a.box[6 * g + q];
+            }
+            if (a.off_copy && a.off) a.off_copy[g] = run.vox;
+        }
+        if (threadIdx.x == 0) carry_s = add(carry, warp_tot[31]);
+        __syncthreads();
+        carry = carry_s;
+        __syncthreads();  // warp_tot and carry_s are rewritten by the next chunk
     }
     if (threadIdx.x == kPlanThreads - 1) {
-        const Counts T = warp_tot[31];
+        const Counts T = carry;
         // Over capacity: report, and give the stage kernels no tiles so that nothing
         // is written past the end of an arena.
         const bool over = (a.off && T.vox > a.capacity) || (a.spec_off && T.spec > a.spec_capacity);
@@ -165,6 +169,16 @@ __global__ void item_count_kernel(int G, const int* keys_out, int item_vox, int*
     }
 }
 }  // namespace
+
+size_t exclusive_scan_temp_bytes(int n) {
+    size_t bytes = 0;
+    cub::DeviceScan::ExclusiveSum(nullptr, bytes, (const int*)nullptr, (int*)nullptr, n);
+    return bytes;
+}
+
+void launch_exclusive_scan(void* temp, size_t temp_bytes, const int* in, int* out, int n, cudaStream_t s) {
+    cub::DeviceScan::ExclusiveSum(temp, temp_bytes, in, out, n, s);
+}
 
 size_t work_order_temp_bytes(int G) {
     size_t sort = 0, scan = 0;

@@ -340,61 +340,68 @@ size_t redist_smem_bytes(int nmax, bool fp64) {
 
 namespace {
 // Per class c, the exclusive scan over grains of ceil(n / redist_units(c)) (n the output
-// box side) for the grains of toff_all (n tiles each) whose n is in class c; one CTA, as
-// plan_kernel.
+// box side) for the grains of toff_all (n tiles each) whose n is in class c; one CTA over
+// chunks of 1024 consecutive grains, each grain's box read once.
 __global__ void __launch_bounds__(1024) redist_class_kernel(int G, const int* toff_all, const int* box,
                                                             int* class_toff) {
     __shared__ int warp_tot[32][kRedistClasses];
+    __shared__ int carry[kRedistClasses];
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const int stride = G + 2;
     const bool none = toff_all[G + 1] == 0;  // the plan overflowed: no tiles at all
-    const int per = (G + blockDim.x) / blockDim.x;  // grains 0..G
-    const int g0 = threadIdx.x * per, g1 = min(G + 1, g0 + per);
-    auto count = [&](int g, int c) {
-        if (none || g < 1 || g > G || toff_all[g + 1] - toff_all[g] <= 0) return 0;
-        const Box b = load_box(box + 6 * g);  // cubes; the largest side bounds every stride
-        const int n = max(b.nx(), max(b.ny(), b.nz()));
-        const int lo = c == 0 ? 0 : redist_side(c - 1);
-        return (n > lo && n <= redist_side(c)) ? (n + redist_units(c) - 1) / redist_units(c) : 0;
-    };
-    int mine[kRedistClasses], incl[kRedistClasses];
-#pragma unroll
-    for (int c = 0; c < kRedistClasses; c++) {
-        mine[c] = 0;
-        for (int g = g0; g < g1; g++) mine[c] += count(g, c);
-        incl[c] = mine[c];
-#pragma unroll
-        for (int o = 1; o < 32; o <<= 1) {
-            const int u = __shfl_up_sync(0xffffffffu, incl[c], o);
-            if (lane >= o) incl[c] += u;
-        }
-        if (lane == 31) warp_tot[warp][c] = incl[c];
-    }
+    if (threadIdx.x < kRedistClasses) carry[threadIdx.x] = 0;
     __syncthreads();
-    if (warp == 0) {
+    for (int g0 = 0; g0 <= G; g0 += blockDim.x) {
+        const int g = g0 + threadIdx.x;
+        int cls = -1, tiles = 0;
+        if (!none && g >= 1 && g <= G && toff_all[g + 1] - toff_all[g] > 0) {
+            const Box b = load_box(box + 6 * g);  // cubes; the largest side bounds every stride
+            const int n = max(b.nx(), max(b.ny(), b.nz()));
+#pragma unroll
+            for (int c = 0; c < kRedistClasses; c++) {
+                const int lo = c == 0 ? 0 : redist_side(c - 1);
+                if (n > lo && n <= redist_side(c)) {
+                    cls = c;
+                    tiles = (n + redist_units(c) - 1) / redist_units(c);
+                }
+            }
+        }
+        int incl[kRedistClasses];
 #pragma unroll
         for (int c = 0; c < kRedistClasses; c++) {
-            const int w = warp_tot[lane][c];
-            int wi = w;
+            incl[c] = cls == c ? tiles : 0;
 #pragma unroll
             for (int o = 1; o < 32; o <<= 1) {
-                const int u = __shfl_up_sync(0xffffffffu, wi, o);
-                if (lane >= o) wi += u;
+                const int u = __shfl_up_sync(0xffffffffu, incl[c], o);
+                if (lane >= o) incl[c] += u;
             }
-            warp_tot[lane][c] = wi;  // inclusive over warps
+            if (lane == 31) warp_tot[warp][c] = incl[c];
         }
-    }
-    __syncthreads();
+        __syncthreads();
+        if (warp == 0) {
 #pragma unroll
-    for (int c = 0; c < kRedistClasses; c++) {
-        int run = (warp > 0 ? warp_tot[warp - 1][c] : 0) + incl[c] - mine[c];
-        int* t = class_toff + (long long)c * stride;
-        for (int g = g0; g < g1; g++) {
-            t[g] = run;
-            run += count(g, c);
+            for (int c = 0; c < kRedistClasses; c++) {
+                int wi = warp_tot[lane][c];
+#pragma unroll
+                for (int o = 1; o < 32; o <<= 1) {
+                    const int u = __shfl_up_sync(0xffffffffu, wi, o);
+                    if (lane >= o) wi += u;
+                }
+                warp_tot[lane][c] = wi;  // inclusive over warps
+            }
         }
-        if (threadIdx.x == blockDim.x - 1) t[G + 1] = warp_tot[31][c];
+        __syncthreads();
+        if (g <= G) {
+#pragma unroll
+            for (int c = 0; c < kRedistClasses; c++)
+                class_toff[(long long)c * stride + g] =
+                    carry[c] + (warp > 0 ? warp_tot[warp - 1][c] : 0) + incl[c] - (cls == c ? tiles : 0);
+        }
+        __syncthreads();
+        if (threadIdx.x < kRedistClasses) carry[threadIdx.x] += warp_tot[31][threadIdx.x];
+        __syncthreads();
     }
+    if (threadIdx.x < kRedistClasses) class_toff[(long long)threadIdx.x * stride + G + 1] = carry[threadIdx.x];
 }
 
 // CTAs of kernel k with `threads` threads and `smem` bytes that fit the device at once.
