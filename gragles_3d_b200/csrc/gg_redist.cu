@@ -40,6 +40,21 @@ struct Intersect {
     }
 };
 
+// q / d for 0 <= q < 2^12 and 1 <= d <= 64, from d's FP32 reciprocal: (q + 1/2) / d lies
+// at least 1/(2d) from an integer and the product's rounding error is below 2^-10.
+// S = 0 (the runtime-pitch kernels, any side): the integer division.
+template <int S>
+__device__ __forceinline__ int div_small(int q, int d, float rd) {
+    if (S) return __float2int_rz(((float)q + 0.5f) * rd);
+    return q / d;
+}
+
+// 4- or 8-byte asynchronous copy to a shared-memory address given as a 32-bit offset.
+template <typename T>
+__device__ __forceinline__ void cp_async_to(uint32_t dst, const T* src) {
+    asm volatile("cp.async.ca.shared.global [%0], [%1], %2;\n" ::"r"(dst), "l"(src), "n"(sizeof(T)) : "memory");
+}
+
 // isgn(s) * h of the reference: h, -h or +0 (isgn is 0 for +-0 and NaN), as a sign copy.
 __device__ __forceinline__ float copysign_t(float h, float s) { return copysignf(h, s); }
 __device__ __forceinline__ double copysign_t(double h, double s) { return copysign(h, s); }
@@ -230,12 +245,16 @@ __global__ void __launch_bounds__(kMaxThreads) redist_xy_kernel(RedistArgs<T> a)
             for (int q = line; q < nx * ny; q += lstride) outg[q] = T(-1);
         if (sweeps) {
             for (int q = line; q < ny * P; q += lstride) O[q] = T(-1);
-            // rows of the intersection, x-adjacent threads on x-adjacent words
-            const int wd = I.xmax - I.xmin;
+            // the rows of the intersection as one flat range, x-adjacent threads on
+            // x-adjacent words: element q is row q / wd, column q % wd
+            const int wd = I.xmax - I.xmin, n = (I.ymax - I.ymin) * wd, inx = ib.nx();
+            const float rwd = 1.f / (float)wd;
             const T* src = a.in.grain_ptr(g) + ib.at(I.ymin, I.xmin, k);
-            T* dst = In + (I.ymin - ob.y0) * P + (I.xmin - ob.x0);
-            for (int yy = 0; yy < I.ymax - I.ymin; yy++, src += ib.nx(), dst += P)
-                for (int xx = line; xx < wd; xx += lstride) cp_async_elem(dst + xx, src + xx);
+            const uint32_t dst = (uint32_t)__cvta_generic_to_shared(In + (I.ymin - ob.y0) * P + (I.xmin - ob.x0));
+            for (int q = line; q < n; q += lstride) {
+                const int r = div_small<S>(q, wd, rwd), c = q - r * wd;
+                cp_async_to(dst + (uint32_t)(sizeof(T) * (r * P + c)), src + (r * inx + c));
+            }
         }
         cp_async_wait_all();
         __syncthreads();
@@ -257,9 +276,13 @@ __global__ void __launch_bounds__(kMaxThreads) redist_xy_kernel(RedistArgs<T> a)
                 sweep_backward_prop(O0 + j, P, PL, I.ymax - 1, ob.y0, I.ymin, j < I.xmax, h);
         }
         __syncthreads();
-        if (sweeps)
-            for (int yy = 0; yy < ny; yy++)
-                for (int xx = line; xx < nx; xx += lstride) outg[yy * nx + xx] = O[yy * P + xx];
+        if (sweeps) {
+            const float rnx = 1.f / (float)nx;
+            for (int q = line; q < nx * ny; q += lstride) {
+                const int r = div_small<S>(q, nx, rnx);
+                outg[q] = O[r * P + (q - r * nx)];
+            }
+        }
         __syncthreads();
     }
 }
@@ -290,16 +313,25 @@ __global__ void __launch_bounds__(kMaxThreads) redist_z_kernel(RedistArgs<T> a) 
         T* Z = reinterpret_cast<T*>(smem_raw) + (S ? u * z_unit_stride(S) : 0);
         T* Zin = Z + PLZ;
         T* outr = a.out.grain_ptr(g) + (long long)(i - ob.y0) * nx;  // OUT(i, x0, z0)
+        const float rnx = 1.f / (float)nx;
         if (unit) {
-            for (int kk = 0; kk < nz; kk++)
-                for (int xx = line; xx < nx; xx += lstride) cp_async_elem(Z + kk * PZ + xx, outr + kk * zs + xx);
+            // the row's [z][x] plane and its input on the intersection, each as one flat
+            // range (element q: z q / width, x q % width), x-adjacent threads on x-adjacent words
+            const uint32_t zd = (uint32_t)__cvta_generic_to_shared(Z);
+            for (int q = line; q < nz * nx; q += lstride) {
+                const int r = div_small<S>(q, nx, rnx), c = q - r * nx;
+                cp_async_to(zd + (uint32_t)(sizeof(T) * (r * PZ + c)), outr + (r * zs + c));
+            }
             if (i >= I.ymin && i < I.ymax) {
-                const int wd = I.xmax - I.xmin;
+                const int wd = I.xmax - I.xmin, n = (I.zmax - I.zmin) * wd;
+                const float rwd = 1.f / (float)wd;
                 const long long izs = (long long)ib.nx() * ib.ny();
                 const T* src = a.in.grain_ptr(g) + ib.at(i, I.xmin, I.zmin);
-                T* dst = Zin + (I.zmin - ob.z0) * PZ + (I.xmin - ob.x0);
-                for (int k = I.zmin; k < I.zmax; k++, src += izs, dst += PZ)
-                    for (int xx = line; xx < wd; xx += lstride) cp_async_elem(dst + xx, src + xx);
+                const uint32_t dst = (uint32_t)__cvta_generic_to_shared(Zin + (I.zmin - ob.z0) * PZ + (I.xmin - ob.x0));
+                for (int q = line; q < n; q += lstride) {
+                    const int r = div_small<S>(q, wd, rwd), c = q - r * wd;
+                    cp_async_to(dst + (uint32_t)(sizeof(T) * (r * PZ + c)), src + (r * izs + c));
+                }
             }
         }
         cp_async_wait_all();
@@ -317,13 +349,13 @@ __global__ void __launch_bounds__(kMaxThreads) redist_z_kernel(RedistArgs<T> a) 
         __syncthreads();
         // clampValues(-delta, delta), dimensionalBufferReal.h:44-57
         if (unit)
-            for (int kk = 0; kk < nz; kk++)
-                for (int xx = line; xx < nx; xx += lstride) {
-                    T v = Z[kk * PZ + xx];
-                    if (v < -delta) v = -delta;
-                    else if (v > delta) v = delta;
-                    outr[kk * zs + xx] = v;
-                }
+            for (int q = line; q < nz * nx; q += lstride) {
+                const int r = div_small<S>(q, nx, rnx), c = q - r * nx;
+                T v = Z[r * PZ + c];
+                if (v < -delta) v = -delta;
+                else if (v > delta) v = delta;
+                outr[r * zs + c] = v;
+            }
         __syncthreads();
     }
 }
