@@ -213,6 +213,8 @@ __device__ __forceinline__ void sweep_backward_in(T* o, int so, int d, int p_sta
 // units spaced so that lane t of the CTA, unit t / S, line t % S, reads bank t mod 32 in
 // every sweep (the unit stride is congruent to S modulo 32, as S (S + 1) is).
 __host__ __device__ constexpr int xy_unit_stride(int S) { return 2 * S * (S + 1) + (32 - S % 32) % 32; }
+static_assert(xy_unit_stride(24) % 4 == 0 && xy_unit_stride(40) % 4 == 0 && xy_unit_stride(56) % 4 == 0,
+              "unit planes start on 16 bytes");
 __host__ __device__ constexpr int z_unit_stride(int S) { return 2 * S * S + S % 32; }
 __host__ __device__ constexpr int class_threads(int S, int U) { return S ? (U * S + 31) / 32 * 32 : kMaxThreads; }
 
@@ -244,7 +246,14 @@ __global__ void __launch_bounds__(kMaxThreads) redist_xy_kernel(RedistArgs<T> a)
         if (unit && !sweeps)  // no xy sweep reaches this slice
             for (int q = line; q < nx * ny; q += lstride) outg[q] = T(-1);
         if (sweeps) {
-            for (int q = line; q < ny * P; q += lstride) O[q] = T(-1);
+            // O (16-byte aligned: every unit stride is a multiple of 4 elements) to -1,
+            // 16 bytes a store
+            constexpr int kPer = 16 / (int)sizeof(T);
+            const uint4 m1 = sizeof(T) == 4 ? make_uint4(0xBF800000u, 0xBF800000u, 0xBF800000u, 0xBF800000u)
+                                            : make_uint4(0u, 0xBFF00000u, 0u, 0xBFF00000u);
+            const int n4 = ny * P / kPer;
+            for (int q = line; q < n4; q += lstride) reinterpret_cast<uint4*>(O)[q] = m1;
+            for (int q = n4 * kPer + line; q < ny * P; q += lstride) O[q] = T(-1);
             // the rows of the intersection as one flat range, x-adjacent threads on
             // x-adjacent words: element q is row q / wd, column q % wd
             const int wd = I.xmax - I.xmin, n = (I.ymax - I.ymin) * wd, inx = ib.nx();
