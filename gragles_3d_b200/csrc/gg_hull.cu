@@ -145,6 +145,7 @@ struct ElemSmem {
     double2* jres;               // kJobMax (mobility, energy)
     int nl, nq, nh, nj, ne, nd, np, np_flat;
     double ubox[6];  // box of the grain's barycenters (lo, hi)
+    int tnt[32];     // triangles of the 32 records being grouped
     int next;  // the work item this warp fetched
 };
 
@@ -470,11 +471,11 @@ __global__ void __launch_bounds__(32) elements_kernel(ElementArgs a) {
             const int excl = incl - nt;
             const int total = __shfl_sync(kFull, incl, 31);
             const unsigned peers = __match_any_sync(kFull, k);
+            // triangles of the earlier records of this record's list among the 32
+            S.tnt[lane] = nt;
+            __syncwarp();
             int before = 0;
-            for (int src = 0; src < 32; src++) {
-                const int w = __shfl_sync(kFull, nt, src);
-                if (src < lane && ((peers >> src) & 1)) before += w;
-            }
+            for (unsigned m = peers & ((1u << lane) - 1u); m; m &= m - 1) before += S.tnt[__ffs(m) - 1];
             const int dst = valid ? S.off[k] + S.fill[k] + before : 0;
             __syncwarp();
             if (valid && 31 - __clz(peers) == lane) S.fill[k] += before + nt;
