@@ -146,6 +146,7 @@ struct ElemSmem {
     int nl, nq, nh, nj, ne, nd, np, np_flat;
     double ubox[6];  // box of the grain's barycenters (lo, hi)
     int tnt[32];     // triangles of the 32 records being grouped
+    int eseq[kLMax]; // the element sequence: (type << 16) | junction or list
     int next;  // the work item this warp fetched
 };
 
@@ -715,135 +716,202 @@ __global__ void __launch_bounds__(32) elements_kernel(ElementArgs a) {
         }
         __syncwarp();
         // 6. the element table in search order: HJ, QJ, TL, GB, with its barycenter
-        //    segments, and the (element, searched ID) pairs
+        //    segments, and the (element, searched ID) pairs.  The sequence is listed first;
+        //    then 32 elements at a time each lane sizes one (IDs, segments, barycenters),
+        //    warp scans place them and each lane writes its own.  An element that does not
+        //    fit a capacity ends the table (the step then reports the overflow).  The ID
+        //    index (dense IDs in first-seen order) is built by one lane.
         for (int q = lane; q < kIHash; q += 32) S.ikey[q] = kNoId;
-        __syncwarp();
-        if (lane == 0) {
+        int* eidoff = S.qlist;  // per element: its first ID; the lists are copied into eseq
+        int* enid = S.hlist;    // per element: its IDs
+        int* esid = S.lslot;    // per TL / GB element e: its searched IDs at 2 e, 2 e + 1
+        {
+            const int nh = S.nh, nq = S.nq;
+            for (int i = lane; i < nh; i += 32) S.eseq[i] = (4 << 16) | S.hlist[i];
+            for (int i = lane; i < nq; i += 32) S.eseq[nh + i] = (3 << 16) | S.qlist[i];
+            int nseq = nh + nq;
+            for (int pass = 2; pass >= 1; pass--)  // TL, then GB, each in key order
+                for (int k0 = 0; k0 < nl; k0 += 32) {
+                    const int k = k0 + lane;
+                    const bool take = k < nl && id_count(S.lists[k]) == pass + 1;
+                    const unsigned m = __ballot_sync(kFull, take);
+                    const int at = nseq + __popc(m & ((1u << lane) - 1u));
+                    if (take && at < kLMax) S.eseq[at] = (pass << 16) | k;
+                    nseq += __popc(m);
+                }
+            if (nseq > kLMax) {  // each element holds a distinct list: cannot happen
+                if (lane == 0) atomicOr(a.err, ERR_BOUNDS);
+                nseq = kLMax;
+            }
+            __syncwarp();
             HullElem* E = a.el.elem + (long long)g * a.el.elem_cap;
             uint32_t* ids = a.el.ids + (long long)g * a.el.id_cap;
             int2* segs = a.el.segs + (long long)g * a.el.seg_cap;
-            int ne = 0, ni = 0, ns = 0, nd = 0, np = 0, pb = 0;
-            bool over = false, over_index = false;
-            // IDs from junction j's segment chain (j >= 0), else the nid IDs of id_src
-            auto emit = [&](int type, const uint32_t* id_src, int j, int nid, int head, bool chained, double en,
-                            double mo) {
-                if (ne >= a.el.elem_cap || ni + nid > a.el.id_cap) { over = true; return; }
-                const int id_off = ni, seg_off = ns;
-                if (j < 0) {
-                    for (int q = 0; q < nid; q++) ids[ni++] = id_src[q];
-                } else {
-                    for (int walk = 0; j >= 0 && walk < kLMax; walk++, j = S.jh[j].id_next) {
-                        const uint32_t* seg = S.jids + (long long)j * kJIds;
-                        for (int q = 0; q < S.jh[j].own && ni < id_off + nid; q++) ids[ni++] = seg[q];
+            int ne = 0, ni = 0, ns = 0, pb = 0;
+            bool over = false;
+            for (int c0 = 0; c0 < nseq; c0 += 32) {
+                const int e = c0 + lane;
+                const bool have = e < nseq;
+                int type = 0, src = 0, nid = 0, nseg = 0, pcnt = 0, head = -1;
+                uint32_t nb[3] = {0u, 0u, 0u};
+                if (have) {
+                    const int v = S.eseq[e];
+                    type = v >> 16;
+                    src = v & 0xFFFF;
+                    if (type >= 3) {
+                        // the junction's IDs: its segment chain, up to J.nids of them
+                        const JHead& J = S.jh[src];
+                        head = J.head;
+                        int n = 0;
+                        for (int j = src, walk = 0; j >= 0 && walk < kLMax && n < J.nids; walk++, j = S.jh[j].id_next)
+                            n += min(S.jh[j].own, J.nids - n);
+                        if (n != J.nids) atomicOr(a.err, ERR_BOUNDS);
+                        nid = n;
+                    } else {
+                        head = src;
+                        const uint32_t* L = S.lists[src];
+                        if (type == 1) {
+                            nb[nid++] = (uint32_t)g != L[0] ? L[0] : L[1];
+                        } else {
+#pragma unroll
+                            for (int q = 0; q < 3; q++)
+                                if ((uint32_t)g != L[q]) {
+#pragma unroll
+                                    for (int r = 0; r < 3; r++)
+                                        if (r == nid) nb[r] = L[q];
+                                    nid++;
+                                }
+                        }
                     }
-                    if (ni != id_off + nid) atomicOr(a.err, ERR_BOUNDS);
-                    nid = ni - id_off;
-                }
-                int nseg = 0, pcnt = 0;
-                for (int k = head; k >= 0; k = chained ? S.next_key[k] : -1) {
-                    if (ns >= a.el.seg_cap) { over = true; break; }
-                    if (k >= kLMax || S.off[k] < 0 || S.off[k] + S.cnt[k] > a.el.bary_cap) {
-                        atomicOr(a.err, ERR_BOUNDS);
-                        break;
-                    }
-                    const int off = S.off[k], cnt = S.cnt[k];
-                    segs[ns++] = make_int2(off, cnt);
-                    nseg++;
-                    S.lflat[k] = pb + pcnt;
-                    S.fill[k] = ne;  // fill is free after the jobs: the list's element
-                    pcnt += cnt;
-                }
-                HullElem& e = E[ne];
-                e.type = type;
-                e.id_off = id_off;
-                e.nids = nid;
-                e.seg_off = seg_off;
-                e.nseg = nseg;
-                e.energy = en;
-                e.mobility = mo;
-                e.area = 0.0;
-                // every barycenter belongs to one element; each element's run starts on a
-                // pair boundary and an odd run gets one padding entry (ebf's pair layout)
-                if (pb + pcnt + (pcnt & 1) > a.el.flat_cap) {
-                    over = true;
-                    pcnt = 0;
-                }
-                e.pbase = pb;
-                e.pcount = pcnt;
-                pb += pcnt + (pcnt & 1);
-                // the IDs projectPointToGrainBoundary compares: all for a high-order
-                // junction, else the first 3 (QJ), 2 (TL), 1 (GB); each element once per ID
-                const int nc = type == 4 ? nid : min(nid, type);
-                for (int q = 0; q < nc; q++) {
-                    const uint32_t id = ids[id_off + q];
-                    unsigned hs = (id * 2654435761u) & (kIHash - 1);
-                    int d = -1;
-                    for (int probe = 0; probe < kIHash; probe++) {
-                        if (S.ikey[hs] == id) { d = S.iden[hs]; break; }
-                        if (S.ikey[hs] == kNoId) {
-                            if (nd >= kIdxMax) break;
-                            S.ikey[hs] = id;
-                            S.iden[hs] = (short)nd;
-                            S.dkey[nd] = id;
-                            S.dcnt[nd] = 0;
-                            S.dlast[nd] = -1;
-                            d = nd++;
+                    for (int k = head, walk = 0; k >= 0 && walk < kLMax; walk++, k = type >= 3 ? S.next_key[k] : -1) {
+                        if (k >= kLMax || S.off[k] < 0 || S.off[k] + S.cnt[k] > a.el.bary_cap) {
+                            atomicOr(a.err, ERR_BOUNDS);
                             break;
                         }
-                        hs = (hs + 1) & (kIHash - 1);
+                        nseg++;
+                        pcnt += S.cnt[k];
                     }
-                    if (d < 0 || np >= kPairMax) { over = over_index = true; break; }
-                    if (S.dlast[d] == ne) continue;
-                    S.dlast[d] = ne;
-                    S.dcnt[d]++;
-                    S.pe[np] = (unsigned short)ne;
-                    S.pd[np] = (unsigned short)d;
-                    np++;
                 }
-                ne++;
-            };
-            for (int i = 0; i < S.nh; i++) {
-                const JHead& J = S.jh[S.hlist[i]];
-                // a junction made from one list keeps that list's energy (1 for HJ)
-                emit(4, nullptr, S.hlist[i], J.nids, J.head, true, 1.0, 1.0);
-            }
-            for (int i = 0; i < S.nq; i++) {
-                const JHead& J = S.jh[S.qlist[i]];
-                emit(3, nullptr, S.qlist[i], J.nids, J.head, true, S.energy[J.head], S.mobility[J.head]);
-            }
-            for (int pass = 2; pass >= 1; pass--)  // TL, then GB, each in key order
-                for (int k = 0; k < nl; k++) {
-                    const int count = id_count(S.lists[k]);
-                    if ((pass == 2 && count != 3) || (pass == 1 && count != 2)) continue;
-                    uint32_t nb[3];
-                    int nn = 0;
-                    if (count == 2) nb[nn++] = (uint32_t)g != S.lists[k][0] ? S.lists[k][0] : S.lists[k][1];
-                    else
-                        for (int q = 0; q < 3; q++)
-                            if ((uint32_t)g != S.lists[k][q]) nb[nn++] = S.lists[k][q];
-                    emit(pass, nb, -1, nn, k, false, S.energy[k], S.mobility[k]);
+                // every element's run starts on a pair boundary; an odd run gets a padding entry
+                const int padded = pcnt + (pcnt & 1);
+                int xi = nid, xs = nseg, xp = padded;
+#pragma unroll
+                for (int o = 1; o < 32; o <<= 1) {
+                    const int ui = __shfl_up_sync(kFull, xi, o), us = __shfl_up_sync(kFull, xs, o),
+                              up = __shfl_up_sync(kFull, xp, o);
+                    if (lane >= o) { xi += ui; xs += us; xp += up; }
                 }
-            // the index: IDs with their element ranges, elements in search order
-            int run = 0;
-            for (int d = 0; d < nd; d++) {
-                S.doff[d] = run;
-                run += S.dcnt[d];
-                S.dcnt[d] = 0;
+                const int id_off = ni + xi - nid, seg_off = ns + xs - nseg, pbase = pb + xp - padded;
+                const bool fits = ne + lane < a.el.elem_cap && id_off + nid <= a.el.id_cap &&
+                                  seg_off + nseg <= a.el.seg_cap && pbase + padded <= a.el.flat_cap;
+                const unsigned bad = __ballot_sync(kFull, have && !fits);
+                const int cnt = bad ? __ffs(bad) - 1 : min(32, nseq - c0);  // elements placed
+                if (lane < cnt) {
+                    const int ei = ne + lane;
+                    if (type >= 3) {
+                        int w = id_off;
+                        for (int j = src, walk = 0; j >= 0 && walk < kLMax && w < id_off + nid; walk++, j = S.jh[j].id_next) {
+                            const uint32_t* seg = S.jids + (long long)j * kJIds;
+                            for (int q = 0; q < S.jh[j].own && w < id_off + nid; q++) ids[w++] = seg[q];
+                        }
+                    } else {
+                        for (int q = 0; q < nid; q++) ids[id_off + q] = nb[q];
+                        esid[2 * ei] = (int)nb[0];
+                        esid[2 * ei + 1] = (int)nb[1];
+                    }
+                    int sg = seg_off, pc = 0;
+                    for (int k = head, walk = 0; k >= 0 && walk < nseg; walk++, k = type >= 3 ? S.next_key[k] : -1) {
+                        const int off = S.off[k], c = S.cnt[k];
+                        segs[sg++] = make_int2(off, c);
+                        S.lflat[k] = pbase + pc;
+                        S.fill[k] = ei;  // fill is free after the jobs: the list's element
+                        pc += c;
+                    }
+                    HullElem& el = E[ei];
+                    el.type = type;
+                    el.id_off = id_off;
+                    el.nids = nid;
+                    el.seg_off = seg_off;
+                    el.nseg = nseg;
+                    // a junction made from one list keeps that list's energy (1 for HJ)
+                    el.energy = type == 4 ? 1.0 : S.energy[head];
+                    el.mobility = type == 4 ? 1.0 : S.mobility[head];
+                    el.area = 0.0;
+                    el.pbase = pbase;
+                    el.pcount = pcnt;
+                    eidoff[ei] = id_off;
+                    enid[ei] = nid;
+                }
+                if (cnt > 0) {
+                    ni += __shfl_sync(kFull, xi, cnt - 1);
+                    ns += __shfl_sync(kFull, xs, cnt - 1);
+                    pb += __shfl_sync(kFull, xp, cnt - 1);
+                }
+                ne += cnt;
+                if (bad) {
+                    over = true;
+                    break;
+                }
             }
-            if (run > a.el.pair_cap) over = over_index = true;
-            unsigned short* pairs = a.el.idx_elem + (long long)g * a.el.pair_cap;
-            for (int q = 0; q < np; q++) {
-                const int d = S.pd[q];
-                const int at = S.doff[d] + S.dcnt[d]++;
-                if (at < a.el.pair_cap) pairs[at] = S.pe[q];
+            __syncwarp();
+            if (lane == 0) {
+                // the index: each element's searched IDs -- all for a high-order junction,
+                // else the first 3 (QJ), 2 (TL), 1 (GB) -- in element order, each element once
+                // per ID; IDs numbered by first appearance
+                int nd = 0, np = 0;
+                bool over_index = false;
+                for (int e = 0; e < ne; e++) {
+                    const int type = S.eseq[e] >> 16, nid = enid[e];
+                    const int nc = type == 4 ? nid : min(nid, type);
+                    for (int q = 0; q < nc; q++) {
+                        const uint32_t id = type <= 2 ? (uint32_t)esid[2 * e + q] : ids[eidoff[e] + q];
+                        unsigned hs = (id * 2654435761u) & (kIHash - 1);
+                        int d = -1;
+                        for (int probe = 0; probe < kIHash; probe++) {
+                            if (S.ikey[hs] == id) { d = S.iden[hs]; break; }
+                            if (S.ikey[hs] == kNoId) {
+                                if (nd >= kIdxMax) break;
+                                S.ikey[hs] = id;
+                                S.iden[hs] = (short)nd;
+                                S.dkey[nd] = id;
+                                S.dcnt[nd] = 0;
+                                S.dlast[nd] = -1;
+                                d = nd++;
+                                break;
+                            }
+                            hs = (hs + 1) & (kIHash - 1);
+                        }
+                        if (d < 0 || np >= kPairMax) { over = over_index = true; break; }
+                        if (S.dlast[d] == e) continue;
+                        S.dlast[d] = e;
+                        S.dcnt[d]++;
+                        S.pe[np] = (unsigned short)e;
+                        S.pd[np] = (unsigned short)d;
+                        np++;
+                    }
+                }
+                // IDs with their element ranges, elements in search order
+                int run = 0;
+                for (int d = 0; d < nd; d++) {
+                    S.doff[d] = run;
+                    run += S.dcnt[d];
+                    S.dcnt[d] = 0;
+                }
+                if (run > a.el.pair_cap) over = over_index = true;
+                unsigned short* pairs = a.el.idx_elem + (long long)g * a.el.pair_cap;
+                for (int q = 0; q < np; q++) {
+                    const int d = S.pd[q];
+                    const int at = S.doff[d] + S.dcnt[d]++;
+                    if (at < a.el.pair_cap) pairs[at] = S.pe[q];
+                }
+                if (over) { atomicOr(a.err, ERR_HULL); atomicOr(a.cap.diag, over_index ? HULL_INDEX : HULL_TABLE); }
+                a.el.n_elem[g] = ne;
+                a.el.n_idx[g] = nd;
+                a.el.n_flat[g] = pb;
+                S.np_flat = pb;
+                S.ne = ne;
+                S.nd = nd;
             }
-            if (over) { atomicOr(a.err, ERR_HULL); atomicOr(a.cap.diag, over_index ? HULL_INDEX : HULL_TABLE); }
-            a.el.n_elem[g] = ne;
-            a.el.n_idx[g] = nd;
-            a.el.n_flat[g] = pb;
-            S.np_flat = pb;
-            S.ne = ne;
-            S.nd = nd;
         }
         __syncwarp();
         {
