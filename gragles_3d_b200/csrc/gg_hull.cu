@@ -376,12 +376,28 @@ __global__ void __launch_bounds__(32) elements_kernel(ElementArgs a) {
         for (int q = lane; q < kLHash; q += 32) S.lslot[q] = -1;
         int nl = 0;
         __syncwarp();
+        // a record's list (32 bytes, two 16-byte loads) and triangle count; the next chunk's
+        // are loaded while this one is deduplicated
+        auto load_rec = [&](int r, uint4& l0, uint4& l1, int& nt) {
+            if (r < nrec) {
+                const uint4* src = reinterpret_cast<const uint4*>(rec_list + 8 * (long long)r);
+                l0 = src[0];
+                l1 = src[1];
+                nt = rec_ntri[r];
+            } else {
+                l0 = l1 = make_uint4(kNoId, kNoId, kNoId, kNoId);
+                nt = 0;
+            }
+        };
+        uint4 n0, n1;
+        int n_nt;
+        load_rec(lane, n0, n1, n_nt);
         for (int base = 0; base < nrec; base += 32) {
             const int r = base + lane;
             const bool valid = r < nrec;
-            uint32_t mine[8];
-#pragma unroll
-            for (int q = 0; q < 8; q++) mine[q] = valid ? rec_list[8 * (long long)r + q] : kNoId;
+            const uint32_t mine[8] = {n0.x, n0.y, n0.z, n0.w, n1.x, n1.y, n1.z, n1.w};
+            const int nt_rec = n_nt;
+            load_rec(r + 32, n0, n1, n_nt);
             const unsigned h = list_hash(mine);
             const unsigned vmask = __ballot_sync(kFull, valid);
             const unsigned peers = __match_any_sync(kFull, h) & vmask;
@@ -433,7 +449,7 @@ __global__ void __launch_bounds__(32) elements_kernel(ElementArgs a) {
                 nl += __popc(fm);
                 found = __shfl_sync(kFull, found, leader);
             }
-            if (valid) rec_ntri[r] = (rec_ntri[r] & 0xFF) | ((found < kLMax && found >= 0 ? found : 0) << 8);
+            if (valid) rec_ntri[r] = (nt_rec & 0xFF) | ((found < kLMax && found >= 0 ? found : 0) << 8);
             __syncwarp();
         }
         if (nl > kLMax) nl = kLMax;
@@ -964,7 +980,16 @@ __global__ void __launch_bounds__(32) elements_kernel(ElementArgs a) {
             float* pf = reinterpret_cast<float*>(a.el.ebf + (long long)g * a.el.flat_cap);
             int* pidx = a.el.eidx + (long long)g * a.el.flat_cap;
             float r2 = 0.f;
+            // the barycenter of the lane's next index is loaded while this one is placed
+            double p0 = 0, p1 = 0, p2 = 0;
+            if (lane < total) { p0 = eb[3 * (long long)lane]; p1 = eb[3 * (long long)lane + 1]; p2 = eb[3 * (long long)lane + 2]; }
             for (int i = lane; i < total; i += 32) {
+                const double b0 = p0, b1 = p1, b2 = p2;
+                if (i + 32 < total) {
+                    p0 = eb[3 * (long long)(i + 32)];
+                    p1 = eb[3 * (long long)(i + 32) + 1];
+                    p2 = eb[3 * (long long)(i + 32) + 2];
+                }
                 int lo = 0, hi = nl - 1;
                 while (lo < hi) {
                     const int mid = (lo + hi + 1) >> 1;
@@ -974,8 +999,7 @@ __global__ void __launch_bounds__(32) elements_kernel(ElementArgs a) {
                 const int base = nl > 0 ? S.lflat[lo] : -1;
                 const int dst = base < 0 ? -1 : base + (i - S.off[lo]);
                 if (dst < 0 || dst >= nflat) continue;  // a list no element holds
-                const double dx = eb[3 * (long long)i] - org[0], dy = eb[3 * (long long)i + 1] - org[1],
-                             dz = eb[3 * (long long)i + 2] - org[2];
+                const double dx = b0 - org[0], dy = b1 - org[1], dz = b2 - org[2];
                 const double w = dx * dx + dy * dy + dz * dz;
                 float* pp = pf + 8 * (dst >> 1) + (dst & 1);  // pair layout: x0 x1 y0 y1 z0 z1 w0 w1
                 pp[0] = (float)dx;
