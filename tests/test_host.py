@@ -265,3 +265,29 @@ def test_rtree_lists_follow_the_reference_order(name):
     off, ids = gg.rtree_lists(boxes, valid)
     assert np.array_equal(off, d["init_list_off"])
     assert np.array_equal(ids, d["init_list_ids"])
+
+
+def test_small_division_by_fp32_reciprocal_is_exact():
+    """The redistancing kernels take a flat element index q apart into (row, column) with
+    trunc((q + 1/2) * fl(1/d)) in FP32 (gg_redist.cu, div_small) for the fixed-side
+    classes: q < 2^12 and d <= 64.  Every such pair, in IEEE FP32 arithmetic as the
+    kernel does it (no fused multiply-add), gives q // d."""
+    q = np.arange(4096, dtype=np.int64)
+    for d in range(1, 65):
+        rd = np.float32(1.0) / np.float32(d)
+        prod = (q.astype(np.float32) + np.float32(0.5)) * rd
+        assert prod.dtype == np.float32
+        assert np.array_equal(np.trunc(prod).astype(np.int64), q // d), f"divisor {d}"
+
+
+def test_marching_cubes_edge_table_is_empty_only_for_uniform_cubes():
+    """The marching-cubes kernel treats a cube as active when its index is neither 0 nor
+    255 (gg_mc.cu, cube_active) instead of looking the edge table up: the table has no
+    other empty entry."""
+    src = open(os.path.join(ROOT, "gragles_3d_b200", "csrc", "gg_mc_tables.inc")).read()
+    body = src[src.index("gg_mc_edge_table"):src.index("gg_mc_tri_table")]
+    body = body[body.index("{") + 1:]
+    vals = [int(v, 16) if v.lower().startswith("0x") else int(v)
+            for v in re.findall(r"0[xX][0-9a-fA-F]+|\b\d+\b", body)][:256]
+    assert len(vals) == 256
+    assert [i for i, v in enumerate(vals) if v == 0] == [0, 255]
