@@ -8,7 +8,10 @@
 // resize of the output box to the new bounding box (dimensionalBuffer.h:120-219).
 //
 // One CTA owns one grain and walks its cubes in the reference's z, y, x order in
-// slabs of whole cube layers.  A block scan of per-cube triangle counts gives each
+// slabs of whole cube layers.  A slab's voxel signs are staged as bits (a warp ballot
+// per 32 voxels); 32 cubes of a row are classified at once from their corners' bit
+// vectors, and only the active cubes (not all corners alike) are listed, in cube
+// order, and processed further.  A block scan of per-cube triangle counts gives each
 // triangle its place in the reference's emission order; the FP64 volume and area
 // terms of a chunk are then added by one thread in that order, so the sums are
 // bit-identical to the reference's sequential loop.  The distinct neighbour IDs

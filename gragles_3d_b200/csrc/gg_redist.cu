@@ -5,21 +5,21 @@
 // intersection except the last runs four sweeps (x forward, x backward, y forward,
 // y backward), then sweeps z forward and backward over all columns, and clamps to
 // +-delta.  Every sweep is a recurrence along one line and the lines of a sweep are
-// independent, so a small CTA (one thread per line: 32 or 64 threads for the usual
-// sides) owns one unit of work at a time:
-//   kernel xy: a CTA per (grain, output z-slice); the slice of the output sits in
-//              shared memory, threads run rows for the x sweeps and columns for the
-//              y sweeps;
-//   kernel z:  a CTA per (grain, output y-row); the [z][x] plane of the row sits in
-//              shared memory and threads run the z recurrences of one column each
-//              (x-adjacent threads touch adjacent words).
-// One unit's buffers are small (two n x n planes), so many CTAs share an SM.
-// The unit's input values on the in/out intersection are staged next to it with
-// coalesced loads (a recurrence that read HBM step by step would wait on every load).
-// Along a line the value that the next step updates is carried in a register, so a
-// step costs its arithmetic and shared-memory loads that do not depend on the chain.  The
-// arithmetic is the reference's, statement by statement (no contraction), and the
-// lines of a sweep run in the reference's order, so the FP64 result is bit-identical.
+// independent, so a thread runs one line, and a CTA runs one to five units side by side
+// (all of one grain; the count is fixed per box-size class so that 120-128 lanes have a
+// line):
+//   kernel xy: a unit is (grain, output z-slice); the slice of the output sits in shared
+//              memory, threads run rows for the x sweeps and columns for the y sweeps;
+//   kernel z:  a unit is (grain, output y-row); the [z][x] plane of the row sits in shared
+//              memory and threads run the z recurrences of one column each (x-adjacent
+//              threads touch adjacent words).
+// A unit's buffers are small (two n x n planes).  Its input values on the in/out
+// intersection are staged next to it with coalesced loads over one flat range (a
+// recurrence that read HBM step by step would wait on every load).  Along a line the
+// value that the next step updates is carried in a register, so a step costs its
+// arithmetic and shared-memory loads that do not depend on the chain.  The arithmetic
+// is the reference's, statement by statement (no contraction), and the lines of a sweep
+// run in the reference's order, so the FP64 result is bit-identical.
 #include "gg_kernels.cuh"
 
 namespace gg {
