@@ -48,9 +48,9 @@ __host__ __device__ constexpr int nbc_dz(int k) { return k >> 2; }
 static_assert(corner_dx(1) == 1 && corner_dz(2) == 0 && corner_dy(7) == 1 && corner_dz(4) == 1, "corner table");
 static_assert(edge_b(3) == 0 && edge_b(7) == 4 && edge_b(6) == 7 && edge_a(11) == 3 && edge_b(11) == 7, "edge table");
 static_assert(nbc_dx(2) == 1 && nbc_dy(3) == 1 && nbc_dx(3) == 0 && nbc_dz(5) == 1, "neighbour corner table");
-// a cube crosses the zero level unless its 8 corners agree: the edge table is 0 exactly
-// for cube indices 0 and 255
-__device__ __forceinline__ bool cube_active(int ci) { return ci != 0 && ci != 255; }
+// A cube crosses the zero level unless its 8 corners agree: the edge table is 0 exactly
+// for cube indices 0 and 255, so the active cubes are found from the corners' sign bits
+// alone (any & ~all over the eight corner bit vectors of a row of 32 cubes).
 
 struct V3 { double x, y, z; };
 

@@ -94,7 +94,7 @@ __device__ __forceinline__ void step_in(T a, T b, T& out_here, T& out_next, T h)
 template <typename T, int MODE>
 __device__ __forceinline__ T* line_steps(T* op, T& cur, int count, int s, int d, T h) {
     int k = 0;
-    if (MODE == 2) {
+    if constexpr (MODE == 2) {
         if (count <= 0) return op;
         T a = op[d];
         for (; k + 4 <= count; k += 4, op += 4 * s) {
@@ -136,28 +136,29 @@ __device__ __forceinline__ T* line_steps(T* op, T& cur, int count, int s, int d,
             a = b;
         }
         return op;
-    }
-    for (; k + 4 <= count; k += 4, op += 4 * s) {
-        T nx[4], src[4];
+    } else {
+        for (; k + 4 <= count; k += 4, op += 4 * s) {
+            T nx[4], src[4];
 #pragma unroll
-        for (int j = 0; j < 4; j++) {
-            nx[j] = op[(j + 1) * s];
-            src[j] = MODE == 1 ? op[d + (j + 1) * s] : nx[j];
-        }
+            for (int j = 0; j < 4; j++) {
+                nx[j] = op[(j + 1) * s];
+                src[j] = MODE == 1 ? op[d + (j + 1) * s] : nx[j];
+            }
 #pragma unroll
-        for (int j = 0; j < 4; j++) {
-            step_prop(src[j], cur, nx[j], h);
-            op[j * s] = cur;
-            cur = nx[j];
+            for (int j = 0; j < 4; j++) {
+                step_prop(src[j], cur, nx[j], h);
+                op[j * s] = cur;
+                cur = nx[j];
+            }
         }
+        for (; k < count; k++, op += s) {
+            T nx = op[s];
+            step_prop(MODE == 1 ? op[d + s] : nx, cur, nx, h);
+            *op = cur;
+            cur = nx;
+        }
+        return op;
     }
-    for (; k < count; k++, op += s) {
-        T nx = op[s];
-        step_prop(MODE == 1 ? op[d + s] : nx, cur, nx, h);
-        *op = cur;
-        cur = nx;
-    }
-    return op;
 }
 
 // Forward sweep over positions p0 .. p_end - 1 of a line with stride so, the input d

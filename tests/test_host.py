@@ -281,9 +281,9 @@ def test_small_division_by_fp32_reciprocal_is_exact():
 
 
 def test_marching_cubes_edge_table_is_empty_only_for_uniform_cubes():
-    """The marching-cubes kernel treats a cube as active when its index is neither 0 nor
-    255 (gg_mc.cu, cube_active) instead of looking the edge table up: the table has no
-    other empty entry."""
+    """The marching-cubes kernel treats a cube as active when its eight corner signs are not
+    all alike (cube index neither 0 nor 255; gg_mc.cu, the row words any & ~all) instead of
+    looking the edge table up: the table has no other empty entry."""
     src = open(os.path.join(ROOT, "gragles_3d_b200", "csrc", "gg_mc_tables.inc")).read()
     body = src[src.index("gg_mc_edge_table"):src.index("gg_mc_tri_table")]
     body = body[body.index("{") + 1:]
