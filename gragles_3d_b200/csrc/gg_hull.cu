@@ -90,7 +90,10 @@ __device__ double energy_of(const HullPhysics& ph, double misori) {
     return 1.0 * (misori / theta_ref) * (1.0 - log(misori / theta_ref));
 }
 
-// Vector3d (a - b).squaredNorm(): Eigen's unrolled sum c0 + (c1 + c2)
+// Vector3d (a - b).squaredNorm(): Eigen's unrolled sum c0 + (c1 + c2).  The reference's
+// junction test sqrt(d2) < 2 is d2 < 4 exactly: sqrt is correctly rounded and monotone, and
+// the largest double below 4, 4 - 2^-51, has its square root below 2 - 2^-53, which rounds
+// to 2 - 2^-52.
 __device__ __forceinline__ double sqdist(const double* a, const double* b) {
     const double d0 = a[0] - b[0], d1 = a[1] - b[1], d2 = a[2] - b[2];
     return d0 * d0 + (d1 * d1 + d2 * d2);
@@ -190,12 +193,12 @@ __device__ void insert_list(ElemSmem& S, unsigned h, int k, int* err) {
 // loads run ahead of the sequential sums).
 __device__ __forceinline__ void bary_sum(const double* b, int n, double& p0, double& p1, double& p2) {
     int i = 0;
-    for (; i + 4 <= n; i += 4) {
-        double v[12];
+    for (; i + 8 <= n; i += 8) {  // 24 loads in flight, the sums in order
+        double v[24];
 #pragma unroll
-        for (int u = 0; u < 12; u++) v[u] = b[3 * i + u];
+        for (int u = 0; u < 24; u++) v[u] = b[3 * i + u];
 #pragma unroll
-        for (int u = 0; u < 4; u++) {
+        for (int u = 0; u < 8; u++) {
             p0 += v[3 * u];
             p1 += v[3 * u + 1];
             p2 += v[3 * u + 2];
@@ -637,7 +640,7 @@ __global__ void __launch_bounds__(32) elements_kernel(ElementArgs a) {
                 int found = -1;
                 for (int j0 = i + 1; j0 < S.nq && found < 0; j0 += 32) {
                     const int j = j0 + lane;
-                    const bool hit = j < S.nq && sqrt(sqdist(ap, S.jh[S.qlist[j]].pos)) < 2;
+                    const bool hit = j < S.nq && sqdist(ap, S.jh[S.qlist[j]].pos) < 4.0;
                     const unsigned m = __ballot_sync(kFull, hit);
                     if (m) found = j0 + __ffs(m) - 1;
                 }
@@ -689,7 +692,7 @@ __global__ void __launch_bounds__(32) elements_kernel(ElementArgs a) {
                     int found = -1;
                     for (int i0 = i; i0 < S.nq && found < 0; i0 += 32) {
                         const int ii = i0 + lane;
-                        const bool hit = ii < S.nq && sqrt(sqdist(S.jh[S.qlist[ii]].pos, hp)) < 2;
+                        const bool hit = ii < S.nq && sqdist(S.jh[S.qlist[ii]].pos, hp) < 4.0;
                         const unsigned m = __ballot_sync(kFull, hit);
                         if (m) found = i0 + __ffs(m) - 1;
                     }
@@ -713,7 +716,7 @@ __global__ void __launch_bounds__(32) elements_kernel(ElementArgs a) {
                     int found = -1;
                     for (int k0 = k; k0 < S.nh && found < 0; k0 += 32) {
                         const int kk = k0 + lane;
-                        const bool hit = kk < S.nh && sqrt(sqdist(ap, S.jh[S.hlist[kk]].pos)) < 2;
+                        const bool hit = kk < S.nh && sqdist(ap, S.jh[S.hlist[kk]].pos) < 4.0;
                         const unsigned m = __ballot_sync(kFull, hit);
                         if (m) found = k0 + __ffs(m) - 1;
                     }
