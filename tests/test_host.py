@@ -291,3 +291,17 @@ def test_marching_cubes_edge_table_is_empty_only_for_uniform_cubes():
             for v in re.findall(r"0[xX][0-9a-fA-F]+|\b\d+\b", body)][:256]
     assert len(vals) == 256
     assert [i for i, v in enumerate(vals) if v == 0] == [0, 255]
+
+
+def test_junction_distance_test_without_square_root():
+    """The element build tests the reference's sqrt(d2) < 2 as d2 < 4 (gg_hull.cu, the
+    junction merges).  With a correctly rounded square root the two agree for every double:
+    checked around 4 (the 2^20 doubles below it, and above) and on random squared
+    distances."""
+    import math
+
+    xs = [4.0 - k * 2.0 ** -51 for k in range(1 << 20)] + [4.0 + k * 2.0 ** -50 for k in range(1024)]
+    rng = np.random.default_rng(3)
+    xs += list(rng.uniform(0.0, 100.0, 200000)) + list(rng.uniform(3.99, 4.01, 200000))
+    for x in xs:
+        assert (math.sqrt(x) < 2) == (x < 4.0), repr(x)
